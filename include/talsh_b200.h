@@ -1,0 +1,91 @@
+/* talsh-b200: device-level C ABI of the sm_100a kernels.
+ *
+ * These entry points sit below the TAL-SH API (talsh.h).  They take device
+ * pointers and a CUDA stream (cudaStream_t passed as void*, NULL = legacy
+ * default stream), launch asynchronously and return 0 on success or a TAL-SH
+ * error code.  They replace the NV-TAL internal interface
+ * (`gpu_tensor_block_{copy,add,contract_dlf,init,scale}`,
+ * reference device_algebra.h:259-274); only talsh.h is a compatibility
+ * promise, this layer is specific to this core.
+ *
+ * Conventions: column-major bodies (dimension 0 fastest); permutations are
+ * 1-based O2N arrays (o2n[i] = output position of input dimension i, as in
+ * the reference's `transp(1:n)` of tensor_block_copy); data kinds R4, R8, C4,
+ * C8 from tensor_algebra.h.  Scale factors follow the reference CPU rules
+ * (real kinds use cmplx8_to_real8(alpha) for add/scale, real(alpha) for
+ * contraction).
+ */
+#ifndef TALSH_B200_CORE_H_
+#define TALSH_B200_CORE_H_
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* dst = permute(src): dst[O2N(idx)] = src[idx]; conj != 0 negates imaginary
+ * parts (C4/C8).  Pure data movement, bit-exact.
+ * Replaces gpu_tensor_block_copy (reference tensor_algebra_gpu_nvidia.cu:4806). */
+int tcTensorPermute(int data_kind, int rank, const int *dims_in, const int *o2n, const void *src,
+                    void *dst, int conj, void *stream);
+
+/* dst += permute(src) * alpha, evaluated per element as d + l*s without FMA
+ * contraction (bit-exact with the reference CPU add).  conj applies to src.
+ * Replaces gpu_tensor_block_add (reference tensor_algebra_gpu_nvidia.cu:5203). */
+int tcTensorPermuteAdd(int data_kind, int rank, const int *dims_in, const int *o2n,
+                       const void *src, void *dst, double alpha_re, double alpha_im, int conj,
+                       void *stream);
+
+/* dst[0..vol) = value.  Replaces gpu_tensor_block_init (:4467). */
+int tcTensorInit(int data_kind, size_t vol, void *dst, double val_re, double val_im, void *stream);
+
+/* dst[0..vol) *= alpha.  Replaces gpu_tensor_block_scale (:4525). */
+int tcTensorScale(int data_kind, size_t vol, void *dst, double alpha_re, double alpha_im,
+                  void *stream);
+
+/* Bytes of device scratch tcTensorNorm1 needs for a tensor of vol elements. */
+size_t tcTensorNorm1Scratch(size_t vol);
+
+/* *result_dev (device double) = sum of |x| over src[0..vol), accumulated in
+ * double with a fixed two-pass reduction (run-to-run deterministic).
+ * scratch: device buffer of at least tcTensorNorm1Scratch(vol) bytes.
+ * No reference GPU counterpart: the reference norm is host-only
+ * (talshTensorImageNorm1_cpu, talshc.cpp:6207). */
+int tcTensorNorm1(int data_kind, size_t vol, const void *src, double *result_dev, void *scratch,
+                  size_t scratch_bytes, void *stream);
+
+/* Bytes of device scratch tcTensorContract needs for this shape (offset
+ * tables of the gather-GEMM, plus the partial sums of a full contraction). */
+size_t tcTensorContractScratch(int data_kind, const int *cptrn, int drank, const int *ddims,
+                               int lrank, const int *ldims, int rrank, const int *rdims);
+
+/* D = beta*D + alpha * contraction(L, R) for a digital pattern cptrn[lrank+rrank]
+ * (reference format: >0 position in D, <0 minus the position in the other
+ * operand).  Indices present in D, L and R at once are not supported
+ * (TALSH_NOT_IMPLEMENTED).  beta = 1 if accumulative else D is overwritten.
+ * conj_bits: bit0 D, bit1 L, bit2 R (complex kinds only).  Rank-0 operands are
+ * single elements of the data kind, resident in device memory.  scratch:
+ * device buffer of tcTensorContractScratch(...) bytes (may be NULL when that is 0).
+ * Replaces gpu_tensor_block_contract_dlf (reference :5847). */
+int tcTensorContract(int data_kind, const int *cptrn, int drank, const int *ddims, int lrank,
+                     const int *ldims, int rrank, const int *rdims, void *D, const void *L,
+                     const void *R, double alpha_re, double alpha_im, int conj_bits,
+                     int accumulative, void *scratch, size_t scratch_bytes, void *stream);
+
+/* Host view of the transpose tile plan (diagnostics): info[0] fused rank,
+ * [1] identity flag, [2] tile volume, [3] input run, [4] output run,
+ * [5] input runs, [6] output runs, [7] input vector width, [8] output vector
+ * width, [9] shared bytes, [10] tile count. */
+int tcPermutePlanInfo(int data_kind, int rank, const int *dims_in, const int *o2n, int *info);
+
+/* Number of kernels this library launched since load (diagnostics). */
+unsigned long long tcKernelLaunchCount(void);
+/* Last CUDA error text seen by the library (diagnostics). */
+const char *tcLastErrorString(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TALSH_B200_CORE_H_ */

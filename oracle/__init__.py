@@ -1,0 +1,165 @@
+"""Oracle for the talsh-b200 hot path -- TEST INFRASTRUCTURE ONLY.
+
+ctypes wrapper over liboracle.so, the plain-C restatement of the reference
+TAL-SH CPU path (see oracle.h for the reference file:line each routine
+follows).  Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline
+leg import this package, as the checker or as the timed CPU baseline; the
+product library never uses it.
+
+Parity status: pinned.  The restatement is checked against every known answer
+the reference's own tests and documents hold for this path (digital patterns
+and matricizations quoted from the reference, the analytic norms of
+test.cpp's test_talsh_c, the explicit-loop residual of test_nwchem_c, the
+patterns of tensor_contractions.txt) and against numpy's independent einsum /
+transpose (tests/test_oracle.py).  The reference's own CPU library is Fortran
+and cannot be compiled here (no Fortran compiler in the image).
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "liboracle.so")
+R4, R8, C4, C8 = 4, 8, 14, 18
+NP_DTYPE = {R4: np.float32, R8: np.float64, C4: np.complex64, C8: np.complex128}
+KIND_OF = {np.dtype(np.float32): R4, np.dtype(np.float64): R8,
+           np.dtype(np.complex64): C4, np.dtype(np.complex128): C8}
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            from .build import build_oracle
+            build_oracle()
+        L = C.CDLL(LIB_PATH)
+        P, I, D, V, Z = C.POINTER, C.c_int, C.c_double, C.c_void_p, C.c_size_t
+        L.orc_str2dig.argtypes = [C.c_char_p, P(I), P(I), P(I), P(I), P(I)]
+        L.orc_contraction_permutations.argtypes = [I, I, I, I, P(I), I, P(I), P(I), P(I), P(I), P(I), P(I), P(I)]
+        L.orc_contr_permutations.argtypes = [I, I, I, I, P(I), I, P(I), P(I), P(I), P(I), P(I), P(I)]
+        L.orc_permute.argtypes = [I, I, P(I), P(I), V, V, I]
+        L.orc_permute_blocked.argtypes = [I, I, P(I), P(I), V, V, I]
+        L.orc_tensor_copy.argtypes = [I, P(I), I, P(I), V, V, I]
+        L.orc_tensor_add.argtypes = [I, P(I), I, P(I), V, V, D, D, I]
+        L.orc_tensor_scale.argtypes = [I, Z, V, D, D, I]
+        L.orc_tensor_init.argtypes = [I, Z, V, D, D, I]
+        L.orc_norm1.argtypes = [I, Z, V]
+        L.orc_norm1.restype = D
+        L.orc_tensor_contract.argtypes = [I, P(I), I, P(I), I, P(I), I, P(I), V, V, V, D, D, I, I]
+        L.orc_cmplx8_to_real8.argtypes = [D, D]
+        L.orc_cmplx8_to_real8.restype = D
+        L.orc_fill_uniform.argtypes = [I, Z, V, C.c_ulonglong]
+        _lib = L
+    return _lib
+
+
+def _iv(seq):
+    seq = list(seq)
+    return (C.c_int * max(1, len(seq)))(*seq)
+
+
+def _ptr(a):
+    return C.c_void_p(a.ctypes.data)
+
+
+def _fort(a):
+    """Fortran-ordered view/copy that keeps 0-d arrays 0-d (np.asfortranarray would not)."""
+    a = np.asarray(a)
+    return a if a.flags["F_CONTIGUOUS"] else np.asfortranarray(a)
+
+
+def str2dig(pattern):
+    """Returns (errc, digital, drank, lrank, rrank, conj_bits)."""
+    dig = (C.c_int * 256)()
+    dr, lr, rr, cj = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+    e = lib().orc_str2dig(pattern.encode(), dig, C.byref(dr), C.byref(lr), C.byref(rr), C.byref(cj))
+    n = max(0, lr.value + rr.value) if e == 0 else 0
+    return e, list(dig[:n]), dr.value, lr.value, rr.value, cj.value
+
+
+def permutations(cptrn, lrank, rrank, conj=0, variant="cpu", gemm_tl=1, gemm_tr=0):
+    """Matricization: (ierr, dprm[1:], lprm[1:], rprm[1:], ncd, nlu, nru, nhu)."""
+    a = _iv(cptrn)
+    d, l, r = (C.c_int * 64)(), (C.c_int * 64)(), (C.c_int * 64)()
+    ncd, nlu, nru, nhu = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+    if variant == "cpu":
+        e = lib().orc_contraction_permutations(gemm_tl, gemm_tr, lrank, rrank, a, conj, d, l, r,
+                                               C.byref(ncd), C.byref(nlu), C.byref(nru), C.byref(nhu))
+    else:
+        e = lib().orc_contr_permutations(gemm_tl, gemm_tr, lrank, rrank, a, conj, d, l, r,
+                                         C.byref(ncd), C.byref(nlu), C.byref(nru))
+    dr = sum(1 for x in cptrn if x > 0) - nhu.value
+    return e, list(d[1:1 + dr]), list(l[1:1 + lrank]), list(r[1:1 + rrank]), ncd.value, nlu.value, nru.value, nhu.value
+
+
+def out_dims(dims_in, o2n):
+    out = [0] * len(dims_in)
+    for i, p in enumerate(o2n):
+        out[p - 1] = dims_in[i]
+    return out
+
+
+def permute(a, o2n, conj=False, blocked=False, nthreads=1):
+    """Returns permute(a) as a Fortran-ordered array; a is Fortran-ordered with dims a.shape."""
+    a = _fort(a)
+    dims = list(a.shape)
+    out = np.empty(out_dims(dims, o2n), dtype=a.dtype, order="F")
+    kind = KIND_OF[a.dtype]
+    if blocked:
+        e = lib().orc_permute_blocked(kind, len(dims), _iv(dims), _iv(o2n), _ptr(a), _ptr(out), nthreads)
+    else:
+        e = lib().orc_permute(kind, len(dims), _iv(dims), _iv(o2n), _ptr(a), _ptr(out), 1 if conj else 0)
+    assert e == 0, e
+    return out
+
+
+def tensor_add(d, l, cptrn, sr=1.0, si=0.0, conj_bits=0):
+    """In place: d += permute(l) * s (reference cpu_tensor_block_add)."""
+    l = _fort(l)
+    assert d.flags["F_CONTIGUOUS"] and d.dtype == l.dtype
+    e = lib().orc_tensor_add(KIND_OF[d.dtype], _iv(cptrn), l.ndim, _iv(l.shape), _ptr(l), _ptr(d), sr, si, conj_bits)
+    assert e == 0, e
+    return d
+
+
+def tensor_copy(d, l, cptrn, conj_bits=0):
+    l = _fort(l)
+    e = lib().orc_tensor_copy(KIND_OF[d.dtype], _iv(cptrn), l.ndim, _iv(l.shape), _ptr(l), _ptr(d), conj_bits)
+    assert e == 0, e
+    return d
+
+
+def tensor_scale(d, sr, si=0.0, conj_bits=0):
+    e = lib().orc_tensor_scale(KIND_OF[d.dtype], d.size, _ptr(d), sr, si, conj_bits)
+    assert e == 0, e
+    return d
+
+
+def norm1(a):
+    a = np.ascontiguousarray(a.ravel(order="F"))
+    return lib().orc_norm1(KIND_OF[a.dtype], a.size, _ptr(a))
+
+
+def tensor_contract(d, l, r, cptrn, sr=1.0, si=0.0, conj_bits=0, accumulative=True):
+    """In place on d (Fortran-ordered): reference tensor_block_contract. Returns ierr."""
+    l = _fort(l)
+    r = _fort(r)
+    assert d.flags["F_CONTIGUOUS"]
+    return lib().orc_tensor_contract(KIND_OF[d.dtype], _iv(cptrn), d.ndim, _iv(d.shape), l.ndim, _iv(l.shape),
+                                     r.ndim, _iv(r.shape), _ptr(d), _ptr(l), _ptr(r), sr, si, conj_bits,
+                                     1 if accumulative else 0)
+
+
+def cmplx8_to_real8(re, im):
+    return lib().orc_cmplx8_to_real8(re, im)
+
+
+def uniform(dims, kind, seed):
+    """Seeded mt19937_64 uniform[-1,1] tensor (complex: re then im per element)."""
+    n = int(np.prod(dims)) if len(dims) else 1
+    a = np.empty(n, dtype=NP_DTYPE[kind])
+    lib().orc_fill_uniform(kind, n, _ptr(a), seed)
+    return a.reshape(dims, order="F") if len(dims) else a.reshape(())

@@ -1,0 +1,34 @@
+// Shared definitions of the talsh-b200 core (host and device code).
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+
+#include "talsh.h"
+#include "talsh_b200.h"
+
+namespace tb {
+
+constexpr int kMaxRank = MAX_TENSOR_RANK;
+
+inline int kind_size(int kind) {
+  switch (kind) {
+    case R4: return 4;
+    case R8: return 8;
+    case C4: return 8;
+    case C8: return 16;
+    default: return 0;
+  }
+}
+inline bool kind_is_complex(int kind) { return kind == C4 || kind == C8; }
+
+// Real approximant of a complex scale factor that keeps the modulus and the
+// sign of the real part (reference cmplx8_to_real8, tensor_algebra_cpu.F90:430-445).
+double cmplx8_to_real8(double re, double im);
+
+// Bookkeeping shared by the CUDA translation units.
+void note_launch(unsigned n = 1);
+void note_cuda_error(const char *what, int code);
+int check_launch(const char *what);  // 0 or TALSH_FAILURE after a kernel launch
+
+}  // namespace tb

@@ -1,0 +1,740 @@
+// Tensor contraction D = beta*D + alpha * sum_contracted L*R for sm_100a.
+//
+// Reference semantics: tensor_block_contract (tensor_algebra_cpu.F90:3675-4358)
+// and gpu_tensor_block_contract_dlf (tensor_algebra_gpu_nvidia.cu:5847-7183):
+// digital pattern, conjugation bits (the D bit flips the L and R bits), real
+// kinds use real(alpha), beta = 1 when accumulative else D is overwritten.
+//
+// Design (no transpose + GEMM + transpose): every operand stays in its own
+// layout.  The contraction is viewed as C[m,n] = sum_k A[m,k] B[k,n] where
+//   m runs over L's uncontracted indices (L order), n over R's uncontracted
+//   indices (R order) and k over the contracted pairs,
+// and three small offset tables (m -> L and D offsets, n -> R and D offsets,
+// k -> L and R offsets) built on the device turn every tile load into a
+// gather and the epilogue into a scatter in D's own layout.  Tile loads are
+// mapped so that the operand's stride-1 index runs across the lanes.
+//  * R8: warp-level DMMA (mma.sync m8n8k4 f64) on a multistage cp.async
+//    pipeline, FP64 end to end.
+//  * R4 / C4 / C8: register-blocked SIMT FMA kernel on the same tables.
+//  * Degenerate patterns: full contraction (dot, deterministic two-pass),
+//    scalar x tensor (the permute-add kernel with a device-side scale) and
+//    scalar x scalar.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+
+#include "common.h"
+
+namespace tb {
+int permute_scaled_by_device_scalar(int kind, int rank, const int *dims, const int *o2n,
+                                    const void *src, void *dst, double alpha_re, double alpha_im,
+                                    const void *scalar_dev, int scalar_conj, int tensor_conj,
+                                    int accumulate, void *stream);
+namespace {
+
+constexpr int kMaxGR = 24;  // max indices per group (m, n or k)
+
+struct TableParams {
+  int nm, nn, nk;
+  int64_t M, N, K;
+  int64_t mext[kMaxGR], mstrL[kMaxGR], mstrD[kMaxGR];
+  int64_t next[kMaxGR], nstrR[kMaxGR], nstrD[kMaxGR];
+  int64_t kext[kMaxGR], kstrL[kMaxGR], kstrR[kMaxGR];
+  int64_t *mL, *mD, *nR, *nD, *kL, *kR;
+};
+
+__global__ void build_tables_kernel(const TableParams T) {
+  const int64_t total = T.M + T.N + T.K;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
+    if (i < T.M) {
+      int64_t r = i, a = 0, b = 0;
+      for (int d = 0; d < T.nm; ++d) {
+        const int64_t c = r % T.mext[d];
+        r /= T.mext[d];
+        a += c * T.mstrL[d];
+        b += c * T.mstrD[d];
+      }
+      T.mL[i] = a;
+      T.mD[i] = b;
+    } else if (i < T.M + T.N) {
+      int64_t r = i - T.M, a = 0, b = 0;
+      for (int d = 0; d < T.nn; ++d) {
+        const int64_t c = r % T.next[d];
+        r /= T.next[d];
+        a += c * T.nstrR[d];
+        b += c * T.nstrD[d];
+      }
+      T.nR[i - T.M] = a;
+      T.nD[i - T.M] = b;
+    } else {
+      int64_t r = i - T.M - T.N, a = 0, b = 0;
+      for (int d = 0; d < T.nk; ++d) {
+        const int64_t c = r % T.kext[d];
+        r /= T.kext[d];
+        a += c * T.kstrL[d];
+        b += c * T.kstrR[d];
+      }
+      T.kL[i - T.M - T.N] = a;
+      T.kR[i - T.M - T.N] = b;
+    }
+  }
+}
+
+struct GemmArgs {
+  int M, N, K;
+  int tiles_m;
+  const int64_t *mL, *mD, *nR, *nD, *kL, *kR;
+  double alpha_re, alpha_im;
+  int beta;       // 1: D += ..., 0: D = ...
+  int a_along_m;  // A tile loads: lanes along m (else along k)
+  int b_along_n;  // B tile loads: lanes along n (else along k)
+  int conj_l, conj_r;
+};
+
+// ---------------------------------------------------------------- R8: DMMA
+__device__ __forceinline__ void cp_async8(void *smem_ptr, const void *gptr, bool valid) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem_ptr);
+  const int n = valid ? 8 : 0;
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gptr), "r"(n));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+__device__ __forceinline__ void dmma_8x8x4(double &c0, double &c1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(c0), "+d"(c1)
+               : "d"(a), "d"(b));
+}
+
+template <int BM, int BN>
+struct DmmaCfg {
+  static constexpr int WM = 32, WN = 32;            // warp tile
+  static constexpr int WARPS_M = BM / WM, WARPS_N = BN / WN;
+  static constexpr int THREADS = WARPS_M * WARPS_N * 32;
+  static constexpr int BK = 16, STAGES = 3;
+  static constexpr int AP = BM + 8, BP = BN + 8;    // pitches: 2-wavefront fragment loads
+  static constexpr size_t SMEM = (size_t)STAGES * BK * (AP + BP) * sizeof(double) +
+                                 (size_t)(2 * BM + 2 * BN) * sizeof(int64_t);
+};
+
+template <int BM, int BN>
+__global__ void __launch_bounds__(DmmaCfg<BM, BN>::THREADS)
+    dgemm_gather_kernel(const double *__restrict__ L, const double *__restrict__ R, double *D,
+                        const GemmArgs a) {
+  using C = DmmaCfg<BM, BN>;
+  constexpr int BK = C::BK, ST = C::STAGES, AP = C::AP, BP = C::BP, NT = C::THREADS;
+  extern __shared__ __align__(16) unsigned char smem[];
+  double *As = reinterpret_cast<double *>(smem);
+  double *Bs = As + ST * BK * AP;
+  int64_t *mLs = reinterpret_cast<int64_t *>(Bs + ST * BK * BP);
+  int64_t *mDs = mLs + BM;
+  int64_t *nRs = mDs + BM;
+  int64_t *nDs = nRs + BN;
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int tile_m = blockIdx.x % a.tiles_m, tile_n = blockIdx.x / a.tiles_m;
+  const int m0 = tile_m * BM, n0 = tile_n * BN;
+  for (int i = tid; i < BM; i += NT) {
+    const int m = m0 + i;
+    mLs[i] = m < a.M ? a.mL[m] : 0;
+    mDs[i] = m < a.M ? a.mD[m] : 0;
+  }
+  for (int i = tid; i < BN; i += NT) {
+    const int n = n0 + i;
+    nRs[i] = n < a.N ? a.nR[n] : 0;
+    nDs[i] = n < a.N ? a.nD[n] : 0;
+  }
+  __syncthreads();
+
+  const int numK = (a.K + BK - 1) / BK;
+  auto load_tile = [&](int kt, int s) {
+    double *as = As + s * BK * AP;
+    double *bs = Bs + s * BK * BP;
+#pragma unroll
+    for (int i = 0; i < (BM * BK) / NT; ++i) {
+      const int idx = tid + i * NT;
+      const int ml = a.a_along_m ? (idx % BM) : (idx / BK);
+      const int kl = a.a_along_m ? (idx / BM) : (idx % BK);
+      const int m = m0 + ml, k = kt * BK + kl;
+      const bool v = (m < a.M) && (k < a.K);
+      const double *src = v ? (L + mLs[ml] + a.kL[k]) : L;
+      cp_async8(as + kl * AP + ml, src, v);
+    }
+#pragma unroll
+    for (int i = 0; i < (BN * BK) / NT; ++i) {
+      const int idx = tid + i * NT;
+      const int nl = a.b_along_n ? (idx % BN) : (idx / BK);
+      const int kl = a.b_along_n ? (idx / BN) : (idx % BK);
+      const int n = n0 + nl, k = kt * BK + kl;
+      const bool v = (n < a.N) && (k < a.K);
+      const double *src = v ? (R + nRs[nl] + a.kR[k]) : R;
+      cp_async8(bs + kl * BP + nl, src, v);
+    }
+  };
+
+  constexpr int FM = C::WM / 8, FN = C::WN / 8;
+  double acc[FM][FN][2];
+#pragma unroll
+  for (int i = 0; i < FM; ++i)
+#pragma unroll
+    for (int j = 0; j < FN; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+
+  const int wm0 = (warp % C::WARPS_M) * C::WM, wn0 = (warp / C::WARPS_M) * C::WN;
+  const int fr = lane >> 2, fc = lane & 3;
+
+#pragma unroll
+  for (int s = 0; s < ST - 1; ++s) {
+    if (s < numK) load_tile(s, s);
+    cp_async_commit();
+  }
+  for (int kt = 0; kt < numK; ++kt) {
+    cp_async_wait<ST - 2>();
+    __syncthreads();
+    const int pre = kt + ST - 1;
+    if (pre < numK) load_tile(pre, pre % ST);
+    cp_async_commit();
+    const double *as = As + (kt % ST) * BK * AP;
+    const double *bs = Bs + (kt % ST) * BK * BP;
+#pragma unroll
+    for (int ks = 0; ks < BK / 4; ++ks) {
+      double af[FM], bf[FN];
+#pragma unroll
+      for (int i = 0; i < FM; ++i) af[i] = as[(ks * 4 + fc) * AP + wm0 + i * 8 + fr];
+#pragma unroll
+      for (int j = 0; j < FN; ++j) bf[j] = bs[(ks * 4 + fc) * BP + wn0 + j * 8 + fr];
+#pragma unroll
+      for (int i = 0; i < FM; ++i)
+#pragma unroll
+        for (int j = 0; j < FN; ++j) dmma_8x8x4(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
+    }
+  }
+  cp_async_wait<0>();
+
+  const double alpha = a.alpha_re;
+#pragma unroll
+  for (int i = 0; i < FM; ++i) {
+    const int ml = wm0 + i * 8 + fr;
+    if (m0 + ml >= a.M) continue;
+#pragma unroll
+    for (int j = 0; j < FN; ++j) {
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int nl = wn0 + j * 8 + fc * 2 + h;
+        if (n0 + nl >= a.N) continue;
+        double *p = D + mDs[ml] + nDs[nl];
+        *p = a.beta ? fma(alpha, acc[i][j][h], *p) : alpha * acc[i][j][h];
+      }
+    }
+  }
+}
+
+// ------------------------------------------------- R4 / C4 / C8: SIMT FMA
+template <typename T> struct Num;
+template <> struct Num<float> {
+  using A = float;
+  __device__ static A zero() { return 0.f; }
+  __device__ static A load(const float &x, bool) { return x; }
+  __device__ static void fma_acc(A &c, A x, A y) { c = fmaf(x, y, c); }
+  __device__ static float out(A acc, float d, double ar, double, int beta) {
+    const float v = acc * (float)ar;
+    return beta ? d + v : v;
+  }
+};
+template <> struct Num<double> {
+  using A = double;
+  __device__ static A zero() { return 0.0; }
+  __device__ static A load(const double &x, bool) { return x; }
+  __device__ static void fma_acc(A &c, A x, A y) { c = fma(x, y, c); }
+  __device__ static double out(A acc, double d, double ar, double, int beta) {
+    return beta ? fma(ar, acc, d) : ar * acc;
+  }
+};
+template <> struct Num<float2> {
+  using A = float2;
+  __device__ static A zero() { return make_float2(0.f, 0.f); }
+  __device__ static A load(const float2 &x, bool cj) { return cj ? make_float2(x.x, -x.y) : x; }
+  __device__ static void fma_acc(A &c, A x, A y) {
+    c.x = fmaf(x.x, y.x, c.x); c.x = fmaf(-x.y, y.y, c.x);
+    c.y = fmaf(x.x, y.y, c.y); c.y = fmaf(x.y, y.x, c.y);
+  }
+  __device__ static float2 out(A acc, float2 d, double ar, double ai, int beta) {
+    const float vr = acc.x * (float)ar - acc.y * (float)ai, vi = acc.x * (float)ai + acc.y * (float)ar;
+    return beta ? make_float2(d.x + vr, d.y + vi) : make_float2(vr, vi);
+  }
+};
+template <> struct Num<double2> {
+  using A = double2;
+  __device__ static A zero() { return make_double2(0.0, 0.0); }
+  __device__ static A load(const double2 &x, bool cj) { return cj ? make_double2(x.x, -x.y) : x; }
+  __device__ static void fma_acc(A &c, A x, A y) {
+    c.x = fma(x.x, y.x, c.x); c.x = fma(-x.y, y.y, c.x);
+    c.y = fma(x.x, y.y, c.y); c.y = fma(x.y, y.x, c.y);
+  }
+  __device__ static double2 out(A acc, double2 d, double ar, double ai, int beta) {
+    const double vr = acc.x * ar - acc.y * ai, vi = acc.x * ai + acc.y * ar;
+    return beta ? make_double2(d.x + vr, d.y + vi) : make_double2(vr, vi);
+  }
+};
+
+constexpr int kSBM = 64, kSBN = 64, kSBK = 16, kSThreads = 256;
+
+template <typename T>
+__global__ void __launch_bounds__(kSThreads)
+    gemm_gather_simt_kernel(const T *__restrict__ L, const T *__restrict__ R, T *D, const GemmArgs a) {
+  using A = typename Num<T>::A;
+  __shared__ A As[kSBK][kSBM + 1];
+  __shared__ A Bs[kSBK][kSBN + 1];
+  __shared__ int64_t mLs[kSBM], mDs[kSBM], nRs[kSBN], nDs[kSBN];
+  const int tid = threadIdx.x;
+  const int tile_m = blockIdx.x % a.tiles_m, tile_n = blockIdx.x / a.tiles_m;
+  const int m0 = tile_m * kSBM, n0 = tile_n * kSBN;
+  for (int i = tid; i < kSBM; i += kSThreads) {
+    const int m = m0 + i;
+    mLs[i] = m < a.M ? a.mL[m] : 0;
+    mDs[i] = m < a.M ? a.mD[m] : 0;
+  }
+  for (int i = tid; i < kSBN; i += kSThreads) {
+    const int n = n0 + i;
+    nRs[i] = n < a.N ? a.nR[n] : 0;
+    nDs[i] = n < a.N ? a.nD[n] : 0;
+  }
+  const int tr = tid % 16, tc = tid / 16;  // 16 x 16 threads, 4 x 4 outputs each
+  A acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = Num<T>::zero();
+  __syncthreads();
+  for (int k0 = 0; k0 < a.K; k0 += kSBK) {
+#pragma unroll
+    for (int i = 0; i < (kSBM * kSBK) / kSThreads; ++i) {
+      const int idx = tid + i * kSThreads;
+      const int ml = a.a_along_m ? (idx % kSBM) : (idx / kSBK);
+      const int kl = a.a_along_m ? (idx / kSBM) : (idx % kSBK);
+      const int m = m0 + ml, k = k0 + kl;
+      As[kl][ml] = (m < a.M && k < a.K) ? Num<T>::load(L[mLs[ml] + a.kL[k]], a.conj_l) : Num<T>::zero();
+    }
+#pragma unroll
+    for (int i = 0; i < (kSBN * kSBK) / kSThreads; ++i) {
+      const int idx = tid + i * kSThreads;
+      const int nl = a.b_along_n ? (idx % kSBN) : (idx / kSBK);
+      const int kl = a.b_along_n ? (idx / kSBN) : (idx % kSBK);
+      const int n = n0 + nl, k = k0 + kl;
+      Bs[kl][nl] = (n < a.N && k < a.K) ? Num<T>::load(R[nRs[nl] + a.kR[k]], a.conj_r) : Num<T>::zero();
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < kSBK; ++kk) {
+      A av[4], bv[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) av[i] = As[kk][tr + 16 * i];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) bv[j] = Bs[kk][tc + 16 * j];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) Num<T>::fma_acc(acc[i][j], av[i], bv[j]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int ml = tr + 16 * i;
+    if (m0 + ml >= a.M) continue;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int nl = tc + 16 * j;
+      if (n0 + nl >= a.N) continue;
+      T *p = D + mDs[ml] + nDs[nl];
+      *p = Num<T>::out(acc[i][j], a.beta ? *p : T(), a.alpha_re, a.alpha_im, a.beta);
+    }
+  }
+}
+
+// ------------------------------------------------------ full contraction
+constexpr int kDotThreads = 256;
+
+__device__ __forceinline__ double2 warp_sum2(double2 v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    v.x += __shfl_down_sync(0xffffffffu, v.x, o);
+    v.y += __shfl_down_sync(0xffffffffu, v.y, o);
+  }
+  return v;
+}
+__device__ double2 block_sum2(double2 v) {
+  __shared__ double2 ws[kDotThreads / 32];
+  v = warp_sum2(v);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) ws[warp] = v;
+  __syncthreads();
+  double2 r = make_double2(0.0, 0.0);
+  if (warp == 0) {
+    r = (lane < kDotThreads / 32) ? ws[lane] : make_double2(0.0, 0.0);
+    r = warp_sum2(r);
+  }
+  return r;
+}
+
+template <typename T> __device__ __forceinline__ double2 as_c(const T &x, bool cj);
+template <> __device__ __forceinline__ double2 as_c<float>(const float &x, bool) { return make_double2(x, 0.0); }
+template <> __device__ __forceinline__ double2 as_c<double>(const double &x, bool) { return make_double2(x, 0.0); }
+template <> __device__ __forceinline__ double2 as_c<float2>(const float2 &x, bool cj) { return make_double2(x.x, cj ? -x.y : x.y); }
+template <> __device__ __forceinline__ double2 as_c<double2>(const double2 &x, bool cj) { return make_double2(x.x, cj ? -x.y : x.y); }
+
+template <typename T> __device__ __forceinline__ void store_c(T *p, double2 v);
+template <> __device__ __forceinline__ void store_c<float>(float *p, double2 v) { *p = (float)v.x; }
+template <> __device__ __forceinline__ void store_c<double>(double *p, double2 v) { *p = v.x; }
+template <> __device__ __forceinline__ void store_c<float2>(float2 *p, double2 v) { *p = make_float2((float)v.x, (float)v.y); }
+template <> __device__ __forceinline__ void store_c<double2>(double2 *p, double2 v) { *p = v; }
+
+template <typename T>
+__global__ void __launch_bounds__(kDotThreads)
+    dot_partial_kernel(const T *__restrict__ L, const T *__restrict__ R, const int64_t *kL,
+                       const int64_t *kR, int64_t K, int64_t chunk, int cl, int cr, double2 *part) {
+  const int64_t beg = (int64_t)blockIdx.x * chunk, end = min(K, beg + chunk);
+  double2 acc = make_double2(0.0, 0.0);
+  for (int64_t k = beg + threadIdx.x; k < end; k += kDotThreads) {
+    const double2 x = as_c<T>(L[kL[k]], cl), y = as_c<T>(R[kR[k]], cr);
+    acc.x += x.x * y.x - x.y * y.y;
+    acc.y += x.x * y.y + x.y * y.x;
+  }
+  const double2 s = block_sum2(acc);
+  if (threadIdx.x == 0) part[blockIdx.x] = s;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kDotThreads)
+    dot_final_kernel(const double2 *part, int n, T *D, double ar, double ai, int beta) {
+  double2 acc = make_double2(0.0, 0.0);
+  for (int i = threadIdx.x; i < n; i += kDotThreads) { acc.x += part[i].x; acc.y += part[i].y; }
+  const double2 s = block_sum2(acc);
+  if (threadIdx.x == 0) {
+    double2 v = make_double2(s.x * ar - s.y * ai, s.x * ai + s.y * ar);
+    if (beta) {
+      const double2 d = as_c<T>(*D, false);
+      v.x += d.x;
+      v.y += d.y;
+    }
+    store_c<T>(D, v);
+  }
+}
+
+// scalar x scalar: d = (beta ? d : 0) + (l*r)*alpha in complex(8) arithmetic.
+template <typename T>
+__global__ void scalar_mul_kernel(const T *L, const T *R, T *D, double ar, double ai, int cl,
+                                  int cr, int beta) {
+  const double2 l = as_c<T>(*L, cl), r = as_c<T>(*R, cr);
+  const double2 p = make_double2(l.x * r.x - l.y * r.y, l.x * r.y + l.y * r.x);
+  double2 v = make_double2(p.x * ar - p.y * ai, p.x * ai + p.y * ar);
+  if (beta) {
+    const double2 d = as_c<T>(*D, false);
+    v.x = d.x + v.x;
+    v.y = d.y + v.y;
+  }
+  store_c<T>(D, v);
+}
+
+int dot_blocks(int64_t K) {
+  int64_t b = (K + 16383) / 16384;
+  return (int)std::max<int64_t>(1, std::min<int64_t>(b, 1024));
+}
+
+struct Analysis {
+  TableParams T;
+  bool a_along_m = true, b_along_n = true;
+  int hyper = 0;
+};
+
+int64_t align_up(int64_t x, int64_t a) { return (x + a - 1) / a * a; }
+
+// Splits the pattern into m / n / k index groups with their strides.
+int analyze(const int *cptrn, int drank, const int *ddims, int lrank, const int *ldims, int rrank,
+            const int *rdims, Analysis &an) {
+  TableParams &T = an.T;
+  std::memset(&T, 0, sizeof(T));
+  int64_t dstr[kMaxRank], lstr[kMaxRank], rstr[kMaxRank];
+  int64_t s = 1;
+  for (int i = 0; i < drank; ++i) { dstr[i] = s; s *= ddims[i]; }
+  s = 1;
+  for (int i = 0; i < lrank; ++i) { lstr[i] = s; s *= ldims[i]; }
+  s = 1;
+  for (int i = 0; i < rrank; ++i) { rstr[i] = s; s *= rdims[i]; }
+  // Validation in the manner of the GPU path (reference :5934-5966).
+  int dseen[kMaxRank] = {0}, lseen[kMaxRank] = {0}, rseen[kMaxRank] = {0};
+  for (int i = 0; i < lrank; ++i) {
+    const int j = cptrn[i];
+    if (j > 0) {
+      if (j > drank || ddims[j - 1] != ldims[i]) return TALSH_INVALID_ARGS;
+      dseen[j - 1]++;
+    } else if (j < 0) {
+      if (-j > rrank || rdims[-j - 1] != ldims[i] || cptrn[lrank - j - 1] != -(i + 1)) return TALSH_INVALID_ARGS;
+      if (rseen[-j - 1]++) return TALSH_INVALID_ARGS;
+    } else {
+      return TALSH_INVALID_ARGS;
+    }
+  }
+  for (int i = 0; i < rrank; ++i) {
+    const int j = cptrn[lrank + i];
+    if (j > 0) {
+      if (j > drank || ddims[j - 1] != rdims[i]) return TALSH_INVALID_ARGS;
+      dseen[j - 1]++;
+    } else if (j < 0) {
+      if (-j > lrank || ldims[-j - 1] != rdims[i] || cptrn[-j - 1] != -(i + 1)) return TALSH_INVALID_ARGS;
+      if (lseen[-j - 1]++) return TALSH_INVALID_ARGS;
+    } else {
+      return TALSH_INVALID_ARGS;
+    }
+  }
+  for (int i = 0; i < drank; ++i) {
+    if (dseen[i] == 2) an.hyper++;
+    else if (dseen[i] != 1) return TALSH_INVALID_ARGS;
+  }
+  if (an.hyper) return TALSH_SUCCESS;
+  int64_t lvol = 1, rvol = 1;
+  for (int i = 0; i < lrank; ++i) lvol *= ldims[i];
+  for (int i = 0; i < rrank; ++i) rvol *= rdims[i];
+  // m: L uncontracted in L order; n: R uncontracted in R order.
+  T.M = T.N = T.K = 1;
+  for (int i = 0; i < lrank; ++i) {
+    if (cptrn[i] > 0 && ldims[i] > 1) {
+      if (T.nm >= kMaxGR) return TALSH_LIMIT_EXCEEDED;
+      T.mext[T.nm] = ldims[i]; T.mstrL[T.nm] = lstr[i]; T.mstrD[T.nm] = dstr[cptrn[i] - 1];
+      T.M *= ldims[i]; T.nm++;
+    }
+  }
+  for (int i = 0; i < rrank; ++i) {
+    if (cptrn[lrank + i] > 0 && rdims[i] > 1) {
+      if (T.nn >= kMaxGR) return TALSH_LIMIT_EXCEEDED;
+      T.next[T.nn] = rdims[i]; T.nstrR[T.nn] = rstr[i]; T.nstrD[T.nn] = dstr[cptrn[lrank + i] - 1];
+      T.N *= rdims[i]; T.nn++;
+    }
+  }
+  // k: follow R's order when R's leading index is contracted and L's is not
+  // (or R is the larger operand), otherwise L's order.
+  const bool l_lead_k = lrank > 0 && cptrn[0] < 0;
+  const bool r_lead_k = rrank > 0 && cptrn[lrank] < 0;
+  const bool k_in_r_order = r_lead_k && (!l_lead_k || rvol > lvol);
+  if (k_in_r_order) {
+    for (int i = 0; i < rrank; ++i) {
+      const int j = cptrn[lrank + i];
+      if (j < 0 && rdims[i] > 1) {
+        if (T.nk >= kMaxGR) return TALSH_LIMIT_EXCEEDED;
+        T.kext[T.nk] = rdims[i]; T.kstrR[T.nk] = rstr[i]; T.kstrL[T.nk] = lstr[-j - 1];
+        T.K *= rdims[i]; T.nk++;
+      }
+    }
+  } else {
+    for (int i = 0; i < lrank; ++i) {
+      const int j = cptrn[i];
+      if (j < 0 && ldims[i] > 1) {
+        if (T.nk >= kMaxGR) return TALSH_LIMIT_EXCEEDED;
+        T.kext[T.nk] = ldims[i]; T.kstrL[T.nk] = lstr[i]; T.kstrR[T.nk] = rstr[-j - 1];
+        T.K *= ldims[i]; T.nk++;
+      }
+    }
+  }
+  // Lane mapping for the tile loads: along the operand's stride-1 group.
+  an.a_along_m = T.nm > 0 && (T.nk == 0 || T.mstrL[0] <= T.kstrL[0]);
+  an.b_along_n = T.nn > 0 && (T.nk == 0 || T.nstrR[0] <= T.kstrR[0]);
+  return TALSH_SUCCESS;
+}
+
+size_t table_bytes(const TableParams &T) {
+  return (size_t)align_up(8 * (2 * T.M + 2 * T.N + 2 * T.K), 256);
+}
+
+int sm_count_dev() {
+  static int cache = 0;
+  if (cache == 0) {
+    int dev = 0, v = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0) v = 148;
+    cache = v;
+  }
+  return cache;
+}
+
+template <int BM, int BN>
+int launch_dmma(const double *L, const double *R, double *D, GemmArgs ga, cudaStream_t st) {
+  using C = DmmaCfg<BM, BN>;
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaFuncSetAttribute(dgemm_gather_kernel<BM, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)C::SMEM);
+    attr_set = true;
+  }
+  ga.tiles_m = (ga.M + BM - 1) / BM;
+  const int64_t tiles = (int64_t)ga.tiles_m * ((ga.N + BN - 1) / BN);
+  if (tiles > 0x7fffffffLL) return TALSH_LIMIT_EXCEEDED;
+  dgemm_gather_kernel<BM, BN><<<(unsigned)tiles, C::THREADS, C::SMEM, st>>>(L, R, D, ga);
+  note_launch();
+  return check_launch("dgemm_gather_kernel");
+}
+
+template <typename T>
+int launch_simt(const void *L, const void *R, void *D, GemmArgs ga, cudaStream_t st) {
+  ga.tiles_m = (ga.M + kSBM - 1) / kSBM;
+  const int64_t tiles = (int64_t)ga.tiles_m * ((ga.N + kSBN - 1) / kSBN);
+  if (tiles > 0x7fffffffLL) return TALSH_LIMIT_EXCEEDED;
+  gemm_gather_simt_kernel<T><<<(unsigned)tiles, kSThreads, 0, st>>>((const T *)L, (const T *)R,
+                                                                     (T *)D, ga);
+  note_launch();
+  return check_launch("gemm_gather_simt_kernel");
+}
+
+template <typename T>
+int launch_dot(const void *L, const void *R, void *D, const int64_t *kL, const int64_t *kR,
+               int64_t K, int cl, int cr, double ar, double ai, int beta, double2 *part,
+               cudaStream_t st) {
+  const int nb = dot_blocks(K);
+  const int64_t chunk = (K + nb - 1) / nb;
+  dot_partial_kernel<T><<<nb, kDotThreads, 0, st>>>((const T *)L, (const T *)R, kL, kR, K, chunk, cl, cr, part);
+  note_launch();
+  dot_final_kernel<T><<<1, kDotThreads, 0, st>>>(part, nb, (T *)D, ar, ai, beta);
+  note_launch();
+  return check_launch("dot_kernels");
+}
+
+template <typename T>
+int launch_scalar(const void *L, const void *R, void *D, double ar, double ai, int cl, int cr,
+                  int beta, cudaStream_t st) {
+  scalar_mul_kernel<T><<<1, 1, 0, st>>>((const T *)L, (const T *)R, (T *)D, ar, ai, cl, cr, beta);
+  note_launch();
+  return check_launch("scalar_mul_kernel");
+}
+
+// Shape / kind checks shared by the scratch query and the launch.
+int check_args(int kind, const int *cptrn, int drank, const int *ddims, int lrank, const int *ldims,
+               int rrank, const int *rdims) {
+  if (kind_size(kind) == 0) return TALSH_INVALID_ARGS;
+  if (drank < 0 || lrank < 0 || rrank < 0 || drank > kMaxRank || lrank > kMaxRank || rrank > kMaxRank)
+    return TALSH_INVALID_ARGS;
+  if ((lrank + rrank > 0 && cptrn == nullptr) || (drank > 0 && ddims == nullptr) ||
+      (lrank > 0 && ldims == nullptr) || (rrank > 0 && rdims == nullptr))
+    return TALSH_INVALID_ARGS;
+  for (int i = 0; i < drank; ++i) if (ddims[i] <= 0) return TALSH_INVALID_ARGS;
+  for (int i = 0; i < lrank; ++i) if (ldims[i] <= 0) return TALSH_INVALID_ARGS;
+  for (int i = 0; i < rrank; ++i) if (rdims[i] <= 0) return TALSH_INVALID_ARGS;
+  return TALSH_SUCCESS;
+}
+
+}  // namespace
+
+// Scratch bytes needed by tcTensorContract for this shape (0 when none).
+size_t contract_scratch_bytes(int kind, const int *cptrn, int drank, const int *ddims, int lrank,
+                              const int *ldims, int rrank, const int *rdims) {
+  if (check_args(kind, cptrn, drank, ddims, lrank, ldims, rrank, rdims)) return 0;
+  if (lrank == 0 || rrank == 0) return 0;
+  Analysis an;
+  if (analyze(cptrn, drank, ddims, lrank, ldims, rrank, rdims, an) || an.hyper) return 0;
+  size_t b = table_bytes(an.T);
+  if (drank == 0) b += (size_t)dot_blocks(an.T.K) * sizeof(double2);
+  return b;
+}
+
+int contract_launch(int kind, const int *cptrn, int drank, const int *ddims, int lrank,
+                    const int *ldims, int rrank, const int *rdims, void *D, const void *L,
+                    const void *R, double alpha_re, double alpha_im, int conj_bits,
+                    int accumulative, void *scratch, size_t scratch_bytes, void *stream) {
+  int rc = check_args(kind, cptrn, drank, ddims, lrank, ldims, rrank, rdims);
+  if (rc) return rc;
+  if (D == nullptr || L == nullptr || R == nullptr) return TALSH_INVALID_ARGS;
+  const bool cplx = kind_is_complex(kind);
+  int cl = 0, cr = 0;
+  if (cplx) {
+    int cb = conj_bits & 7;
+    if (cb & 1) cb ^= 7;  // a conjugated destination conjugates both inputs instead
+    cl = (cb >> 1) & 1;
+    cr = (cb >> 2) & 1;
+  }
+  const double ar = alpha_re, ai = cplx ? alpha_im : 0.0;
+  const int beta = accumulative ? 1 : 0;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (lrank == 0 && rrank == 0) {
+    if (drank != 0) return TALSH_INVALID_ARGS;
+    switch (kind) {
+      case R4: return launch_scalar<float>(L, R, D, alpha_re, alpha_im, cl, cr, beta, st);
+      case R8: return launch_scalar<double>(L, R, D, alpha_re, alpha_im, cl, cr, beta, st);
+      case C4: return launch_scalar<float2>(L, R, D, alpha_re, alpha_im, cl, cr, beta, st);
+      default: return launch_scalar<double2>(L, R, D, alpha_re, alpha_im, cl, cr, beta, st);
+    }
+  }
+  if (lrank == 0 || rrank == 0) {
+    // scalar x tensor: D (+)= permute(T) * (s * alpha), the reference's ADD_TENSOR case.
+    const int trank = lrank ? lrank : rrank;
+    const int *tdims = lrank ? ldims : rdims;
+    const int *tptrn = lrank ? cptrn : cptrn + lrank;
+    if (trank != drank) return TALSH_INVALID_ARGS;
+    for (int i = 0; i < trank; ++i)
+      if (tptrn[i] < 1 || tptrn[i] > drank || ddims[tptrn[i] - 1] != tdims[i]) return TALSH_INVALID_ARGS;
+    return permute_scaled_by_device_scalar(kind, trank, tdims, tptrn, lrank ? L : R, D, alpha_re,
+                                           alpha_im, lrank ? R : L, lrank ? cr : cl,
+                                           lrank ? cl : cr, beta, stream);
+  }
+  Analysis an;
+  if ((rc = analyze(cptrn, drank, ddims, lrank, ldims, rrank, rdims, an)) != 0) return rc;
+  if (an.hyper) return TALSH_NOT_IMPLEMENTED;
+  TableParams T = an.T;
+  const size_t need = table_bytes(T) + (drank == 0 ? (size_t)dot_blocks(T.K) * sizeof(double2) : 0);
+  if (scratch == nullptr || scratch_bytes < need) return TALSH_INVALID_ARGS;
+  if (T.M > 0x7fffffffLL || T.N > 0x7fffffffLL || T.K > 0x7fffffffLL) return TALSH_LIMIT_EXCEEDED;
+  int64_t *base = (int64_t *)scratch;
+  T.mL = base; T.mD = T.mL + T.M; T.nR = T.mD + T.M; T.nD = T.nR + T.N; T.kL = T.nD + T.N; T.kR = T.kL + T.K;
+  {
+    const int64_t total = T.M + T.N + T.K;
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((total + 255) / 256, 4096));
+    build_tables_kernel<<<grid, 256, 0, st>>>(T);
+    note_launch();
+    if ((rc = check_launch("build_tables_kernel")) != 0) return rc;
+  }
+  if (drank == 0) {
+    double2 *part = (double2 *)((char *)scratch + table_bytes(T));
+    switch (kind) {
+      case R4: return launch_dot<float>(L, R, D, T.kL, T.kR, T.K, cl, cr, ar, ai, beta, part, st);
+      case R8: return launch_dot<double>(L, R, D, T.kL, T.kR, T.K, cl, cr, ar, ai, beta, part, st);
+      case C4: return launch_dot<float2>(L, R, D, T.kL, T.kR, T.K, cl, cr, ar, ai, beta, part, st);
+      default: return launch_dot<double2>(L, R, D, T.kL, T.kR, T.K, cl, cr, ar, ai, beta, part, st);
+    }
+  }
+  GemmArgs ga;
+  std::memset(&ga, 0, sizeof(ga));
+  ga.M = (int)T.M; ga.N = (int)T.N; ga.K = (int)T.K;
+  ga.mL = T.mL; ga.mD = T.mD; ga.nR = T.nR; ga.nD = T.nD; ga.kL = T.kL; ga.kR = T.kR;
+  ga.alpha_re = ar; ga.alpha_im = ai; ga.beta = beta;
+  ga.a_along_m = an.a_along_m ? 1 : 0;
+  ga.b_along_n = an.b_along_n ? 1 : 0;
+  ga.conj_l = cl; ga.conj_r = cr;
+  switch (kind) {
+    case R8: {
+      const int64_t big_tiles = ((T.M + 127) / 128) * ((T.N + 127) / 128);
+      if (big_tiles >= 2 * sm_count_dev())
+        return launch_dmma<128, 128>((const double *)L, (const double *)R, (double *)D, ga, st);
+      return launch_dmma<64, 64>((const double *)L, (const double *)R, (double *)D, ga, st);
+    }
+    case R4: return launch_simt<float>(L, R, D, ga, st);
+    case C4: return launch_simt<float2>(L, R, D, ga, st);
+    default: return launch_simt<double2>(L, R, D, ga, st);
+  }
+}
+
+}  // namespace tb
+
+extern "C" size_t tcTensorContractScratch(int data_kind, const int *cptrn, int drank,
+                                          const int *ddims, int lrank, const int *ldims,
+                                          int rrank, const int *rdims) {
+  return tb::contract_scratch_bytes(data_kind, cptrn, drank, ddims, lrank, ldims, rrank, rdims);
+}
+
+extern "C" int tcTensorContract(int data_kind, const int *cptrn, int drank, const int *ddims,
+                                int lrank, const int *ldims, int rrank, const int *rdims, void *D,
+                                const void *L, const void *R, double alpha_re, double alpha_im,
+                                int conj_bits, int accumulative, void *scratch,
+                                size_t scratch_bytes, void *stream) {
+  return tb::contract_launch(data_kind, cptrn, drank, ddims, lrank, ldims, rrank, rdims, D, L, R,
+                             alpha_re, alpha_im, conj_bits, accumulative, scratch, scratch_bytes,
+                             stream);
+}

@@ -1,0 +1,1759 @@
+// The TAL-SH runtime of talsh-b200: implements talsh.h on top of the sm_100a
+// kernels (talsh_b200.h).
+//
+// Behaviour follows the reference runtime talshc.cpp (talshInit :546,
+// talshTensorConstruct :1167, talshTaskFinalize :2064, talshTaskStatus :2336,
+// talshTensorPlace :3318, talshTensorCopy :4530, talshTensorAdd :4795,
+// talshTensorContract :5073): tensors own up to TALSH_MAX_DEV_PRESENT body
+// images, every operation picks a source image per argument, stages images
+// that live elsewhere onto the executing GPU, and applies the two-bit
+// coherence code of each argument when its task completes (D discard, M move,
+// T temporary, K keep).
+//
+// B200-specific design:
+//  * one in-order CUDA stream per GPU carries every task, so data
+//    dependencies between asynchronous tasks are honoured without tracking;
+//  * each task records four events (start, inputs ready, compute done,
+//    finished) that give the TAL-SH task status ladder and timings;
+//  * device memory comes from the stream-ordered CUDA allocator with a byte
+//    budget per GPU (90% of free memory at init by default, environment
+//    variable TALSH_B200_GPU_BUDGET_BYTES overrides it); exceeding the budget
+//    returns TRY_LATER and the operation leaves no trace;
+//  * Host bodies allocated by the library are pinned, so staging copies are
+//    asynchronous DMA transfers.
+// There is no CPU compute path: operations requested on DEV_HOST return
+// TALSH_NOT_AVAILABLE.
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <unordered_map>
+#include <vector>
+
+#include "common.h"
+
+namespace tb {
+int norm1_launch(int data_kind, size_t vol, const void *src, double *result_dev, double *partial,
+                 cudaStream_t st);
+size_t contract_scratch_bytes(int kind, const int *cptrn, int drank, const int *ddims, int lrank,
+                              const int *ldims, int rrank, const int *rdims);
+int contract_launch(int kind, const int *cptrn, int drank, const int *ddims, int lrank,
+                    const int *ldims, int rrank, const int *rdims, void *D, const void *L,
+                    const void *R, double alpha_re, double alpha_im, int conj_bits,
+                    int accumulative, void *scratch, size_t scratch_bytes, void *stream);
+
+namespace {
+
+constexpr unsigned kTwoBits = 3u;
+
+struct AllocRec {
+  int gpu;       // -1: host
+  size_t bytes;
+  bool pinned;   // host only
+};
+
+struct GpuCtx {
+  bool in_use = false;
+  cudaStream_t stream = nullptr;
+  size_t budget = 0, used = 0, peak = 0;
+  double flops = 0.0, bytes = 0.0;
+  unsigned long long tasks_ok = 0, tasks_failed = 0, try_later = 0;
+  std::vector<cudaEvent_t> event_pool;
+};
+
+struct Runtime {
+  bool on = false;
+  GpuCtx gpu[MAX_GPUS_PER_NODE];
+  std::unordered_map<void *, AllocRec> allocs;
+  bool log_ops = false;
+  size_t host_bytes = 0;
+  int mem_policy = MEM_ALLOC_TMP_BUF, mem_fallback = 1;
+};
+Runtime R;
+std::recursive_mutex g_mu;
+
+int node_gpu_count() {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
+
+// ---------------------------------------------------------------- memory
+void *host_alloc(size_t bytes, bool try_pinned) {
+  void *p = nullptr;
+  bool pinned = false;
+  if (try_pinned && cudaHostAlloc(&p, bytes, cudaHostAllocPortable) == cudaSuccess) {
+    pinned = true;
+  } else {
+    cudaGetLastError();
+    p = std::malloc(bytes);
+  }
+  if (p) {
+    R.allocs[p] = AllocRec{-1, bytes, pinned};
+    R.host_bytes += bytes;
+  }
+  return p;
+}
+
+bool any_gpu_in_use() {
+  for (auto &g : R.gpu) if (g.in_use) return true;
+  return false;
+}
+
+int dev_alloc(int gpu, size_t bytes, void **p) {
+  GpuCtx &G = R.gpu[gpu];
+  if (bytes == 0) bytes = 16;
+  bytes = (bytes + 255) & ~size_t(255);
+  if (G.used + bytes > G.budget) { G.try_later++; return TRY_LATER; }
+  cudaSetDevice(gpu);
+  if (cudaMallocAsync(p, bytes, G.stream) != cudaSuccess) {
+    cudaGetLastError();
+    G.try_later++;
+    return TRY_LATER;
+  }
+  G.used += bytes;
+  if (G.used > G.peak) G.peak = G.used;
+  R.allocs[*p] = AllocRec{gpu, bytes, false};
+  return TALSH_SUCCESS;
+}
+
+// Frees library-owned memory (host or device); unknown pointers are ignored.
+int mem_free(void *p) {
+  if (p == nullptr) return TALSH_SUCCESS;
+  auto it = R.allocs.find(p);
+  if (it == R.allocs.end()) return NOT_CLEAN;
+  const AllocRec a = it->second;
+  R.allocs.erase(it);
+  if (a.gpu < 0) {
+    if (a.pinned) cudaFreeHost(p); else std::free(p);
+    R.host_bytes -= a.bytes;
+  } else {
+    GpuCtx &G = R.gpu[a.gpu];
+    cudaSetDevice(a.gpu);
+    cudaFreeAsync(p, G.stream);
+    G.used -= a.bytes;
+  }
+  return TALSH_SUCCESS;
+}
+
+cudaEvent_t event_get(int gpu) {
+  GpuCtx &G = R.gpu[gpu];
+  if (!G.event_pool.empty()) {
+    cudaEvent_t e = G.event_pool.back();
+    G.event_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  cudaSetDevice(gpu);
+  cudaEventCreate(&e);
+  return e;
+}
+void event_put(int gpu, cudaEvent_t e) {
+  if (e) R.gpu[gpu].event_pool.push_back(e);
+}
+
+// ---------------------------------------------------------------- tensors
+size_t shape_volume(const talsh_tens_shape_t *s) {
+  size_t v = 1;
+  for (int i = 0; i < s->num_dim; ++i) v *= (size_t)s->dims[i];
+  return v;
+}
+
+bool healthy(const talsh_tens_t *t) {
+  return t->shape_p != nullptr && t->dev_rsc != nullptr && t->data_kind != nullptr &&
+         t->avail != nullptr && t->ndev >= 0 && t->ndev <= t->dev_rsc_len;
+}
+
+// Releases the memory behind an image descriptor (attached memory is only detached).
+int rsc_release(talsh_dev_rsc_t *r) {
+  int rc = TALSH_SUCCESS;
+  if (r->gmem_p != nullptr && r->mem_attached == 0) rc = mem_free(r->gmem_p);
+  tensDevRsc_clean(r);
+  return rc;
+}
+
+// Discards image i (not allowed when no other available image exists).
+int image_discard(talsh_tens_t *t, int i) {
+  if (i < 0 || i >= t->ndev) return TALSH_INVALID_ARGS;
+  int others = 0;
+  for (int j = 0; j < t->ndev; ++j) if (j != i && t->avail[j] == YEP) ++others;
+  if (others == 0) return TALSH_NOT_ALLOWED;
+  const int rc = rsc_release(&t->dev_rsc[i]);
+  const int last = t->ndev - 1;
+  if (i < last) {
+    t->dev_rsc[i] = t->dev_rsc[last];
+    t->data_kind[i] = t->data_kind[last];
+    t->avail[i] = t->avail[last];
+  }
+  tensDevRsc_clean(&t->dev_rsc[last]);
+  t->data_kind[last] = NO_TYPE;
+  t->avail[last] = NOPE;
+  t->ndev--;
+  return rc;
+}
+
+// Keeps only image i, moved to slot 0.
+int image_discard_other(talsh_tens_t *t, int i) {
+  if (i < 0 || i >= t->ndev || t->avail[i] != YEP) return TALSH_NOT_ALLOWED;
+  int rc = TALSH_SUCCESS;
+  for (int j = 0; j < t->ndev; ++j) {
+    if (j == i) continue;
+    if (rsc_release(&t->dev_rsc[j]) != TALSH_SUCCESS) rc = NOT_CLEAN;
+  }
+  if (i > 0) {
+    t->dev_rsc[0] = t->dev_rsc[i];
+    t->data_kind[0] = t->data_kind[i];
+    t->avail[0] = t->avail[i];
+  }
+  for (int j = 1; j < t->dev_rsc_len; ++j) {
+    tensDevRsc_clean(&t->dev_rsc[j]);
+    t->data_kind[j] = NO_TYPE;
+    t->avail[j] = NOPE;
+  }
+  t->ndev = 1;
+  return rc;
+}
+
+int find_image(const talsh_tens_t *t, int dev_id, const void *p) {
+  for (int i = 0; i < t->ndev; ++i)
+    if (t->dev_rsc[i].dev_id == dev_id && t->dev_rsc[i].gmem_p == p) return i;
+  return -1;
+}
+
+// Preferred image for execution on [dvk, dvn]: that device, then that kind, then Host.
+int choose_image(const talsh_tens_t *t, int dvk, int dvn) {
+  int same_kind = -1, host = -1;
+  for (int i = 0; i < t->ndev; ++i) {
+    if (t->avail[i] != YEP) continue;
+    int dk = DEV_NULL;
+    const int dn = decode_device_id(t->dev_rsc[i].dev_id, &dk);
+    if (dn < 0) continue;
+    if (dk == dvk) {
+      if (dn == dvn) return i;
+      if (same_kind < 0) same_kind = i;
+    }
+    if (dk == DEV_HOST && host < 0) host = i;
+  }
+  return same_kind >= 0 ? same_kind : host;
+}
+
+// ---------------------------------------------------------------- tasks
+struct ArgRec {
+  talsh_tens_t *t = nullptr;
+  int src_dev = -1;        // flat id of the source image
+  void *src_ptr = nullptr;
+  void *dptr = nullptr;    // body used on the executing GPU
+  bool dalloc = false;     // staged copy owned by the task
+  unsigned coh = COPY_T;
+  bool output = false;
+  bool need_input = true;
+  bool copy_back = false;  // output copied back into the source image
+  size_t bytes = 0;
+};
+
+struct TaskRec {
+  int gpu = -1;
+  cudaStream_t st = nullptr;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};  // start, comput, output, finish
+  int nargs = 0;
+  ArgRec a[MAX_TENSOR_OPERANDS];
+  void *scratch = nullptr;
+  int failed = 0;
+  bool finalized = false;
+  double times[4] = {0, 0, 0, 0};  // total, comput, input, output (seconds)
+};
+
+TaskRec *rec_of(const talsh_task_t *t) { return (TaskRec *)t->task_p; }
+
+void release_task_events(TaskRec *tr) {
+  for (auto &e : tr->ev) { event_put(tr->gpu, e); e = nullptr; }
+}
+
+// Applies coherence control and frees task resources (reference talshTaskFinalize :2064).
+int task_finalize(talsh_task_t *task, bool success) {
+  TaskRec *tr = rec_of(task);
+  if (tr == nullptr || tr->finalized) return TALSH_SUCCESS;
+  int rc = TALSH_SUCCESS;
+  if (success) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, tr->ev[0], tr->ev[3]) == cudaSuccess) tr->times[0] = ms * 1e-3;
+    if (cudaEventElapsedTime(&ms, tr->ev[1], tr->ev[2]) == cudaSuccess) tr->times[1] = ms * 1e-3;
+    if (cudaEventElapsedTime(&ms, tr->ev[0], tr->ev[1]) == cudaSuccess) tr->times[2] = ms * 1e-3;
+    if (cudaEventElapsedTime(&ms, tr->ev[2], tr->ev[3]) == cudaSuccess) tr->times[3] = ms * 1e-3;
+    cudaGetLastError();
+    task->exec_time = tr->times[0];
+  }
+  for (int i = tr->nargs - 1; i >= 0; --i) {
+    ArgRec &a = tr->a[i];
+    talsh_tens_t *t = a.t;
+    if (t == nullptr || !healthy(t)) { rc = TALSH_FAILURE; continue; }
+    int img = find_image(t, a.src_dev, a.src_ptr);
+    if (a.dalloc) {
+      if (success && (a.coh == COPY_M || a.coh == COPY_K) && t->ndev < t->dev_rsc_len) {
+        const int k = t->ndev++;
+        t->dev_rsc[k].dev_id = encode_device_id(DEV_NVIDIA_GPU, tr->gpu);
+        t->dev_rsc[k].gmem_p = a.dptr;
+        t->dev_rsc[k].buf_entry = -1;
+        t->dev_rsc[k].mem_attached = 0;
+        t->data_kind[k] = task->data_kind;
+        t->avail[k] = YEP;
+      } else {
+        mem_free(a.dptr);
+      }
+      a.dptr = nullptr;
+    }
+    if (img < 0) continue;
+    if (success && (a.coh == COPY_D || a.coh == COPY_M)) {
+      if (t->avail[img] == NOPE) {
+        if (t->ndev > 1) {
+          if (image_discard(t, img) != TALSH_SUCCESS) rc = NOT_CLEAN;
+        } else {
+          t->avail[img] = YEP;
+        }
+      }
+    } else {
+      t->avail[img] = YEP;
+    }
+  }
+  if (tr->scratch) { mem_free(tr->scratch); tr->scratch = nullptr; }
+  GpuCtx &G = R.gpu[tr->gpu];
+  if (success) {
+    G.tasks_ok++;
+    G.flops += task->flops;
+    G.bytes += task->data_vol;
+  } else {
+    G.tasks_failed++;
+  }
+  tr->finalized = true;
+  task->task_error = success ? (rc == TALSH_SUCCESS ? 0 : 13) : (tr->failed > 0 ? tr->failed : 13);
+  return rc;
+}
+
+// Polls (wait=false) or waits for the task's last event; finalizes when done.
+int task_progress(talsh_task_t *task, bool wait) {
+  TaskRec *tr = rec_of(task);
+  if (tr == nullptr) return TALSH_INVALID_ARGS;
+  if (tr->finalized) return task->task_error == 0 ? TALSH_TASK_COMPLETED : TALSH_TASK_ERROR;
+  cudaSetDevice(tr->gpu);
+  cudaError_t e = wait ? cudaEventSynchronize(tr->ev[3]) : cudaEventQuery(tr->ev[3]);
+  if (e == cudaSuccess) {
+    task_finalize(task, true);
+    return task->task_error == 0 ? TALSH_TASK_COMPLETED : TALSH_TASK_ERROR;
+  }
+  if (e != cudaErrorNotReady) {
+    note_cuda_error("task", (int)e);
+    tr->failed = 14;
+    task_finalize(task, false);
+    return TALSH_TASK_ERROR;
+  }
+  cudaGetLastError();
+  if (cudaEventQuery(tr->ev[2]) == cudaSuccess) return TALSH_TASK_OUTPUT_READY;
+  if (cudaEventQuery(tr->ev[1]) == cudaSuccess) return TALSH_TASK_INPUT_READY;
+  if (cudaEventQuery(tr->ev[0]) == cudaSuccess) return TALSH_TASK_STARTED;
+  cudaGetLastError();
+  return TALSH_TASK_SCHEDULED;
+}
+
+// ------------------------------------------------------- operation driver
+enum OpKind { kOpInit, kOpScale, kOpCopy, kOpAdd, kOpContract, kOpNorm1, kOpPlace };
+
+struct OpSpec {
+  OpKind kind;
+  int nt = 0;                        // tensors: D, L, R
+  talsh_tens_t *t[3] = {nullptr, nullptr, nullptr};
+  unsigned coh_ctrl = 0;
+  int dig[2 * MAX_TENSOR_RANK];
+  int drank = 0, lrank = 0, rrank = 0, conj = 0;
+  double sr = 0.0, si = 0.0;
+  int accumulative = YEP;
+  double *norm_out = nullptr;        // host result of kOpNorm1
+};
+
+// Resolves the execution GPU: returns its ordinal or a negative TAL-SH error.
+int resolve_gpu(int dev_id, int dev_kind, talsh_tens_t *const *ts, int nt, int &err) {
+  int dvk = DEV_NULL, dvn = -1;
+  if (dev_kind == DEV_DEFAULT) {
+    if (dev_id == DEV_DEFAULT) {
+      dvk = DEV_NVIDIA_GPU;  // every operation of this core runs on a GPU
+      dvn = -1;
+    } else {
+      dvn = decode_device_id(dev_id, &dvk);
+      if (dvn < 0) { err = TALSH_INVALID_ARGS; return -1; }
+    }
+  } else {
+    if (valid_device_kind(dev_kind) != YEP) { err = TALSH_INVALID_ARGS; return -1; }
+    dvk = dev_kind;
+    dvn = (dev_id == DEV_DEFAULT) ? -1 : dev_id;
+    if (dvn >= 0 && encode_device_id(dvk, dvn) >= DEV_MAX) { err = TALSH_INVALID_ARGS; return -1; }
+  }
+  if (dvk != DEV_NVIDIA_GPU) { err = TALSH_NOT_AVAILABLE; return -1; }
+  if (dvn < 0) {
+    // a GPU already holding the first tensor, else the first GPU in use
+    for (int k = 0; k < nt && dvn < 0; ++k) {
+      const talsh_tens_t *t = ts[k];
+      for (int i = 0; t && i < t->ndev; ++i) {
+        int dk = DEV_NULL;
+        const int dn = decode_device_id(t->dev_rsc[i].dev_id, &dk);
+        if (dk == DEV_NVIDIA_GPU && dn >= 0 && dn < MAX_GPUS_PER_NODE && R.gpu[dn].in_use) { dvn = dn; break; }
+      }
+    }
+    for (int g = 0; g < MAX_GPUS_PER_NODE && dvn < 0; ++g) if (R.gpu[g].in_use) dvn = g;
+    if (dvn < 0) { err = TALSH_NOT_AVAILABLE; return -1; }
+  }
+  if (dvn >= MAX_GPUS_PER_NODE || !R.gpu[dvn].in_use) { err = TALSH_INVALID_ARGS; return -1; }
+  return dvn;
+}
+
+int kind_size_checked(int kind) { return kind_size(kind); }
+
+int copy_between(void *dst, int dst_dev, const void *src, int src_dev, size_t bytes, cudaStream_t st) {
+  int sk = DEV_NULL, dk = DEV_NULL;
+  const int sn = decode_device_id(src_dev, &sk), dn = decode_device_id(dst_dev, &dk);
+  cudaError_t e;
+  if (sk == DEV_NVIDIA_GPU && dk == DEV_NVIDIA_GPU && sn != dn)
+    e = cudaMemcpyPeerAsync(dst, dn, src, sn, bytes, st);
+  else
+    e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, st);
+  if (e != cudaSuccess) { note_cuda_error("cudaMemcpyAsync", (int)e); return TALSH_FAILURE; }
+  return TALSH_SUCCESS;
+}
+
+// Schedules one operation (the shared body of the reference dispatchers).
+int schedule(OpSpec &op, int dev_id, int dev_kind, talsh_task_t *user_task) {
+  if (!R.on) return TALSH_NOT_INITIALIZED;
+  for (int k = 0; k < op.nt; ++k) {
+    if (op.t[k] == nullptr) return TALSH_INVALID_ARGS;
+    if (talshTensorIsEmpty(op.t[k]) != NOPE) return TALSH_OBJECT_IS_EMPTY;
+    if (!healthy(op.t[k])) return TALSH_FAILURE;
+  }
+  if (user_task != nullptr && talshTaskStatus(user_task) != TALSH_TASK_EMPTY) return TALSH_OBJECT_NOT_EMPTY;
+  int err = 0;
+  const int gpu = resolve_gpu(dev_id, dev_kind, op.t, op.nt, err);
+  if (gpu < 0) return err;
+  const int exec_dev = encode_device_id(DEV_NVIDIA_GPU, gpu);
+  GpuCtx &G = R.gpu[gpu];
+
+  // Images and data kinds.
+  int img[3] = {-1, -1, -1};
+  for (int k = 0; k < op.nt; ++k) {
+    img[k] = choose_image(op.t[k], DEV_NVIDIA_GPU, gpu);
+    if (img[k] < 0) return TALSH_FAILURE;
+  }
+  const int dkind = op.t[0]->data_kind[img[0]];
+  for (int k = 1; k < op.nt; ++k)
+    if (op.t[k]->data_kind[img[k]] != dkind) return TALSH_INVALID_ARGS;
+  const int esz = kind_size_checked(dkind);
+  if (esz == 0) return TALSH_INVALID_ARGS;
+
+  TaskRec *tr = new TaskRec();
+  tr->gpu = gpu;
+  tr->st = G.stream;
+  tr->nargs = op.nt;
+  for (int k = 0; k < op.nt; ++k) {
+    ArgRec &a = tr->a[k];
+    talsh_tens_t *t = op.t[k];
+    a.t = t;
+    a.src_dev = t->dev_rsc[img[k]].dev_id;
+    a.src_ptr = t->dev_rsc[img[k]].gmem_p;
+    a.coh = argument_coherence_get_value(op.coh_ctrl, op.nt, k);
+    a.bytes = shape_volume(t->shape_p) * esz;
+    a.output = (k == 0) && op.kind != kOpNorm1 && op.kind != kOpPlace;
+    a.need_input = !(k == 0 && (op.kind == kOpInit || op.kind == kOpCopy ||
+                               (op.kind == kOpContract && op.accumulative == NOPE)));
+    if (a.src_dev == exec_dev) {
+      a.dptr = a.src_ptr;
+    } else {
+      const int rc = dev_alloc(gpu, a.bytes, &a.dptr);
+      if (rc != TALSH_SUCCESS) {
+        for (int j = 0; j < k; ++j) if (tr->a[j].dalloc) mem_free(tr->a[j].dptr);
+        delete tr;
+        return rc;
+      }
+      a.dalloc = true;
+      a.copy_back = a.output && (a.coh == COPY_T || a.coh == COPY_K);
+    }
+  }
+  size_t scratch = 0;
+  if (op.kind == kOpContract) {
+    int dd[MAX_TENSOR_RANK], ld[MAX_TENSOR_RANK], rd[MAX_TENSOR_RANK];
+    for (int i = 0; i < op.drank; ++i) dd[i] = op.t[0]->shape_p->dims[i];
+    for (int i = 0; i < op.lrank; ++i) ld[i] = op.t[1]->shape_p->dims[i];
+    for (int i = 0; i < op.rrank; ++i) rd[i] = op.t[2]->shape_p->dims[i];
+    scratch = contract_scratch_bytes(dkind, op.dig, op.drank, dd, op.lrank, ld, op.rrank, rd);
+  } else if (op.kind == kOpNorm1) {
+    scratch = tcTensorNorm1Scratch(shape_volume(op.t[0]->shape_p)) + 256;
+  }
+  if (scratch > 0) {
+    const int rc = dev_alloc(gpu, scratch, &tr->scratch);
+    if (rc != TALSH_SUCCESS) {
+      for (int j = 0; j < op.nt; ++j) if (tr->a[j].dalloc) mem_free(tr->a[j].dptr);
+      delete tr;
+      return rc;
+    }
+  }
+  // Resources acquired: commit image bookkeeping (reference: discard other
+  // output images, mark moved/discarded sources unavailable).
+  if (op.kind != kOpNorm1 && op.kind != kOpPlace) {
+    talsh_tens_t *D = op.t[0];
+    const int di = find_image(D, tr->a[0].src_dev, tr->a[0].src_ptr);
+    image_discard_other(D, di);
+    D->avail[0] = NOPE;
+  }
+  for (int k = (op.kind == kOpNorm1 || op.kind == kOpPlace) ? 0 : 1; k < op.nt; ++k) {
+    ArgRec &a = tr->a[k];
+    const int i = find_image(a.t, a.src_dev, a.src_ptr);
+    if (a.coh == COPY_D || (a.coh == COPY_M && a.src_dev != exec_dev)) a.t->avail[i] = NOPE;
+  }
+
+  talsh_task_t *task = user_task;
+  if (task == nullptr) {
+    if (talshTaskCreate(&task) != TALSH_SUCCESS || task == nullptr) return TALSH_FAILURE;
+  }
+  task->task_p = tr;
+  task->task_error = -1;
+  task->dev_kind = DEV_NVIDIA_GPU;
+  task->data_kind = dkind;
+  task->coherence = (int)op.coh_ctrl;
+  task->num_args = op.nt;
+  task->data_vol = 0.0;
+  for (int k = 0; k < op.nt; ++k) {
+    task->tens_args[k].tens_p = op.t[k];
+    task->tens_args[k].source_image = find_image(op.t[k], tr->a[k].src_dev, tr->a[k].src_ptr);
+    task->data_vol += (double)tr->a[k].bytes;
+  }
+  task->flops = 0.0;
+
+  // Enqueue: inputs, compute, outputs.
+  cudaSetDevice(gpu);
+  cudaStream_t st = G.stream;
+  for (auto &e : tr->ev) e = event_get(gpu);
+  int rc = TALSH_SUCCESS;
+  cudaEventRecord(tr->ev[0], st);
+  for (int k = 0; k < op.nt && rc == TALSH_SUCCESS; ++k) {
+    ArgRec &a = tr->a[k];
+    if (a.dalloc && a.need_input) rc = copy_between(a.dptr, exec_dev, a.src_ptr, a.src_dev, a.bytes, st);
+  }
+  cudaEventRecord(tr->ev[1], st);
+  if (rc == TALSH_SUCCESS) {
+    const size_t vol = shape_volume(op.t[0]->shape_p);
+    switch (op.kind) {
+      case kOpInit:
+        rc = tcTensorInit(dkind, vol, tr->a[0].dptr, op.sr, op.si, st);
+        break;
+      case kOpScale:
+        rc = tcTensorScale(dkind, vol, tr->a[0].dptr, op.sr, op.si, st);
+        task->flops = (kind_is_complex(dkind) ? 6.0 : 1.0) * (double)vol;
+        break;
+      case kOpCopy: {
+        const int lconj = ((op.conj >> 1) ^ op.conj) & 1;
+        rc = tcTensorPermute(dkind, op.lrank, op.t[1]->shape_p->dims, op.dig, tr->a[1].dptr,
+                             tr->a[0].dptr, lconj, st);
+        break;
+      }
+      case kOpAdd: {
+        const int lconj = ((op.conj >> 1) ^ op.conj) & 1;
+        rc = tcTensorPermuteAdd(dkind, op.lrank, op.t[1]->shape_p->dims, op.dig, tr->a[1].dptr,
+                                tr->a[0].dptr, op.sr, op.si, lconj, st);
+        task->flops = (kind_is_complex(dkind) ? 8.0 : 2.0) * (double)vol;
+        break;
+      }
+      case kOpContract: {
+        const int *dd = op.t[0]->shape_p->dims, *ld = op.t[1]->shape_p->dims, *rd = op.t[2]->shape_p->dims;
+        rc = contract_launch(dkind, op.dig, op.drank, dd, op.lrank, ld, op.rrank, rd, tr->a[0].dptr,
+                             tr->a[1].dptr, tr->a[2].dptr, op.sr, op.si, op.conj, op.accumulative,
+                             tr->scratch, scratch, st);
+        double m = 1.0, n = 1.0, kk = 1.0;
+        for (int i = 0; i < op.lrank; ++i) (op.dig[i] > 0 ? m : kk) *= (double)ld[i];
+        for (int i = 0; i < op.rrank; ++i) if (op.dig[op.lrank + i] > 0) n *= (double)rd[i];
+        task->flops = (kind_is_complex(dkind) ? 8.0 : 2.0) * m * n * kk;
+        break;
+      }
+      case kOpNorm1: {
+        double *res = (double *)((char *)tr->scratch + scratch - 256);
+        rc = norm1_launch(dkind, vol, tr->a[0].dptr, res, (double *)tr->scratch, st);
+        if (rc == TALSH_SUCCESS && op.norm_out) {
+          const cudaError_t e = cudaMemcpyAsync(op.norm_out, res, sizeof(double), cudaMemcpyDeviceToHost, st);
+          if (e != cudaSuccess) { note_cuda_error("norm1 readback", (int)e); rc = TALSH_FAILURE; }
+        }
+        break;
+      }
+      case kOpPlace:
+        break;
+    }
+  }
+  cudaEventRecord(tr->ev[2], st);
+  for (int k = 0; k < op.nt && rc == TALSH_SUCCESS; ++k) {
+    ArgRec &a = tr->a[k];
+    if (a.copy_back) rc = copy_between(a.src_ptr, a.src_dev, a.dptr, exec_dev, a.bytes, st);
+  }
+  cudaEventRecord(tr->ev[3], st);
+  if (rc != TALSH_SUCCESS) {
+    // Scheduling failed after the task was recorded: the work already queued
+    // must drain before its buffers can be released.
+    cudaStreamSynchronize(st);
+    cudaGetLastError();
+    tr->failed = 20;
+    task_finalize(task, false);
+    if (user_task == nullptr) talshTaskDestroy(task);
+    return TALSH_FAILURE;
+  }
+  if (R.log_ops) std::printf("#TALSH-B200: op %d scheduled on GPU %d\n", (int)op.kind, gpu);
+  if (user_task == nullptr) {
+    int stats = 0;
+    int e = talshTaskWait(task, &stats);
+    if (e == TALSH_SUCCESS && stats != TALSH_TASK_COMPLETED) e = TALSH_TASK_ERROR;
+    const int d = talshTaskDestroy(task);
+    if (e == TALSH_SUCCESS && d != TALSH_SUCCESS) e = d;
+    return e;
+  }
+  return TALSH_SUCCESS;
+}
+
+int parse_and_check(const char *cptrn, OpSpec &op, int want_inputs) {
+  if (cptrn == nullptr) return TALSH_INVALID_ARGS;
+  int dr, lr, rr, cj;
+  if (talsh_get_contr_ptrn_str2dig(cptrn, op.dig, &dr, &lr, &rr, &cj) != 0) return TALSH_INVALID_ARGS;
+  op.drank = dr; op.lrank = lr; op.rrank = rr; op.conj = cj;
+  if (op.t[0] && talshTensorRank(op.t[0]) != dr) return TALSH_INVALID_ARGS;
+  if (op.t[1] && talshTensorRank(op.t[1]) != lr) return TALSH_INVALID_ARGS;
+  if (want_inputs == 2) {
+    if (op.t[2] && talshTensorRank(op.t[2]) != rr) return TALSH_INVALID_ARGS;
+  } else if (rr != 0) {
+    return TALSH_INVALID_ARGS;
+  }
+  if (want_inputs == 1) {  // copy/add: a permutation of D's indices with matching extents
+    if (dr != lr) return TALSH_INVALID_ARGS;
+    for (int i = 0; i < lr; ++i) {
+      const int p = op.dig[i];
+      if (p < 1 || p > dr || op.t[0]->shape_p->dims[p - 1] != op.t[1]->shape_p->dims[i]) return TALSH_INVALID_ARGS;
+    }
+  }
+  return TALSH_SUCCESS;
+}
+
+}  // namespace
+}  // namespace tb
+
+using namespace tb;
+
+// ===================================================================== C ABI
+extern "C" {
+
+double time_sys_sec(void) {
+  return std::chrono::duration<double>(std::chrono::system_clock::now().time_since_epoch()).count();
+}
+double time_high_sec(void) {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+int talsh_tens_no_init(const talsh_tens_data_t *, const talsh_tens_shape_t *, const talsh_tens_signature_t *) {
+  return TALSH_SUCCESS;
+}
+
+int tens_valid_data_kind(int datk, int *datk_size) {
+  int sz = -1;
+  switch (datk) {
+    case NO_TYPE: sz = 0; break;
+    case R4: sz = 4; break;
+    case R8: sz = 8; break;
+    case C4: sz = 8; break;
+    case C8: sz = 16; break;
+    default: break;
+  }
+  if (datk_size) *datk_size = sz;
+  return sz >= 0 ? YEP : NOPE;
+}
+int tens_valid_data_kind_(int datk, int *datk_size) { return tens_valid_data_kind(datk, datk_size); }
+int talshValidDataKind(int datk, int *datk_size) { return tens_valid_data_kind(datk, datk_size); }
+
+int permutation_trivial(const int perm_len, const int *perm, const int base) {
+  for (int i = 0; i < perm_len; ++i) if (perm[base + i] != i + 1) return NOPE;
+  return YEP;
+}
+
+unsigned int argument_coherence_get_value(unsigned int coh_ctrl, unsigned int tot_args, unsigned int arg_num) {
+  return (coh_ctrl >> ((tot_args - (arg_num + 1)) * 2)) & kTwoBits;
+}
+
+int argument_coherence_set_value(unsigned int *coh_ctrl, unsigned int tot_args, unsigned int arg_num,
+                                 unsigned int coh_val) {
+  if (arg_num >= tot_args) return 1;
+  if (coh_val & ~kTwoBits) return 2;
+  const unsigned sh = (tot_args - (arg_num + 1)) * 2;
+  *coh_ctrl = (*coh_ctrl & ~(kTwoBits << sh)) | (coh_val << sh);
+  return 0;
+}
+
+int valid_device_kind(int dev_kind) {
+  return (dev_kind == DEV_NULL || dev_kind == DEV_HOST || dev_kind == DEV_NVIDIA_GPU ||
+          dev_kind == DEV_INTEL_MIC || dev_kind == DEV_AMD_GPU) ? YEP : NOPE;
+}
+
+int encode_device_id(int dev_kind, int dev_num) {
+  switch (dev_kind) {
+    case DEV_HOST: return dev_num == 0 ? 0 : DEV_MAX;
+    case DEV_NVIDIA_GPU: return (dev_num >= 0 && dev_num < MAX_GPUS_PER_NODE) ? 1 + dev_num : DEV_MAX;
+    case DEV_INTEL_MIC: return (dev_num >= 0 && dev_num < MAX_MICS_PER_NODE) ? 1 + MAX_GPUS_PER_NODE + dev_num : DEV_MAX;
+    case DEV_AMD_GPU:
+      return (dev_num >= 0 && dev_num < MAX_AMDS_PER_NODE) ? 1 + MAX_GPUS_PER_NODE + MAX_MICS_PER_NODE + dev_num : DEV_MAX;
+    default: return DEV_MAX;
+  }
+}
+
+int decode_device_id(int dev_id, int *dev_kind) {
+  const int id = dev_id < 0 ? -dev_id : dev_id;
+  int dk = DEV_NULL, dn = DEV_NULL;
+  if (id == 0) { dk = DEV_HOST; dn = 0; }
+  else if (id <= MAX_GPUS_PER_NODE) { dk = DEV_NVIDIA_GPU; dn = id - 1; }
+  else if (id <= MAX_GPUS_PER_NODE + MAX_MICS_PER_NODE) { dk = DEV_INTEL_MIC; dn = id - 1 - MAX_GPUS_PER_NODE; }
+  else if (id <= MAX_GPUS_PER_NODE + MAX_MICS_PER_NODE + MAX_AMDS_PER_NODE) {
+    dk = DEV_AMD_GPU; dn = id - 1 - MAX_GPUS_PER_NODE - MAX_MICS_PER_NODE;
+  }
+  if (dev_kind) *dev_kind = dk;
+  return dn;
+}
+
+int tensDevRsc_clean(talsh_dev_rsc_t *drsc) {
+  if (drsc == nullptr) return -1;
+  drsc->dev_id = DEV_NULL;
+  drsc->gmem_p = nullptr;
+  drsc->buf_entry = -1;
+  drsc->mem_attached = 0;
+  return 0;
+}
+int tensDevRsc_is_empty(talsh_dev_rsc_t *drsc) {
+  if (drsc == nullptr) return TALSH_INVALID_ARGS;
+  return (drsc->dev_id < 0 || drsc->gmem_p == nullptr) ? YEP : NOPE;
+}
+int tensDevRsc_device_id(talsh_dev_rsc_t *drsc) { return drsc ? drsc->dev_id : DEV_NULL; }
+
+int tensShape_create(talsh_tens_shape_t **tshape) {
+  if (tshape == nullptr) return TALSH_INVALID_ARGS;
+  *tshape = (talsh_tens_shape_t *)std::malloc(sizeof(talsh_tens_shape_t));
+  if (*tshape == nullptr) return TRY_LATER;
+  return tensShape_clean(*tshape);
+}
+int tensShape_clean(talsh_tens_shape_t *s) {
+  if (s == nullptr) return TALSH_INVALID_ARGS;
+  s->num_dim = -1; s->dims = nullptr; s->divs = nullptr; s->grps = nullptr;
+  return TALSH_SUCCESS;
+}
+int tensShape_construct(talsh_tens_shape_t *s, int, int rank, const int *dims, const int *divs, const int *grps) {
+  if (s == nullptr || rank < 0 || rank > MAX_TENSOR_RANK) return TALSH_INVALID_ARGS;
+  if (s->num_dim >= 0) return TALSH_OBJECT_NOT_EMPTY;
+  if (rank > 0 && dims == nullptr) return TALSH_INVALID_ARGS;
+  for (int i = 0; i < rank; ++i) if (dims[i] <= 0) return TALSH_INVALID_ARGS;
+  if (rank > 0) {
+    s->dims = (int *)std::malloc(sizeof(int) * rank);
+    s->divs = (int *)std::malloc(sizeof(int) * rank);
+    s->grps = (int *)std::malloc(sizeof(int) * rank);
+    if (!s->dims || !s->divs || !s->grps) { tensShape_destruct(s); return TRY_LATER; }
+    for (int i = 0; i < rank; ++i) {
+      s->dims[i] = dims[i];
+      s->divs[i] = divs ? divs[i] : dims[i];
+      s->grps[i] = grps ? grps[i] : 0;
+    }
+  }
+  s->num_dim = rank;
+  return TALSH_SUCCESS;
+}
+int tensShape_destruct(talsh_tens_shape_t *s) {
+  if (s == nullptr) return TALSH_INVALID_ARGS;
+  std::free(s->dims); std::free(s->divs); std::free(s->grps);
+  return tensShape_clean(s);
+}
+int tensShape_destroy(talsh_tens_shape_t *s) {
+  if (s == nullptr) return TALSH_INVALID_ARGS;
+  tensShape_destruct(s);
+  std::free(s);
+  return TALSH_SUCCESS;
+}
+size_t tensShape_volume(const talsh_tens_shape_t *s) {
+  if (s == nullptr || s->num_dim < 0) return 0;
+  return shape_volume(s);
+}
+int tensShape_rank(const talsh_tens_shape_t *s) { return s ? s->num_dim : -1; }
+
+// ------------------------------------------------------------ control API
+int talshInit(size_t *host_buf_size, int *host_arg_max, int ngpus, int gpu_list[], int nmics,
+              int mic_list[], int namds, int amd_list[]) {
+  (void)mic_list; (void)amd_list;
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (R.on) return TALSH_ALREADY_INITIALIZED;
+  if (ngpus < 0 || ngpus > MAX_GPUS_PER_NODE || nmics < 0 || namds < 0) return TALSH_INVALID_ARGS;
+  if (nmics > 0 || namds > 0) return TALSH_NOT_AVAILABLE;
+  const int avail = ngpus > 0 ? node_gpu_count() : 0;
+  for (int i = 0; i < ngpus; ++i) {
+    if (gpu_list == nullptr || gpu_list[i] < 0 || gpu_list[i] >= avail) return TALSH_INVALID_ARGS;
+    if (i > 0 && gpu_list[i] != gpu_list[i - 1] + 1) return TALSH_INVALID_ARGS;  // consecutive range
+  }
+  const char *env = std::getenv("TALSH_B200_GPU_BUDGET_BYTES");
+  for (int i = 0; i < ngpus; ++i) {
+    const int g = gpu_list[i];
+    GpuCtx &G = R.gpu[g];
+    if (cudaSetDevice(g) != cudaSuccess) { cudaGetLastError(); return TALSH_FAILURE; }
+    if (cudaStreamCreateWithFlags(&G.stream, cudaStreamNonBlocking) != cudaSuccess) return TALSH_FAILURE;
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, g) == cudaSuccess) {
+      uint64_t keep = UINT64_MAX;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    size_t fr = 0, tot = 0;
+    cudaMemGetInfo(&fr, &tot);
+    G.budget = env ? (size_t)std::strtoull(env, nullptr, 10) : (fr / 10) * 9;
+    G.used = G.peak = 0;
+    G.in_use = true;
+  }
+  cudaGetLastError();
+  if (host_arg_max) *host_arg_max = 1 << 20;
+  (void)host_buf_size;  // Host bodies are pinned per tensor; the requested size is reported unchanged
+  R.on = true;
+  return TALSH_SUCCESS;
+}
+
+int talshShutdown(void) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (!R.on) return TALSH_NOT_INITIALIZED;
+  for (int g = 0; g < MAX_GPUS_PER_NODE; ++g) {
+    GpuCtx &G = R.gpu[g];
+    if (!G.in_use) continue;
+    cudaSetDevice(g);
+    cudaStreamSynchronize(G.stream);
+  }
+  for (auto &kv : R.allocs) {
+    if (kv.second.gpu < 0) { if (kv.second.pinned) cudaFreeHost(kv.first); else std::free(kv.first); }
+    else { cudaSetDevice(kv.second.gpu); cudaFree(kv.first); }
+  }
+  R.allocs.clear();
+  R.host_bytes = 0;
+  for (int g = 0; g < MAX_GPUS_PER_NODE; ++g) {
+    GpuCtx &G = R.gpu[g];
+    if (!G.in_use) continue;
+    cudaSetDevice(g);
+    for (cudaEvent_t e : G.event_pool) cudaEventDestroy(e);
+    G.event_pool.clear();
+    cudaStreamDestroy(G.stream);
+    G = GpuCtx();
+  }
+  cudaGetLastError();
+  R.on = false;
+  return TALSH_SUCCESS;
+}
+
+void talshSetMemAllocPolicyHost(int mem_policy, int fallback, int *ierr) {
+  R.mem_policy = mem_policy;
+  R.mem_fallback = fallback;
+  if (ierr) *ierr = TALSH_SUCCESS;
+}
+int talshEnableFastMath(int, int) { return TALSH_NOT_AVAILABLE; }
+int talshDisableFastMath(int, int) { return TALSH_SUCCESS; }
+int talshQueryFastMath(int, int) { return NOPE; }
+
+int talshDeviceCount(int dev_kind, int *dev_count) {
+  if (dev_count == nullptr) return TALSH_INVALID_ARGS;
+  switch (dev_kind) {
+    case DEV_HOST: *dev_count = 1; return TALSH_SUCCESS;
+    case DEV_NVIDIA_GPU: *dev_count = node_gpu_count(); return TALSH_SUCCESS;
+    case DEV_INTEL_MIC:
+    case DEV_AMD_GPU: *dev_count = 0; return TALSH_SUCCESS;
+    default: return TALSH_INVALID_ARGS;
+  }
+}
+int talshFlatDevId(int dev_kind, int dev_num) { return encode_device_id(dev_kind, dev_num); }
+int talshKindDevId(int dev_id, int *dev_kind) { return decode_device_id(dev_id, dev_kind); }
+
+int talshDeviceState(int dev_num, int dev_kind) {
+  int dk = dev_kind, dn = dev_num;
+  if (dev_kind == DEV_NULL) dn = decode_device_id(dev_num, &dk);
+  if (dk == DEV_HOST) return R.on ? DEV_ON : DEV_OFF;
+  if (dk == DEV_NVIDIA_GPU && dn >= 0 && dn < MAX_GPUS_PER_NODE) return R.gpu[dn].in_use ? DEV_ON : DEV_OFF;
+  return DEV_OFF;
+}
+int talshDeviceState_(int dev_num, int dev_kind) { return talshDeviceState(dev_num, dev_kind); }
+
+int talshDeviceBusyLeast(int dev_kind) {
+  if (dev_kind == DEV_NVIDIA_GPU || dev_kind == DEV_NULL) {
+    int best = -1;
+    size_t best_used = (size_t)-1;
+    for (int g = 0; g < MAX_GPUS_PER_NODE; ++g)
+      if (R.gpu[g].in_use && R.gpu[g].used < best_used) { best = g; best_used = R.gpu[g].used; }
+    if (best >= 0) return dev_kind == DEV_NULL ? encode_device_id(DEV_NVIDIA_GPU, best) : best;
+  }
+  if (dev_kind == DEV_HOST || dev_kind == DEV_NULL) return 0;
+  return TALSH_NOT_AVAILABLE;
+}
+int talshDeviceBusyLeast_(int dev_kind) { return talshDeviceBusyLeast(dev_kind); }
+
+int talshDetermineOptimalDevice(const talsh_tens_t *tens0, const talsh_tens_t *tens1, const talsh_tens_t *tens2) {
+  const talsh_tens_t *ts[3] = {tens0, tens1, tens2};
+  for (const talsh_tens_t *t : ts) {
+    if (t == nullptr || t->dev_rsc == nullptr) continue;
+    for (int i = 0; i < t->ndev; ++i) {
+      int dk = DEV_NULL;
+      const int dn = decode_device_id(t->dev_rsc[i].dev_id, &dk);
+      if (dk == DEV_NVIDIA_GPU && dn >= 0 && R.gpu[dn].in_use) return t->dev_rsc[i].dev_id;
+    }
+  }
+  for (int g = 0; g < MAX_GPUS_PER_NODE; ++g) if (R.gpu[g].in_use) return encode_device_id(DEV_NVIDIA_GPU, g);
+  return DEV_NULL;
+}
+
+static int gpu_of(int dev_num, int dev_kind) {
+  int dk = dev_kind, dn = dev_num;
+  if (dev_kind == DEV_NULL) dn = decode_device_id(dev_num, &dk);
+  if (dk != DEV_NVIDIA_GPU || dn < 0 || dn >= MAX_GPUS_PER_NODE) return -1;
+  return dn;
+}
+size_t talshDeviceMemorySize(int dev_num, int dev_kind) {
+  const int g = gpu_of(dev_num, dev_kind);
+  if (g < 0) return 0;
+  cudaDeviceProp p;
+  if (cudaGetDeviceProperties(&p, g) != cudaSuccess) { cudaGetLastError(); return 0; }
+  return p.totalGlobalMem;
+}
+size_t talshDeviceMemorySize_(int dev_num, int dev_kind) { return talshDeviceMemorySize(dev_num, dev_kind); }
+size_t talshDeviceBufferSize(int dev_num, int dev_kind) {
+  const int g = gpu_of(dev_num, dev_kind);
+  return (g >= 0 && R.gpu[g].in_use) ? R.gpu[g].budget : 0;
+}
+size_t talshDeviceBufferSize_(int dev_num, int dev_kind) { return talshDeviceBufferSize(dev_num, dev_kind); }
+size_t talshDeviceTensorSize(int dev_num, int dev_kind) { return talshDeviceBufferSize(dev_num, dev_kind); }
+size_t talshDeviceTensorSize_(int dev_num, int dev_kind) { return talshDeviceTensorSize(dev_num, dev_kind); }
+size_t talshDeviceBufferFreeSize(int dev_num, int dev_kind) {
+  const int g = gpu_of(dev_num, dev_kind);
+  return (g >= 0 && R.gpu[g].in_use) ? R.gpu[g].budget - R.gpu[g].used : 0;
+}
+size_t talshDeviceBufferFreeSize_(int dev_num, int dev_kind) { return talshDeviceBufferFreeSize(dev_num, dev_kind); }
+void *talshDeviceBufferBasePtr(int, int) { return nullptr; }
+void *talshDeviceBufferBasePtr_(int a, int b) { return talshDeviceBufferBasePtr(a, b); }
+double talshDeviceGetFlops(int dev_kind, int dev_id) {
+  double f = 0.0;
+  for (int g = 0; g < MAX_GPUS_PER_NODE; ++g) {
+    if (!R.gpu[g].in_use) continue;
+    if (dev_kind == DEV_NVIDIA_GPU && dev_id != DEV_DEFAULT && dev_id != g) continue;
+    if (dev_kind == DEV_HOST) continue;
+    f += R.gpu[g].flops;
+  }
+  return f;
+}
+void talshMemManagerLogStart(void) {}
+void talshMemManagerLogFinish(void) {}
+void talshTensorOpLogStart(void) { R.log_ops = true; }
+void talshTensorOpLogFinish(void) { R.log_ops = false; }
+
+int talshStats(int dev_id, int dev_kind) {
+  for (int g = 0; g < MAX_GPUS_PER_NODE; ++g) {
+    const GpuCtx &G = R.gpu[g];
+    if (!G.in_use) continue;
+    if (dev_id >= 0 && gpu_of(dev_id, dev_kind) != g) continue;
+    std::printf("#TALSH-B200 GPU %d: tasks ok %llu failed %llu deferred %llu; flops %.6e; bytes %.6e; "
+                "pool used %zu peak %zu budget %zu\n",
+                g, G.tasks_ok, G.tasks_failed, G.try_later, G.flops, G.bytes, G.used, G.peak, G.budget);
+  }
+  std::printf("#TALSH-B200 Host: library-owned bytes %zu\n", R.host_bytes);
+  return TALSH_SUCCESS;
+}
+int talshStats_(int dev_id, int dev_kind) { return talshStats(dev_id, dev_kind); }
+
+// ------------------------------------------------------------- tensors
+int talshTensorCreate(talsh_tens_t **tens_block) {
+  if (tens_block == nullptr) return TALSH_INVALID_ARGS;
+  *tens_block = (talsh_tens_t *)std::malloc(sizeof(talsh_tens_t));
+  if (*tens_block == nullptr) return TRY_LATER;
+  return talshTensorClean(*tens_block);
+}
+
+int talshTensorClean(talsh_tens_t *t) {
+  if (t == nullptr) return TALSH_INVALID_ARGS;
+  t->shape_p = nullptr; t->dev_rsc = nullptr; t->data_kind = nullptr; t->avail = nullptr;
+  t->dev_rsc_len = 0; t->ndev = 0;
+  return TALSH_SUCCESS;
+}
+
+int talshTensorIsEmpty(const talsh_tens_t *t) {
+  if (t == nullptr) return TALSH_INVALID_ARGS;
+  return t->shape_p == nullptr ? YEP : NOPE;
+}
+
+int talshTensorConstruct(talsh_tens_t *t, int data_kind, int tens_rank, const int tens_dims[], int dev_id,
+                         void *ext_mem, int in_hab, talsh_tens_init_i init_method, double init_val_real,
+                         double init_val_imag) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (!R.on) return TALSH_NOT_INITIALIZED;
+  if (t == nullptr) return TALSH_INVALID_ARGS;
+  if (talshTensorIsEmpty(t) != YEP) return TALSH_OBJECT_NOT_EMPTY;
+  int dksize = 0;
+  if (tens_valid_data_kind(data_kind, &dksize) != YEP) return TALSH_INVALID_ARGS;
+  int dev_kind = DEV_NULL;
+  const int dev_num = decode_device_id(dev_id, &dev_kind);
+  if (dev_num < 0) return TALSH_INVALID_ARGS;
+  if (dev_kind != DEV_HOST && dev_kind != DEV_NVIDIA_GPU) return TALSH_NOT_AVAILABLE;
+  if (dev_kind == DEV_NVIDIA_GPU && (dev_num >= MAX_GPUS_PER_NODE || !R.gpu[dev_num].in_use))
+    return TALSH_INVALID_ARGS;
+  int rc = tensShape_create(&t->shape_p);
+  if (rc) return rc;
+  rc = tensShape_construct(t->shape_p, NOPE, tens_rank, tens_dims, nullptr, nullptr);
+  if (rc) { std::free(t->shape_p); t->shape_p = nullptr; return rc == TALSH_OBJECT_NOT_EMPTY ? TALSH_FAILURE : rc; }
+  t->dev_rsc = (talsh_dev_rsc_t *)std::malloc(TALSH_MAX_DEV_PRESENT * sizeof(talsh_dev_rsc_t));
+  t->data_kind = (int *)std::malloc(TALSH_MAX_DEV_PRESENT * sizeof(int));
+  t->avail = (int *)std::malloc(TALSH_MAX_DEV_PRESENT * sizeof(int));
+  if (!t->dev_rsc || !t->data_kind || !t->avail) { talshTensorDestruct(t); return TRY_LATER; }
+  t->dev_rsc_len = TALSH_MAX_DEV_PRESENT;
+  t->ndev = 0;
+  for (int j = 0; j < TALSH_MAX_DEV_PRESENT; ++j) {
+    tensDevRsc_clean(&t->dev_rsc[j]);
+    t->data_kind[j] = NO_TYPE;
+    t->avail[j] = NOPE;
+  }
+  if (ext_mem != nullptr) {
+    t->dev_rsc[0].dev_id = dev_id;
+    t->dev_rsc[0].gmem_p = ext_mem;
+    t->dev_rsc[0].buf_entry = in_hab >= 0 ? in_hab : -1;
+    t->dev_rsc[0].mem_attached = 1;
+    t->data_kind[0] = data_kind;
+    t->avail[0] = YEP;
+    t->ndev = 1;
+    return TALSH_SUCCESS;
+  }
+  if (data_kind == NO_TYPE) return TALSH_SUCCESS;
+  const size_t vol = shape_volume(t->shape_p);
+  const size_t bytes = vol * (size_t)dksize;
+  void *p = nullptr;
+  if (dev_kind == DEV_HOST) {
+    p = host_alloc(bytes, any_gpu_in_use());
+    if (p == nullptr) { talshTensorDestruct(t); return TRY_LATER; }
+  } else {
+    rc = dev_alloc(dev_num, bytes, &p);
+    if (rc) { talshTensorDestruct(t); return rc; }
+  }
+  t->dev_rsc[0].dev_id = dev_id;
+  t->dev_rsc[0].gmem_p = p;
+  t->dev_rsc[0].buf_entry = -1;
+  t->dev_rsc[0].mem_attached = 0;
+  t->data_kind[0] = data_kind;
+  t->avail[0] = YEP;
+  t->ndev = 1;
+  // Initialization (reference :1257-1298): Host bodies are filled here, GPU
+  // bodies by a blocking talshTensorInit.
+  int erc = TALSH_SUCCESS;
+  if (dev_kind == DEV_HOST) {
+    if (init_method != nullptr) {
+      talsh_tens_data_t tdd{p, vol, data_kind};
+      if (init_method(&tdd, t->shape_p, nullptr) != 0) erc = NOT_CLEAN;
+    } else {
+      switch (data_kind) {
+        case R4: { float v = (float)init_val_real; float *q = (float *)p; for (size_t i = 0; i < vol; ++i) q[i] = v; break; }
+        case R8: { double *q = (double *)p; for (size_t i = 0; i < vol; ++i) q[i] = init_val_real; break; }
+        case C4: { float *q = (float *)p; for (size_t i = 0; i < vol; ++i) { q[2 * i] = (float)init_val_real; q[2 * i + 1] = (float)init_val_imag; } break; }
+        case C8: { double *q = (double *)p; for (size_t i = 0; i < vol; ++i) { q[2 * i] = init_val_real; q[2 * i + 1] = init_val_imag; } break; }
+      }
+    }
+  } else {
+    if (talshTensorInit(t, init_val_real, init_val_imag, dev_id, DEV_DEFAULT, COPY_M, nullptr) != TALSH_SUCCESS)
+      erc = NOT_CLEAN;
+  }
+  return erc;
+}
+
+int talshTensorConstruct_(talsh_tens_t *t, int data_kind, int tens_rank, const int tens_dims[], int dev_id,
+                          void *ext_mem, int in_hab, talsh_tens_init_i init_method, double vr, double vi) {
+  return talshTensorConstruct(t, data_kind, tens_rank, tens_dims, dev_id, ext_mem, in_hab, init_method, vr, vi);
+}
+
+int talshTensorImportData(talsh_tens_t *t, int data_kind, const void *ext_data) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (!R.on) return TALSH_NOT_INITIALIZED;
+  if (t == nullptr || ext_data == nullptr) return TALSH_INVALID_ARGS;
+  if (talshTensorIsEmpty(t) != NOPE) return TALSH_OBJECT_IS_EMPTY;
+  int es = 0;
+  if (tens_valid_data_kind(data_kind, &es) != YEP || es <= 0) return TALSH_INVALID_ARGS;
+  const size_t bytes = shape_volume(t->shape_p) * (size_t)es;
+  int found = -1;
+  for (int i = 0; i < t->ndev; ++i) {
+    if (t->data_kind[i] != data_kind || t->avail[i] != YEP) continue;
+    found = i;
+    int dk = DEV_NULL;
+    const int dn = decode_device_id(t->dev_rsc[i].dev_id, &dk);
+    if (dk == DEV_HOST) {
+      std::memcpy(t->dev_rsc[i].gmem_p, ext_data, bytes);
+    } else if (dk == DEV_NVIDIA_GPU) {
+      cudaSetDevice(dn);
+      if (R.gpu[dn].in_use) cudaStreamSynchronize(R.gpu[dn].stream);
+      if (cudaMemcpy(t->dev_rsc[i].gmem_p, ext_data, bytes, cudaMemcpyDefault) != cudaSuccess) {
+        cudaGetLastError();
+        return TALSH_FAILURE;
+      }
+    }
+  }
+  // Other images (other data kinds) are no longer coherent.
+  if (found >= 0)
+    for (int i = t->ndev - 1; i >= 0; --i) if (t->data_kind[i] != data_kind) image_discard(t, i);
+  return found >= 0 ? TALSH_SUCCESS : TALSH_NOT_FOUND;
+}
+
+int talshTensorDestruct(talsh_tens_t *t) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (t == nullptr) return TALSH_INVALID_ARGS;
+  int rc = TALSH_SUCCESS;
+  if (t->dev_rsc != nullptr) {
+    for (int i = 0; i < t->ndev; ++i) {
+      int dk = DEV_NULL;
+      const int dn = decode_device_id(t->dev_rsc[i].dev_id, &dk);
+      if (dk == DEV_NVIDIA_GPU && dn >= 0 && dn < MAX_GPUS_PER_NODE && R.gpu[dn].in_use) {
+        cudaSetDevice(dn);
+        cudaStreamSynchronize(R.gpu[dn].stream);  // no queued task may still use the body
+      }
+      if (rsc_release(&t->dev_rsc[i]) != TALSH_SUCCESS) rc = NOT_CLEAN;
+    }
+  }
+  std::free(t->dev_rsc); std::free(t->data_kind); std::free(t->avail);
+  if (t->shape_p) tensShape_destroy(t->shape_p);
+  talshTensorClean(t);
+  return rc;
+}
+
+int talshTensorDestroy(talsh_tens_t *t) {
+  if (t == nullptr) return TALSH_INVALID_ARGS;
+  const int rc = talshTensorDestruct(t);
+  std::free(t);
+  return rc;
+}
+
+int talshTensorRank(const talsh_tens_t *t) {
+  if (t == nullptr) return -1;
+  if (t->shape_p == nullptr) return -1;
+  return t->shape_p->num_dim;
+}
+
+size_t talshTensorVolume(const talsh_tens_t *t) {
+  if (t == nullptr || t->shape_p == nullptr) return 0;
+  return shape_volume(t->shape_p);
+}
+
+size_t talshTensorSizeAllImages(const talsh_tens_t *t, int *num_images) {
+  if (num_images) *num_images = 0;
+  if (t == nullptr || t->shape_p == nullptr) return 0;
+  size_t total = 0;
+  const size_t vol = shape_volume(t->shape_p);
+  for (int i = 0; i < t->ndev; ++i) { int es = 0; tens_valid_data_kind(t->data_kind[i], &es); total += vol * (size_t)es; }
+  if (num_images) *num_images = t->ndev;
+  return total;
+}
+
+const int *talshTensorDimExtents(const talsh_tens_t *t, int *rank) {
+  if (t == nullptr || t->shape_p == nullptr) { if (rank) *rank = -1; return nullptr; }
+  if (rank) *rank = t->shape_p->num_dim;
+  return t->shape_p->dims;
+}
+
+int talshTensorShape(const talsh_tens_t *t, talsh_tens_shape_t *s) {
+  if (t == nullptr || s == nullptr) return TALSH_INVALID_ARGS;
+  if (t->shape_p == nullptr) return TALSH_OBJECT_IS_EMPTY;
+  if (s->num_dim >= 0) tensShape_destruct(s);
+  return tensShape_construct(s, NOPE, t->shape_p->num_dim, t->shape_p->dims, t->shape_p->divs, t->shape_p->grps);
+}
+
+int talshTensorDataKind(const talsh_tens_t *t, int *num_images, int *data_kinds) {
+  if (t == nullptr || num_images == nullptr || data_kinds == nullptr) return TALSH_INVALID_ARGS;
+  if (t->shape_p == nullptr) return TALSH_OBJECT_IS_EMPTY;
+  *num_images = t->ndev;
+  for (int i = 0; i < t->ndev; ++i) data_kinds[i] = t->data_kind[i];
+  return TALSH_SUCCESS;
+}
+
+int talshTensorReshape(talsh_tens_t *t, int tens_rank, const int tens_dims[]) {
+  if (t == nullptr || t->shape_p == nullptr) return TALSH_INVALID_ARGS;
+  talsh_tens_shape_t s;
+  tensShape_clean(&s);
+  const int rc = tensShape_construct(&s, NOPE, tens_rank, tens_dims, nullptr, nullptr);
+  if (rc) return rc;
+  if (shape_volume(&s) != shape_volume(t->shape_p)) { tensShape_destruct(&s); return TALSH_INVALID_ARGS; }
+  tensShape_destruct(t->shape_p);
+  *t->shape_p = s;
+  return TALSH_SUCCESS;
+}
+
+int talshTensorInUse(const talsh_tens_t *t) {
+  if (t == nullptr || t->shape_p == nullptr) return TALSH_INVALID_ARGS;
+  for (int i = 0; i < t->ndev; ++i) if (t->avail[i] != YEP) return YEP;
+  return NOPE;
+}
+
+int talshTensorPresence(const talsh_tens_t *t, int *ncopies, int copies[], int data_kinds[], int dev_kind, int dev_id) {
+  if (t == nullptr || ncopies == nullptr || copies == nullptr || data_kinds == nullptr) return TALSH_INVALID_ARGS;
+  if (t->shape_p == nullptr) return TALSH_OBJECT_IS_EMPTY;
+  *ncopies = 0;
+  for (int i = 0; i < t->ndev; ++i) {
+    int dk = DEV_NULL;
+    const int dn = decode_device_id(t->dev_rsc[i].dev_id, &dk);
+    if (dev_kind != DEV_NULL && dk != dev_kind) continue;
+    if (dev_kind != DEV_NULL && dev_id >= 0 && dn != dev_id) continue;
+    copies[*ncopies] = t->dev_rsc[i].dev_id;
+    data_kinds[*ncopies] = t->data_kind[i];
+    (*ncopies)++;
+  }
+  return TALSH_SUCCESS;
+}
+int talshTensorPresence_(const talsh_tens_t *t, int *n, int c[], int d[], int k, int i) { return talshTensorPresence(t, n, c, d, k, i); }
+
+int talshTensorGetBodyAccess(talsh_tens_t *t, void **body_p, int data_kind, int dev_id, int dev_kind) {
+  if (t == nullptr || body_p == nullptr) return TALSH_INVALID_ARGS;
+  if (t->shape_p == nullptr) return TALSH_OBJECT_IS_EMPTY;
+  const int flat = (dev_kind == DEV_NULL) ? dev_id : encode_device_id(dev_kind, dev_id);
+  *body_p = nullptr;
+  for (int i = 0; i < t->ndev; ++i) {
+    if (t->dev_rsc[i].dev_id == flat && t->data_kind[i] == data_kind) {
+      if (t->avail[i] != YEP) return TALSH_NOT_ALLOWED;
+      int dk = DEV_NULL;
+      const int dn = decode_device_id(flat, &dk);
+      if (dk == DEV_NVIDIA_GPU && R.gpu[dn].in_use) { cudaSetDevice(dn); cudaStreamSynchronize(R.gpu[dn].stream); }
+      *body_p = t->dev_rsc[i].gmem_p;
+      return TALSH_SUCCESS;
+    }
+  }
+  return TALSH_NOT_FOUND;
+}
+int talshTensorGetBodyAccess_(talsh_tens_t *t, void **b, int k, int i, int dk) { return talshTensorGetBodyAccess(t, b, k, i, dk); }
+int talshTensorGetBodyAccessConst(const talsh_tens_t *t, const void **body_p, int data_kind, int dev_id, int dev_kind) {
+  void *p = nullptr;
+  const int rc = talshTensorGetBodyAccess(const_cast<talsh_tens_t *>(t), &p, data_kind, dev_id, dev_kind);
+  if (body_p) *body_p = p;
+  return rc;
+}
+
+int talshTensorGetScalar(talsh_tens_t *t, double *sr, double *si) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (t == nullptr || sr == nullptr || si == nullptr) return TALSH_INVALID_ARGS;
+  if (t->shape_p == nullptr) return TALSH_OBJECT_IS_EMPTY;
+  if (t->shape_p->num_dim != 0) return TALSH_INVALID_ARGS;
+  for (int i = 0; i < t->ndev; ++i) {
+    if (t->avail[i] != YEP) continue;
+    unsigned char buf[16];
+    int es = 0;
+    tens_valid_data_kind(t->data_kind[i], &es);
+    int dk = DEV_NULL;
+    const int dn = decode_device_id(t->dev_rsc[i].dev_id, &dk);
+    if (dk == DEV_HOST) {
+      std::memcpy(buf, t->dev_rsc[i].gmem_p, es);
+    } else if (dk == DEV_NVIDIA_GPU && R.gpu[dn].in_use) {
+      cudaSetDevice(dn);
+      cudaStreamSynchronize(R.gpu[dn].stream);
+      if (cudaMemcpy(buf, t->dev_rsc[i].gmem_p, es, cudaMemcpyDeviceToHost) != cudaSuccess) {
+        cudaGetLastError();
+        return TALSH_FAILURE;
+      }
+    } else {
+      continue;
+    }
+    switch (t->data_kind[i]) {
+      case R4: { float v; std::memcpy(&v, buf, 4); *sr = v; *si = 0.0; break; }
+      case R8: { double v; std::memcpy(&v, buf, 8); *sr = v; *si = 0.0; break; }
+      case C4: { float v[2]; std::memcpy(v, buf, 8); *sr = v[0]; *si = v[1]; break; }
+      case C8: { double v[2]; std::memcpy(v, buf, 16); *sr = v[0]; *si = v[1]; break; }
+      default: return TALSH_FAILURE;
+    }
+    return TALSH_SUCCESS;
+  }
+  return TALSH_NOT_FOUND;
+}
+
+void talshTensorPrint(const talsh_tens_t *t) {
+  if (t == nullptr || t->shape_p == nullptr) { std::printf("#TENSOR: empty\n"); return; }
+  std::printf("#TENSOR: rank %d: dims (", t->shape_p->num_dim);
+  for (int i = 0; i < t->shape_p->num_dim; ++i) std::printf(i ? ",%d" : "%d", t->shape_p->dims[i]);
+  std::printf(")\n");
+}
+void talshTensorPrintInfo(const talsh_tens_t *t) {
+  talshTensorPrint(t);
+  if (t == nullptr || t->shape_p == nullptr) return;
+  for (int i = 0; i < t->ndev; ++i)
+    std::printf("#  image %d: device %d kind %d avail %d ptr %p attached %d\n", i, t->dev_rsc[i].dev_id,
+                t->data_kind[i], t->avail[i], t->dev_rsc[i].gmem_p, t->dev_rsc[i].mem_attached);
+}
+void talshTensorPrintBody(const talsh_tens_t *t, double thresh) {
+  if (t == nullptr || t->shape_p == nullptr) return;
+  for (int i = 0; i < t->ndev; ++i) {
+    if (t->dev_rsc[i].dev_id != 0) continue;
+    const size_t vol = shape_volume(t->shape_p);
+    for (size_t l = 0; l < vol; ++l) {
+      double re = 0, im = 0;
+      switch (t->data_kind[i]) {
+        case R4: re = ((float *)t->dev_rsc[i].gmem_p)[l]; break;
+        case R8: re = ((double *)t->dev_rsc[i].gmem_p)[l]; break;
+        case C4: re = ((float *)t->dev_rsc[i].gmem_p)[2 * l]; im = ((float *)t->dev_rsc[i].gmem_p)[2 * l + 1]; break;
+        case C8: re = ((double *)t->dev_rsc[i].gmem_p)[2 * l]; im = ((double *)t->dev_rsc[i].gmem_p)[2 * l + 1]; break;
+      }
+      if (std::hypot(re, im) > thresh) std::printf("%zu: %.15e %.15e\n", l, re, im);
+    }
+    return;
+  }
+}
+
+// ------------------------------------------------------------- slices
+int talshTensorSliceCreate(talsh_tens_slice_t **) { return TALSH_NOT_IMPLEMENTED; }
+int talshTensorSliceClean(talsh_tens_slice_t *) { return TALSH_NOT_IMPLEMENTED; }
+int talshTensorSliceConstruct(talsh_tens_slice_t *, const talsh_tens_t *, const size_t *, const int *, const int *, const int *) {
+  return TALSH_NOT_IMPLEMENTED;
+}
+size_t talshTensorSliceVolume(const talsh_tens_slice_t *) { return 0; }
+int talshTensorSliceDestruct(talsh_tens_slice_t *) { return TALSH_NOT_IMPLEMENTED; }
+int talshTensorSliceDestroy(talsh_tens_slice_t *) { return TALSH_NOT_IMPLEMENTED; }
+
+// ------------------------------------------------------------- tasks
+int talshTaskCreate(talsh_task_t **task) {
+  if (task == nullptr) return TALSH_INVALID_ARGS;
+  *task = (talsh_task_t *)std::malloc(sizeof(talsh_task_t));
+  if (*task == nullptr) return TRY_LATER;
+  return talshTaskClean(*task);
+}
+
+int talshTaskClean(talsh_task_t *t) {
+  if (t == nullptr) return TALSH_INVALID_ARGS;
+  t->task_p = nullptr;
+  t->task_error = -1;
+  t->dev_kind = DEV_NULL;
+  t->data_kind = NO_TYPE;
+  t->coherence = -1;
+  t->num_args = 0;
+  for (int i = 0; i < MAX_TENSOR_OPERANDS; ++i) { t->tens_args[i].tens_p = nullptr; t->tens_args[i].source_image = -1; }
+  t->data_vol = 0.0;
+  t->flops = 0.0;
+  t->exec_time = 0.0;
+  return TALSH_SUCCESS;
+}
+
+int talshTaskIsEmpty(const talsh_task_t *t) {
+  if (t == nullptr) return TALSH_INVALID_ARGS;
+  return t->dev_kind == DEV_NULL ? YEP : NOPE;
+}
+
+int talshTaskDestruct(talsh_task_t *t) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (t == nullptr) return TALSH_INVALID_ARGS;
+  if (t->dev_kind == DEV_NULL) return talshTaskClean(t);
+  const int s = talshTaskStatus(t);
+  if (s != TALSH_TASK_COMPLETED && s != TALSH_TASK_ERROR) return TALSH_IN_PROGRESS;
+  TaskRec *tr = rec_of(t);
+  if (tr) { release_task_events(tr); delete tr; }
+  return talshTaskClean(t);
+}
+
+int talshTaskDestroy(talsh_task_t *t) {
+  if (t == nullptr) return TALSH_INVALID_ARGS;
+  const int rc = talshTaskDestruct(t);
+  if (rc == TALSH_IN_PROGRESS) return rc;
+  std::free(t);
+  return rc;
+}
+
+int talshTaskDevId(talsh_task_t *t, int *dev_kind) {
+  if (t == nullptr || t->dev_kind == DEV_NULL || t->task_p == nullptr) return DEV_NULL;
+  if (dev_kind) { *dev_kind = t->dev_kind; return rec_of(t)->gpu; }
+  return encode_device_id(t->dev_kind, rec_of(t)->gpu);
+}
+int talshTaskDevId_(talsh_task_t *t, int *dev_kind) { return talshTaskDevId(t, dev_kind); }
+int talshTaskArgCoherence(const talsh_task_t *t) { return t ? t->coherence : -1; }
+const talshTensArg_t *talshTaskTensArgs(const talsh_task_t *t, int *num_args) {
+  if (t == nullptr) { if (num_args) *num_args = 0; return nullptr; }
+  if (num_args) *num_args = t->num_args;
+  return t->tens_args;
+}
+
+int talshTaskStatus(talsh_task_t *t) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (!R.on) return TALSH_NOT_INITIALIZED;
+  if (t == nullptr) return TALSH_INVALID_ARGS;
+  if (t->dev_kind == DEV_NULL) return TALSH_TASK_EMPTY;
+  if (t->task_error >= 0) return t->task_error > 0 ? TALSH_TASK_ERROR : TALSH_TASK_COMPLETED;
+  if (t->task_p == nullptr) return TALSH_INVALID_ARGS;
+  return task_progress(t, false);
+}
+
+int talshTaskComplete(talsh_task_t *t, int *stats, int *ierr) {
+  if (ierr == nullptr) return TALSH_INVALID_ARGS;
+  if (!R.on) { *ierr = TALSH_NOT_INITIALIZED; return NOPE; }
+  if (t == nullptr || stats == nullptr) { *ierr = TALSH_INVALID_ARGS; return NOPE; }
+  *ierr = TALSH_SUCCESS;
+  const int s = talshTaskStatus(t);
+  if (s == TALSH_TASK_EMPTY) { *stats = s; *ierr = TALSH_OBJECT_IS_EMPTY; return NOPE; }
+  if (s != TALSH_TASK_COMPLETED && s != TALSH_TASK_ERROR && s < TALSH_TASK_EMPTY) { *ierr = s; return NOPE; }
+  *stats = s;
+  return (s == TALSH_TASK_COMPLETED || s == TALSH_TASK_ERROR) ? YEP : NOPE;
+}
+
+int talshTaskWait(talsh_task_t *t, int *stats) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (!R.on) return TALSH_NOT_INITIALIZED;
+  if (t == nullptr || stats == nullptr) return TALSH_INVALID_ARGS;
+  if (t->dev_kind == DEV_NULL) { *stats = TALSH_TASK_EMPTY; return TALSH_OBJECT_IS_EMPTY; }
+  if (t->task_error >= 0) { *stats = t->task_error > 0 ? TALSH_TASK_ERROR : TALSH_TASK_COMPLETED; return TALSH_SUCCESS; }
+  *stats = task_progress(t, true);
+  return TALSH_SUCCESS;
+}
+
+int talshTasksWait(int ntasks, talsh_task_t tasks[], int stats[]) {
+  if (ntasks < 0 || (ntasks > 0 && (tasks == nullptr || stats == nullptr))) return TALSH_INVALID_ARGS;
+  int rc = TALSH_SUCCESS;
+  for (int i = 0; i < ntasks; ++i) {
+    const int e = talshTaskWait(&tasks[i], &stats[i]);
+    if (e != TALSH_SUCCESS && rc == TALSH_SUCCESS) rc = e;
+  }
+  return rc;
+}
+
+int talshTaskTime(talsh_task_t *t, double *total, double *comput, double *input, double *output, double *mmul) {
+  if (t == nullptr || total == nullptr) return TALSH_INVALID_ARGS;
+  int s = talshTaskStatus(t);
+  if (s != TALSH_TASK_COMPLETED) return (s == TALSH_TASK_ERROR) ? TALSH_TASK_ERROR : TALSH_IN_PROGRESS;
+  TaskRec *tr = rec_of(t);
+  if (tr == nullptr) return TALSH_INVALID_ARGS;
+  *total = tr->times[0];
+  if (comput) *comput = tr->times[1];
+  if (input) *input = tr->times[2];
+  if (output) *output = tr->times[3];
+  if (mmul) *mmul = tr->times[1];
+  return TALSH_SUCCESS;
+}
+int talshTaskTime_(talsh_task_t *t, double *a, double *b, double *c, double *d, double *e) { return talshTaskTime(t, a, b, c, d, e); }
+
+void talshTaskPrint(const talsh_task_t *t) {
+  if (t == nullptr) return;
+  std::printf("#TASK: dev_kind %d data_kind %d coherence %d args %d error %d flops %.3e bytes %.3e time %.6f\n",
+              t->dev_kind, t->data_kind, t->coherence, t->num_args, t->task_error, t->flops, t->data_vol, t->exec_time);
+}
+
+// ------------------------------------------------- tensor-operation objects
+int talshTensorOpCreate(talsh_tens_op_t **) { return TALSH_NOT_IMPLEMENTED; }
+int talshTensorOpClean(talsh_tens_op_t *) { return TALSH_NOT_IMPLEMENTED; }
+int talshTensorOpSetArgument(talsh_tens_op_t *, const talsh_tens_t *, const size_t *, const int *) { return TALSH_NOT_IMPLEMENTED; }
+int talshTensorOpSpecify(talsh_tens_op_t *, int, int, const char *, double, double) { return TALSH_NOT_IMPLEMENTED; }
+int talshTensorOpSetExecDevice(talsh_tens_op_t *, int, int) { return TALSH_NOT_IMPLEMENTED; }
+int talshTensorOpActivate(talsh_tens_op_t *) { return TALSH_NOT_IMPLEMENTED; }
+int talshTensorOpLoadInput(talsh_tens_op_t *) { return TALSH_NOT_IMPLEMENTED; }
+int talshTensorOpExecute(talsh_tens_op_t *, int, int) { return TALSH_NOT_IMPLEMENTED; }
+int talshTensorOpTest(talsh_tens_op_t *, int *, int) { return TALSH_NOT_IMPLEMENTED; }
+int talshTensorOpStoreOutput(talsh_tens_op_t *) { return TALSH_NOT_IMPLEMENTED; }
+int talshTensorOpDeactivate(talsh_tens_op_t *) { return TALSH_NOT_IMPLEMENTED; }
+int talshTensorOpDestruct(talsh_tens_op_t *) { return TALSH_NOT_IMPLEMENTED; }
+int talshTensorOpDestroy(talsh_tens_op_t *) { return TALSH_NOT_IMPLEMENTED; }
+int talshTensorOpProgress(talsh_tens_op_t *, int *) { return TALSH_NOT_IMPLEMENTED; }
+size_t talshTensorOpGetArgVolume(const talsh_tens_op_t *, unsigned int) { return 0; }
+size_t talshTensorOpGetArgSize(const talsh_tens_op_t *, unsigned int) { return 0; }
+double talshTensorOpGetByteCount(const talsh_tens_op_t *, unsigned int) { return 0.0; }
+double talshTensorOpGetFlopCount(const talsh_tens_op_t *) { return 0.0; }
+double talshTensorOpGetIntensity(const talsh_tens_op_t *) { return 0.0; }
+int talshTensorOpDecompose2(const talsh_tens_op_t *, talsh_tens_op_t *, talsh_tens_op_t *) { return TALSH_NOT_IMPLEMENTED; }
+void talshTensorOpPrint(const talsh_tens_op_t *) {}
+
+// ------------------------------------------------------ data placement
+int talshTensorPlace(talsh_tens_t *t, int dev_id, int dev_kind, void *dev_mem, int copy_ctrl, talsh_task_t *task) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (!R.on) return TALSH_NOT_INITIALIZED;
+  if (t == nullptr) return TALSH_INVALID_ARGS;
+  if (talshTensorIsEmpty(t) != NOPE) return TALSH_OBJECT_IS_EMPTY;
+  if (!healthy(t)) return TALSH_FAILURE;
+  const int flat = (dev_kind == DEV_DEFAULT) ? dev_id : encode_device_id(dev_kind, dev_id);
+  int dvk = DEV_NULL;
+  const int dvn = decode_device_id(flat, &dvk);
+  if (dvn < 0) return TALSH_INVALID_ARGS;
+  if (copy_ctrl != COPY_M && copy_ctrl != COPY_K) return TALSH_INVALID_ARGS;
+  if (dvk != DEV_HOST && dvk != DEV_NVIDIA_GPU) return TALSH_NOT_AVAILABLE;
+  if (dvk == DEV_NVIDIA_GPU && (dvn >= MAX_GPUS_PER_NODE || !R.gpu[dvn].in_use)) return TALSH_INVALID_ARGS;
+  // Source image: one on the destination device means nothing to do.
+  int src = -1;
+  for (int i = 0; i < t->ndev; ++i) {
+    if (t->avail[i] != YEP) continue;
+    if (t->dev_rsc[i].dev_id == flat) {
+      if (task) { talshTaskClean(task); task->task_error = 0; }
+      return TALSH_SUCCESS;
+    }
+    int dk = DEV_NULL;
+    decode_device_id(t->dev_rsc[i].dev_id, &dk);
+    if (src < 0 || dk == DEV_HOST) src = i;
+  }
+  if (src < 0) return TALSH_NOT_FOUND;
+  int es = 0;
+  tens_valid_data_kind(t->data_kind[src], &es);
+  const size_t bytes = shape_volume(t->shape_p) * (size_t)es;
+  int sk = DEV_NULL;
+  const int sn = decode_device_id(t->dev_rsc[src].dev_id, &sk);
+  const int gpu = (dvk == DEV_NVIDIA_GPU) ? dvn : sn;  // the GPU whose stream moves the data
+  if (sk != DEV_NVIDIA_GPU && dvk != DEV_NVIDIA_GPU) return TALSH_FAILURE;
+  if (gpu < 0 || gpu >= MAX_GPUS_PER_NODE || !R.gpu[gpu].in_use) return TALSH_INVALID_ARGS;
+  // Destination body.
+  void *dst = dev_mem;
+  bool owned = false;
+  if (dst == nullptr) {
+    if (dvk == DEV_HOST) {
+      dst = host_alloc(bytes, true);
+      if (dst == nullptr) return TRY_LATER;
+    } else {
+      const int rc = dev_alloc(dvn, bytes, &dst);
+      if (rc) return rc;
+    }
+    owned = true;
+  }
+  GpuCtx &G = R.gpu[gpu];
+  cudaSetDevice(gpu);
+  talsh_task_t *tk = task;
+  if (tk == nullptr) { if (talshTaskCreate(&tk) != TALSH_SUCCESS) { if (owned) mem_free(dst); return TALSH_FAILURE; } }
+  else if (talshTaskStatus(tk) != TALSH_TASK_EMPTY) { if (owned) mem_free(dst); return TALSH_OBJECT_NOT_EMPTY; }
+  TaskRec *tr = new TaskRec();
+  tr->gpu = gpu;
+  tr->st = G.stream;
+  tr->nargs = 0;  // placement has its own bookkeeping below
+  for (auto &e : tr->ev) e = event_get(gpu);
+  cudaEventRecord(tr->ev[0], G.stream);
+  cudaEventRecord(tr->ev[1], G.stream);
+  int rc = copy_between(dst, flat, t->dev_rsc[src].gmem_p, t->dev_rsc[src].dev_id, bytes, G.stream);
+  cudaEventRecord(tr->ev[2], G.stream);
+  cudaEventRecord(tr->ev[3], G.stream);
+  tk->task_p = tr;
+  tk->task_error = -1;
+  tk->dev_kind = DEV_NVIDIA_GPU;
+  tk->data_kind = t->data_kind[src];
+  tk->coherence = copy_ctrl;
+  tk->num_args = 1;
+  tk->tens_args[0].tens_p = t;
+  tk->tens_args[0].source_image = src;
+  tk->data_vol = (double)bytes;
+  if (rc != TALSH_SUCCESS) {
+    cudaStreamSynchronize(G.stream);
+    if (owned) mem_free(dst);
+    tr->failed = 20;
+    task_finalize(tk, false);
+    if (task == nullptr) talshTaskDestroy(tk);
+    return TALSH_FAILURE;
+  }
+  // The new image becomes visible right away (reads of it are ordered on the
+  // same stream); the moved source is discarded once the copy finished.
+  if (t->ndev >= t->dev_rsc_len) { cudaStreamSynchronize(G.stream); if (owned) mem_free(dst); return TALSH_LIMIT_EXCEEDED; }
+  const int k = t->ndev++;
+  t->dev_rsc[k].dev_id = flat;
+  t->dev_rsc[k].gmem_p = dst;
+  t->dev_rsc[k].buf_entry = -1;
+  t->dev_rsc[k].mem_attached = owned ? 0 : 1;
+  t->data_kind[k] = t->data_kind[src];
+  t->avail[k] = YEP;
+  if (copy_ctrl == COPY_M) {
+    cudaStreamSynchronize(G.stream);
+    image_discard(t, src);
+  }
+  if (task == nullptr) {
+    int stats = 0;
+    int e = talshTaskWait(tk, &stats);
+    if (e == TALSH_SUCCESS && stats != TALSH_TASK_COMPLETED) e = TALSH_TASK_ERROR;
+    talshTaskDestroy(tk);
+    return e;
+  }
+  return TALSH_SUCCESS;
+}
+int talshTensorPlace_(talsh_tens_t *t, int a, int b, void *c, int d, talsh_task_t *e) { return talshTensorPlace(t, a, b, c, d, e); }
+
+int talshTensorDiscard(talsh_tens_t *t, int dev_id, int dev_kind) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (!R.on) return TALSH_NOT_INITIALIZED;
+  if (t == nullptr) return TALSH_INVALID_ARGS;
+  if (talshTensorIsEmpty(t) != NOPE) return TALSH_OBJECT_IS_EMPTY;
+  const int flat = (dev_kind == DEV_NULL) ? dev_id : encode_device_id(dev_kind, dev_id);
+  for (int i = t->ndev - 1; i >= 0; --i) {
+    if (t->dev_rsc[i].dev_id != flat) continue;
+    int dk = DEV_NULL;
+    const int dn = decode_device_id(flat, &dk);
+    if (dk == DEV_NVIDIA_GPU && R.gpu[dn].in_use) { cudaSetDevice(dn); cudaStreamSynchronize(R.gpu[dn].stream); }
+    return image_discard(t, i);
+  }
+  return TALSH_SUCCESS;
+}
+int talshTensorDiscard_(talsh_tens_t *t, int a, int b) { return talshTensorDiscard(t, a, b); }
+
+int talshTensorDiscardOther(talsh_tens_t *t, int dev_id, int dev_kind) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (!R.on) return TALSH_NOT_INITIALIZED;
+  if (t == nullptr) return TALSH_INVALID_ARGS;
+  if (talshTensorIsEmpty(t) != NOPE) return TALSH_OBJECT_IS_EMPTY;
+  const int flat = (dev_kind == DEV_NULL) ? dev_id : encode_device_id(dev_kind, dev_id);
+  for (int i = 0; i < t->ndev; ++i) {
+    if (t->dev_rsc[i].dev_id != flat) continue;
+    for (int g = 0; g < MAX_GPUS_PER_NODE; ++g)
+      if (R.gpu[g].in_use) { cudaSetDevice(g); cudaStreamSynchronize(R.gpu[g].stream); }
+    return image_discard_other(t, i);
+  }
+  return TALSH_NOT_FOUND;
+}
+int talshTensorDiscardOther_(talsh_tens_t *t, int a, int b) { return talshTensorDiscardOther(t, a, b); }
+
+// ------------------------------------------------------ tensor operations
+int talshTensorInit(talsh_tens_t *d, double vr, double vi, int dev_id, int dev_kind, int copy_ctrl, talsh_task_t *task) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  OpSpec op;
+  op.kind = kOpInit;
+  op.nt = 1;
+  op.t[0] = d;
+  op.coh_ctrl = (unsigned)copy_ctrl;
+  op.sr = vr;
+  op.si = vi;
+  if (copy_ctrl < 0 || copy_ctrl > 3) return TALSH_INVALID_ARGS;
+  return schedule(op, dev_id, dev_kind, task);
+}
+int talshTensorInit_(talsh_tens_t *d, double a, double b, int c, int e, int f, talsh_task_t *g) { return talshTensorInit(d, a, b, c, e, f, g); }
+
+int talshTensorScale(talsh_tens_t *d, double vr, double vi, int dev_id, int dev_kind, int copy_ctrl, talsh_task_t *task) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  OpSpec op;
+  op.kind = kOpScale;
+  op.nt = 1;
+  op.t[0] = d;
+  op.coh_ctrl = (unsigned)copy_ctrl;
+  op.sr = vr;
+  op.si = vi;
+  if (copy_ctrl < 0 || copy_ctrl > 3) return TALSH_INVALID_ARGS;
+  return schedule(op, dev_id, dev_kind, task);
+}
+int talshTensorScale_(talsh_tens_t *d, double a, double b, int c, int e, int f, talsh_task_t *g) { return talshTensorScale(d, a, b, c, e, f, g); }
+
+int talshTensorSlice(talsh_tens_t *, talsh_tens_t *, const int *, int, int, int, int, talsh_task_t *) { return TALSH_NOT_IMPLEMENTED; }
+int talshTensorSlice_(talsh_tens_t *a, talsh_tens_t *b, const int *c, int d, int e, int f, int g, talsh_task_t *h) {
+  return talshTensorSlice(a, b, c, d, e, f, g, h);
+}
+int talshTensorInsert(talsh_tens_t *, talsh_tens_t *, const int *, int, int, int, int, talsh_task_t *) { return TALSH_NOT_IMPLEMENTED; }
+int talshTensorInsert_(talsh_tens_t *a, talsh_tens_t *b, const int *c, int d, int e, int f, int g, talsh_task_t *h) {
+  return talshTensorInsert(a, b, c, d, e, f, g, h);
+}
+
+int talshTensorCopy(const char *cptrn, talsh_tens_t *d, talsh_tens_t *l, int dev_id, int dev_kind, int copy_ctrl,
+                    talsh_task_t *task) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (!R.on) return TALSH_NOT_INITIALIZED;
+  if (d == nullptr || l == nullptr) return TALSH_INVALID_ARGS;
+  if (talshTensorIsEmpty(d) != NOPE || talshTensorIsEmpty(l) != NOPE) return TALSH_OBJECT_IS_EMPTY;
+  if (copy_ctrl < 0 || copy_ctrl > 15) return TALSH_INVALID_ARGS;
+  OpSpec op;
+  op.kind = kOpCopy;
+  op.nt = 2;
+  op.t[0] = d;
+  op.t[1] = l;
+  op.coh_ctrl = (unsigned)copy_ctrl;
+  const int rc = parse_and_check(cptrn, op, 1);
+  if (rc) return rc;
+  return schedule(op, dev_id, dev_kind, task);
+}
+int talshTensorCopy_(const char *p, talsh_tens_t *d, talsh_tens_t *l, int a, int b, int c, talsh_task_t *t) {
+  return talshTensorCopy(p, d, l, a, b, c, t);
+}
+
+int talshTensorAdd(const char *cptrn, talsh_tens_t *d, talsh_tens_t *l, double sr, double si, int dev_id, int dev_kind,
+                   int copy_ctrl, talsh_task_t *task) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (!R.on) return TALSH_NOT_INITIALIZED;
+  if (d == nullptr || l == nullptr) return TALSH_INVALID_ARGS;
+  if (talshTensorIsEmpty(d) != NOPE || talshTensorIsEmpty(l) != NOPE) return TALSH_OBJECT_IS_EMPTY;
+  if (copy_ctrl < 0 || copy_ctrl > 15) return TALSH_INVALID_ARGS;
+  OpSpec op;
+  op.kind = kOpAdd;
+  op.nt = 2;
+  op.t[0] = d;
+  op.t[1] = l;
+  op.coh_ctrl = (unsigned)copy_ctrl;
+  op.sr = sr;
+  op.si = si;
+  const int rc = parse_and_check(cptrn, op, 1);
+  if (rc) return rc;
+  return schedule(op, dev_id, dev_kind, task);
+}
+int talshTensorAdd_(const char *p, talsh_tens_t *d, talsh_tens_t *l, double a, double b, int c, int e, int f, talsh_task_t *t) {
+  return talshTensorAdd(p, d, l, a, b, c, e, f, t);
+}
+
+int talshTensorContract(const char *cptrn, talsh_tens_t *d, talsh_tens_t *l, talsh_tens_t *r, double sr, double si,
+                        int dev_id, int dev_kind, int copy_ctrl, int accumulative, talsh_task_t *task) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (!R.on) return TALSH_NOT_INITIALIZED;
+  if (d == nullptr || l == nullptr || r == nullptr) return TALSH_INVALID_ARGS;
+  if (talshTensorIsEmpty(d) != NOPE || talshTensorIsEmpty(l) != NOPE || talshTensorIsEmpty(r) != NOPE)
+    return TALSH_OBJECT_IS_EMPTY;
+  if (copy_ctrl < 0 || copy_ctrl > 63) return TALSH_INVALID_ARGS;
+  OpSpec op;
+  op.kind = kOpContract;
+  op.nt = 3;
+  op.t[0] = d;
+  op.t[1] = l;
+  op.t[2] = r;
+  op.coh_ctrl = (unsigned)copy_ctrl;
+  op.sr = sr;
+  op.si = si;
+  op.accumulative = accumulative == NOPE ? NOPE : YEP;
+  const int rc = parse_and_check(cptrn, op, 2);
+  if (rc) return rc;
+  return schedule(op, dev_id, dev_kind, task);
+}
+int talshTensorContract_(const char *p, talsh_tens_t *d, talsh_tens_t *l, talsh_tens_t *r, double a, double b, int c,
+                         int e, int f, int g, talsh_task_t *t) {
+  return talshTensorContract(p, d, l, r, a, b, c, e, f, g, t);
+}
+
+int talshTensorContractXL(const char *cptrn, talsh_tens_t *d, talsh_tens_t *l, talsh_tens_t *r, double sr, double si,
+                          int dev_id, int dev_kind, int accumulative) {
+  // Without out-of-core decomposition yet: a blocking contraction on one GPU.
+  return talshTensorContract(cptrn, d, l, r, sr, si, dev_id, dev_kind, COPY_MTT, accumulative, nullptr);
+}
+int talshTensorContractXL_(const char *p, talsh_tens_t *d, talsh_tens_t *l, talsh_tens_t *r, double a, double b, int c,
+                           int e, int f) {
+  return talshTensorContractXL(p, d, l, r, a, b, c, e, f);
+}
+
+int talshTensorDecomposeSVD(const char *, talsh_tens_t *, talsh_tens_t *, talsh_tens_t *, talsh_tens_t *, const char, int, int) {
+  return TALSH_NOT_IMPLEMENTED;
+}
+int talshTensorDecomposeSVDL(const char *, talsh_tens_t *, talsh_tens_t *, talsh_tens_t *, int, int) { return TALSH_NOT_IMPLEMENTED; }
+int talshTensorDecomposeSVDR(const char *, talsh_tens_t *, talsh_tens_t *, talsh_tens_t *, int, int) { return TALSH_NOT_IMPLEMENTED; }
+int talshTensorDecomposeSVDLR(const char *, talsh_tens_t *, talsh_tens_t *, talsh_tens_t *, int, int) { return TALSH_NOT_IMPLEMENTED; }
+int talshTensorOrthogonalizeSVD(const char *, talsh_tens_t *, int, int) { return TALSH_NOT_IMPLEMENTED; }
+int talshTensorOrthogonalizeMGS(talsh_tens_t *, int, int *, int, int) { return TALSH_NOT_IMPLEMENTED; }
+
+double talshTensorImageNorm1_cpu(const talsh_tens_t *t) {
+  if (t == nullptr || t->shape_p == nullptr) return -1.0;
+  for (int i = 0; i < t->ndev; ++i) {
+    if (t->dev_rsc[i].dev_id != 0) continue;
+    const size_t n = shape_volume(t->shape_p);
+    const void *p = t->dev_rsc[i].gmem_p;
+    double s = 0.0;
+    switch (t->data_kind[i]) {
+      case R4: for (size_t j = 0; j < n; ++j) s += (double)std::fabs(((const float *)p)[j]); break;
+      case R8: for (size_t j = 0; j < n; ++j) s += std::fabs(((const double *)p)[j]); break;
+      case C4: for (size_t j = 0; j < n; ++j) s += (double)std::hypot(((const float *)p)[2 * j], ((const float *)p)[2 * j + 1]); break;
+      case C8: for (size_t j = 0; j < n; ++j) s += std::hypot(((const double *)p)[2 * j], ((const double *)p)[2 * j + 1]); break;
+      default: return -1.0;
+    }
+    return s;
+  }
+  return -1.0;
+}
+
+double talshTensorNorm1(talsh_tens_t *t, int dev_id, int dev_kind) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (!R.on || t == nullptr || talshTensorIsEmpty(t) != NOPE) return -1.0;
+  double *out = nullptr;
+  if (cudaMallocHost((void **)&out, sizeof(double)) != cudaSuccess) { cudaGetLastError(); return -1.0; }
+  *out = -1.0;
+  OpSpec op;
+  op.kind = kOpNorm1;
+  op.nt = 1;
+  op.t[0] = t;
+  op.coh_ctrl = COPY_T;  // a staged copy of a Host image is temporary
+  op.norm_out = out;
+  const int rc = schedule(op, dev_id, dev_kind, nullptr);
+  const double v = (rc == TALSH_SUCCESS) ? *out : -1.0;
+  cudaFreeHost(out);
+  return v;
+}
+double talshTensorNorm1_(talsh_tens_t *t, int dev_id, int dev_kind) { return talshTensorNorm1(t, dev_id, dev_kind); }
+
+}  // extern "C"
