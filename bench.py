@@ -1,0 +1,543 @@
+"""talsh-b200 benchmark: the transpose/add sweep (C2) on B200, plus the C1/C3
+contraction rates, against the reference algorithm on the host cores.
+
+Workload (one step): the seeded C2 sweep -- ranks 2..6, every permutation of
+ranks 2..4 and 64 random permutations of ranks 5 and 6, extents drawn
+log-uniformly for a total volume of 2^20..2^28 elements (odd extents 17/31/97
+and unit extents included), R4 and R8; each case runs one transpose
+D = TRN(L) and one transpose-add D += TRN(L)*alpha (alpha cycling through
+1, 0.5, -1.25).  Metric: algorithmic HBM bytes (2*vol*esize per transpose,
+3*vol*esize per add) / device time, in GB/s.
+
+  value      the whole sweep per step, inputs resident in HBM, replayed from a
+             CUDA graph; consecutive cases use input regions 1 GiB apart so no
+             case reads another case's data out of L2 (the L2 is 126 MB).
+  e2e        the same sweep through talshTensorCopy/talshTensorAdd on pinned
+             Host tensors (COPY_TT: every step moves L (and D for adds) to the
+             GPU and D back).
+  roofline   permute_tiled_kernel launches timed one by one with CUDA events.
+  contract   C1 and C3 FP64 contractions through talshTensorContract on
+             GPU-resident tensors (TFLOP/s, error vs an FP64 reference).
+  cpu_baseline  the reference's cache-blocked CPU transpose (restated in the
+             oracle, OpenMP over all host cores) on a bounded sample of the sweep.
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+Multi-GPU (torchrun): every rank runs the whole sweep on its own GPU (replicas,
+weak scaling: the transposes are independent units); value = all ranks' bytes
+/ the slowest rank's time.
+"""
+import argparse
+import ctypes as C
+import itertools
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+R4, R8, C4, C8 = 4, 8, 14, 18
+ESIZE = {R4: 4, R8: 8, C4: 8, C8: 16}
+METRIC = "transpose GB/s"
+SLOT = 1 << 30          # 1 GiB input/output regions
+NSLOT = 4               # regions rotated between consecutive cases
+ALPHAS = [(1.0, 0.0), (0.5, 0.0), (-1.25, 0.0)]
+
+
+def c2_cases(seed=2024):
+    """The seeded C2 sweep: list of (kind, dims, o2n)."""
+    rng = np.random.default_rng(seed)
+    perms = []
+    for rank in (2, 3, 4):
+        perms += [(rank, tuple(p)) for p in itertools.permutations(range(1, rank + 1))]
+    for rank in (5, 6):
+        perms += [(rank, tuple(int(x) + 1 for x in rng.permutation(rank))) for _ in range(64)]
+    cases = []
+    for kind in (R4, R8):
+        for n, (rank, o2n) in enumerate(perms):
+            vol = 2.0 ** rng.uniform(20, 28)
+            w = rng.dirichlet(np.ones(rank))
+            dims = [max(2, int(round(vol ** wi))) for wi in w]
+            r = rng.random()
+            if r < 0.35:
+                dims[rng.integers(rank)] = int(rng.choice([17, 31, 97]))
+            elif r < 0.45 and rank > 2:
+                dims[rng.integers(rank)] = 1
+            while np.prod(dims, dtype=np.int64) > 2 ** 28:
+                dims[int(np.argmax(dims))] //= 2
+            while np.prod(dims, dtype=np.int64) < 2 ** 20:
+                dims[int(np.argmin(dims))] *= 2
+            cases.append((kind, [int(d) for d in dims], list(o2n)))
+    return cases
+
+
+def case_bytes(kind, dims):
+    return int(np.prod(dims, dtype=np.int64)) * ESIZE[kind]
+
+
+def pattern(o2n, add):
+    lab = "abcdefgh"
+    d = [None] * len(o2n)
+    for i, p in enumerate(o2n):
+        d[p - 1] = lab[i]
+    return "D(%s)%s=L(%s)" % (",".join(d), "+" if add else "", ",".join(lab[:len(o2n)]))
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons while running."""
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.rows = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.QUERY,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def stop(self):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        if self.thread is not None:
+            self.thread.join(timeout=5)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+        sm = [num(r[1]) for r in self.rows if num(r[1])]
+        mx = [num(r[2]) for r in self.rows if num(r[2])]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def measured_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def profile_traffic_ratio():
+    """DRAM bytes / algorithmic bytes of permute_tiled_kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "permute_tiled_kernel_c2.md")
+    try:
+        for line in open(path):
+            if line.startswith("traffic_over_algorithmic:"):
+                return float(line.split(":")[1].split()[0])
+    except OSError:
+        pass
+    return None
+
+
+# ----------------------------------------------------------------- CPU side
+def cpu_sample_cases(cases, budget_elems=1 << 24):
+    """A bounded sample of the sweep for the host cores: every 8th case, volume capped."""
+    out = []
+    for i, (kind, dims, o2n) in enumerate(cases):
+        if i % 8:
+            continue
+        dims = list(dims)
+        while np.prod(dims, dtype=np.int64) > budget_elems:
+            dims[int(np.argmax(dims))] //= 2
+        out.append((kind, dims, o2n))
+    return out
+
+
+def run_cpu_baseline(cases, seconds_budget=20.0):
+    import oracle as O
+    O.lib()
+    threads = os.cpu_count() or 1
+    sample = cpu_sample_cases(cases)
+    arrays = {}
+    total_bytes, total_time = 0.0, 0.0
+    rng = np.random.default_rng(0)
+    t_start = time.time()
+    n_done = 0
+    for i, (kind, dims, o2n) in enumerate(sample):
+        vol = int(np.prod(dims, dtype=np.int64))
+        dt = np.float32 if kind == R4 else np.float64
+        a = np.asfortranarray(rng.standard_normal(vol).astype(dt).reshape(dims, order="F"))
+        out = np.empty(O.out_dims(dims, o2n), dtype=dt, order="F")
+        L = O.lib()
+        iv = lambda s: (C.c_int * max(1, len(s)))(*s)
+        t0 = time.perf_counter()
+        L.orc_permute_blocked(kind, len(dims), iv(dims), iv(o2n), C.c_void_p(a.ctypes.data),
+                              C.c_void_p(out.ctypes.data), threads)
+        dt_s = time.perf_counter() - t0
+        total_bytes += 2.0 * vol * ESIZE[kind]
+        total_time += dt_s
+        n_done += 1
+        if time.time() - t_start > seconds_budget:
+            break
+    gbs = total_bytes / total_time / 1e9 if total_time > 0 else 0.0
+    return {"value": gbs, "unit": "GB/s", "cores": threads, "kind": "port",
+            "sample": "%d of %d sweep transposes (every 8th case, volume capped at 2^24 elements), "
+                      "cache-blocked OpenMP transpose restating tensor_block_copy_dlf_r8, %.1f GB moved in %.2f s"
+                      % (n_done, len(cases), total_bytes / 1e9, total_time)}, total_time
+
+
+# ----------------------------------------------------------------- GPU side
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="talsh_b200", choices=["talsh_b200", "reference"])
+    ap.add_argument("--e2e-steps", type=int, default=1)
+    ap.add_argument("--no-contract", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    cases = c2_cases()
+    config = {"workload": "C2 transpose/add sweep: ranks 2-6, %d cases x (transpose + add), R4/R8, "
+                          "volumes 2^20..2^28 (seed 2024)" % len(cases),
+              "ops_per_step": 2 * len(cases), "l2": "inputs rotated over 4 x 1 GiB regions (> 126 MB L2)",
+              "parallelism": "replicas" if world > 1 else "single GPU"}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        for _ in range(args.warmup):
+            pass
+        vals = []
+        base = None
+        for _ in range(max(1, args.steps)):
+            base, _t = run_cpu_baseline(cases, seconds_budget=max(5.0, 60.0 / max(1, args.steps)))
+            vals.append(base["value"])
+        v = statistics.median(vals)
+        base["value"] = v
+        line = {"metric": METRIC, "value": v, "unit": "GB/s", "n_gpus": args.gpus, "steps": args.steps,
+                "warmup": args.warmup, "higher_is_better": True, "impl": "reference", "dtype": "f32/f64",
+                "data": "synthetic", "config": config, "cpu_baseline": base, "vs_baseline": None,
+                "e2e": {"value": v, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+
+    import torch
+    import tal_sh_b200 as T
+
+    if world > 1:
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    dev = torch.device("cuda", local if world > 1 else 0)
+    torch.cuda.set_device(dev)
+    L = T.lib()
+    stream = torch.cuda.current_stream(dev)
+
+    # Resident buffers: NSLOT regions for L and for D.
+    lbuf = torch.empty(NSLOT * SLOT, dtype=torch.uint8, device=dev)
+    dbuf = torch.empty(NSLOT * SLOT, dtype=torch.uint8, device=dev)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(1234 + rank)
+    lbuf.view(torch.float32).uniform_(-1.0, 1.0, generator=gen)
+    dbuf.view(torch.float32).uniform_(-1.0, 1.0, generator=gen)
+    base_l, base_d = lbuf.data_ptr(), dbuf.data_ptr()
+    iv = T.ivec
+
+    ops = []
+    for i, (kind, dims, o2n) in enumerate(cases):
+        b = case_bytes(kind, dims)
+        slot = (i % NSLOT) if b <= SLOT else 0
+        if b > SLOT:
+            assert b <= NSLOT * SLOT
+        src, dst = base_l + slot * SLOT, base_d + slot * SLOT
+        a = ALPHAS[i % len(ALPHAS)]
+        ops.append((kind, dims, o2n, src, dst, False, (0.0, 0.0), 2 * b))
+        ops.append((kind, dims, o2n, src, dst, True, a, 3 * b))
+    step_bytes = float(sum(o[7] for o in ops))
+
+    def launch(op, s=None):
+        kind, dims, o2n, src, dst, add, a, _ = op
+        if s is None:
+            s = torch.cuda.current_stream(dev).cuda_stream  # the capture stream inside a graph capture
+        if add:
+            rc = L.tcTensorPermuteAdd(kind, len(dims), iv(dims), iv(o2n), src, dst, a[0], a[1], 0, s)
+        else:
+            rc = L.tcTensorPermute(kind, len(dims), iv(dims), iv(o2n), src, dst, 0, s)
+        if rc != 0:
+            raise RuntimeError("launch failed %d: %s" % (rc, L.tcLastErrorString()))
+
+    def run_sweep():
+        s = torch.cuda.current_stream(dev).cuda_stream
+        for op in ops:
+            launch(op, s)
+
+    # Warm-up (also fills plan/occupancy caches before graph capture).
+    for _ in range(max(1, args.warmup)):
+        run_sweep()
+    torch.cuda.synchronize(dev)
+
+    # Per-launch timing for the roofline (one eager pass).
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in ops]
+    for op, (e0, e1) in zip(ops, evs):
+        e0.record(stream)
+        launch(op)
+        e1.record(stream)
+    torch.cuda.synchronize(dev)
+    durs = [e0.elapsed_time(e1) * 1e-3 for e0, e1 in evs]
+    copy_t = sum(d for d, op in zip(durs, ops) if not op[5])
+    add_t = sum(d for d, op in zip(durs, ops) if op[5])
+    copy_b = sum(op[7] for op in ops if not op[5])
+    add_b = sum(op[7] for op in ops if op[5])
+    launch_avg_bytes = step_bytes / len(ops)
+    launch_avg_s = sum(durs) / len(ops)
+
+    # CUDA graph of the whole sweep (falls back to eager launches).
+    graph = None
+    try:
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=stream):
+            run_sweep()
+        graph = g
+        graph.replay()
+        torch.cuda.synchronize(dev)
+    except Exception as exc:  # capture unsupported: time eager launches
+        print("graph capture failed (%s); timing eager launches" % exc, file=sys.stderr)
+        graph = None
+        torch.cuda.synchronize(dev)
+    stream = torch.cuda.current_stream(dev)
+    for _ in range(args.warmup):
+        graph.replay() if graph is not None else run_sweep()
+    launches_before = L.tcKernelLaunchCount()
+    sampler = ClockSampler(dev.index if dev.index is not None else 0)
+    sampler.start()
+    time.sleep(0.3)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for _ in range(args.steps):
+        graph.replay() if graph is not None else run_sweep()
+    t1.record(stream)
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    sampler.stop()
+    elapsed = t0.elapsed_time(t1) * 1e-3
+    gpu_launches = len(ops) * args.steps if graph is not None else int(L.tcKernelLaunchCount() - launches_before)
+    if world > 1:
+        tt = torch.tensor([elapsed], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        elapsed = float(tt.item())
+    value = step_bytes * args.steps * world / elapsed / 1e9
+    ms_per_step = elapsed / args.steps * 1e3
+
+    # Bit-exact spot check of one case against the oracle (small, outside timing).
+    check = None
+    if rank == 0:
+        import oracle as O
+        kind, dims, o2n, src, dst, add, a, _ = ops[0]
+        vol = int(np.prod(dims))
+        nb = vol * ESIZE[kind]
+        dt = np.float32 if kind == R4 else np.float64
+        launch(ops[0])
+        torch.cuda.synchronize(dev)
+        lin = lbuf[(src - base_l):(src - base_l) + nb].cpu().numpy().view(dt).reshape(dims, order="F")
+        out = dbuf[(dst - base_d):(dst - base_d) + nb].cpu().numpy().view(dt)
+        check = bool(out.tobytes() == O.permute(lin, o2n).tobytes(order="F"))
+
+    # End to end through the public API with pinned Host buffers.
+    e2e = None
+    if args.e2e_steps > 0:
+        hl = torch.empty(2 * SLOT, dtype=torch.uint8, pin_memory=True)
+        hd = torch.empty(2 * SLOT, dtype=torch.uint8, pin_memory=True)
+        hl.view(torch.float32).uniform_(-1.0, 1.0)
+        hd.zero_()
+        hb, ha = C.c_size_t(0), C.c_int(0)
+        rc = L.talshInit(C.byref(hb), C.byref(ha), 1, T.ivec([dev.index or 0]), 0, None, 0, None)
+        assert rc in (0, T.TALSH_ALREADY_INITIALIZED), rc
+        tens = []
+        for kind, dims, o2n in cases:
+            lt = T.Tens(); dt_ = T.Tens()
+            L.talshTensorClean(C.byref(lt)); L.talshTensorClean(C.byref(dt_))
+            outd = [0] * len(dims)
+            for i, p in enumerate(o2n):
+                outd[p - 1] = dims[i]
+            assert L.talshTensorConstruct(C.byref(lt), kind, len(dims), iv(dims), 0, hl.data_ptr(), -1, None, 0.0, 0.0) == 0
+            assert L.talshTensorConstruct(C.byref(dt_), kind, len(dims), iv(outd), 0, hd.data_ptr(), -1, None, 0.0, 0.0) == 0
+            tens.append((lt, dt_, pattern(o2n, False).encode(), pattern(o2n, True).encode()))
+        h2d = d2h = 0
+        for (kind, dims, o2n) in cases:
+            b = case_bytes(kind, dims)
+            h2d += b + 2 * b  # copy: L; add: L and D
+            d2h += b + b
+        gdev = dev.index or 0
+
+        def e2e_step():
+            for i, (lt, dt_, pc, pa) in enumerate(tens):
+                a = ALPHAS[i % len(ALPHAS)]
+                rc1 = L.talshTensorCopy(pc, C.byref(dt_), C.byref(lt), gdev, T.DEV_NVIDIA_GPU, T.COPY_TT, None)
+                rc2 = L.talshTensorAdd(pa, C.byref(dt_), C.byref(lt), a[0], a[1], gdev, T.DEV_NVIDIA_GPU, T.COPY_TT, None)
+                if rc1 or rc2:
+                    raise RuntimeError("e2e op failed %d %d" % (rc1, rc2))
+        e2e_step()  # warm-up
+        torch.cuda.synchronize(dev)
+        t = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            e2e_step()
+        torch.cuda.synchronize(dev)
+        e2e_s = time.perf_counter() - t
+        if world > 1:
+            tt = torch.tensor([e2e_s], device=dev)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            e2e_s = float(tt.item())
+        for lt, dt_, _, _ in tens:
+            L.talshTensorDestruct(C.byref(lt)); L.talshTensorDestruct(C.byref(dt_))
+        e2e = {"value": step_bytes * args.e2e_steps * world / e2e_s / 1e9, "unit": "GB/s",
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+               "path": "talshTensorCopy + talshTensorAdd, pinned Host tensors, COPY_TT, blocking calls",
+               "steps": args.e2e_steps}
+
+    # Contractions (FP64) through talshTensorContract on GPU-resident tensors.
+    contract = None
+    if not args.no_contract:
+        contract = bench_contractions(T, L, torch, dev)
+
+    del lbuf, dbuf
+    peak, peak_kind = measured_peak()
+    achieved = launch_avg_bytes / launch_avg_s / 1e9
+    ratio = profile_traffic_ratio()
+    roofline = {"kernel": "permute_tiled_kernel (transpose and transpose-add)", "bound": "hbm",
+                "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)",
+                "traffic": (ratio * launch_avg_bytes) if ratio else None,
+                "launches": len(ops), "avg_launch_bytes": launch_avg_bytes, "avg_launch_us": launch_avg_s * 1e6,
+                "transpose_gbs": copy_b / copy_t / 1e9, "add_gbs": add_b / add_t / 1e9}
+
+    if rank == 0:
+        cpu = None
+        if not args.no_cpu and world == 1:
+            cpu, _ = run_cpu_baseline(cases)
+        line = {"metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32/f64 (R4/R8)", "data": "synthetic", "config": config,
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": gpu_launches,
+                "clocks": sampler.summary(), "contract": contract, "check_bit_exact": check,
+                "graph": graph is not None}
+        print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def bench_contractions(T, L, torch, dev):
+    """C1 and C3 FP64 contraction rates (talshTensorContract, GPU-resident operands)."""
+    hb, ha = C.c_size_t(0), C.c_int(0)
+    rc = L.talshInit(C.byref(hb), C.byref(ha), 1, T.ivec([dev.index or 0]), 0, None, 0, None)
+    assert rc in (0, T.TALSH_ALREADY_INITIALIZED)
+    gpu = 1 + (dev.index or 0)
+    out = {}
+    specs = [("C1", "D(a,b,i,j)+=L(a,k,c,i)*R(c,b,k,j)", [32] * 4, [32] * 4, [32] * 4, 20),
+             ("C3b", "D(a,b,i,j)+=L(a,k,c,i)*R(c,b,k,j)", [192, 192, 64, 64], [192, 64, 192, 64],
+              [192, 192, 64, 64], 3),
+             ("C3a", "D(a,b,i,j)+=L(a,b,c,d)*R(c,d,i,j)", [192, 192, 64, 64], [192] * 4, [192, 192, 64, 64], 2)]
+    for name, pat, dd, ld, rd, reps in specs:
+        tens = []
+        for dims, init in ((dd, 0.0), (ld, 0.0), (rd, 0.0)):
+            t = T.Tens()
+            L.talshTensorClean(C.byref(t))
+            rc = L.talshTensorConstruct(C.byref(t), T.R8, 4, T.ivec(dims), gpu, None, -1, None, init, 0.0)
+            if rc != 0:
+                return {"error": "construct %d" % rc}
+            tens.append(t)
+        # fill L and R with normal values scaled by 1/sqrt(contracted volume)
+        ptrs = []
+        for t, dims in zip(tens, (dd, ld, rd)):
+            p = C.c_void_p()
+            assert L.talshTensorGetBodyAccess(C.byref(t), C.byref(p), T.R8, gpu, T.DEV_NULL) == 0
+            ptrs.append(p.value)
+        kvol = 1
+        e, dig, dr, lr, rr, cj = T.parse_pattern(pat)
+        for i, v in enumerate(dig[:lr]):
+            if v < 0:
+                kvol *= ld[i]
+        views = []
+        for p, dims in zip(ptrs, (dd, ld, rd)):
+            n = int(np.prod(dims))
+            views.append(torch.as_tensor(_DevArray(p, n), device=dev))
+        gen = torch.Generator(device=dev)
+        gen.manual_seed(7)
+        views[1].normal_(generator=gen).mul_(kvol ** -0.5)
+        views[2].normal_(generator=gen).mul_(kvol ** -0.5)
+        torch.cuda.synchronize(dev)
+        flops = 2.0 * np.prod(dd) * kvol
+        run = lambda: L.talshTensorContract(pat.encode(), C.byref(tens[0]), C.byref(tens[1]), C.byref(tens[2]),
+                                           1.0, 0.0, gpu, T.DEV_NULL, T.COPY_MTT, T.NOPE, None)
+        assert run() == 0
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            assert run() == 0
+        torch.cuda.synchronize(dev)
+        dt = (time.perf_counter() - t0) / reps
+        # FP64 reference on the GPU (torch einsum over cuBLAS DGEMM), outside the timing.
+        import re
+        toks = re.findall(r"\(([^)]*)\)", pat)
+        sD, sL, sR = [t.split(",") for t in toks]
+        labels = sorted(set(sD + sL + sR))
+        m = {x: "abcdefghij"[i] for i, x in enumerate(labels)}
+        spec = "".join(m[x] for x in reversed(sL)) + "," + "".join(m[x] for x in reversed(sR)) + "->" + \
+            "".join(m[x] for x in reversed(sD))
+        lv = views[1].view(*reversed(ld))
+        rv = views[2].view(*reversed(rd))
+        ref = torch.einsum(spec, lv, rv)
+        got = views[0].view(*reversed(dd))
+        err = float(torch.linalg.norm(got - ref) / torch.linalg.norm(ref))
+        out[name] = {"pattern": pat, "tflops": flops / dt / 1e12, "ms": dt * 1e3, "flop": flops,
+                     "rel_err_vs_fp64": err, "dtype": "f64", "path": "talshTensorContract, GPU-resident"}
+        for t in tens:
+            L.talshTensorDestruct(C.byref(t))
+        del views, ref, got, lv, rv
+    return out
+
+
+class _DevArray:
+    """__cuda_array_interface__ wrapper for a device body owned by TAL-SH."""
+
+    def __init__(self, ptr, n):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": "<f8", "data": (ptr, False), "version": 3}
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,179 @@
+"""CPU-only checks of the drop-in boundary: libtalsh.so loads and exports every
+function include/*.h declares; the product's pattern parser and permutation
+solvers agree with the oracle; the runtime's host logic works without a GPU."""
+import ctypes as C
+import itertools
+import json
+import os
+import random
+import re
+
+import numpy as np
+import pytest
+
+import oracle as O
+import tal_sh_b200 as T
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GOLD = os.path.join(ROOT, "tests", "golden")
+
+
+def declared_functions(path):
+    text = open(path).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    text = re.sub(r"//[^\n]*", "", text)
+    text = re.sub(r"^\s*#[^\n]*", "", text, flags=re.M)
+    text = re.sub(r"typedef[^;]*;", "", text)
+    names = set()
+    for m in re.finditer(r"([A-Za-z_]\w*)\s*\(([^;{}]*)\)\s*;", text):
+        if m.group(1) not in ("TALSH_DEFAULT", "int", "void", "double", "size_t"):
+            names.add(m.group(1))
+    return names
+
+
+@pytest.mark.parametrize("header", ["talsh.h", "tensor_algebra.h", "talsh_b200.h"])
+def test_library_exports_every_declared_symbol(built, header):
+    L = T.lib()
+    names = declared_functions(os.path.join(ROOT, "include", header))
+    assert len(names) > 5
+    missing = [n for n in sorted(names) if not hasattr(L, n)]
+    assert not missing, missing
+
+
+def test_headers_compile_as_c_and_cpp(built, tmp_path):
+    src = tmp_path / "t.c"
+    src.write_text('#include "talsh.h"\n#include "talsh_b200.h"\nint main(void){talsh_tens_t t; talshTensorClean(&t); return 0;}\n')
+    import subprocess
+    for cc, ext in (("gcc", "c"), ("g++", "cpp")):
+        f = tmp_path / ("t." + ext)
+        f.write_text(src.read_text())
+        subprocess.run([cc, "-I", os.path.join(ROOT, "include"), "-c", str(f), "-o", str(tmp_path / ("t_" + ext + ".o"))],
+                       check=True)
+
+
+def test_struct_layouts_match_reference_abi():
+    # talsh.h:87-94 and :110-121 on LP64
+    assert C.sizeof(T.Tens) == 40
+    assert C.sizeof(T.DevRsc) == 24
+    assert C.sizeof(T.Task) == 8 + 4 * 5 + 4 + 16 * 4 + 24
+
+
+def _pattern_corpus():
+    g = json.load(open(os.path.join(GOLD, "tensor_contractions.json")))
+    pats = [c["pattern"] for c in g]
+    pats += ["D(a,b,i,j)+=L(a,k,c,i)*R(c,b,k,j)", "D(i,c,a,b)=L(a,b,c,i)", "D(a,a)+=L(a)*R(a)", "D(a)+=L(a,b)",
+             "D(a,,b)+=L(a,b)", "D+(a)+=L(a,b)*R+(b)", "D(a,b)+=L(a,b)*2.0", "D()=L()", "X(a|b)+=Y(b|a)",
+             "D(a,b)+=L(a,c)*R(c,b)*S(d)", "D(a,b+)+=L(b+,a)", "D(a,b", "D(1a,b2)=L(b2,1a)", "D(a)+=L(a)*R(a)",
+             "D(a,b)+=L(a,c,c)*R(b)", "", "*", "D(a)*3", "D(a)+=L(a)*R()*", "  D(a)=L(a)  ", "D(a_b)=L(a_b)",
+             "D(a,b)+=L+(a,c)*R(c,b)", "D(ab,cd)+=L(cd,ef)*R(ef,ab)", "D(a)+=L(a,b)*R(b)*2", "D(a)+=L(a,b)*R(c)"]
+    rng = random.Random(7)
+    for _ in range(300):  # random well-formed and perturbed patterns
+        labels = list("abcdefghij")
+        rng.shuffle(labels)
+        nd, nc = rng.randint(0, 4), rng.randint(0, 3)
+        dl, cl = labels[:nd], labels[nd:nd + nc]
+        split = rng.randint(0, nd)
+        lidx, ridx = dl[:split] + cl, dl[split:] + cl
+        rng.shuffle(lidx)
+        rng.shuffle(ridx)
+        p = "D(%s)+=L%s(%s)*R%s(%s)" % (",".join(dl), rng.choice(["", "+"]), ",".join(lidx),
+                                           rng.choice(["", "+"]), ",".join(ridx))
+        if rng.random() < 0.3:
+            i = rng.randrange(len(p))
+            p = p[:i] + rng.choice(["a", ",", ")", "(", "+", "*", "|"]) + p[i + 1:]
+        pats.append(p)
+    return pats
+
+
+def test_parser_matches_oracle(built):
+    for p in _pattern_corpus():
+        assert T.parse_pattern(p) == O.str2dig(p), p
+
+
+def _product_permutations(fn, cptrn, lr, rr, conj, tl=1, tr=0):
+    L = T.lib()
+    d, l, r = (C.c_int * 64)(), (C.c_int * 64)(), (C.c_int * 64)()
+    ncd, nlu, nru, nhu, ierr = C.c_int(), C.c_int(), C.c_int(), C.c_int(), C.c_int()
+    if fn == "cpu":
+        L.get_contraction_permutations(tl, tr, lr, rr, T.ivec(cptrn), conj, d, l, r, C.byref(ncd), C.byref(nlu),
+                                       C.byref(nru), C.byref(nhu), C.byref(ierr))
+    else:
+        L.get_contr_permutations(tl, tr, lr, rr, T.ivec(cptrn), conj, d, l, r, C.byref(ncd), C.byref(nlu),
+                                 C.byref(nru), C.byref(ierr))
+    dr = sum(1 for x in cptrn if x > 0) - nhu.value
+    return ierr.value, list(d[1:1 + dr]), list(l[1:1 + lr]), list(r[1:1 + rr]), ncd.value, nlu.value, nru.value, nhu.value
+
+
+def test_permutation_solvers_match_oracle(built):
+    for p in _pattern_corpus():
+        e, dig, dr, lr, rr, cj = O.str2dig(p)
+        if e != 0:
+            continue
+        for conj in {0, cj, 2, 4, 1}:
+            for tl, tr in ((1, 0), (0, 0), (1, 1)):
+                a = _product_permutations("cpu", dig, lr, rr, conj, tl, tr)
+                b = O.permutations(dig, lr, rr, conj, "cpu", tl, tr)
+                assert a[0] == b[0] and (a[0] != 0 or a == b), (p, conj, a, b)
+                a = _product_permutations("gpu", dig, lr, rr, conj, tl, tr)
+                b = O.permutations(dig, lr, rr, conj, "gpu", tl, tr)
+                assert (a[0] != 0) == (b[0] != 0) and (a[0] != 0 or a == b), (p, conj, a, b)
+
+
+def test_device_id_codec_and_coherence(built):
+    L = T.lib()
+    k = C.c_int()
+    assert L.encode_device_id(T.DEV_HOST, 0) == 0
+    assert L.encode_device_id(T.DEV_NVIDIA_GPU, 3) == 4
+    assert L.decode_device_id(4, C.byref(k)) == 3 and k.value == T.DEV_NVIDIA_GPU
+    assert L.decode_device_id(0, C.byref(k)) == 0 and k.value == T.DEV_HOST
+    assert L.talshFlatDevId(T.DEV_NVIDIA_GPU, 8) == 25  # DEV_MAX: out of range
+    assert T.COPY_MTT == 26 and T.COPY_TT == 10
+    for coh in range(64):
+        vals = [L.argument_coherence_get_value(coh, 3, i) for i in range(3)]
+        assert vals == [(coh >> 4) & 3, (coh >> 2) & 3, coh & 3]
+        c = C.c_uint(0)
+        for i, v in enumerate(vals):
+            assert L.argument_coherence_set_value(C.byref(c), 3, i, v) == 0
+        assert c.value == coh
+
+
+def test_host_runtime_without_gpu(built):
+    """Host-side object logic with no GPU in the session: construction, queries,
+    Host 1-norm, and every compute request refused (no CPU compute path)."""
+    L = T.lib()
+    hb, ha = C.c_size_t(0), C.c_int(0)
+    assert L.talshInit(C.byref(hb), C.byref(ha), 0, None, 0, None, 0, None) == 0
+    try:
+        assert L.talshInit(C.byref(hb), C.byref(ha), 0, None, 0, None, 0, None) == T.TALSH_ALREADY_INITIALIZED
+        d = T.Tensor([3, 4, 5], T.R8, dev_id=0, init=0.5)
+        assert d.volume() == 60 and L.talshTensorRank(d.ref) == 3
+        assert np.all(d.host_array() == 0.5)
+        assert L.talshTensorImageNorm1_cpu(d.ref) == pytest.approx(30.0)
+        ext = np.asfortranarray(np.arange(12, dtype=np.complex128).reshape(3, 4, order="F") * (1 - 1j))
+        c = T.Tensor([3, 4], T.C8, dev_id=0, ext=ext)
+        assert L.talshTensorImageNorm1_cpu(c.ref) == pytest.approx(np.abs(ext).sum())
+        body = C.c_void_p()
+        assert L.talshTensorGetBodyAccess(c.ref, C.byref(body), T.C8, 0, T.DEV_HOST) == 0
+        assert body.value == ext.ctypes.data
+        n, copies, kinds = C.c_int(), (C.c_int * 16)(), (C.c_int * 16)()
+        assert L.talshTensorPresence(c.ref, C.byref(n), copies, kinds, T.DEV_NULL, -1) == 0
+        assert n.value == 1 and copies[0] == 0 and kinds[0] == T.C8
+        l = T.Tensor([5, 3, 4], T.R8, dev_id=0, init=1.0)
+        assert L.talshTensorAdd(b"D(a,b,c)+=L(c,a,b)", d.ref, l.ref, 1.0, 0.0, 0, T.DEV_HOST, T.COPY_MT, None) == T.TALSH_NOT_AVAILABLE
+        assert L.talshTensorAdd(b"D(a,b,c)+=L(c,a,b)", d.ref, l.ref, 1.0, 0.0, -1, -1, T.COPY_MT, None) == T.TALSH_NOT_AVAILABLE
+        assert L.talshTensorAdd(b"D(a,b,c)+=L(c,a,b", d.ref, l.ref, 1.0, 0.0, -1, -1, T.COPY_MT, None) == T.TALSH_INVALID_ARGS
+        assert L.talshTensorNorm1(d.ref, -1, -1) == -1.0
+        assert L.talshTensorContract(b"D(a,b,c)+=L(c,a,b)*R()", d.ref, l.ref, l.ref, 1.0, 0.0, 0, T.DEV_HOST,
+                                     T.COPY_MTT, T.YEP, None) == T.TALSH_INVALID_ARGS  # rank mismatch of R
+        sc = T.Tensor([], T.R8, dev_id=0, init=2.5)
+        re_, im_ = C.c_double(), C.c_double()
+        assert L.talshTensorGetScalar(sc.ref, C.byref(re_), C.byref(im_)) == 0 and re_.value == 2.5
+        task = T.Task()
+        assert L.talshTaskClean(C.byref(task)) == 0 and L.talshTaskIsEmpty(C.byref(task)) == T.YEP
+        assert L.talshTaskStatus(C.byref(task)) == T.TALSH_TASK_EMPTY
+        for t in (d, c, l, sc):
+            assert t.destruct() == 0
+        assert L.talshTensorIsEmpty(d.ref) == T.YEP
+    finally:
+        assert L.talshShutdown() == 0
+    assert L.talshShutdown() == T.TALSH_NOT_INITIALIZED
