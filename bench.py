@@ -326,7 +326,7 @@ def main():
     graph = None
     try:
         g = torch.cuda.CUDAGraph()
-        with torch.cuda.graph(g, stream=stream):
+        with torch.cuda.graph(g):  # captured on torch's side stream, replayed on the current one
             run_sweep()
         graph = g
         graph.replay()
@@ -468,6 +468,21 @@ def bench_contractions(T, L, torch, dev):
     assert rc in (0, T.TALSH_ALREADY_INITIALIZED)
     gpu = 1 + (dev.index or 0)
     out = {}
+    # FP64 denominator measured here: cuBLAS DGEMM (torch.matmul, float64) at 8192^3.
+    a = torch.randn(8192, 8192, dtype=torch.float64, device=dev)
+    b = torch.randn(8192, 8192, dtype=torch.float64, device=dev)
+    torch.matmul(a, b)
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(3):
+        torch.matmul(a, b)
+    e1.record()
+    torch.cuda.synchronize(dev)
+    dgemm_tflops = 3 * 2.0 * 8192 ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e12
+    out["fp64_peak"] = {"tflops": dgemm_tflops, "source": "measured: cuBLAS DGEMM 8192^3 (torch.matmul float64)",
+                        "nominal_tflops": 40.0}
+    del a, b
     specs = [("C1", "D(a,b,i,j)+=L(a,k,c,i)*R(c,b,k,j)", [32] * 4, [32] * 4, [32] * 4, 20),
              ("C3b", "D(a,b,i,j)+=L(a,k,c,i)*R(c,b,k,j)", [192, 192, 64, 64], [192, 64, 192, 64],
               [192, 192, 64, 64], 3),
@@ -524,7 +539,8 @@ def bench_contractions(T, L, torch, dev):
         ref = torch.einsum(spec, lv, rv)
         got = views[0].view(*reversed(dd))
         err = float(torch.linalg.norm(got - ref) / torch.linalg.norm(ref))
-        out[name] = {"pattern": pat, "tflops": flops / dt / 1e12, "ms": dt * 1e3, "flop": flops,
+        out[name] = {"pattern": pat, "tflops": flops / dt / 1e12, "frac_of_dgemm": flops / dt / 1e12 / dgemm_tflops,
+                     "ms": dt * 1e3, "flop": flops,
                      "rel_err_vs_fp64": err, "dtype": "f64", "path": "talshTensorContract, GPU-resident"}
         for t in tens:
             L.talshTensorDestruct(C.byref(t))

@@ -42,7 +42,12 @@ def copy_ctrl(*codes):
     return v
 
 
-COPY_MT, COPY_TT, COPY_MTT, COPY_TTT = copy_ctrl("M", "T"), copy_ctrl("T", "T"), copy_ctrl("M", "T", "T"), copy_ctrl("T", "T", "T")
+for _a in "DMTK":
+    for _b in "DMTK":
+        globals()["COPY_" + _a + _b] = copy_ctrl(_a, _b)
+        for _c in "DMTK":
+            globals()["COPY_" + _a + _b + _c] = copy_ctrl(_a, _b, _c)
+del _a, _b, _c
 
 NP_DTYPE = {R4: np.float32, R8: np.float64, C4: np.complex64, C8: np.complex128}
 KIND_OF = {np.dtype(np.float32): R4, np.dtype(np.float64): R8,

@@ -25,6 +25,7 @@
 
 #include <algorithm>
 #include <climits>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <unordered_map>
@@ -36,10 +37,23 @@ namespace tb {
 namespace {
 
 constexpr int kThreads = 256;
-constexpr int kMaxFR = 40;       // max fused rank (every fused extent is >= 2)
-constexpr int kTileBytes = 32768;  // shared tile budget (bytes of elements)
-constexpr int kMaxLo = 2048;     // output run length bound (ySm table)
-constexpr int kMaxRuns = 1024;   // run count bound (rIn / wOut tables)
+constexpr int kMinBlocks = 3;      // resident CTAs per SM the register budget is sized for
+constexpr int kMaxFR = 40;         // max fused rank (every fused extent is >= 2)
+constexpr int kTileBytes = 32768;  // bytes of one tile buffer (two buffers per CTA)
+constexpr int kMaxTabLo = 4096;    // output run length when B needs a table (more than 3 dims)
+constexpr int kMaxRuns = 1024;     // run count bound (run tables live in shared memory)
+constexpr int kChunk = 256;        // elements (vectors on the write side) per warp chunk
+
+// Mixed-radix decomposition of an index over up to 3 tile dimensions with
+// precomputed magic divisors; groups of more dimensions use shared tables.
+struct GroupMap {
+  int n;              // dimensions (0..3), or -1: use the shared table
+  int32_t ext[3];     // tile extents
+  uint32_t mg[2], sh[2];
+  int64_t gstr[3];    // global strides (input for read runs, output for write runs)
+  int32_t sstr[3];    // shared-memory strides
+  int mask;           // which coordinate is the partially covered split dimension (-1: none)
+};
 
 struct PermParams {
   int rank;
@@ -47,9 +61,15 @@ struct PermParams {
   uint32_t mg_li, sh_li, mg_lo, sh_lo;
   int a_last, b_last, a_pre, b_pre;
   int a_in_B, b_in_A;
+  int y_step;         // 1: the VOUT elements y..y+VOUT-1 share all but the first B coordinate
+  int nch_r, nch_w;   // warp chunks per input run (kChunk elements) / output run (kChunk*VOUT)
+  uint32_t mg_cr, sh_cr, mg_cw, sh_cw;
+  int ytab;           // 1: output-run positions come from the shared table ySm
+  GroupMap rmap, wmap, ymap;
   int nra, nwb, nb;
   int conj;
-  int off_rin, off_rc, off_wout, off_wsm, off_wc, off_ysm;
+  int off_rin, off_rc, off_wout, off_wsm, off_wc, off_ysm, off_tab_end;
+  int buf_elems;      // elements per tile buffer (whole 128-byte rows)
   int64_t num_tiles;
   double s_re, s_im;
   const void *sdev;  // optional device scalar multiplying the scale (rank-0 operand)
@@ -79,6 +99,45 @@ void make_magic(uint32_t d, uint32_t &mg, uint32_t &sh) {
 }
 __device__ __forceinline__ uint32_t fast_div(uint32_t n, uint32_t mg, uint32_t sh) {
   return (__umulhi(n, mg) + n) >> sh;
+}
+
+// Bank swizzle of a shared-memory element index: the position inside each
+// 128-byte row is XORed with a fold of the row number.  It is a bijection on
+// every row, keeps unit-stride accesses conflict-free and spreads power-of-two
+// strides (the output-run stride inside an input run) over all banks.
+template <typename T>
+__device__ __forceinline__ int swz(int idx) {
+  constexpr int SB = sizeof(T) == 4 ? 5 : (sizeof(T) == 8 ? 4 : 3);  // log2(elements per row)
+  const int row = idx >> SB;
+  return idx ^ ((row ^ (row >> SB)) & ((1 << SB) - 1));
+}
+
+struct Coords {
+  int64_t goff;
+  int32_t soff;
+  int32_t mask;
+};
+
+__device__ __forceinline__ Coords decompose(const GroupMap &g, uint32_t idx) {
+  Coords c{0, 0, 0};
+  if (g.n <= 0) return c;
+  if (g.n == 1) {
+    c.goff = (int64_t)idx * g.gstr[0];
+    c.soff = (int32_t)idx * g.sstr[0];
+    c.mask = (int32_t)idx;
+    return c;
+  }
+  const uint32_t q0 = fast_div(idx, g.mg[0], g.sh[0]);
+  const uint32_t c0 = idx - q0 * (uint32_t)g.ext[0];
+  uint32_t c1 = q0, c2 = 0;
+  if (g.n == 3) {
+    c2 = fast_div(q0, g.mg[1], g.sh[1]);
+    c1 = q0 - c2 * (uint32_t)g.ext[1];
+  }
+  c.goff = (int64_t)c0 * g.gstr[0] + (int64_t)c1 * g.gstr[1] + (int64_t)c2 * g.gstr[2];
+  c.soff = (int32_t)(c0 * g.sstr[0] + c1 * g.sstr[1] + c2 * g.sstr[2]);
+  c.mask = (int32_t)(g.mask == 0 ? c0 : (g.mask == 1 ? c1 : c2));
+  return c;
 }
 
 // ---- element arithmetic (explicit rounding, never contracted into FMA) ----
@@ -169,15 +228,53 @@ __device__ __forceinline__ void st_pack(T *p, const Pack<T, N> &v) {
   *reinterpret_cast<Pack<T, N> *>(p) = v;
 }
 
-__device__ void compute_setup(const PermParams &P, int64_t tile, TileSetup &S) {
+// Asynchronous global -> shared copy of one element (LDGSTS); the element size
+// is 4, 8 or 16 bytes and both addresses are element-aligned.
+template <int BYTES>
+__device__ __forceinline__ void cp_async_elem(void *smem_ptr, const void *gptr) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem_ptr);
+  if constexpr (BYTES == 16)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gptr));
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(s), "l"(gptr), "n"(BYTES));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cp_async_wait_1() { asm volatile("cp.async.wait_group 1;\n" ::); }
+
+// Tile coordinates of one CTA, advanced by gridDim.x tiles at a time with
+// mixed-radix carries (no divisions per tile).  Held by thread 0 in shared memory.
+struct TileCursor {
+  int32_t c[kMaxFR];
+  int32_t step[kMaxFR];
+};
+
+__device__ void cursor_init(const PermParams &P, TileCursor &cur, int64_t first, int64_t step) {
+  for (int i = 0; i < P.rank; ++i) {
+    const int64_t nt = P.ntile[i];
+    cur.c[i] = (int32_t)(first % nt);
+    first /= nt;
+    cur.step[i] = (int32_t)(step % nt);
+    step /= nt;
+  }
+}
+
+__device__ void cursor_advance(const PermParams &P, TileCursor &cur) {
+  int carry = 0;
+  for (int i = 0; i < P.rank; ++i) {
+    const int32_t nt = (int32_t)P.ntile[i];
+    int32_t v = cur.c[i] + cur.step[i] + carry;
+    carry = 0;
+    if (v >= nt) { v -= nt; carry = 1; }
+    cur.c[i] = v;
+  }
+}
+
+__device__ void make_setup(const PermParams &P, const TileCursor &cur, TileSetup &S) {
   int64_t in_base = 0, out_base = 0;
   int ta = P.tl[P.a_last], tb = P.tl[P.b_last];
   for (int i = 0; i < P.rank; ++i) {
-    const int64_t nt = P.ntile[i];
-    if (nt == 1) continue;
-    const int64_t c = tile % nt;
-    tile /= nt;
-    const int64_t start = c * P.tl[i];
+    if (P.ntile[i] == 1) continue;
+    const int64_t start = (int64_t)cur.c[i] * P.tl[i];
     in_base += start * P.istr[i];
     out_base += start * P.ostr[i];
     const int rem = (int)min((int64_t)P.tl[i], P.ext[i] - start);
@@ -192,21 +289,27 @@ __device__ void compute_setup(const PermParams &P, int64_t tile, TileSetup &S) {
   S.tb_lim = P.b_in_A ? INT_MAX : tb;
 }
 
-template <typename T, int VIN, int VOUT, int OP>
-__global__ void __launch_bounds__(kThreads) permute_tiled_kernel(const T *__restrict__ src,
-                                                                 T *dst, const PermParams P) {
+template <typename T, int VOUT, int OP>
+__global__ void __launch_bounds__(kThreads, kMinBlocks)
+    permute_tiled_kernel(const T *__restrict__ src, T *dst, const PermParams P) {
   extern __shared__ __align__(16) unsigned char smem[];
-  T *tile = reinterpret_cast<T *>(smem);
+  T *buf0 = reinterpret_cast<T *>(smem);
+  T *buf1 = buf0 + P.buf_elems;
   int64_t *rIn = reinterpret_cast<int64_t *>(smem + P.off_rin);
   int32_t *rC = reinterpret_cast<int32_t *>(smem + P.off_rc);
   int64_t *wOut = reinterpret_cast<int64_t *>(smem + P.off_wout);
   int32_t *wSm = reinterpret_cast<int32_t *>(smem + P.off_wsm);
   int32_t *wC = reinterpret_cast<int32_t *>(smem + P.off_wc);
   int32_t *ySm = reinterpret_cast<int32_t *>(smem + P.off_ysm);
-  __shared__ TileSetup setup[2];
+  __shared__ TileSetup setup[3];
+  __shared__ TileCursor cursor;
 
   const int tid = threadIdx.x;
-  // Run tables for the full tile shape (shared by all tiles of this CTA).
+  const int64_t G = gridDim.x;
+  // Per-CTA shared tables, valid for every tile of this plan: run offsets of
+  // the input runs (global offset + coordinate of the output split dimension)
+  // and of the output runs (global offset, shared offset, coordinate of the
+  // input split dimension), and the shared offset of every output-run position.
   for (int r = tid; r < P.Ri; r += kThreads) {
     int rem = r, cb = 0;
     int64_t off = 0;
@@ -218,7 +321,7 @@ __global__ void __launch_bounds__(kThreads) permute_tiled_kernel(const T *__rest
       if (d == P.b_last) cb = c;
     }
     rIn[r] = off;
-    rC[r] = cb;
+    rC[r] = P.b_in_A ? 0 : cb;
   }
   for (int r = tid; r < P.Ro; r += kThreads) {
     int rem = r, ca = 0, sm = 0;
@@ -233,109 +336,136 @@ __global__ void __launch_bounds__(kThreads) permute_tiled_kernel(const T *__rest
     }
     wOut[r] = off;
     wSm[r] = sm;
-    wC[r] = ca;
+    wC[r] = P.a_in_B ? 0 : ca;
   }
-  for (int y = tid; y < P.Lo; y += kThreads) {
-    int rem = y, sm = 0;
-    for (int k = 0; k < P.nb; ++k) {
-      const int d = P.b_dims[k];
-      const int c = rem % P.tl[d];
-      rem /= P.tl[d];
-      sm += c * P.smstr[d];
+  if (P.ytab) {
+    for (int y = tid; y < P.Lo; y += kThreads) {
+      int rem = y, sm = 0;
+      for (int k = 0; k < P.nb; ++k) {
+        const int d = P.b_dims[k];
+        const int c = rem % P.tl[d];
+        rem /= P.tl[d];
+        sm += c * P.smstr[d];
+      }
+      ySm[y] = sm;
     }
-    ySm[y] = sm;
   }
-  if (tid == 0 && blockIdx.x < P.num_tiles) compute_setup(P, blockIdx.x, setup[0]);
+  if (tid == 0 && blockIdx.x < P.num_tiles) {
+    cursor_init(P, cursor, blockIdx.x, G);
+    make_setup(P, cursor, setup[0]);
+    cursor_advance(P, cursor);
+    if (blockIdx.x + G < P.num_tiles) {
+      make_setup(P, cursor, setup[1]);
+      cursor_advance(P, cursor);
+    }
+  }
   __syncthreads();
 
-  constexpr int kTileElems = kTileBytes / (int)sizeof(T);
-  constexpr int KR = (kTileElems + kThreads * VIN - 1) / (kThreads * VIN);
-  constexpr int KW = (kTileElems + kThreads * VOUT - 1) / (kThreads * VOUT);
   const bool cj = P.conj != 0;
   double sr = P.s_re, si = P.s_im;
   effective_scale<T>(P.sdev, P.sdev_kind, P.sdev_conj, sr, si);
+  const int lane = tid & 31, warp = tid >> 5;
+  constexpr int kWarps = kThreads / 32;
 
-  int it = 0;
-  for (int64_t t = blockIdx.x; t < P.num_tiles; t += gridDim.x, ++it) {
-    const TileSetup S = setup[it & 1];
-    // ---- read phase: global (input runs) -> shared ----
-    {
-      Pack<T, VIN> v[KR];
-      int sidx[KR];
-#pragma unroll
-      for (int k = 0; k < KR; ++k) {
-        const int e = (tid + k * kThreads) * VIN;
-        sidx[k] = -1;
-        if (e < P.V) {
-          const int r = (int)fast_div((uint32_t)e, P.mg_li, P.sh_li);
-          const int x = e - r * P.Li;
-          if (x < S.li_act && rC[r] < S.tb_lim) {
-            v[k] = ld_pack<T, VIN>(src + (S.in_base + rIn[r] + x));
-            sidx[k] = x + r * P.Li_pad;
-          }
-        }
-      }
-#pragma unroll
-      for (int k = 0; k < KR; ++k) {
-        if (sidx[k] >= 0) {
-#pragma unroll
-          for (int j = 0; j < VIN; ++j) tile[sidx[k] + j] = v[k].v[j];
-        }
-      }
+  // Read phase: warps take chunks of input runs (chunk = up to 256 elements);
+  // one table lookup per chunk, then every lane streams elements 32 apart.
+  auto issue_loads = [&](const TileSetup &S, T *buf) {
+    const int nch = P.nch_r, total = P.Ri * nch;
+    for (int it = warp; it < total; it += kWarps) {
+      const int r = (int)fast_div((uint32_t)it, P.mg_cr, P.sh_cr);
+      const int x0 = (it - r * nch) * kChunk;
+      if (rC[r] >= S.tb_lim) continue;
+      const int xe = min(x0 + kChunk, S.li_act);
+      const T *g = src + (S.in_base + rIn[r]);
+      const int sb = r * P.Li;
+#pragma unroll 4
+      for (int x = x0 + lane; x < xe; x += 32) cp_async_elem<sizeof(T)>(buf + swz<T>(sb + x), g + x);
     }
+  };
+
+  int64_t t = blockIdx.x;
+  if (t < P.num_tiles) issue_loads(setup[0], buf0);
+  cp_async_commit();
+  for (int iter = 0; t < P.num_tiles; t += G, ++iter) {
+    const int64_t tn = t + G;
+    if (tn < P.num_tiles) issue_loads(setup[(iter + 1) % 3], (iter & 1) ? buf0 : buf1);
+    cp_async_commit();
+    if (tid == 0 && tn + G < P.num_tiles) {
+      make_setup(P, cursor, setup[(iter + 2) % 3]);
+      cursor_advance(P, cursor);
+    }
+    cp_async_wait_1();
     __syncthreads();
-    // ---- write phase: shared -> global (output runs) ----
-    {
-      Pack<T, VOUT> v[KW];
-      int64_t goff[KW];
+    // Write phase: warps take chunks of output runs; lanes move VOUT elements
+    // per step with one (vector) store.
+    const TileSetup S = setup[iter % 3];
+    const T *buf = (iter & 1) ? buf1 : buf0;
+    const int nch = P.nch_w, total = P.Ro * nch;
+    for (int it = warp; it < total; it += kWarps) {
+      const int r = (int)fast_div((uint32_t)it, P.mg_cw, P.sh_cw);
+      const int y0 = (it - r * nch) * (kChunk * VOUT);
+      if (wC[r] >= S.ta_lim) continue;
+      const int ye = min(y0 + kChunk * VOUT, S.lo_act);
+      T *g = dst + (S.out_base + wOut[r]);
+      const int ws = wSm[r];
+      constexpr int U = (OP == kOpAdd) ? 4 : 2;  // steps per batch (adds keep U loads of D in flight)
+      for (int yb = y0 + lane * VOUT; yb < ye; yb += 32 * VOUT * U) {
+        Pack<T, VOUT> v[U];
+        bool ok[U];
 #pragma unroll
-      for (int k = 0; k < KW; ++k) {
-        const int e = (tid + k * kThreads) * VOUT;
-        goff[k] = -1;
-        if (e < P.V) {
-          const int r = (int)fast_div((uint32_t)e, P.mg_lo, P.sh_lo);
-          const int y = e - r * P.Lo;
-          if (y < S.lo_act && wC[r] < S.ta_lim) {
-            const int base = wSm[r];
+        for (int u = 0; u < U; ++u) {
+          const int y = yb + u * 32 * VOUT;
+          ok[u] = y < ye;
+          if (!ok[u]) continue;
+          if (P.ytab) {
+            if (P.y_step) {
+              const int base = ws + ySm[y];
 #pragma unroll
-            for (int j = 0; j < VOUT; ++j) {
-              T x = tile[base + ySm[y + j]];
-              if (cj) x = Arith<T>::conj(x);
-              v[k].v[j] = x;
+              for (int j = 0; j < VOUT; ++j) v[u].v[j] = buf[swz<T>(base + j * P.ymap.sstr[0])];
+            } else {
+#pragma unroll
+              for (int j = 0; j < VOUT; ++j) v[u].v[j] = buf[swz<T>(ws + ySm[y + j])];
             }
-            goff[k] = S.out_base + wOut[r] + y;
+          } else {
+            if (P.y_step) {
+              const int base = ws + decompose(P.ymap, (uint32_t)y).soff;
+#pragma unroll
+              for (int j = 0; j < VOUT; ++j) v[u].v[j] = buf[swz<T>(base + j * P.ymap.sstr[0])];
+            } else {
+#pragma unroll
+              for (int j = 0; j < VOUT; ++j) v[u].v[j] = buf[swz<T>(ws + decompose(P.ymap, (uint32_t)(y + j)).soff)];
+            }
+          }
+          if (cj) {
+#pragma unroll
+            for (int j = 0; j < VOUT; ++j) v[u].v[j] = Arith<T>::conj(v[u].v[j]);
           }
         }
-      }
-      if constexpr (OP == kOpAdd) {
-        Pack<T, VOUT> d[KW];
+        if constexpr (OP == kOpAdd) {
+          Pack<T, VOUT> d[U];
 #pragma unroll
-        for (int k = 0; k < KW; ++k)
-          if (goff[k] >= 0) d[k] = ld_pack<T, VOUT>(dst + goff[k]);
+          for (int u = 0; u < U; ++u)
+            if (ok[u]) d[u] = ld_pack<T, VOUT>(g + yb + u * 32 * VOUT);
 #pragma unroll
-        for (int k = 0; k < KW; ++k) {
-          if (goff[k] >= 0) {
+          for (int u = 0; u < U; ++u) {
+            if (!ok[u]) continue;
 #pragma unroll
-            for (int j = 0; j < VOUT; ++j) d[k].v[j] = Arith<T>::axpy(d[k].v[j], v[k].v[j], sr, si);
-            st_pack<T, VOUT>(dst + goff[k], d[k]);
+            for (int j = 0; j < VOUT; ++j) d[u].v[j] = Arith<T>::axpy(d[u].v[j], v[u].v[j], sr, si);
+            st_pack<T, VOUT>(g + yb + u * 32 * VOUT, d[u]);
+          }
+        } else {
+#pragma unroll
+          for (int u = 0; u < U; ++u) {
+            if (!ok[u]) continue;
+            if constexpr (OP == kOpScaleCopy) {
+#pragma unroll
+              for (int j = 0; j < VOUT; ++j) v[u].v[j] = Arith<T>::mul(v[u].v[j], sr, si);
+            }
+            st_pack<T, VOUT>(g + yb + u * 32 * VOUT, v[u]);
           }
         }
-      } else if constexpr (OP == kOpScaleCopy) {
-#pragma unroll
-        for (int k = 0; k < KW; ++k) {
-          if (goff[k] >= 0) {
-#pragma unroll
-            for (int j = 0; j < VOUT; ++j) v[k].v[j] = Arith<T>::mul(v[k].v[j], sr, si);
-            st_pack<T, VOUT>(dst + goff[k], v[k]);
-          }
-        }
-      } else {
-#pragma unroll
-        for (int k = 0; k < KW; ++k)
-          if (goff[k] >= 0) st_pack<T, VOUT>(dst + goff[k], v[k]);
       }
     }
-    if (tid == 0 && t + gridDim.x < P.num_tiles) compute_setup(P, t + gridDim.x, setup[(it + 1) & 1]);
     __syncthreads();
   }
 }
@@ -427,6 +557,19 @@ int fuse_dims(int rank, const int *dims, const int *o2n, Fused &F) {
   return TALSH_SUCCESS;
 }
 
+// Tile buffer budget in bytes: kTileBytes, or TALSH_B200_TILE_BYTES (4096..49152) for tuning.
+int tile_bytes() {
+  static int v = 0;
+  if (v == 0) {
+    v = kTileBytes;
+    if (const char *e = std::getenv("TALSH_B200_TILE_BYTES")) {
+      const int t = std::atoi(e);
+      if (t >= 4096 && t <= 49152) v = t;
+    }
+  }
+  return v;
+}
+
 struct Plan {
   bool linear = false;
   int64_t vol = 0;
@@ -434,6 +577,17 @@ struct Plan {
   int vin = 1, vout = 1;
   size_t smem = 0;
 };
+
+// Next tile extent for a split dimension: about twice the current one, but
+// chosen so that the dimension divides into equal tiles (little masked work).
+int64_t balanced_grow(int64_t ext, int64_t cur) {
+  for (int64_t target = cur * 2; target < ext; target += cur) {
+    const int64_t pieces = (ext + target - 1) / target;
+    const int64_t t = (ext + pieces - 1) / pieces;
+    if (t > cur) return t;
+  }
+  return ext;
+}
 
 int build_plan(int esize, const Fused &F, Plan &plan) {
   plan.vol = F.vol;
@@ -449,7 +603,12 @@ int build_plan(int esize, const Fused &F, Plan &plan) {
   s = 1;
   for (int k = 0; k < n; ++k) { P.ostr[q[k]] = s; s *= P.ext[q[k]]; }
 
-  const int elems_max = kTileBytes / esize;
+  // Small tensors get smaller tiles so that every SM still holds a few of them.
+  int elems_max = tile_bytes() / esize;
+  {
+    const int64_t slots = 148LL * kMinBlocks * 2;
+    while (elems_max > 1024 && F.vol / elems_max < slots) elems_max /= 2;
+  }
   const int run_min = esize >= 16 ? 16 : 32;
   // Initial groups: shortest prefixes reaching run_min elements.
   int na = 0, nb = 0;
@@ -489,8 +648,28 @@ int build_plan(int esize, const Fused &F, Plan &plan) {
     G.Lo = 1;
     for (int k = 0; k < nb_; ++k) G.Lo *= G.tl[q[k]];
   };
+  // Groups of more than three tile dimensions fall back to shared tables,
+  // which bound their length; everything else only has the tile budget.
+  auto group_dims = [&](const Geo &G, int na_, int nb_, int &nra, int &nwb) {
+    bool inA[kMaxFR] = {false}, inB[kMaxFR] = {false};
+    for (int i = 0; i < na_; ++i) inA[i] = true;
+    for (int k = 0; k < nb_; ++k) inB[q[k]] = true;
+    nra = nwb = 0;
+    for (int i = 0; i < n; ++i) {
+      if (G.tl[i] <= 1) continue;
+      if (!inA[i]) ++nra;
+      if (!inB[i]) ++nwb;
+    }
+  };
+  int cur_na = na, cur_nb = nb;
   auto acceptable = [&](const Geo &G) {
-    return G.V <= elems_max && G.Lo <= kMaxLo && G.V / G.Li <= kMaxRuns && G.V / G.Lo <= kMaxRuns;
+    if (G.V > elems_max) return false;
+    int nra, nwb;
+    group_dims(G, cur_na, cur_nb, nra, nwb);
+    (void)nra; (void)nwb;
+    if (cur_nb > 3 && G.Lo > kMaxTabLo) return false;  // B positions need the table
+    if (G.V / G.Li > kMaxRuns || G.V / G.Lo > kMaxRuns) return false;
+    return true;
   };
   Geo G;
   geometry(na, tA, nb, tB, G);
@@ -513,7 +692,7 @@ int build_plan(int esize, const Fused &F, Plan &plan) {
       if (growA) {
         const int al = na - 1;
         if (G.tl[al] < P.ext[al]) {
-          tA2 = std::min<int64_t>(P.ext[al], G.tl[al] * 2);
+          tA2 = balanced_grow(P.ext[al], G.tl[al]);
         } else if (na < n) {
           na2 = na + 1;
           tA2 = std::min<int64_t>(P.ext[na2 - 1], std::max<int64_t>(2, G.tl[na2 - 1]));
@@ -523,7 +702,7 @@ int build_plan(int esize, const Fused &F, Plan &plan) {
       } else {
         const int bl = q[nb - 1];
         if (G.tl[bl] < P.ext[bl]) {
-          tB2 = std::min<int64_t>(P.ext[bl], G.tl[bl] * 2);
+          tB2 = balanced_grow(P.ext[bl], G.tl[bl]);
         } else if (nb < n) {
           nb2 = nb + 1;
           tB2 = std::min<int64_t>(P.ext[q[nb2 - 1]], std::max<int64_t>(2, G.tl[q[nb2 - 1]]));
@@ -533,8 +712,12 @@ int build_plan(int esize, const Fused &F, Plan &plan) {
       }
       Geo G2;
       geometry(na2, tA2, nb2, tB2, G2);
-      if (acceptable(G2)) {
+      cur_na = na2; cur_nb = nb2;
+      const bool ok = acceptable(G2);
+      cur_na = na; cur_nb = nb;
+      if (ok) {
         na = na2; nb = nb2; tA = tA2; tB = tB2; G = G2;
+        cur_na = na; cur_nb = nb;
         done = true;
       }
     }
@@ -562,7 +745,7 @@ int build_plan(int esize, const Fused &F, Plan &plan) {
   P.a_in_B = inB[P.a_last] ? 1 : 0;
   P.b_in_A = inA[P.b_last] ? 1 : 0;
   // shared layout: x over A (input order) contiguous, runs over U\A with pitch Li_pad
-  P.Li_pad = (P.Li % 2 == 0) ? P.Li + 1 : P.Li;
+  P.Li_pad = P.Li;  // no padding: shared indices are bank-swizzled instead
   {
     int32_t st = 1;
     for (int i = 0; i < na; ++i) { P.smstr[i] = st; st *= P.tl[i]; }
@@ -582,38 +765,57 @@ int build_plan(int esize, const Fused &F, Plan &plan) {
   }
   make_magic((uint32_t)P.Li, P.mg_li, P.sh_li);
   make_magic((uint32_t)P.Lo, P.mg_lo, P.sh_lo);
-  // Vector widths: every run start, run length and partial run length must be
-  // a multiple of the vector (16 bytes) on that side.
+  P.nch_r = (P.Li + kChunk - 1) / kChunk;
+  make_magic((uint32_t)P.nch_r, P.mg_cr, P.sh_cr);
+  // Group maps: read runs over U\A (input strides), write runs over U\B
+  // (output strides), output-run positions over B (shared strides only).
+  auto fill_map = [&](GroupMap &g, const int8_t *dims, int nd, bool output_side, int mask_dim) {
+    std::memset(&g, 0, sizeof(g));
+    g.mask = -1;
+    if (nd > 3) { g.n = -1; return; }
+    g.n = nd;
+    for (int k = 0; k < nd; ++k) {
+      const int d = dims[k];
+      g.ext[k] = P.tl[d];
+      g.gstr[k] = output_side ? P.ostr[d] : P.istr[d];
+      g.sstr[k] = P.smstr[d];
+      if (d == mask_dim) g.mask = k;
+    }
+    for (int k = 0; k < 2 && k < nd; ++k) make_magic((uint32_t)g.ext[k], g.mg[k], g.sh[k]);
+  };
+  fill_map(P.rmap, P.ra_dims, P.nra, false, P.b_in_A ? -1 : P.b_last);
+  fill_map(P.wmap, P.wb_dims, P.nwb, true, P.a_in_B ? -1 : P.a_last);
+  fill_map(P.ymap, P.b_dims, P.nb, false, -1);
+  // Output vector width: every output run start, run length and partial run
+  // length must be a multiple of 16 bytes.  Reads are element-granular
+  // asynchronous copies and need no alignment beyond the element.
   const int vec = 16 / esize;
-  plan.vin = plan.vout = 1;
+  plan.vin = 1;
+  plan.vout = 1;
   if (vec > 1) {
-    auto side_ok = [&](bool in_side) {
-      const int L = in_side ? P.Li : P.Lo;
-      if (L % vec) return false;
-      const int last = in_side ? P.a_last : P.b_last;
-      const int pre = in_side ? P.a_pre : P.b_pre;
-      const int64_t partial = P.ext[last] % P.tl[last];
-      if (partial && ((int64_t)pre * partial) % vec) return false;
-      for (int i = 0; i < n; ++i) {
-        const int64_t st = in_side ? P.istr[i] : P.ostr[i];
-        const bool in_group = in_side ? inA[i] : inB[i];
-        if (!in_group && P.tl[i] > 1 && st % vec) return false;      // run offsets
-        if (P.ntile[i] > 1 && (P.tl[i] * st) % vec) return false;    // tile bases
-      }
-      return true;
-    };
-    if (side_ok(true)) plan.vin = vec;
-    if (side_ok(false)) plan.vout = vec;
+    bool ok = (P.Lo % vec) == 0;
+    const int64_t partial = P.ext[P.b_last] % P.tl[P.b_last];
+    if (partial && ((int64_t)P.b_pre * partial) % vec) ok = false;
+    for (int i = 0; i < n && ok; ++i) {
+      if (!inB[i] && P.tl[i] > 1 && P.ostr[i] % vec) ok = false;       // run offsets
+      if (P.ntile[i] > 1 && (P.tl[i] * P.ostr[i]) % vec) ok = false;   // tile bases
+    }
+    if (ok) plan.vout = vec;
   }
-  // Shared memory carve-up.
-  size_t off = (size_t)P.Ri * P.Li_pad * esize;
+  // Shared memory: two tile buffers, then the tables that are in use.
+  // each buffer is rounded up to whole 128-byte rows: the swizzle permutes within rows
+  const size_t buf_elems = (((size_t)P.Ri * P.Li_pad * esize + 127) / 128) * 128 / esize;
+  P.buf_elems = (int)buf_elems;
+  size_t off = 2 * buf_elems * esize;
   off = (off + 15) & ~size_t(15);
+  P.ytab = (P.Lo <= kMaxTabLo || P.ymap.n < 0) ? 1 : 0;
   P.off_rin = (int)off; off += (size_t)P.Ri * 8;
   P.off_wout = (int)off; off += (size_t)P.Ro * 8;
   P.off_rc = (int)off; off += (size_t)P.Ri * 4;
   P.off_wsm = (int)off; off += (size_t)P.Ro * 4;
   P.off_wc = (int)off; off += (size_t)P.Ro * 4;
-  P.off_ysm = (int)off; off += (size_t)P.Lo * 4;
+  P.off_ysm = (int)off; if (P.ytab) off += (size_t)P.Lo * 4;
+  P.off_tab_end = (int)off;
   plan.smem = off;
   return TALSH_SUCCESS;
 }
@@ -629,18 +831,34 @@ int sm_count(int dev) {
   return cache[dev];
 }
 
+// Resident CTAs per SM for a kernel with `smem` dynamic bytes.  The kernel's
+// dynamic shared-memory limit is raised once to the device maximum, so plans of
+// any size can share the same kernel function.
 int blocks_per_sm(const void *fn, size_t smem) {
   static std::mutex mu;
   static std::unordered_map<uint64_t, int> cache;
-  const uint64_t key = (uint64_t)(uintptr_t)fn ^ ((uint64_t)smem << 48);
+  static std::unordered_map<const void *, bool> raised;
   std::lock_guard<std::mutex> lk(mu);
+  if (!raised[fn]) {
+    int dev = 0, optin = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) optin = 0;
+    cudaFuncAttributes fa;
+    const int static_bytes = (cudaFuncGetAttributes(&fa, fn) == cudaSuccess) ? (int)fa.sharedSizeBytes : 1024;
+    if (optin - static_bytes > 48 * 1024)
+      cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - static_bytes);
+    cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    cudaGetLastError();
+    raised[fn] = true;
+  }
+  const uint64_t key = (uint64_t)(uintptr_t)fn ^ ((uint64_t)smem << 44);
   auto it = cache.find(key);
   if (it != cache.end()) return it->second;
   int nb = 0;
-  if (smem > 48 * 1024)
-    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, kThreads, smem) != cudaSuccess || nb < 1)
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, kThreads, smem) != cudaSuccess || nb < 1) {
+    cudaGetLastError();
     nb = 1;
+  }
   cache[key] = nb;
   return nb;
 }
@@ -680,9 +898,11 @@ int launch_typed(const Plan &plan, const void *src, void *dst, int conj, const S
   P.sdev_kind = sc.sdev_kind;
   P.sdev_conj = sc.sdev_conj;
   constexpr int VEC = 16 / sizeof(T);
-  const bool src_al = ((uintptr_t)src % 16) == 0, dst_al = ((uintptr_t)dst % 16) == 0;
-  const int vin = (plan.vin > 1 && src_al) ? VEC : 1;
+  const bool dst_al = ((uintptr_t)dst % 16) == 0;
   const int vout = (plan.vout > 1 && dst_al) ? VEC : 1;
+  P.y_step = (P.ymap.n >= 1 && P.ymap.ext[0] % vout == 0) ? 1 : 0;
+  P.nch_w = (P.Lo + kChunk * vout - 1) / (kChunk * vout);
+  make_magic((uint32_t)P.nch_w, P.mg_cw, P.sh_cw);
   auto run = [&](auto kern) {
     const void *fn = (const void *)kern;
     const int bps = blocks_per_sm(fn, plan.smem);
@@ -690,12 +910,10 @@ int launch_typed(const Plan &plan, const void *src, void *dst, int conj, const S
     kern<<<grid, kThreads, plan.smem, st>>>((const T *)src, (T *)dst, P);
   };
   if constexpr (VEC > 1) {
-    if (vin > 1 && vout > 1) run(permute_tiled_kernel<T, VEC, VEC, OP>);
-    else if (vin > 1) run(permute_tiled_kernel<T, VEC, 1, OP>);
-    else if (vout > 1) run(permute_tiled_kernel<T, 1, VEC, OP>);
-    else run(permute_tiled_kernel<T, 1, 1, OP>);
+    if (vout > 1) run(permute_tiled_kernel<T, VEC, OP>);
+    else run(permute_tiled_kernel<T, 1, OP>);
   } else {
-    run(permute_tiled_kernel<T, 1, 1, OP>);
+    run(permute_tiled_kernel<T, 1, OP>);
   }
   note_launch();
   return check_launch("permute_tiled_kernel");

@@ -106,8 +106,8 @@ def test_plan_properties(talsh):
     L = T.lib()
     info = (C.c_int * 12)()
     assert L.tcPermutePlanInfo(T.R8, 4, T.ivec([32, 32, 32, 32]), T.ivec([3, 4, 2, 1]), info) == 0
-    assert info[0] == 4 and info[1] == 0 and info[3] >= 32 and info[4] >= 32  # coalesced runs
-    assert info[7] == 2 and info[8] == 2  # 16-byte vectors on both sides
+    assert info[0] == 3 and info[1] == 0 and info[3] >= 32 and info[4] >= 32  # (a,b) fuse; coalesced runs
+    assert info[8] == 2  # 16-byte vector stores on the output side
     assert L.tcPermutePlanInfo(T.R8, 3, T.ivec([4, 5, 6]), T.ivec([1, 2, 3]), info) == 0
     assert info[1] == 1  # identity fuses to a straight copy
 

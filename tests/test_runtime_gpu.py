@@ -113,7 +113,9 @@ def test_init_scale_norm(talsh, kind):
     assert same_bits(Z, ref)
     x = host_tensor(X)
     n1 = L.talshTensorNorm1(x.ref, 0, T.DEV_NVIDIA_GPU)
-    assert abs(n1 - O.norm1(X)) <= 1e-12 * O.norm1(X)
+    # moduli of C4 elements are single precision (last-ulp differences between libm and CUDA)
+    tol = 1e-6 if kind == T.C4 else 1e-12
+    assert abs(n1 - O.norm1(X)) <= tol * O.norm1(X)
     assert L.talshTensorNorm1(x.ref, 0, T.DEV_NVIDIA_GPU) == n1  # deterministic
     assert [img[0] for img in x.images()] == [0]  # the staged copy was temporary
     x.destruct()
