@@ -73,6 +73,29 @@ int tcTensorContract(int data_kind, const int *cptrn, int drank, const int *ddim
                      const void *R, double alpha_re, double alpha_im, int conj_bits,
                      int accumulative, void *scratch, size_t scratch_bytes, void *stream);
 
+/* Size of the fixed scratch array behind tcTensorContractNoAlloc: 8 MiB per GPU. */
+#define TC_CONTRACT_NOALLOC_SCRATCH_BYTES ((size_t)8 << 20)
+
+/* tcTensorContract without caller scratch and without any allocation, for
+ * callers that cannot allocate device memory (code running inside an
+ * allocator or memory-pool callback, a host whose device budget belongs to
+ * another runtime, a loop where the implicit synchronisation of cudaMalloc is
+ * not allowed).  Same arguments and results as tcTensorContract minus the
+ * scratch pair.  Its scratch is one array of TC_CONTRACT_NOALLOC_SCRATCH_BYTES
+ * compiled into the library, held on every GPU that loads the library until
+ * exit.  Shapes whose tcTensorContractScratch(...) exceeds that size are
+ * rejected with TALSH_LIMIT_EXCEEDED (tcLastErrorString says why).  The first
+ * call on a device looks up the array's device address, so make that first
+ * call before any stream capture.  All calls share the one array: calls that
+ * may overlap on the GPU (other streams, other host threads) race and must be
+ * serialised by the caller.  No counterpart in the reference. */
+int tcTensorContractNoAlloc(int data_kind, const int *cptrn, int drank, const int *ddims,
+                            int lrank, const int *ldims, int rrank, const int *rdims, void *D,
+                            const void *L, const void *R, double alpha_re, double alpha_im,
+                            int conj_bits, int accumulative, void *stream);
+/* TC_CONTRACT_NOALLOC_SCRATCH_BYTES as compiled into the loaded library. */
+size_t tcTensorContractNoAllocMaxScratch(void);
+
 /* Host view of the transpose tile plan (diagnostics): info[0] fused rank,
  * [1] identity flag, [2] tile volume, [3] input run, [4] output run,
  * [5] input runs, [6] output runs, [7] input vector width, [8] output vector

@@ -145,6 +145,9 @@ _PROTOS = {
     "tcTensorContractScratch": (_Z, [_I, _P(_I), _I, _P(_I), _I, _P(_I), _I, _P(_I)]),
     "tcTensorContract": (_I, [_I, _P(_I), _I, _P(_I), _I, _P(_I), _I, _P(_I), _V, _V, _V, _D, _D,
                               _I, _I, _V, _Z, _V]),
+    "tcTensorContractNoAlloc": (_I, [_I, _P(_I), _I, _P(_I), _I, _P(_I), _I, _P(_I), _V, _V, _V, _D,
+                                     _D, _I, _I, _V]),
+    "tcTensorContractNoAllocMaxScratch": (_Z, []),
     "tcPermutePlanInfo": (_I, [_I, _I, _P(_I), _P(_I), _P(_I)]),
     "tcKernelLaunchCount": (C.c_ulonglong, []),
     "tcLastErrorString": (_S, []),

@@ -29,6 +29,7 @@ double cmplx8_to_real8(double re, double im);
 // Bookkeeping shared by the CUDA translation units.
 void note_launch(unsigned n = 1);
 void note_cuda_error(const char *what, int code);
+void note_error_text(const char *msg);  // sets the text tcLastErrorString returns
 int check_launch(const char *what);  // 0 or TALSH_FAILURE after a kernel launch
 
 }  // namespace tb

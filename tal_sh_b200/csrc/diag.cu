@@ -23,6 +23,11 @@ void note_cuda_error(const char *what, int code) {
                 cudaGetErrorString((cudaError_t)code), code);
 }
 
+void note_error_text(const char *msg) {
+  std::lock_guard<std::mutex> lk(g_err_mu);
+  std::snprintf(g_last_err, sizeof(g_last_err), "%s", msg);
+}
+
 int check_launch(const char *what) {
   const cudaError_t e = cudaGetLastError();
   if (e == cudaSuccess) return TALSH_SUCCESS;
