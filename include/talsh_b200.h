@@ -99,7 +99,7 @@ size_t tcTensorContractNoAllocMaxScratch(void);
 /* Host view of the transpose tile plan (diagnostics): info[0] fused rank,
  * [1] identity flag, [2] tile volume, [3] input run, [4] output run,
  * [5] input runs, [6] output runs, [7] input vector width, [8] output vector
- * width, [9] shared bytes, [10] tile count. */
+ * width, [9] shared bytes, [10] tile count, [11] per-element tables in use. */
 int tcPermutePlanInfo(int data_kind, int rank, const int *dims_in, const int *o2n, int *info);
 
 /* Number of kernels this library launched since load (diagnostics). */

@@ -28,6 +28,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
+#include <type_traits>
 #include <unordered_map>
 #include <vector>
 
@@ -42,7 +43,7 @@ constexpr int kMaxFR = 40;         // max fused rank (every fused extent is >= 2
 constexpr int kTileBytes = 32768;  // bytes of one tile buffer (two buffers per CTA)
 constexpr int kMaxTabLo = 4096;    // output run length when B needs a table (more than 3 dims)
 constexpr int kMaxRuns = 1024;     // run count bound (run tables live in shared memory)
-constexpr int kChunk = 256;        // elements (vectors on the write side) per warp chunk
+constexpr int kStages = 3;              // tile buffers per CTA: loads run kStages - 1 tiles ahead
 
 // Mixed-radix decomposition of an index over up to 3 tile dimensions with
 // precomputed magic divisors; groups of more dimensions use shared tables.
@@ -62,13 +63,17 @@ struct PermParams {
   int a_last, b_last, a_pre, b_pre;
   int a_in_B, b_in_A;
   int y_step;         // 1: the VOUT elements y..y+VOUT-1 share all but the first B coordinate
-  int nch_r, nch_w;   // warp chunks per input run (kChunk elements) / output run (kChunk*VOUT)
-  uint32_t mg_cr, sh_cr, mg_cw, sh_cw;
+  int swz;            // 1: shared indices are bank-swizzled (Li_pad == Li), 0: rows padded to Li_pad
+  int nv;             // vectors (VOUT elements) per output run
+  uint32_t mg_nv, sh_nv;
   int ytab;           // 1: output-run positions come from the shared table ySm
   GroupMap rmap, wmap, ymap;
   int nra, nwb, nb;
   int conj;
   int off_rin, off_rc, off_wout, off_wsm, off_wc, off_ysm, off_tab_end;
+  int reg;            // 1: permute_reg_kernel (per-thread register tables)
+  int ta_rem, tb_rem; // extents of the last (cut-short) tile along a_last / b_last
+  int pre_bA, pre_aB; // tile volume of A below b_last (b_last in A) / of B before a_last (a_last in B)
   int buf_elems;      // elements per tile buffer (whole 128-byte rows)
   int64_t num_tiles;
   double s_re, s_im;
@@ -78,6 +83,8 @@ struct PermParams {
   int64_t istr[kMaxFR];
   int64_t ostr[kMaxFR];
   int64_t ntile[kMaxFR];
+  uint32_t mg_ts[kMaxFR], sh_ts[kMaxFR];  // magic divisors of the tile-index stride of each dimension
+  uint32_t mg_nt[kMaxFR], sh_nt[kMaxFR];  // and of its tile count
   int32_t tl[kMaxFR];
   int32_t smstr[kMaxFR];
   int8_t ra_dims[kMaxFR];
@@ -88,6 +95,8 @@ struct PermParams {
 struct TileSetup {
   int64_t in_base, out_base;
   int li_act, lo_act, ta_lim, tb_lim;
+  int full;  // 1: no split dimension is cut short in this tile (no masking needed)
+  int type;  // bit 0: a_last cut short, bit 1: b_last cut short
 };
 
 // Fast unsigned division for n < 2^31 (Granlund-Montgomery round-up method).
@@ -238,46 +247,39 @@ __device__ __forceinline__ void cp_async_elem(void *smem_ptr, const void *gptr) 
   else
     asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(s), "l"(gptr), "n"(BYTES));
 }
+template <int BYTES>
+__device__ __forceinline__ void cp_async_s(uint32_t s, const void *gptr) {
+  if constexpr (BYTES == 16)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gptr));
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(s), "l"(gptr), "n"(BYTES));
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
-__device__ __forceinline__ void cp_async_wait_1() { asm volatile("cp.async.wait_group 1;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
 
-// Tile coordinates of one CTA, advanced by gridDim.x tiles at a time with
-// mixed-radix carries (no divisions per tile).  Held by thread 0 in shared memory.
-struct TileCursor {
-  int32_t c[kMaxFR];
-  int32_t step[kMaxFR];
+// Per-dimension tiling data, copied to shared memory so that the lanes of a
+// warp read different dimensions without serialising on the constant cache.
+struct DimS {
+  int64_t istr, ostr, ext;
+  int32_t tl, nt;
+  uint32_t mg_ts, sh_ts, mg_nt, sh_nt;
 };
 
-__device__ void cursor_init(const PermParams &P, TileCursor &cur, int64_t first, int64_t step) {
-  for (int i = 0; i < P.rank; ++i) {
-    const int64_t nt = P.ntile[i];
-    cur.c[i] = (int32_t)(first % nt);
-    first /= nt;
-    cur.step[i] = (int32_t)(step % nt);
-    step /= nt;
-  }
-}
-
-__device__ void cursor_advance(const PermParams &P, TileCursor &cur) {
-  int carry = 0;
-  for (int i = 0; i < P.rank; ++i) {
-    const int32_t nt = (int32_t)P.ntile[i];
-    int32_t v = cur.c[i] + cur.step[i] + carry;
-    carry = 0;
-    if (v >= nt) { v -= nt; carry = 1; }
-    cur.c[i] = v;
-  }
-}
-
-__device__ void make_setup(const PermParams &P, const TileCursor &cur, TileSetup &S) {
+// Setup of tile t computed by one thread (coordinates by magic division of
+// the tile index).  The lanes of a warp compute different tiles at once.
+__device__ void setup_one(const PermParams &P, const DimS *D, int64_t t, TileSetup &S) {
   int64_t in_base = 0, out_base = 0;
   int ta = P.tl[P.a_last], tb = P.tl[P.b_last];
   for (int i = 0; i < P.rank; ++i) {
-    if (P.ntile[i] == 1) continue;
-    const int64_t start = (int64_t)cur.c[i] * P.tl[i];
-    in_base += start * P.istr[i];
-    out_base += start * P.ostr[i];
-    const int rem = (int)min((int64_t)P.tl[i], P.ext[i] - start);
+    const DimS d = D[i];
+    if (d.nt <= 1) continue;
+    const uint32_t qt = fast_div((uint32_t)t, d.mg_ts, d.sh_ts);
+    const uint32_t c = qt - fast_div(qt, d.mg_nt, d.sh_nt) * (uint32_t)d.nt;
+    const int64_t start = (int64_t)c * d.tl;
+    in_base += start * d.istr;
+    out_base += start * d.ostr;
+    const int rem = (int)min((int64_t)d.tl, d.ext - start);
     if (i == P.a_last) ta = rem;
     if (i == P.b_last) tb = rem;
   }
@@ -287,30 +289,60 @@ __device__ void make_setup(const PermParams &P, const TileCursor &cur, TileSetup
   S.lo_act = P.b_pre * tb;
   S.ta_lim = P.a_in_B ? INT_MAX : ta;
   S.tb_lim = P.b_in_A ? INT_MAX : tb;
+  S.full = (ta == P.tl[P.a_last] && tb == P.tl[P.b_last]) ? 1 : 0;
+  S.type = (ta < P.tl[P.a_last] ? 1 : 0) | (tb < P.tl[P.b_last] ? 2 : 0);
 }
 
-template <typename T, int VOUT, int OP>
-__global__ void __launch_bounds__(kThreads, kMinBlocks)
-    permute_tiled_kernel(const T *__restrict__ src, T *dst, const PermParams P) {
-  extern __shared__ __align__(16) unsigned char smem[];
-  T *buf0 = reinterpret_cast<T *>(smem);
-  T *buf1 = buf0 + P.buf_elems;
-  int64_t *rIn = reinterpret_cast<int64_t *>(smem + P.off_rin);
-  int32_t *rC = reinterpret_cast<int32_t *>(smem + P.off_rc);
-  int64_t *wOut = reinterpret_cast<int64_t *>(smem + P.off_wout);
-  int32_t *wSm = reinterpret_cast<int32_t *>(smem + P.off_wsm);
-  int32_t *wC = reinterpret_cast<int32_t *>(smem + P.off_wc);
-  int32_t *ySm = reinterpret_cast<int32_t *>(smem + P.off_ysm);
-  __shared__ TileSetup setup[3];
-  __shared__ TileCursor cursor;
+// Setups of the CTA's iterations it0 .. it0 + 31 (tile blockIdx.x + it * gridDim.x),
+// one per lane of warp 0, into a ring of kRing entries.
+constexpr int kRing = 64;
+__device__ __forceinline__ void fill_setups(const PermParams &P, const DimS *D, int it0, TileSetup *ring) {
+  if (threadIdx.x < 32) {
+    const int it = it0 + (int)threadIdx.x;
+    const int64_t t = (int64_t)blockIdx.x + (int64_t)it * gridDim.x;
+    if (t < P.num_tiles) setup_one(P, D, t, ring[it % kRing]);
+  }
+}
 
+// Stores the valid ones of N output vectors (adds: all loads of D are issued
+// before any store).
+template <typename T, int VOUT, int OP, int N>
+__device__ __forceinline__ void emit_masked(T *const *gp, Pack<T, VOUT> *v, const bool *ok, double sr,
+                                            double si) {
+  if constexpr (OP == kOpAdd) {
+    Pack<T, VOUT> d[N];
+#pragma unroll
+    for (int u = 0; u < N; ++u)
+      if (ok[u]) d[u] = ld_pack<T, VOUT>(gp[u]);
+#pragma unroll
+    for (int u = 0; u < N; ++u) {
+      if (!ok[u]) continue;
+#pragma unroll
+      for (int j = 0; j < VOUT; ++j) d[u].v[j] = Arith<T>::axpy(d[u].v[j], v[u].v[j], sr, si);
+      st_pack<T, VOUT>(gp[u], d[u]);
+    }
+  } else {
+#pragma unroll
+    for (int u = 0; u < N; ++u) {
+      if (!ok[u]) continue;
+      if constexpr (OP == kOpScaleCopy) {
+#pragma unroll
+        for (int j = 0; j < VOUT; ++j) v[u].v[j] = Arith<T>::mul(v[u].v[j], sr, si);
+      }
+      st_pack<T, VOUT>(gp[u], v[u]);
+    }
+  }
+}
+
+// Run tables of a plan (per-CTA, shared memory): input-run offsets and the
+// coordinate of the output split dimension; output-run offsets, shared row
+// offsets and the coordinate of the input split dimension; shared offset of
+// every output-run position.
+template <int NT>
+__device__ void build_run_tables(const PermParams &P, int64_t *rIn, int32_t *rC, int64_t *wOut,
+                                 int32_t *wSm, int32_t *wC, int32_t *ySm) {
   const int tid = threadIdx.x;
-  const int64_t G = gridDim.x;
-  // Per-CTA shared tables, valid for every tile of this plan: run offsets of
-  // the input runs (global offset + coordinate of the output split dimension)
-  // and of the output runs (global offset, shared offset, coordinate of the
-  // input split dimension), and the shared offset of every output-run position.
-  for (int r = tid; r < P.Ri; r += kThreads) {
+  for (int r = tid; r < P.Ri; r += NT) {
     int rem = r, cb = 0;
     int64_t off = 0;
     for (int k = 0; k < P.nra; ++k) {
@@ -323,7 +355,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
     rIn[r] = off;
     rC[r] = P.b_in_A ? 0 : cb;
   }
-  for (int r = tid; r < P.Ro; r += kThreads) {
+  for (int r = tid; r < P.Ro; r += NT) {
     int rem = r, ca = 0, sm = 0;
     int64_t off = 0;
     for (int k = 0; k < P.nwb; ++k) {
@@ -339,7 +371,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
     wC[r] = P.a_in_B ? 0 : ca;
   }
   if (P.ytab) {
-    for (int y = tid; y < P.Lo; y += kThreads) {
+    for (int y = tid; y < P.Lo; y += NT) {
       int rem = y, sm = 0;
       for (int k = 0; k < P.nb; ++k) {
         const int d = P.b_dims[k];
@@ -350,121 +382,271 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
       ySm[y] = sm;
     }
   }
-  if (tid == 0 && blockIdx.x < P.num_tiles) {
-    cursor_init(P, cursor, blockIdx.x, G);
-    make_setup(P, cursor, setup[0]);
-    cursor_advance(P, cursor);
-    if (blockIdx.x + G < P.num_tiles) {
-      make_setup(P, cursor, setup[1]);
-      cursor_advance(P, cursor);
+}
+
+// Transpose / transpose-add with per-thread register tables.  Every tile of a
+// plan has the same shape, so each thread's K read elements and K / VOUT write
+// vectors have fixed offsets relative to the tile bases: they are computed once
+// per CTA and held in registers (global offset, shared byte offset, and a
+// 3-bit class: bit 0 the element lies beyond the last tile's extent along
+// a_last, bit 1 likewise along b_last, bit 2 the slot is unused).  A tile
+// moves each element with one asynchronous copy in and one shared load plus
+// one (vector) store out; cut-short tiles mask by class.
+template <typename T, int K, int VOUT, int OP, bool SWZ>
+__global__ void __launch_bounds__(kThreads, K <= 4 ? 4 : 3)
+    permute_reg_kernel(const T *__restrict__ src, T *dst, const PermParams P) {
+  constexpr int KW = K / VOUT;  // write vectors per thread
+  extern __shared__ __align__(16) unsigned char smem[];
+  T *buf0 = reinterpret_cast<T *>(smem);
+  __shared__ TileSetup setup[kRing];
+  __shared__ DimS dimS[kMaxFR];
+  const int tid = threadIdx.x;
+  const int64_t G = gridDim.x;
+
+  // Global offsets (elements, from the tile base), shared byte offsets (16-bit
+  // pairs: the stage buffers are below 64 KB), classes (3 bits per slot).
+  int32_t rg[K], wg[KW];
+  uint32_t rs2[K / 2], ws2[K / 2];
+  uint32_t rcls = 0, wcls = 0;
+  auto half = [](const uint32_t *a, int i) -> uint32_t { return (i & 1) ? (a[i >> 1] >> 16) : (a[i >> 1] & 0xffffu); };
+  {
+    // Run tables live in shared memory only while the register tables are built.
+    int64_t *rIn = reinterpret_cast<int64_t *>(smem + P.off_rin);
+    int32_t *rC = reinterpret_cast<int32_t *>(smem + P.off_rc);
+    int64_t *wOut = reinterpret_cast<int64_t *>(smem + P.off_wout);
+    int32_t *wSm = reinterpret_cast<int32_t *>(smem + P.off_wsm);
+    int32_t *wC = reinterpret_cast<int32_t *>(smem + P.off_wc);
+    int32_t *ySm = reinterpret_cast<int32_t *>(smem + P.off_ysm);
+    build_run_tables<kThreads>(P, rIn, rC, wOut, wSm, wC, ySm);
+    if (tid < P.rank) {
+      DimS d;
+      d.istr = P.istr[tid];
+      d.ostr = P.ostr[tid];
+      d.ext = P.ext[tid];
+      d.tl = P.tl[tid];
+      d.nt = (int32_t)P.ntile[tid];
+      d.mg_ts = P.mg_ts[tid];
+      d.sh_ts = P.sh_ts[tid];
+      d.mg_nt = P.mg_nt[tid];
+      d.sh_nt = P.sh_nt[tid];
+      dimS[tid] = d;
     }
+    __syncthreads();
+    auto sh = [](int p) -> uint32_t { return (uint32_t)(SWZ ? swz<T>(p) : p) * (uint32_t)sizeof(T); };
+    auto cls_of = [&](int ca, int cb) -> uint32_t {
+      return (ca >= P.ta_rem ? 1u : 0u) | (cb >= P.tb_rem ? 2u : 0u);
+    };
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const int e = tid + k * kThreads;
+      rg[k] = 0;
+      if ((k & 1) == 0) rs2[k >> 1] = 0;
+      uint32_t c = 4u;
+      if (e < P.V) {
+        const int r = (int)fast_div((uint32_t)e, P.mg_li, P.sh_li);
+        const int x = e - r * P.Li;
+        rg[k] = (int32_t)(rIn[r] + x);
+        rs2[k >> 1] |= sh(r * P.Li_pad + x) << (16 * (k & 1));
+        const int ca = x / P.a_pre;
+        const int cb = P.b_in_A ? (x / P.pre_bA) % P.tl[P.b_last] : rC[r];
+        c = cls_of(ca, cb);
+      }
+      rcls |= c << (3 * k);
+    }
+    const int nv = P.nv, total = P.Ro * nv;
+#pragma unroll
+    for (int k = 0; k < KW; ++k) {
+      const int f = tid + k * kThreads;
+      wg[k] = 0;
+#pragma unroll
+      for (int j = 0; j < VOUT; ++j)
+        if (((k * VOUT + j) & 1) == 0) ws2[(k * VOUT + j) >> 1] = 0;
+      uint32_t c = 4u;
+      if (f < total) {
+        const int r = (int)fast_div((uint32_t)f, P.mg_nv, P.sh_nv);
+        const int y = (f - r * nv) * VOUT;
+        wg[k] = (int32_t)(wOut[r] + y);
+#pragma unroll
+        for (int j = 0; j < VOUT; ++j) {
+          const int yj = y + j;
+          const int p = wSm[r] + (P.ytab ? ySm[yj] : decompose(P.ymap, (uint32_t)yj).soff);
+          ws2[(k * VOUT + j) >> 1] |= sh(p) << (16 * ((k * VOUT + j) & 1));
+        }
+        const int cb = y / P.b_pre;
+        const int ca = P.a_in_B ? (y / P.pre_aB) % P.tl[P.a_last] : wC[r];
+        c = cls_of(ca, cb);
+      }
+      wcls |= c << (3 * k);
+    }
+    __syncthreads();  // the run tables' space becomes tile buffers
   }
+  fill_setups(P, dimS, 0, setup);
+  fill_setups(P, dimS, 32, setup);
   __syncthreads();
 
   const bool cj = P.conj != 0;
   double sr = P.s_re, si = P.s_im;
   effective_scale<T>(P.sdev, P.sdev_kind, P.sdev_conj, sr, si);
-  const int lane = tid & 31, warp = tid >> 5;
-  constexpr int kWarps = kThreads / 32;
+  const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(buf0);
+  const uint32_t stage_bytes = (uint32_t)P.buf_elems * (uint32_t)sizeof(T);
 
-  // Read phase: warps take chunks of input runs (chunk = up to 256 elements);
-  // one table lookup per chunk, then every lane streams elements 32 apart.
+  auto issue_loads = [&](const TileSetup &S, int stage) {
+    const T *g = src + S.in_base;
+    const uint32_t sb = sbase + (uint32_t)stage * stage_bytes;
+    const uint32_t m = (uint32_t)S.type | 4u;
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+      if (((rcls >> (3 * k)) & m) == 0) cp_async_s<sizeof(T)>(sb + half(rs2, k), g + rg[k]);
+  };
+
+  int64_t t = blockIdx.x;
+#pragma unroll
+  for (int k = 0; k < kStages - 1; ++k) {
+    if (t + k * G < P.num_tiles) issue_loads(setup[k], k);
+    cp_async_commit();
+  }
+  for (int iter = 0; t < P.num_tiles; t += G, ++iter) {
+    const int64_t tn = t + (kStages - 1) * G;
+    if (tn < P.num_tiles)
+      issue_loads(setup[(iter + kStages - 1) % kRing], (iter + kStages - 1) % kStages);
+    cp_async_commit();
+    if ((iter & 31) == 0 && iter > 0) fill_setups(P, dimS, iter + 32, setup);
+    cp_async_wait<kStages - 1>();
+    __syncthreads();
+    const TileSetup S = setup[iter % kRing];
+    const char *sbytes = reinterpret_cast<const char *>(smem) + (size_t)(iter % kStages) * stage_bytes;
+    T *g = dst + S.out_base;
+    const uint32_t m = (uint32_t)S.type | 4u;
+    // Batches of up to 4 vectors bound the live registers.
+    constexpr int WB = KW < 4 ? KW : 4;
+#pragma unroll
+    for (int c0 = 0; c0 < KW; c0 += WB) {
+      Pack<T, VOUT> v[WB];
+      T *gp[WB];
+      bool ok[WB];
+#pragma unroll
+      for (int u = 0; u < WB; ++u) {
+        const int k = c0 + u;
+        ok[u] = ((wcls >> (3 * k)) & m) == 0;
+        gp[u] = g + wg[k];
+        if (ok[u]) {
+#pragma unroll
+          for (int j = 0; j < VOUT; ++j) {
+            const T x = *reinterpret_cast<const T *>(sbytes + half(ws2, k * VOUT + j));
+            v[u].v[j] = cj ? Arith<T>::conj(x) : x;
+          }
+        }
+      }
+      emit_masked<T, VOUT, OP, WB>(gp, v, ok, sr, si);
+    }
+    __syncthreads();
+  }
+}
+
+// Transpose / transpose-add for plans whose tiles span more than 32-bit
+// offsets (tensors of more than 2^31 elements): positions come from the
+// shared run tables (64-bit offsets) for every element.
+template <typename T, int VOUT, int OP, bool SWZ>
+__global__ void __launch_bounds__(kThreads, kMinBlocks)
+    permute_tiled_kernel(const T *__restrict__ src, T *dst, const PermParams P) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  T *buf0 = reinterpret_cast<T *>(smem);
+  int64_t *rIn = reinterpret_cast<int64_t *>(smem + P.off_rin);
+  int32_t *rC = reinterpret_cast<int32_t *>(smem + P.off_rc);
+  int64_t *wOut = reinterpret_cast<int64_t *>(smem + P.off_wout);
+  int32_t *wSm = reinterpret_cast<int32_t *>(smem + P.off_wsm);
+  int32_t *wC = reinterpret_cast<int32_t *>(smem + P.off_wc);
+  int32_t *ySm = reinterpret_cast<int32_t *>(smem + P.off_ysm);
+  __shared__ TileSetup setup[kRing];
+  __shared__ DimS dimS[kMaxFR];
+  const int tid = threadIdx.x;
+  const int64_t G = gridDim.x;
+  build_run_tables<kThreads>(P, rIn, rC, wOut, wSm, wC, ySm);
+  if (tid < P.rank) {
+    DimS d;
+    d.istr = P.istr[tid];
+    d.ostr = P.ostr[tid];
+    d.ext = P.ext[tid];
+    d.tl = P.tl[tid];
+    d.nt = (int32_t)P.ntile[tid];
+    d.mg_ts = P.mg_ts[tid];
+    d.sh_ts = P.sh_ts[tid];
+    d.mg_nt = P.mg_nt[tid];
+    d.sh_nt = P.sh_nt[tid];
+    dimS[tid] = d;
+  }
+  __syncthreads();
+  fill_setups(P, dimS, 0, setup);
+  fill_setups(P, dimS, 32, setup);
+  __syncthreads();
+
+  const bool cj = P.conj != 0;
+  double sr = P.s_re, si = P.s_im;
+  effective_scale<T>(P.sdev, P.sdev_kind, P.sdev_conj, sr, si);
+  auto sh = [](int p) -> int { return SWZ ? swz<T>(p) : p; };
+  const int pitch = P.Li_pad;
+  const int nv = P.nv, total = P.Ro * nv;
+  const int ystr = P.ymap.sstr[0];
+  auto ypos = [&](int ws, int y) -> int {
+    return ws + (P.ytab ? ySm[y] : decompose(P.ymap, (uint32_t)y).soff);
+  };
+  auto tile_buf = [&](int k) -> T * { return buf0 + (size_t)(k % kStages) * P.buf_elems; };
   auto issue_loads = [&](const TileSetup &S, T *buf) {
-    const int nch = P.nch_r, total = P.Ri * nch;
-    for (int it = warp; it < total; it += kWarps) {
-      const int r = (int)fast_div((uint32_t)it, P.mg_cr, P.sh_cr);
-      const int x0 = (it - r * nch) * kChunk;
-      if (rC[r] >= S.tb_lim) continue;
-      const int xe = min(x0 + kChunk, S.li_act);
-      const T *g = src + (S.in_base + rIn[r]);
-      const int sb = r * P.Li;
-#pragma unroll 4
-      for (int x = x0 + lane; x < xe; x += 32) cp_async_elem<sizeof(T)>(buf + swz<T>(sb + x), g + x);
+    const T *g = src + S.in_base;
+#pragma unroll 2
+    for (int e = tid; e < P.V; e += kThreads) {
+      const int r = (int)fast_div((uint32_t)e, P.mg_li, P.sh_li);
+      const int x = e - r * P.Li;
+      if (!S.full && (x >= S.li_act || rC[r] >= S.tb_lim)) continue;
+      cp_async_elem<sizeof(T)>(buf + sh(r * pitch + x), g + (rIn[r] + x));
     }
   };
 
   int64_t t = blockIdx.x;
-  if (t < P.num_tiles) issue_loads(setup[0], buf0);
-  cp_async_commit();
-  for (int iter = 0; t < P.num_tiles; t += G, ++iter) {
-    const int64_t tn = t + G;
-    if (tn < P.num_tiles) issue_loads(setup[(iter + 1) % 3], (iter & 1) ? buf0 : buf1);
+#pragma unroll
+  for (int k = 0; k < kStages - 1; ++k) {
+    if (t + k * G < P.num_tiles) issue_loads(setup[k], tile_buf(k));
     cp_async_commit();
-    if (tid == 0 && tn + G < P.num_tiles) {
-      make_setup(P, cursor, setup[(iter + 2) % 3]);
-      cursor_advance(P, cursor);
-    }
-    cp_async_wait_1();
+  }
+  for (int iter = 0; t < P.num_tiles; t += G, ++iter) {
+    const int64_t tn = t + (kStages - 1) * G;
+    if (tn < P.num_tiles) issue_loads(setup[(iter + kStages - 1) % kRing], tile_buf(iter + kStages - 1));
+    cp_async_commit();
+    if ((iter & 31) == 0 && iter > 0) fill_setups(P, dimS, iter + 32, setup);
+    cp_async_wait<kStages - 1>();
     __syncthreads();
-    // Write phase: warps take chunks of output runs; lanes move VOUT elements
-    // per step with one (vector) store.
-    const TileSetup S = setup[iter % 3];
-    const T *buf = (iter & 1) ? buf1 : buf0;
-    const int nch = P.nch_w, total = P.Ro * nch;
-    for (int it = warp; it < total; it += kWarps) {
-      const int r = (int)fast_div((uint32_t)it, P.mg_cw, P.sh_cw);
-      const int y0 = (it - r * nch) * (kChunk * VOUT);
-      if (wC[r] >= S.ta_lim) continue;
-      const int ye = min(y0 + kChunk * VOUT, S.lo_act);
-      T *g = dst + (S.out_base + wOut[r]);
-      const int ws = wSm[r];
-      constexpr int U = (OP == kOpAdd) ? 4 : 2;  // steps per batch (adds keep U loads of D in flight)
-      for (int yb = y0 + lane * VOUT; yb < ye; yb += 32 * VOUT * U) {
-        Pack<T, VOUT> v[U];
-        bool ok[U];
+    const TileSetup S = setup[iter % kRing];
+    const T *buf = tile_buf(iter);
+    T *g = dst + S.out_base;
+    constexpr int U = 4;  // vectors per batch: U shared gathers (and loads of D) in flight
+    for (int f0 = tid; f0 < total; f0 += U * kThreads) {
+      Pack<T, VOUT> v[U];
+      T *gp[U];
+      bool ok[U];
 #pragma unroll
-        for (int u = 0; u < U; ++u) {
-          const int y = yb + u * 32 * VOUT;
-          ok[u] = y < ye;
-          if (!ok[u]) continue;
-          if (P.ytab) {
-            if (P.y_step) {
-              const int base = ws + ySm[y];
+      for (int u = 0; u < U; ++u) {
+        const int f = f0 + u * kThreads;
+        const int r = (int)fast_div((uint32_t)f, P.mg_nv, P.sh_nv);
+        const int y = (f - r * nv) * VOUT;
+        ok[u] = f < total && (S.full || (y < S.lo_act && wC[r] < S.ta_lim));
+        gp[u] = g;
+        if (!ok[u]) continue;
+        const int ws = wSm[r];
+        if (P.y_step) {
+          const int base = ypos(ws, y);
 #pragma unroll
-              for (int j = 0; j < VOUT; ++j) v[u].v[j] = buf[swz<T>(base + j * P.ymap.sstr[0])];
-            } else {
-#pragma unroll
-              for (int j = 0; j < VOUT; ++j) v[u].v[j] = buf[swz<T>(ws + ySm[y + j])];
-            }
-          } else {
-            if (P.y_step) {
-              const int base = ws + decompose(P.ymap, (uint32_t)y).soff;
-#pragma unroll
-              for (int j = 0; j < VOUT; ++j) v[u].v[j] = buf[swz<T>(base + j * P.ymap.sstr[0])];
-            } else {
-#pragma unroll
-              for (int j = 0; j < VOUT; ++j) v[u].v[j] = buf[swz<T>(ws + decompose(P.ymap, (uint32_t)(y + j)).soff)];
-            }
-          }
-          if (cj) {
-#pragma unroll
-            for (int j = 0; j < VOUT; ++j) v[u].v[j] = Arith<T>::conj(v[u].v[j]);
-          }
-        }
-        if constexpr (OP == kOpAdd) {
-          Pack<T, VOUT> d[U];
-#pragma unroll
-          for (int u = 0; u < U; ++u)
-            if (ok[u]) d[u] = ld_pack<T, VOUT>(g + yb + u * 32 * VOUT);
-#pragma unroll
-          for (int u = 0; u < U; ++u) {
-            if (!ok[u]) continue;
-#pragma unroll
-            for (int j = 0; j < VOUT; ++j) d[u].v[j] = Arith<T>::axpy(d[u].v[j], v[u].v[j], sr, si);
-            st_pack<T, VOUT>(g + yb + u * 32 * VOUT, d[u]);
-          }
+          for (int j = 0; j < VOUT; ++j) v[u].v[j] = buf[sh(base + j * ystr)];
         } else {
 #pragma unroll
-          for (int u = 0; u < U; ++u) {
-            if (!ok[u]) continue;
-            if constexpr (OP == kOpScaleCopy) {
-#pragma unroll
-              for (int j = 0; j < VOUT; ++j) v[u].v[j] = Arith<T>::mul(v[u].v[j], sr, si);
-            }
-            st_pack<T, VOUT>(g + yb + u * 32 * VOUT, v[u]);
-          }
+          for (int j = 0; j < VOUT; ++j) v[u].v[j] = buf[sh(ypos(ws, y + j))];
         }
+        if (cj) {
+#pragma unroll
+          for (int j = 0; j < VOUT; ++j) v[u].v[j] = Arith<T>::conj(v[u].v[j]);
+        }
+        gp[u] = g + (wOut[r] + y);
       }
+      emit_masked<T, VOUT, OP, U>(gp, v, ok, sr, si);
     }
     __syncthreads();
   }
@@ -557,6 +739,18 @@ int fuse_dims(int rank, const int *dims, const int *o2n, Fused &F) {
   return TALSH_SUCCESS;
 }
 
+// Elements per thread of permute_reg_kernel (its tile is at most 256 x this):
+// 8, or 4 for 16-byte elements; TALSH_B200_REG_K=4 selects 4 for every kind.
+int reg_k(int esize) {
+  static int forced = -1;
+  if (forced < 0) {
+    const char *e = std::getenv("TALSH_B200_REG_K");
+    forced = (e && std::atoi(e) == 4) ? 4 : 0;
+  }
+  if (esize >= 16) return 4;
+  return forced ? forced : 8;
+}
+
 // Tile buffer budget in bytes: kTileBytes, or TALSH_B200_TILE_BYTES (4096..49152) for tuning.
 int tile_bytes() {
   static int v = 0;
@@ -581,6 +775,9 @@ struct Plan {
 // Next tile extent for a split dimension: about twice the current one, but
 // chosen so that the dimension divides into equal tiles (little masked work).
 int64_t balanced_grow(int64_t ext, int64_t cur) {
+  // An exact divisor up to 3x leaves no cut-short tile along this dimension.
+  for (int64_t t = cur + 1; t <= std::min(ext, cur * 3); ++t)
+    if (ext % t == 0) return t;
   for (int64_t target = cur * 2; target < ext; target += cur) {
     const int64_t pieces = (ext + target - 1) / target;
     const int64_t t = (ext + pieces - 1) / pieces;
@@ -589,7 +786,9 @@ int64_t balanced_grow(int64_t ext, int64_t cur) {
   return ext;
 }
 
-int build_plan(int esize, const Fused &F, Plan &plan) {
+// out_major: tile index order follows the output's dimensions (copies), else
+// the input's (adds, whose output sectors are read before they are written).
+int build_plan(int esize, const Fused &F, Plan &plan, bool out_major = true) {
   plan.vol = F.vol;
   if (F.n <= 1) { plan.linear = true; return TALSH_SUCCESS; }
   PermParams &P = plan.P;
@@ -603,11 +802,12 @@ int build_plan(int esize, const Fused &F, Plan &plan) {
   s = 1;
   for (int k = 0; k < n; ++k) { P.ostr[q[k]] = s; s *= P.ext[q[k]]; }
 
-  // Small tensors get smaller tiles so that every SM still holds a few of them.
-  int elems_max = tile_bytes() / esize;
+  // Tile budget: at most reg_k(esize) elements per thread of the register-table
+  // kernel.  Small tensors get smaller tiles so that every SM still holds a few.
+  int elems_max = std::min(tile_bytes() / esize, kThreads * reg_k(esize));
   {
     const int64_t slots = 148LL * kMinBlocks * 2;
-    while (elems_max > 1024 && F.vol / elems_max < slots) elems_max /= 2;
+    while (elems_max / 2 >= 1024 && F.vol / elems_max < slots) elems_max /= 2;  // floor 1024: every plan fits
   }
   const int run_min = esize >= 16 ? 16 : 32;
   // Initial groups: shortest prefixes reaching run_min elements.
@@ -619,6 +819,7 @@ int build_plan(int esize, const Fused &F, Plan &plan) {
       if (pre * P.ext[i] >= run_min || i == n - 1) {
         na = i + 1;
         tA = std::min<int64_t>(P.ext[i], (run_min + pre - 1) / pre);
+        tA = (P.ext[i] + (P.ext[i] + tA - 1) / tA - 1) / ((P.ext[i] + tA - 1) / tA);  // equal pieces
         break;
       }
       pre *= P.ext[i];
@@ -627,7 +828,9 @@ int build_plan(int esize, const Fused &F, Plan &plan) {
     for (int k = 0; k < n; ++k) {
       if (pre * P.ext[q[k]] >= run_min || k == n - 1) {
         nb = k + 1;
-        tB = std::min<int64_t>(P.ext[q[k]], (run_min + pre - 1) / pre);
+        const int64_t e = P.ext[q[k]];
+        tB = std::min<int64_t>(e, (run_min + pre - 1) / pre);
+        tB = (e + (e + tB - 1) / tB - 1) / ((e + tB - 1) / tB);  // equal pieces
         break;
       }
       pre *= P.ext[q[k]];
@@ -728,8 +931,19 @@ int build_plan(int esize, const Fused &F, Plan &plan) {
     P.tl[i] = (int32_t)G.tl[i];
     P.ntile[i] = (P.ext[i] + G.tl[i] - 1) / G.tl[i];
   }
+  // Tile index order.  Output-major for copies: the tiles in flight at any time
+  // write neighbouring stretches of the output, so the sectors that straddle
+  // two tiles are completed in L2 before they are written back (a misaligned
+  // output run otherwise costs a read-modify-write).  Input-major for adds,
+  // which read the output sectors anyway.
   P.num_tiles = 1;
-  for (int i = 0; i < n; ++i) P.num_tiles *= P.ntile[i];
+  for (int k = 0; k < n; ++k) {
+    const int i = out_major ? q[k] : k;
+    make_magic((uint32_t)P.num_tiles, P.mg_ts[i], P.sh_ts[i]);  // tile-index stride of dimension i
+    make_magic((uint32_t)P.ntile[i], P.mg_nt[i], P.sh_nt[i]);
+    P.num_tiles *= P.ntile[i];
+  }
+  if (P.num_tiles >= INT_MAX) return TALSH_LIMIT_EXCEEDED;  // tile indices use 32-bit magic division
   P.V = (int)G.V;
   P.Li = (int)G.Li;
   P.Lo = (int)G.Lo;
@@ -744,8 +958,14 @@ int build_plan(int esize, const Fused &F, Plan &plan) {
   for (int k = 0; k < nb; ++k) inB[q[k]] = true;
   P.a_in_B = inB[P.a_last] ? 1 : 0;
   P.b_in_A = inA[P.b_last] ? 1 : 0;
-  // shared layout: x over A (input order) contiguous, runs over U\A with pitch Li_pad
-  P.Li_pad = P.Li;  // no padding: shared indices are bank-swizzled instead
+  // Shared layout: x over A (input order) contiguous, input runs over U\A with
+  // row pitch Li_pad.  The write phase walks the output's fastest dimension
+  // q[0] with shared stride smstr[q[0]].  When q[0] lies inside A (and is not
+  // its first dimension) that stride is a product of A extents, often a power
+  // of two: the indices are then bank-swizzled.  Otherwise the stride is a
+  // multiple of the row pitch, which is made odd.
+  P.swz = (inA[q[0]] && q[0] != 0) ? 1 : 0;
+  P.Li_pad = P.swz ? P.Li : (P.Li % 2 == 0 ? P.Li + 1 : P.Li);
   {
     int32_t st = 1;
     for (int i = 0; i < na; ++i) { P.smstr[i] = st; st *= P.tl[i]; }
@@ -765,8 +985,6 @@ int build_plan(int esize, const Fused &F, Plan &plan) {
   }
   make_magic((uint32_t)P.Li, P.mg_li, P.sh_li);
   make_magic((uint32_t)P.Lo, P.mg_lo, P.sh_lo);
-  P.nch_r = (P.Li + kChunk - 1) / kChunk;
-  make_magic((uint32_t)P.nch_r, P.mg_cr, P.sh_cr);
   // Group maps: read runs over U\A (input strides), write runs over U\B
   // (output strides), output-run positions over B (shared strides only).
   auto fill_map = [&](GroupMap &g, const int8_t *dims, int nd, bool output_side, int mask_dim) {
@@ -802,13 +1020,27 @@ int build_plan(int esize, const Fused &F, Plan &plan) {
     }
     if (ok) plan.vout = vec;
   }
-  // Shared memory: two tile buffers, then the tables that are in use.
-  // each buffer is rounded up to whole 128-byte rows: the swizzle permutes within rows
+  // Shared memory: kStages tile buffers and the run tables.  Each buffer is
+  // rounded up to whole 128-byte rows: the swizzle permutes within rows.  The
+  // register-table kernel reads the run tables only before its first tile, so
+  // they overlay the buffers when they fit there.
   const size_t buf_elems = (((size_t)P.Ri * P.Li_pad * esize + 127) / 128) * 128 / esize;
   P.buf_elems = (int)buf_elems;
-  size_t off = 2 * buf_elems * esize;
-  off = (off + 15) & ~size_t(15);
+  const size_t bufs = (size_t)kStages * buf_elems * esize;
   P.ytab = (P.Lo <= kMaxTabLo || P.ymap.n < 0) ? 1 : 0;
+  const size_t run_tabs = (size_t)P.Ri * 12 + (size_t)P.Ro * 16 + (P.ytab ? (size_t)P.Lo * 4 : 0) + 16;
+  int64_t span_in = 0, span_out = 0;
+  for (int i = 0; i < n; ++i) {
+    span_in += (int64_t)(P.tl[i] - 1) * P.istr[i];
+    span_out += (int64_t)(P.tl[i] - 1) * P.ostr[i];
+  }
+  // TALSH_B200_PERMUTE_GENERIC=1 sends every plan to the generic kernel (for tests).
+  static const bool force_generic = [] {
+    const char *e = std::getenv("TALSH_B200_PERMUTE_GENERIC");
+    return e && std::atoi(e) == 1;
+  }();
+  P.reg = (!force_generic && span_in < INT_MAX && span_out < INT_MAX && P.V <= kThreads * reg_k(esize)) ? 1 : 0;
+  size_t off = (P.reg && run_tabs <= bufs) ? 0 : ((bufs + 15) & ~size_t(15));
   P.off_rin = (int)off; off += (size_t)P.Ri * 8;
   P.off_wout = (int)off; off += (size_t)P.Ro * 8;
   P.off_rc = (int)off; off += (size_t)P.Ri * 4;
@@ -816,6 +1048,15 @@ int build_plan(int esize, const Fused &F, Plan &plan) {
   P.off_wc = (int)off; off += (size_t)P.Ro * 4;
   P.off_ysm = (int)off; if (P.ytab) off += (size_t)P.Lo * 4;
   P.off_tab_end = (int)off;
+  off = std::max(off, bufs);
+  {
+    P.ta_rem = (int)(P.ext[P.a_last] - (P.ntile[P.a_last] - 1) * P.tl[P.a_last]);
+    P.tb_rem = (int)(P.ext[P.b_last] - (P.ntile[P.b_last] - 1) * P.tl[P.b_last]);
+    P.pre_bA = 1;
+    for (int i = 0; i < P.b_last && P.b_in_A; ++i) P.pre_bA *= P.tl[i];
+    P.pre_aB = 1;
+    for (int k = 0; k < nb && P.a_in_B && q[k] != P.a_last; ++k) P.pre_aB *= P.tl[q[k]];
+  }
   plan.smem = off;
   return TALSH_SUCCESS;
 }
@@ -901,19 +1142,36 @@ int launch_typed(const Plan &plan, const void *src, void *dst, int conj, const S
   const bool dst_al = ((uintptr_t)dst % 16) == 0;
   const int vout = (plan.vout > 1 && dst_al) ? VEC : 1;
   P.y_step = (P.ymap.n >= 1 && P.ymap.ext[0] % vout == 0) ? 1 : 0;
-  P.nch_w = (P.Lo + kChunk * vout - 1) / (kChunk * vout);
-  make_magic((uint32_t)P.nch_w, P.mg_cw, P.sh_cw);
+  P.nv = P.Lo / vout;
+  make_magic((uint32_t)P.nv, P.mg_nv, P.sh_nv);
   auto run = [&](auto kern) {
     const void *fn = (const void *)kern;
     const int bps = blocks_per_sm(fn, plan.smem);
     const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(P.num_tiles, (int64_t)sms * bps));
     kern<<<grid, kThreads, plan.smem, st>>>((const T *)src, (T *)dst, P);
   };
-  if constexpr (VEC > 1) {
-    if (vout > 1) run(permute_tiled_kernel<T, VEC, OP>);
-    else run(permute_tiled_kernel<T, 1, OP>);
+  if (P.reg) {
+    auto run_k = [&](auto kc) {
+      constexpr int K = decltype(kc)::value;
+      if (P.swz) {
+        if (vout > 1) run(permute_reg_kernel<T, K, VEC, OP, true>);
+        else run(permute_reg_kernel<T, K, 1, OP, true>);
+      } else {
+        if (vout > 1) run(permute_reg_kernel<T, K, VEC, OP, false>);
+        else run(permute_reg_kernel<T, K, 1, OP, false>);
+      }
+    };
+    if (P.V <= kThreads * 4) run_k(std::integral_constant<int, 4>{});
+    else run_k(std::integral_constant<int, 8>{});
+    note_launch();
+    return check_launch("permute_reg_kernel");
+  }
+  if (P.swz) {
+    if (vout > 1) run(permute_tiled_kernel<T, VEC, OP, true>);
+    else run(permute_tiled_kernel<T, 1, OP, true>);
   } else {
-    run(permute_tiled_kernel<T, 1, OP>);
+    if (vout > 1) run(permute_tiled_kernel<T, VEC, OP, false>);
+    else run(permute_tiled_kernel<T, 1, OP, false>);
   }
   note_launch();
   return check_launch("permute_tiled_kernel");
@@ -943,7 +1201,7 @@ int permute_entry(int kind, int rank, const int *dims, const int *o2n, const voi
   if (rank == 0) { F.n = 0; F.vol = 1; }
   else if ((rc = fuse_dims(rank, dims, o2n, F)) != 0) return rc;
   Plan plan;
-  if ((rc = build_plan(kind_size(kind), F, plan)) != 0) return rc;
+  if ((rc = build_plan(kind_size(kind), F, plan, OP != kOpAdd)) != 0) return rc;
   cudaStream_t st = (cudaStream_t)stream;
   switch (kind) {
     case R4: return launch_typed<float, OP>(plan, src, dst, conj, sc, st);
@@ -1010,6 +1268,7 @@ extern "C" int tcPermutePlanInfo(int data_kind, int rank, const int *dims_in, co
     info[5] = plan.P.Ri; info[6] = plan.P.Ro; info[7] = plan.vin; info[8] = plan.vout;
     info[9] = (int)plan.smem;
     info[10] = (int)std::min<int64_t>(plan.P.num_tiles, INT_MAX);
+    info[11] = plan.P.reg;
   }
   return 0;
 }

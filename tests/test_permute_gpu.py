@@ -2,6 +2,9 @@
 bit-exact against the oracle (reference tensor_block_copy / tensor_block_add)."""
 import ctypes as C
 import itertools
+import os
+import subprocess
+import sys
 
 import numpy as np
 import pytest
@@ -11,6 +14,7 @@ import tal_sh_b200 as T
 from gpu_util import fort, gpu_add, gpu_copy, rand, same_bits
 
 pytestmark = pytest.mark.gpu
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 KINDS = [T.R4, T.R8, T.C4, T.C8]
 LAB = "abcdefgh"
 
@@ -100,6 +104,78 @@ def test_large_volumes_bit_exact(talsh, kind):
         D = fort(np.zeros(O.out_dims(list(dims), o2n), dtype=L.dtype))
         assert gpu_copy(patterns(len(dims), o2n), D, L) == 0
         assert same_bits(D, O.permute(L, list(o2n))), (dims, o2n)
+
+
+@pytest.mark.parametrize("kind", KINDS)
+def test_table_path_bit_exact(talsh, kind):
+    """Tensors large enough for the per-element tables, with extents that leave
+    cut-short tiles along either split dimension or both (copy, add, conj)."""
+    rng = np.random.default_rng(kind + 40)
+    lib = T.lib()
+    info = (C.c_int * 12)()
+    cases = [((97, 131, 17, 23), (4, 3, 1, 2)), ((25, 9, 9, 10, 121), (3, 2, 1, 4, 5)),
+             ((2, 347, 2, 241, 31), (1, 5, 4, 3, 2)), ((1321, 2, 31, 61), (3, 4, 1, 2)),
+             ((30, 47, 2, 17, 113), (4, 3, 5, 2, 1)), ((17, 3, 40961), (1, 3, 2)),
+             ((5, 7, 11, 13, 17, 3), (6, 4, 2, 5, 1, 3))]
+    used = 0
+    for dims, o2n in cases:
+        assert lib.tcPermutePlanInfo(kind, len(dims), T.ivec(dims), T.ivec(o2n), info) == 0
+        used += info[11]
+        L = rand(dims, kind, rng)
+        D = fort(np.full(O.out_dims(list(dims), o2n), np.nan, dtype=L.dtype))
+        assert gpu_copy(patterns(len(dims), o2n), D, L) == 0
+        assert same_bits(D, O.permute(L, list(o2n))), (dims, o2n)
+        D0 = rand(O.out_dims(list(dims), o2n), kind, rng)
+        D = D0.copy(order="F")
+        assert gpu_add(patterns(len(dims), o2n).replace(")=L", ")+=L"), D, L, 0.75, 0.0) == 0
+        ref = D0.copy(order="F")
+        O.tensor_add(ref, L, list(o2n), 0.75, 0.0)
+        assert same_bits(D, ref), ("add", dims, o2n)
+    assert used >= len(cases) - 1  # the cases are meant to take the table path
+
+
+def test_generic_kernel_bit_exact(built):
+    """The generic kernel (64-bit run tables, used when a tile spans more than
+    2^31 elements) is forced for every plan in a child process and checked on
+    small and table-sized cases, copy and add, every kind."""
+    code = r"""
+import ctypes as C, itertools, sys
+sys.path.insert(0, %r); sys.path.insert(0, %r)
+import numpy as np
+import oracle as O, tal_sh_b200 as T
+from gpu_util import fort, rand, same_bits, gpu_copy, gpu_add
+L = T.lib()
+hb, ha = C.c_size_t(0), C.c_int(0)
+assert L.talshInit(C.byref(hb), C.byref(ha), 1, T.ivec([0]), 0, None, 0, None) == 0
+info = (C.c_int * 12)()
+LAB = "abcdefgh"
+def pat(o2n, add):
+    d = [None] * len(o2n)
+    for i, p in enumerate(o2n): d[p - 1] = LAB[i]
+    return "D(%%s)%%s=L(%%s)" %% (",".join(d), "+" if add else "", ",".join(LAB[:len(o2n)]))
+rng = np.random.default_rng(5)
+cases = [((17, 31, 3), (3, 1, 2)), ((5, 6, 7, 3), (4, 3, 2, 1)), ((97, 131, 17, 23), (4, 3, 1, 2)),
+         ((25, 9, 9, 10, 121), (3, 2, 1, 4, 5)), ((64, 32, 3), (2, 1, 3))]
+for kind in (T.R4, T.R8, T.C4, T.C8):
+    for dims, o2n in cases:
+        assert L.tcPermutePlanInfo(kind, len(dims), T.ivec(dims), T.ivec(o2n), info) == 0
+        assert info[11] == 0
+        A = rand(dims, kind, rng)
+        D = fort(np.full(O.out_dims(list(dims), o2n), np.nan, dtype=A.dtype))
+        assert gpu_copy(pat(o2n, False), D, A) == 0
+        assert same_bits(D, O.permute(A, list(o2n))), (kind, dims, o2n)
+        D0 = rand(O.out_dims(list(dims), o2n), kind, rng)
+        D = D0.copy(order="F")
+        assert gpu_add(pat(o2n, True), D, A, -1.25, 0.0) == 0
+        ref = D0.copy(order="F"); O.tensor_add(ref, A, list(o2n), -1.25, 0.0)
+        assert same_bits(D, ref), ("add", kind, dims, o2n)
+assert L.talshShutdown() == 0
+print("OK")
+""" % (ROOT, os.path.join(ROOT, "tests"))
+    env = dict(os.environ, TALSH_B200_PERMUTE_GENERIC="1")
+    p = subprocess.run([sys.executable, "-c", code], env=env, stdout=subprocess.PIPE, stderr=subprocess.STDOUT,
+                       text=True, timeout=600)
+    assert p.returncode == 0 and "OK" in p.stdout, p.stdout
 
 
 def test_plan_properties(talsh):
