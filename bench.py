@@ -15,7 +15,8 @@ D = TRN(L) and one transpose-add D += TRN(L)*alpha (alpha cycling through
   e2e        the same sweep through talshTensorCopy/talshTensorAdd on pinned
              Host tensors (COPY_TT: every step moves L (and D for adds) to the
              GPU and D back).
-  roofline   permute_tiled_kernel launches timed one by one with CUDA events.
+  roofline   the sweep's kernel launches (permute_reg_kernel, linear_kernel for
+             permutations that fuse to a straight copy) timed one by one with CUDA events.
   contract   C1 and C3 FP64 contractions through talshTensorContract on
              GPU-resident tensors (TFLOP/s, error vs an FP64 reference).
   cpu_baseline  the reference's cache-blocked CPU transpose (restated in the
@@ -154,8 +155,8 @@ def measured_peak():
 
 
 def profile_traffic_ratio():
-    """DRAM bytes / algorithmic bytes of permute_tiled_kernel from the committed ncu summary."""
-    path = os.path.join(ROOT, "profiles", "permute_tiled_kernel_c2.md")
+    """DRAM bytes / algorithmic bytes of the sweep's launches from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "permute_reg_kernel_c2_sweep.md")
     try:
         for line in open(path):
             if line.startswith("traffic_over_algorithmic:"):
@@ -217,6 +218,40 @@ def run_cpu_baseline(cases, seconds_budget=20.0):
 
 
 # ----------------------------------------------------------------- GPU side
+def profile_case(spec, op):
+    """One transpose (or transpose-add) of a given shape, four launches, for profilers."""
+    import torch
+    import tal_sh_b200 as T
+    kname, dims, o2n = spec.split(":")
+    kind = {"R4": R4, "R8": R8, "C4": C4, "C8": C8}[kname]
+    dims = [int(x) for x in dims.split(",")]
+    o2n = [int(x) for x in o2n.split(",")]
+    L = T.lib()
+    nbytes = case_bytes(kind, dims)
+    src = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+    dst = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+    src.view(torch.float32).uniform_(-1.0, 1.0)
+    dst.view(torch.float32).uniform_(-1.0, 1.0)
+    info = (C.c_int * 12)()
+    L.tcPermutePlanInfo(kind, len(dims), T.ivec(dims), T.ivec(o2n), info)
+    s = torch.cuda.current_stream().cuda_stream
+    for rep in range(4):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        if op == "add":
+            rc = L.tcTensorPermuteAdd(kind, len(dims), T.ivec(dims), T.ivec(o2n), src.data_ptr(), dst.data_ptr(),
+                                      0.5, 0.0, 0, s)
+        else:
+            rc = L.tcTensorPermute(kind, len(dims), T.ivec(dims), T.ivec(o2n), src.data_ptr(), dst.data_ptr(), 0, s)
+        e1.record()
+        torch.cuda.synchronize()
+        if rc != 0:
+            raise RuntimeError("launch failed %d: %s" % (rc, L.tcLastErrorString()))
+        moved = (3 if op == "add" else 2) * nbytes
+        print(json.dumps({"case": spec, "op": op, "rep": rep, "plan": list(info),
+                          "gbs": moved / (e0.elapsed_time(e1) * 1e-3) / 1e9}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -226,7 +261,13 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--no-contract", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--profile-case", default=None,
+                    help="KIND:d1,d2,..:p1,p2,.. -- run one transpose four times (for ncu) and exit")
+    ap.add_argument("--profile-op", default="copy", choices=["copy", "add"])
     args = ap.parse_args()
+    if args.profile_case:
+        profile_case(args.profile_case, args.profile_op)
+        return
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -443,7 +484,7 @@ def main():
     peak, peak_kind = measured_peak()
     achieved = launch_avg_bytes / launch_avg_s / 1e9
     ratio = profile_traffic_ratio()
-    roofline = {"kernel": "permute_tiled_kernel (transpose and transpose-add)", "bound": "hbm",
+    roofline = {"kernel": "permute_reg_kernel (transpose and transpose-add)", "bound": "hbm",
                 "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)",
                 "traffic": (ratio * launch_avg_bytes) if ratio else None,
