@@ -73,6 +73,28 @@ int tcTensorContract(int data_kind, const int *cptrn, int drank, const int *ddim
                      const void *R, double alpha_re, double alpha_im, int conj_bits,
                      int accumulative, void *scratch, size_t scratch_bytes, void *stream);
 
+/* Bytes of device scratch tcTensorContractSplit needs (0 when the form does
+ * not apply: not R8, or an operand of rank 0). */
+size_t tcTensorContractSplitScratch(int data_kind, const int *cptrn, int drank, const int *ddims,
+                                    int lrank, const int *ldims, int rrank, const int *rdims,
+                                    int slices);
+
+/* Split-precision R8 contraction on the tensor cores (tcgen05 kind::i8): the
+ * operands are permuted to matrices, cut into `slices` int8 slices of 7 bits
+ * per row with power-of-two row scales, all slice pairs (s, t) with
+ * s + t <= slices + 1 are multiplied exactly in int32 and recombined in FP64
+ * (the Ozaki scheme).  Same pattern, alpha/accumulative and D layout rules as
+ * tcTensorContract; slices 2..7, 0 = 6 (relative error about sqrt(K)*2^-46 on
+ * random data, below 1e-10 for contracted volumes up to ~10^8).  Indices
+ * present in D, L and R at once return TALSH_NOT_IMPLEMENTED.  Inputs must be
+ * finite.  The north-star's split-precision form of
+ * gpu_tensor_block_contract_dlf (reference :5847); no reference counterpart. */
+int tcTensorContractSplit(int data_kind, const int *cptrn, int drank, const int *ddims, int lrank,
+                          const int *ldims, int rrank, const int *rdims, void *D, const void *L,
+                          const void *R, double alpha_re, double alpha_im, int conj_bits,
+                          int accumulative, int slices, void *scratch, size_t scratch_bytes,
+                          void *stream);
+
 /* Size of the fixed scratch array behind tcTensorContractNoAlloc: 8 MiB per GPU. */
 #define TC_CONTRACT_NOALLOC_SCRATCH_BYTES ((size_t)8 << 20)
 

@@ -127,6 +127,8 @@ _PROTOS = {
     "talshTensorContractXL": (_I, [_S, _P(Tens), _P(Tens), _P(Tens), _D, _D, _I, _I, _I]),
     "talshTensorImageNorm1_cpu": (_D, [_P(Tens)]),
     "talshTensorNorm1": (_D, [_P(Tens), _I, _I]),
+    "talshContractSlicesSet": (_I, [_I]),
+    "talshContractSlicesGet": (_I, []),
     "talsh_get_contr_ptrn_str2dig": (_I, [_S, _P(_I), _P(_I), _P(_I), _P(_I), _P(_I)]),
     "get_contr_permutations": (None, [_I, _I, _I, _I, _P(_I), _I, _P(_I), _P(_I), _P(_I),
                                       _P(_I), _P(_I), _P(_I), _P(_I)]),
@@ -148,6 +150,9 @@ _PROTOS = {
     "tcTensorContractNoAlloc": (_I, [_I, _P(_I), _I, _P(_I), _I, _P(_I), _I, _P(_I), _V, _V, _V, _D,
                                      _D, _I, _I, _V]),
     "tcTensorContractNoAllocMaxScratch": (_Z, []),
+    "tcTensorContractSplitScratch": (_Z, [_I, _P(_I), _I, _P(_I), _I, _P(_I), _I, _P(_I), _I]),
+    "tcTensorContractSplit": (_I, [_I, _P(_I), _I, _P(_I), _I, _P(_I), _I, _P(_I), _V, _V, _V, _D, _D,
+                                   _I, _I, _I, _V, _Z, _V]),
     "tcPermutePlanInfo": (_I, [_I, _I, _P(_I), _P(_I), _P(_I)]),
     "tcKernelLaunchCount": (C.c_ulonglong, []),
     "tcLastErrorString": (_S, []),

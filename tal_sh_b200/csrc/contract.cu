@@ -723,6 +723,39 @@ int contract_launch(int kind, const int *cptrn, int drank, const int *ddims, int
 
 }  // namespace tb
 
+namespace tb {
+// Offset tables (m -> L, D; n -> R, D; k -> L, R) for callers that only need
+// the D scatter: bytes for given M, N, K, and a launch that builds them.
+size_t contract_tables_bytes(int64_t M, int64_t N, int64_t K) {
+  TableParams T;
+  std::memset(&T, 0, sizeof(T));
+  T.M = M; T.N = N; T.K = K;
+  return table_bytes(T);
+}
+
+int contract_build_tables(const int *cptrn, int drank, const int *ddims, int lrank, const int *ldims,
+                          int rrank, const int *rdims, void *tables, cudaStream_t st, int64_t &M,
+                          int64_t &N, int64_t &K, const int64_t **mD, const int64_t **nD) {
+  int rc = check_args(R8, cptrn, drank, ddims, lrank, ldims, rrank, rdims);
+  if (rc) return rc;
+  Analysis an;
+  if ((rc = analyze(cptrn, drank, ddims, lrank, ldims, rrank, rdims, an)) != 0) return rc;
+  if (an.hyper) return TALSH_NOT_IMPLEMENTED;
+  TableParams T = an.T;
+  int64_t *base = (int64_t *)tables;
+  T.mL = base; T.mD = T.mL + T.M; T.nR = T.mD + T.M; T.nD = T.nR + T.N; T.kL = T.nD + T.N; T.kR = T.kL + T.K;
+  const int64_t total = T.M + T.N + T.K;
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((total + 255) / 256, 4096));
+  build_tables_kernel<<<grid, 256, 0, st>>>(T);
+  note_launch();
+  if ((rc = check_launch("build_tables_kernel")) != 0) return rc;
+  M = T.M; N = T.N; K = T.K;
+  *mD = T.mD;
+  *nD = T.nD;
+  return TALSH_SUCCESS;
+}
+}  // namespace tb
+
 extern "C" size_t tcTensorContractScratch(int data_kind, const int *cptrn, int drank,
                                           const int *ddims, int lrank, const int *ldims,
                                           int rrank, const int *rdims) {

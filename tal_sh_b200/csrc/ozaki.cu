@@ -1,0 +1,465 @@
+// Split-precision R8 tensor contraction on the 5th-generation tensor cores.
+//
+// D = beta*D + alpha * sum_k A[m,k] B[k,n] in FP64 accuracy from exact int8
+// products (the Ozaki scheme with integer slices):
+//  1. L and R are permuted into row-major matrices A (M x K) and Bt (N x K)
+//     by the transpose kernel (k fastest, the same k order on both sides).
+//  2. Each row of A is scaled by a power of two 2^-e so that |x| < 1 and cut
+//     into S slices of 7 bits: x = sum_s a_s 2^(-7 s) + r, a_s in [-127, 127],
+//     |r| < 2^(-7 S).  Every step is exact in FP64 (scaling by 2^k, truncation
+//     and subtraction of the truncated part).  Bt likewise per row (column of B).
+//  3. For every anti-diagonal g = s + t (2 <= g <= S + 1) the products
+//     P_g = sum_{s+t=g} A_s Bt_t^T are exact int8 x int8 -> int32 sums.  One
+//     CTA keeps the S accumulators P_2 .. P_{S+1} of a 128 x 64 tile in tensor
+//     memory (S x 64 columns) and issues tcgen05.mma kind::i8 for all slice
+//     pairs of each 64-byte K block; shared-memory operands use the
+//     no-swizzle K-major canonical layout (8-row x 16-byte core matrices).
+//  4. The epilogue reads the accumulators (tcgen05.ld) and forms
+//     C = 2^(e_m + f_n) * sum_g 2^(-7 g) P_g in FP64, then D = alpha*C (+ D).
+// Slice pairs with s + t > S + 1 are dropped; with S = 6 the relative error
+// against an FP64 contraction is about sqrt(K) * 2^-46 for random data.
+// The int32 sums are exact while (S) * K * 127^2 < 2^31; longer contractions
+// are split into K chunks that accumulate into D.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+
+#include "common.h"
+
+namespace tb {
+int permute_launch_o2n(int kind, int rank, const int *dims, const int *o2n, const void *src, void *dst,
+                       cudaStream_t st);
+size_t contract_tables_bytes(int64_t M, int64_t N, int64_t K);
+int contract_build_tables(const int *cptrn, int drank, const int *ddims, int lrank, const int *ldims,
+                          int rrank, const int *rdims, void *tables, cudaStream_t st, int64_t &M,
+                          int64_t &N, int64_t &K, const int64_t **mD, const int64_t **nD);
+
+namespace {
+
+constexpr int kOzBM = 128;        // tile rows (m), the UMMA M
+constexpr int kOzBN = 64;         // tile columns (n), the UMMA N
+constexpr int kOzBK = 64;         // K bytes per stage (two UMMA K steps of 32)
+constexpr int kOzThreads = 128;   // four warps: loads, MMA issue (thread 0), epilogue
+constexpr int kOzStages = 2;
+constexpr int kOzMaxSlices = 7;
+constexpr uint32_t kSpinLimit = 1u << 22;  // bounded mbarrier waits (seconds at most)
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+// Shared-memory matrix descriptor: no swizzle, K-major.  Core matrices are
+// 8 rows x 16 bytes (128 contiguous bytes); lbo = byte distance between the
+// two 16-byte K halves of an MMA, sbo = byte distance between 8-row groups.
+__device__ __forceinline__ uint64_t make_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+// Instruction descriptor of kind::i8: int32 accumulator, signed A and B, both
+// K-major, M = 128, N = 64.
+constexpr uint32_t kIdescI8 = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kOzBN >> 3) << 17) |
+                              ((uint32_t)(kOzBM >> 4) << 24);
+
+__device__ __forceinline__ void mma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(kIdescI8), "r"(accumulate));
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t *bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                   smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try(uint64_t *bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.b32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Bounded wait: false (and the error flag set) when the phase never completes.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *err) {
+  for (uint32_t i = 0; i < kSpinLimit; ++i)
+    if (mbar_try(bar, parity)) return true;
+  atomicExch(err, 1);
+  return false;
+}
+
+__device__ __forceinline__ void cp16(uint32_t s, const void *g) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(g));
+}
+
+// Row split: one CTA per (padded) row; 256 threads.
+__global__ void __launch_bounds__(256) oz_split_rows(const double *__restrict__ X, int64_t rows,
+                                                     int64_t K, int64_t rows_p, int64_t Kp, int S,
+                                                     int8_t *__restrict__ slices, int32_t *expo) {
+  const int64_t r = blockIdx.x;
+  const int tid = threadIdx.x;
+  __shared__ double red[8];
+  __shared__ int e_sh;
+  const double *x = X + r * K;
+  double mx = 0.0;
+  if (r < rows)
+    for (int64_t k = tid; k < K; k += 256) mx = fmax(mx, fabs(x[k]));
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  if ((tid & 31) == 0) red[tid >> 5] = mx;
+  __syncthreads();
+  if (tid == 0) {
+    double m = 0.0;
+    for (int w = 0; w < 8; ++w) m = fmax(m, red[w]);
+    // m = f * 2^e with f in [0.5, 1): scaled entries lie in (-1, 1).
+    e_sh = (m > 0.0) ? ilogb(m) + 1 : 0;
+    expo[r] = e_sh;
+  }
+  __syncthreads();
+  const int e = e_sh;
+  const int64_t plane = rows_p * Kp;
+  for (int64_t k = tid; k < Kp; k += 256) {
+    double v = (r < rows && k < K) ? scalbn(x[k], -e) : 0.0;
+    for (int s = 0; s < S; ++s) {
+      const double y = v * 128.0;  // |y| < 128
+      const double t = trunc(y);   // in [-127, 127]
+      slices[s * plane + r * Kp + k] = (int8_t)(int)t;
+      v = y - t;                   // exact remainder, |v| < 1
+    }
+  }
+}
+
+struct OzArgs {
+  const int8_t *A;   // [S][Mp][Kp]
+  const int8_t *B;   // [S][Np][Kp]
+  int64_t Mp, Np, Kp;
+  int64_t kb0, kb1;  // K-block range [kb0, kb1) of this launch (64-byte blocks)
+  int S;
+  const int32_t *ea, *eb;
+  double *D;
+  const int64_t *mD, *nD;
+  int64_t M, N;
+  double alpha;
+  int beta;
+  int *err;
+  uint32_t tmem_cols;  // S x 64 columns of int32 accumulators, rounded up to a power of two
+};
+
+// Shared layout of one stage: S A-tiles (128 rows x 64 B) then S B-tiles (64 rows x 64 B),
+// each in the canonical K-major layout: offset(row, c) = c*(rows*16) + (row/8)*128 + (row%8)*16
+// for the 16-byte chunk c in 0..3.
+constexpr int kATileBytes = kOzBM * kOzBK;
+constexpr int kBTileBytes = kOzBN * kOzBK;
+
+__global__ void __launch_bounds__(kOzThreads, 1) oz_gemm_kernel(const OzArgs a) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ __align__(8) uint64_t mbar[kOzStages];
+  __shared__ uint32_t tmem_base_sh;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int S = a.S;
+  const int stage_bytes = S * (kATileBytes + kBTileBytes);
+  const int64_t tm = blockIdx.x, tn = blockIdx.y;
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(&tmem_base_sh)),
+                 "r"(a.tmem_cols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+  }
+  if (tid == 0) {
+    for (int s = 0; s < kOzStages; ++s)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[s])));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::);
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::);
+  const uint32_t tmem = tmem_base_sh;
+  const uint32_t sbase = smem_u32(smem);
+
+  auto load_stage = [&](int st, int64_t kb) {
+    const uint32_t sst = sbase + (uint32_t)(st * stage_bytes);
+    for (int s = 0; s < S; ++s) {
+      const int8_t *ga = a.A + (int64_t)s * a.Mp * a.Kp + (tm * kOzBM) * a.Kp + kb * kOzBK;
+      const uint32_t sa = sst + (uint32_t)(s * kATileBytes);
+      for (int i = tid; i < kOzBM * 4; i += kOzThreads) {  // 128 rows x 4 chunks
+        const int row = i >> 2, c = i & 3;
+        cp16(sa + c * (kOzBM * 16) + (row >> 3) * 128 + (row & 7) * 16, ga + (int64_t)row * a.Kp + c * 16);
+      }
+      const int8_t *gb = a.B + (int64_t)s * a.Np * a.Kp + (tn * kOzBN) * a.Kp + kb * kOzBK;
+      const uint32_t sb = sst + (uint32_t)(S * kATileBytes + s * kBTileBytes);
+      for (int i = tid; i < kOzBN * 4; i += kOzThreads) {  // 64 rows x 4 chunks
+        const int row = i >> 2, c = i & 3;
+        cp16(sb + c * (kOzBN * 16) + (row >> 3) * 128 + (row & 7) * 16, gb + (int64_t)row * a.Kp + c * 16);
+      }
+    }
+    asm volatile("cp.async.commit_group;\n" ::);
+  };
+
+  const int64_t nkb = a.kb1 - a.kb0;
+  bool ok = true;
+  load_stage(0, a.kb0);
+  for (int64_t it = 0; it < nkb; ++it) {
+    const int st = (int)(it & 1);
+    if (it + 1 < nkb) {
+      // The other stage was read by the MMAs of iteration it - 1.
+      if (it >= 1 && ok) ok = mbar_wait(&mbar[st ^ 1], (uint32_t)(((it - 1) >> 1) & 1), a.err);
+      load_stage(st ^ 1, a.kb0 + it + 1);
+      asm volatile("cp.async.wait_group 1;\n" ::);
+    } else {
+      asm volatile("cp.async.wait_group 0;\n" ::);
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (tid == 0 && ok) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::);
+      const uint32_t sst = sbase + (uint32_t)(st * stage_bytes);
+      for (int g = 2; g <= S + 1; ++g) {
+        const uint32_t dcol = tmem + (uint32_t)((g - 2) * kOzBN);
+        for (int s = 1; s < g; ++s) {
+          const int t = g - s;
+          const uint32_t sa = sst + (uint32_t)((s - 1) * kATileBytes);
+          const uint32_t sb = sst + (uint32_t)(S * kATileBytes + (t - 1) * kBTileBytes);
+#pragma unroll
+          for (int j = 0; j < 2; ++j) {  // two K steps of 32 bytes: chunks 2j, 2j+1
+            const uint64_t ad = make_desc(sa + j * 2 * (kOzBM * 16), kOzBM * 16, 128);
+            const uint64_t bd = make_desc(sb + j * 2 * (kOzBN * 16), kOzBN * 16, 128);
+            mma_i8(dcol, ad, bd, (it > 0 || s > 1 || j > 0) ? 1u : 0u);
+          }
+        }
+      }
+      mma_commit(&mbar[st]);
+    }
+  }
+  // All MMAs are done once the last commit has arrived (completion is in order).
+  if (nkb > 0 && ok) ok = mbar_wait(&mbar[(nkb - 1) & 1], (uint32_t)(((nkb - 1) >> 1) & 1), a.err);
+  ok = __syncthreads_and(ok) != 0;  // block-uniform: tcgen05.ld below is warp-collective
+  asm volatile("tcgen05.fence::after_thread_sync;" ::);
+
+  if (ok) {
+    // Epilogue: warp w owns TMEM lanes (tile rows) 32w .. 32w + 31.
+    const int64_t m = tm * kOzBM + warp * 32 + lane;
+    const bool mrow = m < a.M;
+    const int em = mrow ? a.ea[m] : 0;
+    const int64_t dm = mrow ? a.mD[m] : 0;
+    for (int c = 0; c < kOzBN / 16; ++c) {
+      double acc[16];
+#pragma unroll
+      for (int i = 0; i < 16; ++i) acc[i] = 0.0;
+      for (int g = 2; g <= S + 1; ++g) {
+        uint32_t v[16];
+        const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)((g - 2) * kOzBN + c * 16);
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+            : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+              "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]),
+              "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+            : "r"(taddr));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        const double w = scalbn(1.0, -7 * g);
+#pragma unroll
+        for (int i = 0; i < 16; ++i) acc[i] += (double)(int32_t)v[i] * w;
+      }
+      if (mrow) {
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+          const int64_t n = tn * kOzBN + c * 16 + i;
+          if (n < a.N) {
+            double *p = a.D + dm + a.nD[n];
+            const double val = a.alpha * scalbn(acc[i], em + a.eb[n]);
+            *p = a.beta ? (*p + val) : val;
+          }
+        }
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::);
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(a.tmem_cols));
+}
+
+int64_t round_up(int64_t x, int64_t a) { return (x + a - 1) / a * a; }
+
+struct OzPlan {
+  int64_t M, N, K, Mp, Np, Kp;
+  size_t off_A64, off_B64, off_As, off_Bs, off_ea, off_eb, off_tab, off_err, total;
+};
+
+void oz_plan(int64_t M, int64_t N, int64_t K, int S, OzPlan &p) {
+  p.M = M; p.N = N; p.K = K;
+  p.Mp = round_up(std::max<int64_t>(M, 1), kOzBM);
+  p.Np = round_up(std::max<int64_t>(N, 1), kOzBN);
+  p.Kp = round_up(std::max<int64_t>(K, 1), kOzBK);
+  size_t off = 0;
+  auto take = [&](size_t bytes) { const size_t o = off; off = (off + bytes + 255) & ~size_t(255); return o; };
+  p.off_A64 = take((size_t)M * K * 8);
+  p.off_B64 = take((size_t)N * K * 8);
+  p.off_As = take((size_t)S * p.Mp * p.Kp);
+  p.off_Bs = take((size_t)S * p.Np * p.Kp);
+  p.off_ea = take((size_t)p.Mp * 4);
+  p.off_eb = take((size_t)p.Np * 4);
+  p.off_tab = take(contract_tables_bytes(M, N, K));
+  p.off_err = take(16);
+  p.total = off;
+}
+
+// O2N of an operand into (k..., own uncontracted..., unit dims...), k in the
+// shared order (R's order when R leads with a contracted index and L does not
+// or R is larger, else L's -- the order the tables use as well).
+void operand_o2n(const int *cptrn, int lrank, const int *ldims, int rrank, const int *rdims,
+                 bool left, int *o2n) {
+  int64_t lvol = 1, rvol = 1;
+  for (int i = 0; i < lrank; ++i) lvol *= ldims[i];
+  for (int i = 0; i < rrank; ++i) rvol *= rdims[i];
+  const bool l_lead_k = lrank > 0 && cptrn[0] < 0;
+  const bool r_lead_k = rrank > 0 && cptrn[lrank] < 0;
+  const bool k_in_r_order = r_lead_k && (!l_lead_k || rvol > lvol);
+  const int rank = left ? lrank : rrank;
+  const int *dims = left ? ldims : rdims;
+  const int *pat = left ? cptrn : cptrn + lrank;
+  int kpos[kMaxRank];
+  for (int i = 0; i < rank; ++i) kpos[i] = -1;
+  int nk = 0;
+  if (k_in_r_order) {
+    for (int j = 0; j < rrank; ++j) {
+      const int v = cptrn[lrank + j];
+      if (v < 0 && rdims[j] > 1) {
+        const int li = -v - 1;
+        kpos[left ? li : j] = nk++;
+      }
+    }
+  } else {
+    for (int i = 0; i < lrank; ++i) {
+      const int v = cptrn[i];
+      if (v < 0 && ldims[i] > 1) {
+        const int rj = -v - 1;
+        kpos[left ? i : rj] = nk++;
+      }
+    }
+  }
+  int pos = nk;
+  for (int i = 0; i < rank; ++i)
+    if (pat[i] > 0 && dims[i] > 1) o2n[i] = ++pos;
+  for (int i = 0; i < rank; ++i) {
+    if (kpos[i] >= 0) o2n[i] = kpos[i] + 1;
+    else if (dims[i] <= 1) o2n[i] = ++pos;
+  }
+}
+
+}  // namespace
+
+size_t contract_split_scratch(int kind, const int *cptrn, int drank, const int *ddims, int lrank,
+                              const int *ldims, int rrank, const int *rdims, int slices) {
+  if (kind != R8 || lrank == 0 || rrank == 0 || drank == 0) return 0;
+  int64_t M = 1, N = 1, K = 1;
+  for (int i = 0; i < lrank; ++i) (cptrn[i] > 0 ? M : K) *= ldims[i];
+  for (int i = 0; i < rrank; ++i)
+    if (cptrn[lrank + i] > 0) N *= rdims[i];
+  if (slices <= 0) slices = 6;
+  OzPlan p;
+  oz_plan(M, N, K, slices, p);
+  return p.total;
+}
+
+int contract_split_launch(int kind, const int *cptrn, int drank, const int *ddims, int lrank,
+                          const int *ldims, int rrank, const int *rdims, void *D, const void *L,
+                          const void *R, double alpha_re, int accumulative, int slices, void *scratch,
+                          size_t scratch_bytes, void *stream) {
+  if (kind != R8) return TALSH_NOT_IMPLEMENTED;
+  if (lrank == 0 || rrank == 0 || drank == 0) return TALSH_NOT_IMPLEMENTED;
+  if (slices <= 0) slices = 6;
+  if (slices < 2 || slices > kOzMaxSlices) return TALSH_INVALID_ARGS;
+  if (D == nullptr || L == nullptr || R == nullptr || cptrn == nullptr) return TALSH_INVALID_ARGS;
+  const size_t need = contract_split_scratch(kind, cptrn, drank, ddims, lrank, ldims, rrank, rdims, slices);
+  if (need == 0 || scratch == nullptr || scratch_bytes < need) return TALSH_INVALID_ARGS;
+  cudaStream_t st = (cudaStream_t)stream;
+  char *base = (char *)scratch;
+  int64_t M, N, K;
+  const int64_t *mD = nullptr, *nD = nullptr;
+  OzPlan p;
+  {
+    int64_t M0 = 1, N0 = 1, K0 = 1;
+    for (int i = 0; i < lrank; ++i) (cptrn[i] > 0 ? M0 : K0) *= ldims[i];
+    for (int i = 0; i < rrank; ++i)
+      if (cptrn[lrank + i] > 0) N0 *= rdims[i];
+    oz_plan(M0, N0, K0, slices, p);
+  }
+  int rc = contract_build_tables(cptrn, drank, ddims, lrank, ldims, rrank, rdims, base + p.off_tab, st, M, N,
+                                 K, &mD, &nD);
+  if (rc) return rc;
+  if (M != p.M || N != p.N || K != p.K) return TALSH_NOT_IMPLEMENTED;  // hyper-indices or unit-only groups
+  int o2n[kMaxRank];
+  operand_o2n(cptrn, lrank, ldims, rrank, rdims, true, o2n);
+  if ((rc = permute_launch_o2n(R8, lrank, ldims, o2n, L, base + p.off_A64, st)) != 0) return rc;
+  operand_o2n(cptrn, lrank, ldims, rrank, rdims, false, o2n);
+  if ((rc = permute_launch_o2n(R8, rrank, rdims, o2n, R, base + p.off_B64, st)) != 0) return rc;
+  int8_t *As = (int8_t *)(base + p.off_As);
+  int8_t *Bs = (int8_t *)(base + p.off_Bs);
+  int32_t *ea = (int32_t *)(base + p.off_ea);
+  int32_t *eb = (int32_t *)(base + p.off_eb);
+  int *err = (int *)(base + p.off_err);
+  cudaMemsetAsync(err, 0, sizeof(int), st);
+  if (p.Mp > 0x7fffffffLL || p.Np > 0x7fffffffLL) return TALSH_LIMIT_EXCEEDED;
+  oz_split_rows<<<(unsigned)p.Mp, 256, 0, st>>>((const double *)(base + p.off_A64), M, K, p.Mp, p.Kp, slices,
+                                                As, ea);
+  note_launch();
+  oz_split_rows<<<(unsigned)p.Np, 256, 0, st>>>((const double *)(base + p.off_B64), N, K, p.Np, p.Kp, slices,
+                                                Bs, eb);
+  note_launch();
+  if ((rc = check_launch("oz_split_rows")) != 0) return rc;
+  // K chunks keep every int32 accumulator exact: slices * Kc * 127^2 < 2^31.
+  const int64_t kc_max = ((int64_t)0x7fffffff / ((int64_t)slices * 127 * 127)) / kOzBK;
+  const int64_t nkb = p.Kp / kOzBK;
+  const int smem = kOzStages * slices * (kATileBytes + kBTileBytes);
+  static bool attr_done = false;
+  if (!attr_done) {
+    cudaFuncSetAttribute(oz_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         kOzStages * kOzMaxSlices * (kATileBytes + kBTileBytes));
+    attr_done = true;
+  }
+  OzArgs a;
+  a.A = As; a.B = Bs; a.Mp = p.Mp; a.Np = p.Np; a.Kp = p.Kp; a.S = slices;
+  a.ea = ea; a.eb = eb; a.D = (double *)D; a.mD = mD; a.nD = nD; a.M = M; a.N = N;
+  a.alpha = alpha_re; a.err = err;
+  a.tmem_cols = 32;
+  while (a.tmem_cols < (uint32_t)(slices * kOzBN)) a.tmem_cols <<= 1;
+  const dim3 grid((unsigned)(p.Mp / kOzBM), (unsigned)(p.Np / kOzBN));
+  if (grid.y > 65535) return TALSH_LIMIT_EXCEEDED;
+  for (int64_t kb = 0; kb < nkb; kb += kc_max) {
+    a.kb0 = kb;
+    a.kb1 = std::min(nkb, kb + kc_max);
+    a.beta = (kb == 0) ? (accumulative ? 1 : 0) : 1;
+    oz_gemm_kernel<<<grid, kOzThreads, smem, st>>>(a);
+    note_launch();
+    if ((rc = check_launch("oz_gemm_kernel")) != 0) return rc;
+  }
+  return TALSH_SUCCESS;
+}
+
+}  // namespace tb
+
+extern "C" size_t tcTensorContractSplitScratch(int data_kind, const int *cptrn, int drank,
+                                               const int *ddims, int lrank, const int *ldims,
+                                               int rrank, const int *rdims, int slices) {
+  return tb::contract_split_scratch(data_kind, cptrn, drank, ddims, lrank, ldims, rrank, rdims, slices);
+}
+
+extern "C" int tcTensorContractSplit(int data_kind, const int *cptrn, int drank, const int *ddims,
+                                     int lrank, const int *ldims, int rrank, const int *rdims, void *D,
+                                     const void *L, const void *R, double alpha_re, double alpha_im,
+                                     int conj_bits, int accumulative, int slices, void *scratch,
+                                     size_t scratch_bytes, void *stream) {
+  (void)alpha_im;
+  (void)conj_bits;
+  return tb::contract_split_launch(data_kind, cptrn, drank, ddims, lrank, ldims, rrank, rdims, D, L, R,
+                                   alpha_re, accumulative, slices, scratch, scratch_bytes, stream);
+}

@@ -1232,6 +1232,13 @@ extern "C" int tcTensorPermuteAdd(int data_kind, int rank, const int *dims_in, c
 }
 
 namespace tb {
+// dst = permute(src) on a given stream, for the library's own staging steps.
+int permute_launch_o2n(int kind, int rank, const int *dims, const int *o2n, const void *src, void *dst,
+                       cudaStream_t st) {
+  ScaleArgs sc;
+  return permute_entry<kOpCopy>(kind, rank, dims, o2n, src, dst, 0, sc, (void *)st);
+}
+
 // dst (+)= permute(src) * (scalar_dev * alpha): the scalar-times-tensor case of a
 // contraction, with the scale combined on the device (no host round trip).
 int permute_scaled_by_device_scalar(int kind, int rank, const int *dims, const int *o2n,

@@ -27,6 +27,7 @@
 
 #include <chrono>
 #include <cmath>
+#include <atomic>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -41,6 +42,12 @@ int norm1_launch(int data_kind, size_t vol, const void *src, double *result_dev,
                  cudaStream_t st);
 size_t contract_scratch_bytes(int kind, const int *cptrn, int drank, const int *ddims, int lrank,
                               const int *ldims, int rrank, const int *rdims);
+size_t contract_split_scratch(int kind, const int *cptrn, int drank, const int *ddims, int lrank,
+                              const int *ldims, int rrank, const int *rdims, int slices);
+int contract_split_launch(int kind, const int *cptrn, int drank, const int *ddims, int lrank,
+                          const int *ldims, int rrank, const int *rdims, void *D, const void *L,
+                          const void *R, double alpha_re, int accumulative, int slices, void *scratch,
+                          size_t scratch_bytes, void *stream);
 int contract_launch(int kind, const int *cptrn, int drank, const int *ddims, int lrank,
                     const int *ldims, int rrank, const int *rdims, void *D, const void *L,
                     const void *R, double alpha_re, double alpha_im, int conj_bits,
@@ -75,6 +82,10 @@ struct Runtime {
 };
 Runtime R;
 std::recursive_mutex g_mu;
+// R8 contraction form: 0 = plain FP64 (the drop-in default), 2..7 = split
+// precision with that many int8 slices (TALSH_B200_R8_SLICES or
+// talshContractSlicesSet).
+std::atomic<int> g_r8_slices{0};
 
 int node_gpu_count() {
   int n = 0;
@@ -265,6 +276,7 @@ struct TaskRec {
   int nargs = 0;
   ArgRec a[MAX_TENSOR_OPERANDS];
   void *scratch = nullptr;
+  int split_slices = 0;  // > 0: the contraction runs in the split-precision form
   int failed = 0;
   bool finalized = false;
   double times[4] = {0, 0, 0, 0};  // total, comput, input, output (seconds)
@@ -486,7 +498,20 @@ int schedule(OpSpec &op, int dev_id, int dev_kind, talsh_task_t *user_task) {
     for (int i = 0; i < op.drank; ++i) dd[i] = op.t[0]->shape_p->dims[i];
     for (int i = 0; i < op.lrank; ++i) ld[i] = op.t[1]->shape_p->dims[i];
     for (int i = 0; i < op.rrank; ++i) rd[i] = op.t[2]->shape_p->dims[i];
-    scratch = contract_scratch_bytes(dkind, op.dig, op.drank, dd, op.lrank, ld, op.rrank, rd);
+    const int sl = g_r8_slices.load();
+    const size_t split = (sl > 0 && dkind == R8 && op.conj == 0)
+                             ? contract_split_scratch(dkind, op.dig, op.drank, dd, op.lrank, ld, op.rrank, rd, sl)
+                             : 0;
+    bool hyper = false;
+    for (int i = 0; i < op.lrank && !hyper; ++i)
+      for (int j = 0; j < op.rrank; ++j)
+        if (op.dig[i] > 0 && op.dig[i] == op.dig[op.lrank + j]) { hyper = true; break; }
+    if (split > 0 && !hyper) {
+      scratch = split;
+      tr->split_slices = sl;
+    } else {
+      scratch = contract_scratch_bytes(dkind, op.dig, op.drank, dd, op.lrank, ld, op.rrank, rd);
+    }
   } else if (op.kind == kOpNorm1) {
     scratch = tcTensorNorm1Scratch(shape_volume(op.t[0]->shape_p)) + 256;
   }
@@ -566,9 +591,14 @@ int schedule(OpSpec &op, int dev_id, int dev_kind, talsh_task_t *user_task) {
       }
       case kOpContract: {
         const int *dd = op.t[0]->shape_p->dims, *ld = op.t[1]->shape_p->dims, *rd = op.t[2]->shape_p->dims;
-        rc = contract_launch(dkind, op.dig, op.drank, dd, op.lrank, ld, op.rrank, rd, tr->a[0].dptr,
-                             tr->a[1].dptr, tr->a[2].dptr, op.sr, op.si, op.conj, op.accumulative,
-                             tr->scratch, scratch, st);
+        if (tr->split_slices > 0)
+          rc = contract_split_launch(dkind, op.dig, op.drank, dd, op.lrank, ld, op.rrank, rd, tr->a[0].dptr,
+                                     tr->a[1].dptr, tr->a[2].dptr, op.sr, op.accumulative, tr->split_slices,
+                                     tr->scratch, scratch, st);
+        else
+          rc = contract_launch(dkind, op.dig, op.drank, dd, op.lrank, ld, op.rrank, rd, tr->a[0].dptr,
+                               tr->a[1].dptr, tr->a[2].dptr, op.sr, op.si, op.conj, op.accumulative,
+                               tr->scratch, scratch, st);
         double m = 1.0, n = 1.0, kk = 1.0;
         for (int i = 0; i < op.lrank; ++i) (op.dig[i] > 0 ? m : kk) *= (double)ld[i];
         for (int i = 0; i < op.rrank; ++i) if (op.dig[op.lrank + i] > 0) n *= (double)rd[i];
@@ -799,6 +829,10 @@ int talshInit(size_t *host_buf_size, int *host_arg_max, int ngpus, int gpu_list[
     if (i > 0 && gpu_list[i] != gpu_list[i - 1] + 1) return TALSH_INVALID_ARGS;  // consecutive range
   }
   const char *env = std::getenv("TALSH_B200_GPU_BUDGET_BYTES");
+  if (const char *sl = std::getenv("TALSH_B200_R8_SLICES")) {
+    const int v = std::atoi(sl);
+    if (v == 0 || (v >= 2 && v <= 7)) g_r8_slices = v;
+  }
   for (int i = 0; i < ngpus; ++i) {
     const int g = gpu_list[i];
     GpuCtx &G = R.gpu[g];
@@ -1759,5 +1793,13 @@ double talshTensorNorm1(talsh_tens_t *t, int dev_id, int dev_kind) {
   return v;
 }
 double talshTensorNorm1_(talsh_tens_t *t, int dev_id, int dev_kind) { return talshTensorNorm1(t, dev_id, dev_kind); }
+
+int talshContractSlicesSet(int slices) {
+  if (slices != 0 && (slices < 2 || slices > 7)) return TALSH_INVALID_ARGS;
+  g_r8_slices = slices;
+  return TALSH_SUCCESS;
+}
+
+int talshContractSlicesGet(void) { return g_r8_slices.load(); }
 
 }  // extern "C"
