@@ -252,6 +252,53 @@ def profile_case(spec, op):
                           "gbs": moved / (e0.elapsed_time(e1) * 1e-3) / 1e9}))
 
 
+C3_PATTERNS = {"C3a": "D(a,b,i,j)+=L(a,b,c,d)*R(c,d,i,j)", "C3b": "D(a,b,i,j)+=L(a,k,c,i)*R(c,b,k,j)"}
+
+
+def c3_dims(name, v, o):
+    """Extents of D, L, R for the coupled-cluster shapes (a,b,c,d virtual; i,j,k occupied)."""
+    ext = dict(a=v, b=v, c=v, d=v, i=o, j=o, k=o)
+    labels = [t.split(",") for t in __import__("re").findall(r"\(([^)]*)\)", C3_PATTERNS[name])]
+    return [[ext[x] for x in g] for g in labels]
+
+
+def profile_contract(spec):
+    """One contraction of a C3 shape through the device ABI, four launches, for profilers."""
+    import torch
+    import tal_sh_b200 as T
+    parts = spec.split(":")
+    name, v, o = parts[0], int(parts[1]), int(parts[2])
+    slices = int(parts[3]) if len(parts) > 3 else 0
+    dd, ld, rd = c3_dims(name, v, o)
+    L = T.lib()
+    e, dig, dr, lr, rr, _ = T.parse_pattern(C3_PATTERNS[name])
+    args = (R8, T.ivec(dig), dr, T.ivec(dd), lr, T.ivec(ld), rr, T.ivec(rd))
+    g = torch.Generator(device="cuda")
+    g.manual_seed(7)
+    Lt = torch.randn(int(np.prod(ld)), dtype=torch.float64, device="cuda", generator=g)
+    Rt = torch.randn(int(np.prod(rd)), dtype=torch.float64, device="cuda", generator=g)
+    D = torch.zeros(int(np.prod(dd)), dtype=torch.float64, device="cuda")
+    need = L.tcTensorContractSplitScratch(*args, slices) if slices else L.tcTensorContractScratch(*args)
+    sc = torch.empty(max(need, 1), dtype=torch.uint8, device="cuda")
+    s = torch.cuda.current_stream().cuda_stream
+    kvol = np.sqrt(float(np.prod(ld)) * float(np.prod(rd)) / float(np.prod(dd)))  # contracted volume
+    flop = 2.0 * np.prod(dd) * kvol
+    for rep in range(4):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        if slices:
+            rc = L.tcTensorContractSplit(*args, D.data_ptr(), Lt.data_ptr(), Rt.data_ptr(), 1.0, 0.0, 0, 0, slices,
+                                         sc.data_ptr(), need, s)
+        else:
+            rc = L.tcTensorContract(*args, D.data_ptr(), Lt.data_ptr(), Rt.data_ptr(), 1.0, 0.0, 0, 0,
+                                    sc.data_ptr(), need, s)
+        e1.record()
+        torch.cuda.synchronize()
+        if rc != 0:
+            raise RuntimeError("contraction failed %d: %s" % (rc, L.tcLastErrorString()))
+        print(json.dumps({"case": spec, "rep": rep, "tflops": flop / (e0.elapsed_time(e1) * 1e-3) / 1e12}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -264,9 +311,15 @@ def main():
     ap.add_argument("--profile-case", default=None,
                     help="KIND:d1,d2,..:p1,p2,.. -- run one transpose four times (for ncu) and exit")
     ap.add_argument("--profile-op", default="copy", choices=["copy", "add"])
+    ap.add_argument("--profile-contract", default=None,
+                    help="C3a|C3b:v:o[:slices] -- run one FP64 contraction (plain, or split with slices) "
+                         "four times (for ncu) and exit")
     args = ap.parse_args()
     if args.profile_case:
         profile_case(args.profile_case, args.profile_op)
+        return
+    if args.profile_contract:
+        profile_contract(args.profile_contract)
         return
 
     world = int(os.environ.get("WORLD_SIZE", "1"))

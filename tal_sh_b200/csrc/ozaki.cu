@@ -20,10 +20,13 @@
 // against an FP64 contraction is about sqrt(K) * 2^-46 for random data.
 // The int32 sums are exact while (S) * K * 127^2 < 2^31; longer contractions
 // are split into K chunks that accumulate into D.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
+#include <mutex>
 
 #include "common.h"
 
@@ -55,6 +58,14 @@ __device__ __forceinline__ uint32_t smem_u32(const void *p) {
 __device__ __forceinline__ uint64_t make_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
   return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
          ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+// Shared-memory matrix descriptor, 32-byte swizzle, K-major: rows of 32 bytes
+// (one UMMA K step of int8) as written by a TMA box of {32 bytes, rows} with
+// CU_TENSOR_MAP_SWIZZLE_32B; 8-row groups 256 bytes apart.
+__device__ __forceinline__ uint64_t make_desc_sw32(uint32_t saddr) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | (1ull << 16) | ((uint64_t)(256 >> 4) << 32) | (1ull << 46) |
+         (6ull << 61);
 }
 
 // Instruction descriptor of kind::i8: int32 accumulator, signed A and B, both
@@ -287,7 +298,281 @@ __global__ void __launch_bounds__(kOzThreads, 1) oz_gemm_kernel(const OzArgs a) 
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(a.tmem_cols));
 }
 
+// ---------------------------------------------------------------------------
+// Warp-specialised mainloop.  Warp 0: one thread issues the TMA tile copies of
+// each stage (2-D tensor maps over the slice matrices, boxes of 16 bytes x
+// rows, which land exactly in the canonical K-major layout).  Warp 1: one
+// thread issues the MMAs of a stage once its copies have landed and commits
+// them to the stage's "empty" barrier; warp 1 also owns the tensor memory.
+// Warps 2-5: epilogue, TMEM lane quadrant (warp % 4).
+// ---------------------------------------------------------------------------
+constexpr int kOzWsThreads = 192;
+constexpr int kWsBK = 32;                    // K bytes per stage: one UMMA K step
+constexpr int kWsATile = kOzBM * kWsBK;      // 4 KB
+constexpr int kWsGroupM = 8;                 // m tiles per raster group (L2 reuse of A and B)
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void tma_load_2d(uint32_t sdst, const CUtensorMap *map, int x, int y,
+                                            uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+          sdst),
+      "l"((uint64_t)map), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
+}
+
+struct OzWsArgs {
+  int64_t Mp, Np;
+  int tiles_m, tiles_n;
+  int64_t kb0, kb1;
+  int S, nst;
+  const int32_t *ea, *eb;
+  double *D;
+  const int64_t *mD, *nD;
+  int64_t M, N;
+  double alpha;
+  int beta;
+  int *err;
+  uint32_t tmem_cols;
+};
+
+constexpr int kWsBN = 128;                    // tile columns of the pass kernel (UMMA N)
+constexpr int kWsBTile128 = kWsBN * kWsBK;    // 4 KB
+constexpr int kWsDiagPerPass = 3;             // accumulators per pass: 3 x 128 TMEM columns
+constexpr uint32_t kIdescI8N128 = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kWsBN >> 3) << 17) |
+                                  ((uint32_t)(kOzBM >> 4) << 24);
+
+__device__ __forceinline__ void mma_i8_n128(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
+                                            uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(kIdescI8N128), "r"(accumulate));
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// 128 x 128 output tile.  The anti-diagonals g = 2 .. S+1 are processed in
+// passes of up to three (3 x 128 int32 TMEM columns); pass p streams K once,
+// with only the slices its diagonals use, and its epilogue adds the pass's
+// contribution into D before the next pass reuses the accumulators.
+__global__ void __launch_bounds__(kOzWsThreads, 1)
+    oz_gemm_ws_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
+                      const OzWsArgs a) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  constexpr int kMaxStages = 8;
+  __shared__ __align__(8) uint64_t full[kMaxStages], empty[kMaxStages], done, drained;
+  __shared__ uint32_t tmem_base_sh;
+  __shared__ int abort_sh;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int S = a.S, nst = a.nst;
+  const int slot_bytes = S * (kWsATile + kWsBTile128);  // a stage slot holds the largest pass
+  const int npass = (S + kWsDiagPerPass - 1) / kWsDiagPerPass;
+  int tm, tn;
+  {
+    const int id = blockIdx.x;
+    const int per_group = kWsGroupM * a.tiles_n;
+    const int grp = id / per_group;
+    const int first_m = grp * kWsGroupM;
+    const int gm = min(kWsGroupM, a.tiles_m - first_m);
+    const int r = id - grp * per_group;
+    tm = first_m + r % gm;
+    tn = r / gm;
+  }
+  const int64_t nkb = a.kb1 - a.kb0;
+  auto pass_g0 = [&](int p) { return 2 + p * kWsDiagPerPass; };
+  auto pass_g1 = [&](int p) { return min(S + 1, pass_g0(p) + kWsDiagPerPass - 1); };
+
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(&tmem_base_sh)),
+                 "r"(a.tmem_cols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+  }
+  if (tid == 0) {
+    for (int i = 0; i < nst; ++i) {
+      mbar_init(&full[i], 1);
+      mbar_init(&empty[i], 1);
+    }
+    mbar_init(&done, 1);
+    mbar_init(&drained, 128);
+    abort_sh = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::);
+    asm volatile("prefetch.tensormap [%0];" ::"l"((uint64_t)&mapA) : "memory");
+    asm volatile("prefetch.tensormap [%0];" ::"l"((uint64_t)&mapB) : "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::);
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::);
+  const uint32_t tmem = tmem_base_sh;
+  const uint32_t sbase = (smem_u32(smem) + 1023u) & ~1023u;  // swizzled tiles need aligned bases
+
+  if (warp == 0) {
+    if (lane == 0) {
+      int64_t itg = 0;  // stage-ring iteration across passes
+      for (int p = 0; p < npass && !*(volatile int *)&abort_sh; ++p) {
+        const int smax = pass_g1(p) - 1;
+        const uint32_t bytes = (uint32_t)(smax * (kWsATile + kWsBTile128));
+        for (int64_t it = 0; it < nkb; ++it, ++itg) {
+          const int st = (int)(itg % nst);
+          if (itg >= nst && !mbar_wait(&empty[st], (uint32_t)(((itg / nst) - 1) & 1), a.err)) {
+            atomicExch(&abort_sh, 1);
+            break;
+          }
+          if (*(volatile int *)&abort_sh) break;
+          mbar_expect_tx(&full[st], bytes);
+          const uint32_t sst = sbase + (uint32_t)(st * slot_bytes);
+          const int kx = (int)((a.kb0 + it) * kWsBK);
+          for (int s = 0; s < smax; ++s) {
+            const uint32_t sa = sst + (uint32_t)(s * kWsATile);
+            const uint32_t sb = sst + (uint32_t)(S * kWsATile + s * kWsBTile128);
+            tma_load_2d(sa, &mapA, kx, (int)(s * a.Mp + tm * kOzBM), &full[st]);
+            tma_load_2d(sb, &mapB, kx, (int)(s * a.Np + tn * kWsBN), &full[st]);
+          }
+        }
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      int64_t itg = 0;
+      for (int p = 0; p < npass; ++p) {
+        if (p > 0 && !mbar_wait(&drained, (uint32_t)((p - 1) & 1), a.err)) atomicExch(&abort_sh, 1);
+        if (*(volatile int *)&abort_sh) {
+          mma_commit(&done);
+          continue;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::);
+        const int g0 = pass_g0(p), g1 = pass_g1(p);
+        for (int64_t it = 0; it < nkb; ++it, ++itg) {
+          const int st = (int)(itg % nst);
+          if (!mbar_wait(&full[st], (uint32_t)((itg / nst) & 1), a.err)) {
+            atomicExch(&abort_sh, 1);
+            break;
+          }
+          asm volatile("tcgen05.fence::after_thread_sync;" ::);
+          const uint32_t sst = sbase + (uint32_t)(st * slot_bytes);
+          for (int g = g0; g <= g1; ++g) {
+            const uint32_t dcol = tmem + (uint32_t)((g - g0) * kWsBN);
+            for (int s1 = 1; s1 < g; ++s1) {
+              const uint32_t sa = sst + (uint32_t)((s1 - 1) * kWsATile);
+              const uint32_t sb = sst + (uint32_t)(S * kWsATile + (g - s1 - 1) * kWsBTile128);
+              mma_i8_n128(dcol, make_desc_sw32(sa), make_desc_sw32(sb), (it > 0 || s1 > 1) ? 1u : 0u);
+            }
+          }
+          mma_commit(&empty[st]);
+        }
+        mma_commit(&done);  // this pass's accumulators are complete
+      }
+    }
+  } else {
+    const int q = warp & 3;
+    const int64_t m = (int64_t)tm * kOzBM + q * 32 + lane;
+    const bool mrow = m < a.M;
+    const int em = mrow ? a.ea[m] : 0;
+    const int64_t dm = mrow ? a.mD[m] : 0;
+    for (int p = 0; p < npass; ++p) {
+      bool ok = mbar_wait(&done, (uint32_t)(p & 1), a.err);
+      ok = ok && !*(volatile int *)&abort_sh;
+      ok = __all_sync(0xffffffffu, ok);
+      asm volatile("tcgen05.fence::after_thread_sync;" ::);
+      const int g0 = pass_g0(p), g1 = pass_g1(p);
+      const bool first = (p == 0);
+      if (ok) {
+        for (int c = 0; c < kWsBN / 16; ++c) {
+          double acc[16];
+#pragma unroll
+          for (int i = 0; i < 16; ++i) acc[i] = 0.0;
+          for (int g = g0; g <= g1; ++g) {
+            uint32_t v[16];
+            const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)((g - g0) * kWsBN + c * 16);
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+                  "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]),
+                  "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+                : "r"(taddr));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            const double w = scalbn(1.0, -7 * g);
+#pragma unroll
+            for (int i = 0; i < 16; ++i) acc[i] += (double)(int32_t)v[i] * w;
+          }
+          if (mrow) {
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+              const int64_t n = (int64_t)tn * kWsBN + c * 16 + i;
+              if (n < a.N) {
+                double *ptr = a.D + dm + a.nD[n];
+                const double val = a.alpha * scalbn(acc[i], em + a.eb[n]);
+                *ptr = (first && !a.beta) ? val : (*ptr + val);
+              }
+            }
+          }
+        }
+      }
+      asm volatile("tcgen05.fence::before_thread_sync;" ::);
+      mbar_arrive(&drained);
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::);
+  __syncthreads();
+  if (warp == 1)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(a.tmem_cols));
+}
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no -lcuda).
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *,
+                                  CUtensorMapInterleave, CUtensorMapSwizzle, CUtensorMapL2promotion,
+                                  CUtensorMapFloatOOBfill);
+EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (EncodeTiledFn)p;
+    cudaGetLastError();
+  });
+  return fn;
+}
+
+// 2-D map over a [rows][Kp] int8 matrix, box 32 bytes (one UMMA K step) x
+// box_rows, 32-byte swizzle (the layout make_desc_sw32 describes).
+bool make_slice_map(CUtensorMap *map, const void *base, int64_t Kp, int64_t rows, int box_rows) {
+  EncodeTiledFn fn = encode_fn();
+  if (fn == nullptr) return false;
+  const cuuint64_t dims[2] = {(cuuint64_t)Kp, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)Kp};
+  const cuuint32_t box[2] = {(cuuint32_t)kWsBK, (cuuint32_t)box_rows};
+  const cuuint32_t estr[2] = {1u, 1u};
+  return fn(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<void *>(base), dims, strides, box, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_32B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 int64_t round_up(int64_t x, int64_t a) { return (x + a - 1) / a * a; }
+
+constexpr int kOzWsSmem = 208 * 1024;  // dynamic shared bytes for the stage ring (+1 KB alignment slack)
+
+// TALSH_B200_SPLIT_SIMPLE=1 selects the single-loop kernel (for tests).
+bool oz_force_simple() {
+  static const bool v = [] {
+    const char *e = std::getenv("TALSH_B200_SPLIT_SIMPLE");
+    return e && std::atoi(e) == 1;
+  }();
+  return v;
+}
 
 struct OzPlan {
   int64_t M, N, K, Mp, Np, Kp;
@@ -297,7 +582,7 @@ struct OzPlan {
 void oz_plan(int64_t M, int64_t N, int64_t K, int S, OzPlan &p) {
   p.M = M; p.N = N; p.K = K;
   p.Mp = round_up(std::max<int64_t>(M, 1), kOzBM);
-  p.Np = round_up(std::max<int64_t>(N, 1), kOzBN);
+  p.Np = round_up(std::max<int64_t>(N, 1), 128);  // multiple of both kernels' tile width
   p.Kp = round_up(std::max<int64_t>(K, 1), kOzBK);
   size_t off = 0;
   auto take = [&](size_t bytes) { const size_t o = off; off = (off + bytes + 255) & ~size_t(255); return o; };
@@ -434,6 +719,41 @@ int contract_split_launch(int kind, const int *cptrn, int drank, const int *ddim
   while (a.tmem_cols < (uint32_t)(slices * kOzBN)) a.tmem_cols <<= 1;
   const dim3 grid((unsigned)(p.Mp / kOzBM), (unsigned)(p.Np / kOzBN));
   if (grid.y > 65535) return TALSH_LIMIT_EXCEEDED;
+  // Warp-specialised TMA pipeline when the tensor maps can be encoded (the
+  // slice matrices' row counts must fit the 32-bit TMA coordinates).
+  CUtensorMap mapA, mapB;
+  const bool ws = !oz_force_simple() && (int64_t)slices * p.Mp < 0x7fffffffLL &&
+                  (int64_t)slices * p.Np < 0x7fffffffLL && make_slice_map(&mapA, As, p.Kp, slices * p.Mp, kOzBM) &&
+                  make_slice_map(&mapB, Bs, p.Kp, slices * p.Np, kWsBN);
+  if (ws) {
+    const int stage_bytes = slices * (kWsATile + kWsBTile128);
+    const int nst = std::max(2, std::min(8, kOzWsSmem / stage_bytes));
+    const int64_t nkb32 = p.Kp / kWsBK, kc32 = kc_max * (kOzBK / kWsBK);
+    const int64_t tiles = (p.Mp / kOzBM) * (p.Np / kWsBN);
+    if (tiles > 0x7fffffffLL) return TALSH_LIMIT_EXCEEDED;
+    static bool ws_attr = false;
+    if (!ws_attr) {
+      cudaFuncSetAttribute(oz_gemm_ws_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kOzWsSmem + 1024);
+      ws_attr = true;
+    }
+    OzWsArgs w;
+    w.Mp = p.Mp; w.Np = p.Np; w.S = slices; w.nst = nst;
+    w.tiles_m = (int)(p.Mp / kOzBM);
+    w.tiles_n = (int)(p.Np / kWsBN);
+    w.ea = ea; w.eb = eb; w.D = (double *)D; w.mD = mD; w.nD = nD; w.M = M; w.N = N;
+    w.alpha = alpha_re; w.err = err;
+    w.tmem_cols = 32;
+    while (w.tmem_cols < (uint32_t)(std::min(slices, kWsDiagPerPass) * kWsBN)) w.tmem_cols <<= 1;
+    for (int64_t kb = 0; kb < nkb32; kb += kc32) {
+      w.kb0 = kb;
+      w.kb1 = std::min(nkb32, kb + kc32);
+      w.beta = (kb == 0) ? (accumulative ? 1 : 0) : 1;
+      oz_gemm_ws_kernel<<<(unsigned)tiles, kOzWsThreads, nst * stage_bytes + 1024, st>>>(mapA, mapB, w);
+      note_launch();
+      if ((rc = check_launch("oz_gemm_ws_kernel")) != 0) return rc;
+    }
+    return TALSH_SUCCESS;
+  }
   for (int64_t kb = 0; kb < nkb; kb += kc_max) {
     a.kb0 = kb;
     a.kb1 = std::min(nkb, kb + kc_max);

@@ -117,3 +117,26 @@ def test_split_through_talsh_contract(talsh):
     finally:
         assert L.talshContractSlicesSet(0) == 0
     assert rel_err(D - D0, ref - D0) <= TOL_SPLIT6
+
+
+def test_split_single_loop_kernel():
+    """The single-loop kernel (used when tensor maps cannot be encoded) gives the
+    same accuracy; forced in a child process."""
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    code = r"""
+import sys
+sys.path.insert(0, %r); sys.path.insert(0, %r)
+import torch
+import test_split_gpu as t
+for pat, ext in t.CASES[:3]:
+    err = t._run(torch, pat, ext, 6)
+    assert err <= t.TOL_SPLIT6, (pat, err)
+print("OK")
+""" % (root, os.path.join(root, "tests"))
+    env = dict(os.environ, TALSH_B200_SPLIT_SIMPLE="1")
+    p = subprocess.run([sys.executable, "-c", code], env=env, stdout=subprocess.PIPE, stderr=subprocess.STDOUT,
+                       text=True, timeout=600)
+    assert p.returncode == 0 and "OK" in p.stdout, p.stdout
