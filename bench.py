@@ -581,6 +581,26 @@ def bench_contractions(T, L, torch, dev):
     out["fp64_peak"] = {"tflops": dgemm_tflops, "source": "measured: cuBLAS DGEMM 8192^3 (torch.matmul float64)",
                         "nominal_tflops": 40.0}
     del a, b
+    # int8 tensor denominator for the split form: cuBLAS int8 GEMM (torch._int_mm) at 8192^3.
+    int8_tops = None
+    try:
+        a8 = torch.randint(-127, 128, (8192, 8192), dtype=torch.int8, device=dev)
+        b8 = torch.randint(-127, 128, (8192, 8192), dtype=torch.int8, device=dev)
+        torch._int_mm(a8, b8)
+        torch.cuda.synchronize(dev)
+        e0.record()
+        for _ in range(5):
+            torch._int_mm(a8, b8)
+        e1.record()
+        torch.cuda.synchronize(dev)
+        int8_tops = 5 * 2.0 * 8192 ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e12
+        del a8, b8
+    except Exception as exc:  # no int8 GEMM in this torch build
+        print("int8 reference GEMM unavailable: %s" % exc, file=sys.stderr)
+    out["int8_peak"] = {"tops": int8_tops, "source": "measured: cuBLAS int8 GEMM 8192^3 (torch._int_mm)",
+                        "nominal_tops": 4500.0}
+    slices = 6
+    products = slices * (slices + 1) // 2  # int8 slice products per FP64 product
     specs = [("C1", "D(a,b,i,j)+=L(a,k,c,i)*R(c,b,k,j)", [32] * 4, [32] * 4, [32] * 4, 20),
              ("C3b", "D(a,b,i,j)+=L(a,k,c,i)*R(c,b,k,j)", [192, 192, 64, 64], [192, 64, 192, 64],
               [192, 192, 64, 64], 3),
@@ -617,13 +637,16 @@ def bench_contractions(T, L, torch, dev):
         flops = 2.0 * np.prod(dd) * kvol
         run = lambda: L.talshTensorContract(pat.encode(), C.byref(tens[0]), C.byref(tens[1]), C.byref(tens[2]),
                                            1.0, 0.0, gpu, T.DEV_NULL, T.COPY_MTT, T.NOPE, None)
-        assert run() == 0
-        torch.cuda.synchronize(dev)
-        t0 = time.perf_counter()
-        for _ in range(reps):
+
+        def timed():
             assert run() == 0
-        torch.cuda.synchronize(dev)
-        dt = (time.perf_counter() - t0) / reps
+            torch.cuda.synchronize(dev)
+            t0 = time.perf_counter()
+            for _ in range(reps):
+                assert run() == 0
+            torch.cuda.synchronize(dev)
+            return (time.perf_counter() - t0) / reps
+        dt = timed()
         # FP64 reference on the GPU (torch einsum over cuBLAS DGEMM), outside the timing.
         import re
         toks = re.findall(r"\(([^)]*)\)", pat)
@@ -640,6 +663,19 @@ def bench_contractions(T, L, torch, dev):
         out[name] = {"pattern": pat, "tflops": flops / dt / 1e12, "frac_of_dgemm": flops / dt / 1e12 / dgemm_tflops,
                      "ms": dt * 1e3, "flop": flops,
                      "rel_err_vs_fp64": err, "dtype": "f64", "path": "talshTensorContract, GPU-resident"}
+        # The same contraction in the split-precision form (int8 slices on tcgen05).
+        assert L.talshContractSlicesSet(slices) == 0
+        try:
+            dts = timed()
+        finally:
+            assert L.talshContractSlicesSet(0) == 0
+        errs = float(torch.linalg.norm(got - ref) / torch.linalg.norm(ref))
+        tops = flops * products / dts / 1e12
+        out[name + "_split%d" % slices] = {
+            "tflops_fp64_equiv": flops / dts / 1e12, "speedup_vs_plain": dt / dts, "ms": dts * 1e3,
+            "rel_err_vs_fp64": errs, "int8_tops_issued": tops,
+            "frac_of_int8_gemm": (tops / int8_tops) if int8_tops else None,
+            "path": "talshTensorContract with talshContractSlicesSet(%d), GPU-resident" % slices}
         for t in tens:
             L.talshTensorDestruct(C.byref(t))
         del views, ref, got, lv, rv
