@@ -95,6 +95,36 @@ int tcTensorContractSplit(int data_kind, const int *cptrn, int drank, const int 
                           int accumulative, int slices, void *scratch, size_t scratch_bytes,
                           void *stream);
 
+/* Batched contractions (many small tasks, one launch per tile configuration). */
+#define TC_BATCH_MAX_RANK 8
+typedef struct {
+  int data_kind;                      /* R4, R8, C4, C8 */
+  int drank, lrank, rrank;            /* each at most TC_BATCH_MAX_RANK */
+  int cptrn[2 * TC_BATCH_MAX_RANK];   /* digital pattern, lrank + rrank entries */
+  int ddims[TC_BATCH_MAX_RANK], ldims[TC_BATCH_MAX_RANK], rdims[TC_BATCH_MAX_RANK];
+  void *D;                            /* device pointers */
+  const void *L, *R;
+  double alpha_re, alpha_im;
+  int conj_bits, accumulative;
+} tcContractTask;
+
+/* Bytes of device scratch tcTensorContractBatch needs for these tasks (0 when
+ * a task is invalid). */
+size_t tcTensorContractBatchScratch(int ntasks, const tcContractTask *tasks);
+
+/* Runs every task with tcTensorContract's semantics.  The tasks' offset
+ * tables are built by one launch and the GEMM tiles of all tasks run in one
+ * persistent launch per tile configuration (DMMA 64x64 or 32x32 for R8, SIMT
+ * for R4/C4/C8), each CTA finding its task from a tile prefix sum (a full
+ * contraction is a 1 x 1 tile: its sum order differs from tcTensorContract's
+ * two-pass dot product); scalar operands and hyper-indices take the
+ * single-task path.
+ * Tasks must not write overlapping D regions (they run concurrently).  The
+ * north-star's batched form of gpu_tensor_block_contract_dlf; no reference
+ * counterpart (the reference schedules one task per call). */
+int tcTensorContractBatch(int ntasks, const tcContractTask *tasks, void *scratch, size_t scratch_bytes,
+                          void *stream);
+
 /* Size of the fixed scratch array behind tcTensorContractNoAlloc: 8 MiB per GPU. */
 #define TC_CONTRACT_NOALLOC_SCRATCH_BYTES ((size_t)8 << 20)
 

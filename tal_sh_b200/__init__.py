@@ -82,6 +82,19 @@ class Task(C.Structure):
                 ("flops", C.c_double), ("exec_time", C.c_double)]
 
 
+TC_BATCH_MAX_RANK = 8
+
+
+class ContractTask(C.Structure):
+    """tcContractTask (talsh_b200.h): one contraction of a batch, device pointers."""
+    _fields_ = [("data_kind", C.c_int), ("drank", C.c_int), ("lrank", C.c_int), ("rrank", C.c_int),
+                ("cptrn", C.c_int * (2 * TC_BATCH_MAX_RANK)), ("ddims", C.c_int * TC_BATCH_MAX_RANK),
+                ("ldims", C.c_int * TC_BATCH_MAX_RANK), ("rdims", C.c_int * TC_BATCH_MAX_RANK),
+                ("D", C.c_void_p), ("L", C.c_void_p), ("R", C.c_void_p),
+                ("alpha_re", C.c_double), ("alpha_im", C.c_double),
+                ("conj_bits", C.c_int), ("accumulative", C.c_int)]
+
+
 _P = C.POINTER
 _I, _D, _V, _S, _Z = C.c_int, C.c_double, C.c_void_p, C.c_char_p, C.c_size_t
 _PROTOS = {
@@ -151,6 +164,8 @@ _PROTOS = {
                                      _D, _I, _I, _V]),
     "tcTensorContractNoAllocMaxScratch": (_Z, []),
     "tcTensorContractSplitScratch": (_Z, [_I, _P(_I), _I, _P(_I), _I, _P(_I), _I, _P(_I), _I]),
+    "tcTensorContractBatchScratch": (_Z, [_I, _P(ContractTask)]),
+    "tcTensorContractBatch": (_I, [_I, _P(ContractTask), _V, _Z, _V]),
     "tcTensorContractSplit": (_I, [_I, _P(_I), _I, _P(_I), _I, _P(_I), _I, _P(_I), _V, _V, _V, _D, _D,
                                    _I, _I, _I, _V, _Z, _V]),
     "tcPermutePlanInfo": (_I, [_I, _I, _P(_I), _P(_I), _P(_I)]),

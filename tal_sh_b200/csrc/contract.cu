@@ -23,6 +23,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <vector>
 
 #include "common.h"
 
@@ -120,13 +121,14 @@ struct DmmaCfg {
                                  (size_t)(2 * BM + 2 * BN) * sizeof(int64_t);
 };
 
+// One BM x BN tile of a gather-GEMM (shared by the single-contraction kernel and
+// the batched one).
 template <int BM, int BN>
-__global__ void __launch_bounds__(DmmaCfg<BM, BN>::THREADS)
-    dgemm_gather_kernel(const double *__restrict__ L, const double *__restrict__ R, double *D,
-                        const GemmArgs a) {
+__device__ __forceinline__ void dmma_tile(const double *__restrict__ L, const double *__restrict__ R,
+                                          double *D, const GemmArgs &a, int tile_m, int tile_n,
+                                          unsigned char *smem) {
   using C = DmmaCfg<BM, BN>;
   constexpr int BK = C::BK, ST = C::STAGES, AP = C::AP, BP = C::BP, NT = C::THREADS;
-  extern __shared__ __align__(16) unsigned char smem[];
   double *As = reinterpret_cast<double *>(smem);
   double *Bs = As + ST * BK * AP;
   int64_t *mLs = reinterpret_cast<int64_t *>(Bs + ST * BK * BP);
@@ -135,7 +137,6 @@ __global__ void __launch_bounds__(DmmaCfg<BM, BN>::THREADS)
   int64_t *nDs = nRs + BN;
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int tile_m = blockIdx.x % a.tiles_m, tile_n = blockIdx.x / a.tiles_m;
   const int m0 = tile_m * BM, n0 = tile_n * BN;
   for (int i = tid; i < BM; i += NT) {
     const int m = m0 + i;
@@ -231,6 +232,14 @@ __global__ void __launch_bounds__(DmmaCfg<BM, BN>::THREADS)
   }
 }
 
+template <int BM, int BN>
+__global__ void __launch_bounds__(DmmaCfg<BM, BN>::THREADS)
+    dgemm_gather_kernel(const double *__restrict__ L, const double *__restrict__ R, double *D,
+                        const GemmArgs a) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  dmma_tile<BM, BN>(L, R, D, a, blockIdx.x % a.tiles_m, blockIdx.x / a.tiles_m, smem);
+}
+
 // ------------------------------------------------- R4 / C4 / C8: SIMT FMA
 template <typename T> struct Num;
 template <> struct Num<float> {
@@ -282,14 +291,13 @@ template <> struct Num<double2> {
 constexpr int kSBM = 64, kSBN = 64, kSBK = 16, kSThreads = 256;
 
 template <typename T>
-__global__ void __launch_bounds__(kSThreads)
-    gemm_gather_simt_kernel(const T *__restrict__ L, const T *__restrict__ R, T *D, const GemmArgs a) {
+__device__ __forceinline__ void simt_tile(const T *__restrict__ L, const T *__restrict__ R, T *D,
+                                          const GemmArgs &a, int tile_m, int tile_n) {
   using A = typename Num<T>::A;
   __shared__ A As[kSBK][kSBM + 1];
   __shared__ A Bs[kSBK][kSBN + 1];
   __shared__ int64_t mLs[kSBM], mDs[kSBM], nRs[kSBN], nDs[kSBN];
   const int tid = threadIdx.x;
-  const int tile_m = blockIdx.x % a.tiles_m, tile_n = blockIdx.x / a.tiles_m;
   const int m0 = tile_m * kSBM, n0 = tile_n * kSBN;
   for (int i = tid; i < kSBM; i += kSThreads) {
     const int m = m0 + i;
@@ -352,6 +360,12 @@ __global__ void __launch_bounds__(kSThreads)
       *p = Num<T>::out(acc[i][j], a.beta ? *p : T(), a.alpha_re, a.alpha_im, a.beta);
     }
   }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kSThreads)
+    gemm_gather_simt_kernel(const T *__restrict__ L, const T *__restrict__ R, T *D, const GemmArgs a) {
+  simt_tile<T>(L, R, D, a, blockIdx.x % a.tiles_m, blockIdx.x / a.tiles_m);
 }
 
 // ------------------------------------------------------ full contraction
@@ -770,4 +784,310 @@ extern "C" int tcTensorContract(int data_kind, const int *cptrn, int drank, cons
   return tb::contract_launch(data_kind, cptrn, drank, ddims, lrank, ldims, rrank, rdims, D, L, R,
                              alpha_re, alpha_im, conj_bits, accumulative, scratch, scratch_bytes,
                              stream);
+}
+
+// ---------------------------------------------------------------------------
+// Batched contractions: many (small) contractions in one table launch and one
+// persistent gather-GEMM launch per tile configuration.  Each task's compact
+// descriptor (index groups, strides, GEMM arguments, operand pointers) is
+// uploaded once; CTAs walk a flat list of tiles over all tasks of a
+// configuration and find their task by binary search in its tile prefix sums.
+// ---------------------------------------------------------------------------
+namespace tb {
+namespace {
+
+constexpr int kBMaxG = 8;  // max dimensions per index group of a batched task
+
+struct BatchDesc {
+  int nm, nn, nk;
+  int32_t mext[kBMaxG], next[kBMaxG], kext[kBMaxG];
+  int64_t mstrL[kBMaxG], mstrD[kBMaxG], nstrR[kBMaxG], nstrD[kBMaxG], kstrL[kBMaxG], kstrR[kBMaxG];
+  GemmArgs a;
+  const void *L, *R;
+  void *D;
+};
+
+// Tile configurations of the batch: 0 = DMMA 64x64, 1 = DMMA 32x32 (R8),
+// 2 = SIMT 64x64 (R4, C4, C8: one list per kind).
+enum : int { kCfgD64 = 0, kCfgD32 = 1, kCfgS4 = 2, kCfgS14 = 3, kCfgS18 = 4, kNumCfg = 5 };
+
+__global__ void __launch_bounds__(256) batch_tables_kernel(const BatchDesc *descs) {
+  const BatchDesc &d = descs[blockIdx.y];
+  const int64_t M = d.a.M, N = d.a.N, K = d.a.K;
+  const int64_t total = M + N + K;
+  int64_t *mL = const_cast<int64_t *>(d.a.mL), *mD = const_cast<int64_t *>(d.a.mD);
+  int64_t *nR = const_cast<int64_t *>(d.a.nR), *nD = const_cast<int64_t *>(d.a.nD);
+  int64_t *kL = const_cast<int64_t *>(d.a.kL), *kR = const_cast<int64_t *>(d.a.kR);
+  for (int64_t i = (int64_t)blockIdx.x * 256 + threadIdx.x; i < total; i += (int64_t)gridDim.x * 256) {
+    if (i < M) {
+      int64_t r = i, x = 0, y = 0;
+      for (int g = 0; g < d.nm; ++g) {
+        const int64_t c = r % d.mext[g];
+        r /= d.mext[g];
+        x += c * d.mstrL[g];
+        y += c * d.mstrD[g];
+      }
+      mL[i] = x;
+      mD[i] = y;
+    } else if (i < M + N) {
+      int64_t r = i - M, x = 0, y = 0;
+      for (int g = 0; g < d.nn; ++g) {
+        const int64_t c = r % d.next[g];
+        r /= d.next[g];
+        x += c * d.nstrR[g];
+        y += c * d.nstrD[g];
+      }
+      nR[i - M] = x;
+      nD[i - M] = y;
+    } else {
+      int64_t r = i - M - N, x = 0, y = 0;
+      for (int g = 0; g < d.nk; ++g) {
+        const int64_t c = r % d.kext[g];
+        r /= d.kext[g];
+        x += c * d.kstrL[g];
+        y += c * d.kstrR[g];
+      }
+      kL[i - M - N] = x;
+      kR[i - M - N] = y;
+    }
+  }
+}
+
+// Task owning flat tile w: largest j with prefix[j] <= w.
+__device__ __forceinline__ int find_task(const int64_t *prefix, int n, int64_t w) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (prefix[mid] <= w) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+template <int BM, int BN>
+__global__ void __launch_bounds__(DmmaCfg<BM, BN>::THREADS)
+    dmma_batch_kernel(const BatchDesc *descs, const int32_t *list, const int64_t *prefix, int n,
+                      int64_t total) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  for (int64_t w = blockIdx.x; w < total; w += gridDim.x) {
+    const int j = find_task(prefix, n, w);
+    const BatchDesc &d = descs[list[j]];
+    const GemmArgs a = d.a;
+    const int local = (int)(w - prefix[j]);
+    dmma_tile<BM, BN>((const double *)d.L, (const double *)d.R, (double *)d.D, a, local % a.tiles_m,
+                      local / a.tiles_m, smem);
+    __syncthreads();  // the next tile rewrites the shared run tables
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kSThreads)
+    simt_batch_kernel(const BatchDesc *descs, const int32_t *list, const int64_t *prefix, int n,
+                      int64_t total) {
+  for (int64_t w = blockIdx.x; w < total; w += gridDim.x) {
+    const int j = find_task(prefix, n, w);
+    const BatchDesc &d = descs[list[j]];
+    const GemmArgs a = d.a;
+    const int local = (int)(w - prefix[j]);
+    simt_tile<T>((const T *)d.L, (const T *)d.R, (T *)d.D, a, local % a.tiles_m, local / a.tiles_m);
+    __syncthreads();
+  }
+}
+
+struct BatchPlan {
+  std::vector<BatchDesc> descs;
+  std::vector<int> cfg;          // per task: configuration, or -1 = single-task fallback
+  std::vector<int64_t> tab_off;  // per task: offset of its tables (int64 elements)
+  std::vector<size_t> fb_scratch;
+  std::vector<size_t> fb_off;
+  std::vector<int32_t> list[kNumCfg];
+  std::vector<int64_t> prefix[kNumCfg];
+  size_t off_desc = 0, off_list[kNumCfg] = {}, off_prefix[kNumCfg] = {}, off_tab = 0, off_fb = 0, total = 0;
+};
+
+int batch_cfg_of(int kind, int64_t M, int64_t N) {
+  switch (kind) {
+    case R8: return (M >= 48 && N >= 48) ? kCfgD64 : kCfgD32;
+    case R4: return kCfgS4;
+    case C4: return kCfgS14;
+    default: return kCfgS18;
+  }
+}
+
+int batch_plan(int ntasks, const tcContractTask *tasks, BatchPlan &bp) {
+  if (ntasks < 0 || ntasks > 65535 || (ntasks > 0 && tasks == nullptr)) return TALSH_INVALID_ARGS;
+  bp.descs.assign(ntasks, BatchDesc());
+  bp.cfg.assign(ntasks, -1);
+  bp.tab_off.assign(ntasks, 0);
+  bp.fb_scratch.assign(ntasks, 0);
+  bp.fb_off.assign(ntasks, 0);
+  int64_t tab = 0;
+  for (int t = 0; t < ntasks; ++t) {
+    const tcContractTask &x = tasks[t];
+    if (x.drank > TC_BATCH_MAX_RANK || x.lrank > TC_BATCH_MAX_RANK || x.rrank > TC_BATCH_MAX_RANK)
+      return TALSH_INVALID_ARGS;
+    int rc = check_args(x.data_kind, x.cptrn, x.drank, x.ddims, x.lrank, x.ldims, x.rrank, x.rdims);
+    if (rc) return rc;
+    if (x.D == nullptr || x.L == nullptr || x.R == nullptr) return TALSH_INVALID_ARGS;
+    Analysis an;
+    bool batchable = x.lrank > 0 && x.rrank > 0;  // a full contraction (D of rank 0) is a 1 x 1 GEMM
+    if (batchable) {
+      if ((rc = analyze(x.cptrn, x.drank, x.ddims, x.lrank, x.ldims, x.rrank, x.rdims, an)) != 0) return rc;
+      batchable = !an.hyper && an.T.nm <= kBMaxG && an.T.nn <= kBMaxG && an.T.nk <= kBMaxG &&
+                  an.T.M <= 0x7fffffffLL && an.T.N <= 0x7fffffffLL && an.T.K <= 0x7fffffffLL;
+    }
+    if (!batchable) {  // scalar operands, hyper-indices: single-task path
+      bp.fb_scratch[t] = contract_scratch_bytes(x.data_kind, x.cptrn, x.drank, x.ddims, x.lrank, x.ldims,
+                                                x.rrank, x.rdims);
+      continue;
+    }
+    const TableParams &T = an.T;
+    BatchDesc &d = bp.descs[t];
+    d.nm = T.nm; d.nn = T.nn; d.nk = T.nk;
+    for (int g = 0; g < T.nm; ++g) { d.mext[g] = (int32_t)T.mext[g]; d.mstrL[g] = T.mstrL[g]; d.mstrD[g] = T.mstrD[g]; }
+    for (int g = 0; g < T.nn; ++g) { d.next[g] = (int32_t)T.next[g]; d.nstrR[g] = T.nstrR[g]; d.nstrD[g] = T.nstrD[g]; }
+    for (int g = 0; g < T.nk; ++g) { d.kext[g] = (int32_t)T.kext[g]; d.kstrL[g] = T.kstrL[g]; d.kstrR[g] = T.kstrR[g]; }
+    const bool cplx = kind_is_complex(x.data_kind);
+    int cl = 0, cr = 0;
+    if (cplx) {
+      int cb = x.conj_bits & 7;
+      if (cb & 1) cb ^= 7;
+      cl = (cb >> 1) & 1;
+      cr = (cb >> 2) & 1;
+    }
+    GemmArgs &a = d.a;
+    std::memset(&a, 0, sizeof(a));
+    a.M = (int)T.M; a.N = (int)T.N; a.K = (int)T.K;
+    a.alpha_re = x.alpha_re; a.alpha_im = cplx ? x.alpha_im : 0.0;
+    a.beta = x.accumulative ? 1 : 0;
+    a.a_along_m = an.a_along_m ? 1 : 0;
+    a.b_along_n = an.b_along_n ? 1 : 0;
+    a.conj_l = cl; a.conj_r = cr;
+    d.L = x.L; d.R = x.R; d.D = x.D;
+    const int c = batch_cfg_of(x.data_kind, T.M, T.N);
+    const int bm = (c == kCfgD32) ? 32 : 64, bn = bm;
+    a.tiles_m = (int)((T.M + bm - 1) / bm);
+    const int64_t tiles = (int64_t)a.tiles_m * ((T.N + bn - 1) / bn);
+    bp.cfg[t] = c;
+    bp.tab_off[t] = tab;
+    tab += 2 * (T.M + T.N + T.K);
+    auto &pl = bp.prefix[c];
+    if (pl.empty()) pl.push_back(0);
+    bp.list[c].push_back(t);
+    pl.push_back(pl.back() + tiles);
+  }
+  size_t off = 0;
+  auto take = [&](size_t bytes) { const size_t o = off; off = (off + bytes + 255) & ~size_t(255); return o; };
+  bp.off_desc = take(sizeof(BatchDesc) * (size_t)std::max(ntasks, 1));
+  for (int c = 0; c < kNumCfg; ++c) {
+    bp.off_list[c] = take(sizeof(int32_t) * bp.list[c].size());
+    bp.off_prefix[c] = take(sizeof(int64_t) * bp.prefix[c].size());
+  }
+  bp.off_tab = take(sizeof(int64_t) * (size_t)tab);
+  for (int t = 0; t < ntasks; ++t)
+    if (bp.cfg[t] < 0) bp.fb_off[t] = take(bp.fb_scratch[t]);
+  bp.total = off;
+  return TALSH_SUCCESS;
+}
+
+template <int BM, int BN>
+int launch_dmma_batch(const BatchPlan &bp, int c, char *base, cudaStream_t st) {
+  using C = DmmaCfg<BM, BN>;
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(dmma_batch_kernel<BM, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
+    attr = true;
+  }
+  const int64_t total = bp.prefix[c].back();
+  int bps = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, dmma_batch_kernel<BM, BN>, C::THREADS, C::SMEM) !=
+          cudaSuccess || bps < 1)
+    bps = 1;
+  cudaGetLastError();
+  const int64_t grid = std::min<int64_t>(total, (int64_t)sm_count_dev() * bps);
+  dmma_batch_kernel<BM, BN><<<(unsigned)grid, C::THREADS, C::SMEM, st>>>(
+      (const BatchDesc *)(base + bp.off_desc), (const int32_t *)(base + bp.off_list[c]),
+      (const int64_t *)(base + bp.off_prefix[c]), (int)bp.list[c].size(), total);
+  note_launch();
+  return check_launch("dmma_batch_kernel");
+}
+
+template <typename T>
+int launch_simt_batch(const BatchPlan &bp, int c, char *base, cudaStream_t st) {
+  const int64_t total = bp.prefix[c].back();
+  int bps = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, simt_batch_kernel<T>, kSThreads, 0) != cudaSuccess ||
+      bps < 1)
+    bps = 1;
+  cudaGetLastError();
+  const int64_t grid = std::min<int64_t>(total, (int64_t)sm_count_dev() * bps);
+  simt_batch_kernel<T><<<(unsigned)grid, kSThreads, 0, st>>>(
+      (const BatchDesc *)(base + bp.off_desc), (const int32_t *)(base + bp.off_list[c]),
+      (const int64_t *)(base + bp.off_prefix[c]), (int)bp.list[c].size(), total);
+  note_launch();
+  return check_launch("simt_batch_kernel");
+}
+
+}  // namespace
+}  // namespace tb
+
+extern "C" size_t tcTensorContractBatchScratch(int ntasks, const tcContractTask *tasks) {
+  tb::BatchPlan bp;
+  if (tb::batch_plan(ntasks, tasks, bp) != TALSH_SUCCESS) return 0;
+  return bp.total;
+}
+
+extern "C" int tcTensorContractBatch(int ntasks, const tcContractTask *tasks, void *scratch,
+                                     size_t scratch_bytes, void *stream) {
+  using namespace tb;
+  if (ntasks == 0) return TALSH_SUCCESS;
+  BatchPlan bp;
+  int rc = batch_plan(ntasks, tasks, bp);
+  if (rc) return rc;
+  if (scratch == nullptr || scratch_bytes < bp.total) return TALSH_INVALID_ARGS;
+  cudaStream_t st = (cudaStream_t)stream;
+  char *base = (char *)scratch;
+  int64_t *tabs = (int64_t *)(base + bp.off_tab);
+  int64_t max_entries = 0;
+  for (int t = 0; t < ntasks; ++t) {
+    if (bp.cfg[t] < 0) continue;
+    GemmArgs &a = bp.descs[t].a;
+    int64_t *p = tabs + bp.tab_off[t];
+    a.mL = p; a.mD = p + a.M; a.nR = a.mD + a.M; a.nD = a.nR + a.N; a.kL = a.nD + a.N; a.kR = a.kL + a.K;
+    max_entries = std::max<int64_t>(max_entries, (int64_t)a.M + a.N + a.K);
+  }
+  // Descriptors and work lists (pageable source: the copy is staged before it returns).
+  cudaError_t e = cudaMemcpyAsync(base + bp.off_desc, bp.descs.data(), sizeof(BatchDesc) * ntasks,
+                                  cudaMemcpyHostToDevice, st);
+  for (int c = 0; c < kNumCfg && e == cudaSuccess; ++c) {
+    if (bp.list[c].empty()) continue;
+    e = cudaMemcpyAsync(base + bp.off_list[c], bp.list[c].data(), sizeof(int32_t) * bp.list[c].size(),
+                        cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(base + bp.off_prefix[c], bp.prefix[c].data(), sizeof(int64_t) * bp.prefix[c].size(),
+                          cudaMemcpyHostToDevice, st);
+  }
+  if (e != cudaSuccess) {
+    note_cuda_error("batch descriptor upload", (int)e);
+    return TALSH_FAILURE;
+  }
+  if (max_entries > 0) {
+    const int gx = (int)std::max<int64_t>(1, std::min<int64_t>((max_entries + 255) / 256, 64));
+    batch_tables_kernel<<<dim3(gx, ntasks), 256, 0, st>>>((const BatchDesc *)(base + bp.off_desc));
+    note_launch();
+    if ((rc = check_launch("batch_tables_kernel")) != 0) return rc;
+  }
+  if (!bp.list[kCfgD64].empty() && (rc = launch_dmma_batch<64, 64>(bp, kCfgD64, base, st)) != 0) return rc;
+  if (!bp.list[kCfgD32].empty() && (rc = launch_dmma_batch<32, 32>(bp, kCfgD32, base, st)) != 0) return rc;
+  if (!bp.list[kCfgS4].empty() && (rc = launch_simt_batch<float>(bp, kCfgS4, base, st)) != 0) return rc;
+  if (!bp.list[kCfgS14].empty() && (rc = launch_simt_batch<float2>(bp, kCfgS14, base, st)) != 0) return rc;
+  if (!bp.list[kCfgS18].empty() && (rc = launch_simt_batch<double2>(bp, kCfgS18, base, st)) != 0) return rc;
+  for (int t = 0; t < ntasks; ++t) {
+    if (bp.cfg[t] >= 0) continue;
+    const tcContractTask &x = tasks[t];
+    rc = contract_launch(x.data_kind, x.cptrn, x.drank, x.ddims, x.lrank, x.ldims, x.rrank, x.rdims, x.D, x.L,
+                         x.R, x.alpha_re, x.alpha_im, x.conj_bits, x.accumulative,
+                         bp.fb_scratch[t] ? base + bp.fb_off[t] : nullptr, bp.fb_scratch[t], stream);
+    if (rc) return rc;
+  }
+  return TALSH_SUCCESS;
 }

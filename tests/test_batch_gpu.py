@@ -1,0 +1,111 @@
+"""Batched contractions (tcTensorContractBatch): every task equals the same
+contraction run alone through tcTensorContract, and the FP64 oracle."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import oracle as O
+import tal_sh_b200 as T
+from gpu_util import fort, rel_err
+
+pytestmark = pytest.mark.gpu
+
+NPT = {T.R4: np.float32, T.R8: np.float64, T.C4: np.complex64, T.C8: np.complex128}
+TOL = {T.R8: 1e-12, T.C8: 1e-12, T.R4: 2e-5, T.C4: 2e-5}
+
+
+def random_task(rng, kind, emax=24, vmax=1 << 16):
+    """Random contraction: L and R share nc contracted indices; D holds the rest in a random order."""
+    while True:
+        nc = int(rng.integers(1, 4))
+        lu = int(rng.integers(0, 4))
+        ru = int(rng.integers(0, 4))
+        if nc + lu < 1 or nc + ru < 1:
+            continue
+        ext = [int(x) for x in np.exp(rng.uniform(np.log(4), np.log(emax), nc + lu + ru)).round()]
+        c, l, r = list(range(nc)), list(range(nc, nc + lu)), list(range(nc + lu, nc + lu + ru))
+        Lidx = list(rng.permutation(c + l))
+        Ridx = list(rng.permutation(c + r))
+        Didx = list(rng.permutation(l + r))
+        vol = lambda idx: int(np.prod([ext[i] for i in idx])) if idx else 1
+        if max(vol(Lidx), vol(Ridx), vol(Didx)) <= vmax:
+            break
+    cptrn = []
+    for i in Lidx:
+        cptrn.append(Didx.index(i) + 1 if i not in c else -(Ridx.index(i) + 1))
+    for i in Ridx:
+        cptrn.append(Didx.index(i) + 1 if i not in c else -(Lidx.index(i) + 1))
+    dims = lambda idx: [ext[i] for i in idx]
+    return dict(kind=kind, cptrn=cptrn, dd=dims(Didx), ld=dims(Lidx), rd=dims(Ridx))
+
+
+def rnd(rng, dims, kind):
+    x = rng.uniform(-1, 1, dims) if dims else np.asarray(rng.uniform(-1, 1))
+    if kind in (T.C4, T.C8):
+        x = x + 1j * (rng.uniform(-1, 1, dims) if dims else rng.uniform(-1, 1))
+    return fort(np.asarray(x).astype(NPT[kind]))
+
+
+def test_batch_matches_single_and_oracle(talsh):
+    torch = pytest.importorskip("torch")
+    lib = T.lib()
+    rng = np.random.default_rng(2024)
+    kinds = [T.R8] * 60 + [T.C8] * 40 + [T.R4] * 10 + [T.C4] * 10
+    specs = [random_task(rng, k) for k in kinds]
+    # two more full contractions (1 x 1 tiles in the batch) and a scalar-by-tensor task (single-task path)
+    specs.append(dict(kind=T.R8, cptrn=[-2, -1, -2, -1], dd=[], ld=[9, 7], rd=[7, 9]))
+    specs.append(dict(kind=T.C8, cptrn=[-1, -1], dd=[], ld=[33], rd=[33]))
+    specs.append(dict(kind=T.R8, cptrn=[2, 1], dd=[5, 6], ld=[6, 5], rd=[]))
+    dev = lambda a: torch.from_numpy(np.asarray(a).ravel(order="F").copy()).cuda()
+    tasks = (T.ContractTask * len(specs))()
+    keep, singles = [], []
+    for t, sp in zip(tasks, specs):
+        kind = sp["kind"]
+        Lh, Rh, D0 = rnd(rng, sp["ld"], kind), rnd(rng, sp["rd"], kind), rnd(rng, sp["dd"], kind)
+        acc = bool(rng.integers(0, 2))
+        alpha = (0.5, 0.0) if kind in (T.R4, T.R8) else (0.5, -0.25)
+        d, l, r, d1 = dev(D0), dev(Lh), dev(Rh), dev(D0)
+        keep.append((sp, Lh, Rh, D0, acc, alpha, d, l, r, d1))
+        t.data_kind, t.drank, t.lrank, t.rrank = kind, len(sp["dd"]), len(sp["ld"]), len(sp["rd"])
+        for i, v in enumerate(sp["cptrn"]):
+            t.cptrn[i] = v
+        for arr, name in ((sp["dd"], "ddims"), (sp["ld"], "ldims"), (sp["rd"], "rdims")):
+            for i, v in enumerate(arr):
+                getattr(t, name)[i] = v
+        t.D, t.L, t.R = d.data_ptr(), l.data_ptr(), r.data_ptr()
+        t.alpha_re, t.alpha_im = alpha
+        t.conj_bits, t.accumulative = 0, 1 if acc else 0
+    need = lib.tcTensorContractBatchScratch(len(specs), tasks)
+    assert need > 0
+    scratch = torch.empty(need, dtype=torch.uint8, device="cuda")
+    s = torch.cuda.current_stream().cuda_stream
+    launches = lib.tcKernelLaunchCount()
+    assert lib.tcTensorContractBatch(len(specs), tasks, scratch.data_ptr(), need, s) == 0, lib.tcLastErrorString()
+    torch.cuda.synchronize()
+    batched_launches = lib.tcKernelLaunchCount() - launches
+    assert batched_launches <= 6 + 1  # tables + one launch per configuration + the scalar-by-tensor task
+    for sp, Lh, Rh, D0, acc, alpha, d, l, r, d1 in keep:
+        kind = sp["kind"]
+        args = (kind, T.ivec(sp["cptrn"]), len(sp["dd"]), T.ivec(sp["dd"]), len(sp["ld"]), T.ivec(sp["ld"]),
+                len(sp["rd"]), T.ivec(sp["rd"]))
+        ns = lib.tcTensorContractScratch(*args)
+        sc = torch.empty(max(ns, 1), dtype=torch.uint8, device="cuda")
+        assert lib.tcTensorContract(*args, d1.data_ptr(), l.data_ptr(), r.data_ptr(), alpha[0], alpha[1], 0,
+                                    1 if acc else 0, sc.data_ptr(), ns, s) == 0
+        torch.cuda.synchronize()
+        got, single = d.cpu().numpy(), d1.cpu().numpy()
+        if sp["dd"]:  # same tile arithmetic as the single-task path (its full contraction is a two-pass dot)
+            assert got.tobytes() == single.tobytes(), sp
+        ref = D0.copy(order="F")
+        assert O.tensor_contract(ref, Lh, Rh, sp["cptrn"], alpha[0], alpha[1], 0, acc) == 0
+        assert rel_err(got.reshape(ref.shape, order="F"), ref) <= TOL[kind], sp
+
+
+def test_batch_rejects_bad_tasks(talsh):
+    lib = T.lib()
+    tasks = (T.ContractTask * 1)()
+    tasks[0].data_kind, tasks[0].drank, tasks[0].lrank, tasks[0].rrank = T.R8, 9, 1, 1
+    assert lib.tcTensorContractBatchScratch(1, tasks) == 0
+    assert lib.tcTensorContractBatch(1, tasks, None, 0, None) == T.TALSH_INVALID_ARGS
+    assert lib.tcTensorContractBatch(0, tasks, None, 0, None) == 0
