@@ -532,6 +532,7 @@ def main():
     contract = None
     if not args.no_contract:
         contract = bench_contractions(T, L, torch, dev)
+        contract["C4_batch"] = bench_batch(T, L, torch, dev)
 
     del lbuf, dbuf
     peak, peak_kind = measured_peak()
@@ -680,6 +681,99 @@ def bench_contractions(T, L, torch, dev):
             L.talshTensorDestruct(C.byref(t))
         del views, ref, got, lv, rv
     return out
+
+
+def c4_tasks(seed=4096, ntasks=4096, cap=1 << 21):
+    """The C4 batch: operand ranks 2-6, 1-3 contracted indices, extents log-uniform in [4, 48],
+    random index orders, R8/C8 half and half, every operand at most 2^21 elements."""
+    rng = np.random.default_rng(seed)
+    out = []
+    while len(out) < ntasks:
+        nc = int(rng.integers(1, 4))
+        lrank, rrank = int(rng.integers(max(2, nc), 7)), int(rng.integers(max(2, nc), 7))
+        lu, ru = lrank - nc, rrank - nc
+        ext = [int(round(x)) for x in np.exp(rng.uniform(np.log(4), np.log(48), nc + lu + ru))]
+        c, lo, ro = list(range(nc)), list(range(nc, nc + lu)), list(range(nc + lu, nc + lu + ru))
+        Li, Ri, Di = list(rng.permutation(c + lo)), list(rng.permutation(c + ro)), list(rng.permutation(lo + ro))
+        vol = lambda idx: int(np.prod([ext[i] for i in idx])) if idx else 1
+        if max(vol(Li), vol(Ri), vol(Di)) > cap:
+            continue
+        cptrn = [Di.index(i) + 1 if i not in c else -(Ri.index(i) + 1) for i in Li] + \
+                [Di.index(i) + 1 if i not in c else -(Li.index(i) + 1) for i in Ri]
+        kind = R8 if len(out) % 2 == 0 else C8
+        out.append((kind, cptrn, [ext[i] for i in Di], [ext[i] for i in Li], [ext[i] for i in Ri],
+                    vol(lo) * vol(ro) * vol(c)))  # M * N * K
+    return out
+
+
+def bench_batch(T, L, torch, dev):
+    """C4: 4096 small contractions, batched (tcTensorContractBatch) vs one call per task."""
+    tasks = c4_tasks()
+    es = {R8: 8, C8: 16}
+    flops = sum((2.0 if k == R8 else 8.0) * mnk for k, _, _, _, _, mnk in tasks)
+    # inputs: one random pool shared read-only by all tasks; outputs: one region per task
+    maxin = max(max(int(np.prod(ld)), int(np.prod(rd))) * es[k] for k, _, _, ld, rd, _ in tasks)
+    pool = torch.empty(2 * maxin + 256, dtype=torch.uint8, device=dev)
+    pool.view(torch.float64).uniform_(-1.0, 1.0)
+    douts, off = [], 0
+    for k, _, dd, _, _, _ in tasks:
+        douts.append(off)
+        off += (max(1, int(np.prod(dd))) * es[k] + 255) // 256 * 256
+    dbuf = torch.zeros(off, dtype=torch.uint8, device=dev)
+    arr = (T.ContractTask * len(tasks))()
+    for t, (k, cp, dd, ld, rd, _), do in zip(arr, tasks, douts):
+        t.data_kind, t.drank, t.lrank, t.rrank = k, len(dd), len(ld), len(rd)
+        for i, v in enumerate(cp):
+            t.cptrn[i] = v
+        for i, v in enumerate(dd):
+            t.ddims[i] = v
+        for i, v in enumerate(ld):
+            t.ldims[i] = v
+        for i, v in enumerate(rd):
+            t.rdims[i] = v
+        t.D = dbuf.data_ptr() + do
+        t.L = pool.data_ptr()
+        t.R = pool.data_ptr() + maxin
+        t.alpha_re, t.alpha_im, t.conj_bits, t.accumulative = 1.0, 0.0, 0, 1
+    s = torch.cuda.current_stream(dev).cuda_stream
+    need = L.tcTensorContractBatchScratch(len(tasks), arr)
+    scratch = torch.empty(need, dtype=torch.uint8, device=dev)
+
+    def batched():
+        rc = L.tcTensorContractBatch(len(tasks), arr, scratch.data_ptr(), need, s)
+        if rc:
+            raise RuntimeError("batch failed %d: %s" % (rc, L.tcLastErrorString()))
+
+    single_need = max(L.tcTensorContractScratch(k, T.ivec(cp), len(dd), T.ivec(dd), len(ld), T.ivec(ld),
+                                                len(rd), T.ivec(rd)) for k, cp, dd, ld, rd, _ in tasks)
+    sscr = torch.empty(max(single_need, 1), dtype=torch.uint8, device=dev)
+    prepared = [(k, T.ivec(cp), len(dd), T.ivec(dd), len(ld), T.ivec(ld), len(rd), T.ivec(rd), t.D, t.L, t.R)
+                for (k, cp, dd, ld, rd, _), t in zip(tasks, arr)]
+
+    def per_task():
+        for k, cp, dr, dd, lr, ld, rr, rd, D, Lp, Rp in prepared:
+            rc = L.tcTensorContract(k, cp, dr, dd, lr, ld, rr, rd, D, Lp, Rp, 1.0, 0.0, 0, 1, sscr.data_ptr(),
+                                    single_need, s)
+            if rc:
+                raise RuntimeError("task failed %d" % rc)
+
+    res = {}
+    for name, fn in (("batched", batched), ("per_task", per_task)):
+        fn()
+        torch.cuda.synchronize(dev)
+        reps = 3
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            fn()
+        torch.cuda.synchronize(dev)
+        dt = (time.perf_counter() - t0) / reps
+        res[name] = {"ms": dt * 1e3, "tasks_per_s": len(tasks) / dt, "tflops": flops / dt / 1e12}
+    res["speedup"] = res["per_task"]["ms"] / res["batched"]["ms"]
+    res["config"] = ("4096 tasks, operand ranks 2-6, 1-3 contracted indices, extents log-uniform [4,48], "
+                     "R8/C8 alternating, operands <= 2^21 elements (seed 4096); timed host call to completion, "
+                     "descriptor upload included")
+    res["flop"] = flops
+    return res
 
 
 class _DevArray:

@@ -232,6 +232,157 @@ __device__ __forceinline__ void dmma_tile(const double *__restrict__ L, const do
   }
 }
 
+// Complex-double tile on the FP64 tensor pipe: real and imaginary parts are
+// gathered into separate shared planes and C_re += A_re B_re - A_im B_im,
+// C_im += A_re B_im + A_im B_re run as four DMMA products.
+template <int BM, int BN>
+struct ZmmaCfg {
+  using D = DmmaCfg<BM, BN>;
+  static constexpr size_t SMEM = 2 * (size_t)D::STAGES * D::BK * (D::AP + D::BP) * sizeof(double) +
+                                 (size_t)(2 * BM + 2 * BN) * sizeof(int64_t);
+};
+
+__device__ __forceinline__ void cp_async16(void *smem_lo, void *smem_hi, const void *gptr, bool valid) {
+  // one double2 element: real part to one plane, imaginary part to the other
+  cp_async8(smem_lo, gptr, valid);
+  cp_async8(smem_hi, (const char *)gptr + 8, valid);
+}
+
+template <int BM, int BN>
+__device__ __forceinline__ void zmma_tile(const double2 *__restrict__ L, const double2 *__restrict__ R,
+                                          double2 *D, const GemmArgs &a, int tile_m, int tile_n,
+                                          unsigned char *smem) {
+  using C = DmmaCfg<BM, BN>;
+  constexpr int BK = C::BK, ST = C::STAGES, AP = C::AP, BP = C::BP, NT = C::THREADS;
+  double *Ar = reinterpret_cast<double *>(smem);
+  double *Ai = Ar + ST * BK * AP;
+  double *Br = Ai + ST * BK * AP;
+  double *Bi = Br + ST * BK * BP;
+  int64_t *mLs = reinterpret_cast<int64_t *>(Bi + ST * BK * BP);
+  int64_t *mDs = mLs + BM;
+  int64_t *nRs = mDs + BM;
+  int64_t *nDs = nRs + BN;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int m0 = tile_m * BM, n0 = tile_n * BN;
+  for (int i = tid; i < BM; i += NT) {
+    const int m = m0 + i;
+    mLs[i] = m < a.M ? a.mL[m] : 0;
+    mDs[i] = m < a.M ? a.mD[m] : 0;
+  }
+  for (int i = tid; i < BN; i += NT) {
+    const int n = n0 + i;
+    nRs[i] = n < a.N ? a.nR[n] : 0;
+    nDs[i] = n < a.N ? a.nD[n] : 0;
+  }
+  __syncthreads();
+  const int numK = (a.K + BK - 1) / BK;
+  auto load_tile = [&](int kt, int s) {
+#pragma unroll
+    for (int i = 0; i < (BM * BK) / NT; ++i) {
+      const int idx = tid + i * NT;
+      const int ml = a.a_along_m ? (idx % BM) : (idx / BK);
+      const int kl = a.a_along_m ? (idx / BM) : (idx % BK);
+      const int m = m0 + ml, k = kt * BK + kl;
+      const bool v = (m < a.M) && (k < a.K);
+      const double2 *src = v ? (L + mLs[ml] + a.kL[k]) : L;
+      const int o = s * BK * AP + kl * AP + ml;
+      cp_async16(Ar + o, Ai + o, src, v);
+    }
+#pragma unroll
+    for (int i = 0; i < (BN * BK) / NT; ++i) {
+      const int idx = tid + i * NT;
+      const int nl = a.b_along_n ? (idx % BN) : (idx / BK);
+      const int kl = a.b_along_n ? (idx / BN) : (idx % BK);
+      const int n = n0 + nl, k = kt * BK + kl;
+      const bool v = (n < a.N) && (k < a.K);
+      const double2 *src = v ? (R + nRs[nl] + a.kR[k]) : R;
+      const int o = s * BK * BP + kl * BP + nl;
+      cp_async16(Br + o, Bi + o, src, v);
+    }
+  };
+  constexpr int FM = C::WM / 8, FN = C::WN / 8;
+  double cr[FM][FN][2], ci[FM][FN][2];
+#pragma unroll
+  for (int i = 0; i < FM; ++i)
+#pragma unroll
+    for (int j = 0; j < FN; ++j) cr[i][j][0] = cr[i][j][1] = ci[i][j][0] = ci[i][j][1] = 0.0;
+  const int wm0 = (warp % C::WARPS_M) * C::WM, wn0 = (warp / C::WARPS_M) * C::WN;
+  const int fr = lane >> 2, fc = lane & 3;
+  const double sl = a.conj_l ? -1.0 : 1.0, sr = a.conj_r ? -1.0 : 1.0;
+#pragma unroll
+  for (int s = 0; s < ST - 1; ++s) {
+    if (s < numK) load_tile(s, s);
+    cp_async_commit();
+  }
+  for (int kt = 0; kt < numK; ++kt) {
+    cp_async_wait<ST - 2>();
+    __syncthreads();
+    const int pre = kt + ST - 1;
+    if (pre < numK) load_tile(pre, pre % ST);
+    cp_async_commit();
+    const int so = (kt % ST);
+#pragma unroll
+    for (int ks = 0; ks < BK / 4; ++ks) {
+      double ar[FM], ai[FM], nai[FM], br[FN], bi[FN];
+#pragma unroll
+      for (int i = 0; i < FM; ++i) {
+        const int o = so * BK * AP + (ks * 4 + fc) * AP + wm0 + i * 8 + fr;
+        ar[i] = Ar[o];
+        ai[i] = sl * Ai[o];
+        nai[i] = -ai[i];
+      }
+#pragma unroll
+      for (int j = 0; j < FN; ++j) {
+        const int o = so * BK * BP + (ks * 4 + fc) * BP + wn0 + j * 8 + fr;
+        br[j] = Br[o];
+        bi[j] = sr * Bi[o];
+      }
+#pragma unroll
+      for (int i = 0; i < FM; ++i)
+#pragma unroll
+        for (int j = 0; j < FN; ++j) {
+          dmma_8x8x4(cr[i][j][0], cr[i][j][1], ar[i], br[j]);
+          dmma_8x8x4(cr[i][j][0], cr[i][j][1], nai[i], bi[j]);
+          dmma_8x8x4(ci[i][j][0], ci[i][j][1], ar[i], bi[j]);
+          dmma_8x8x4(ci[i][j][0], ci[i][j][1], ai[i], br[j]);
+        }
+    }
+  }
+  cp_async_wait<0>();
+  const double alr = a.alpha_re, ali = a.alpha_im;
+#pragma unroll
+  for (int i = 0; i < FM; ++i) {
+    const int ml = wm0 + i * 8 + fr;
+    if (m0 + ml >= a.M) continue;
+#pragma unroll
+    for (int j = 0; j < FN; ++j) {
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int nl = wn0 + j * 8 + fc * 2 + h;
+        if (n0 + nl >= a.N) continue;
+        double2 *p = D + mDs[ml] + nDs[nl];
+        const double vr = cr[i][j][h] * alr - ci[i][j][h] * ali;
+        const double vi = cr[i][j][h] * ali + ci[i][j][h] * alr;
+        if (a.beta) {
+          const double2 d = *p;
+          *p = make_double2(d.x + vr, d.y + vi);
+        } else {
+          *p = make_double2(vr, vi);
+        }
+      }
+    }
+  }
+  __syncthreads();  // the next tile of a persistent caller rewrites the shared planes
+}
+
+template <int BM, int BN>
+__global__ void __launch_bounds__(DmmaCfg<BM, BN>::THREADS)
+    zgemm_gather_kernel(const double2 *__restrict__ L, const double2 *__restrict__ R, double2 *D,
+                        const GemmArgs a) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  zmma_tile<BM, BN>(L, R, D, a, blockIdx.x % a.tiles_m, blockIdx.x / a.tiles_m, smem);
+}
+
 template <int BM, int BN>
 __global__ void __launch_bounds__(DmmaCfg<BM, BN>::THREADS)
     dgemm_gather_kernel(const double *__restrict__ L, const double *__restrict__ R, double *D,
@@ -863,33 +1014,41 @@ __device__ __forceinline__ int find_task(const int64_t *prefix, int n, int64_t w
   return lo;
 }
 
+// Dynamic work distribution: CTAs take the next flat tile from a counter; the
+// host orders the tasks by decreasing K (longest tiles first).
+__device__ __forceinline__ int64_t next_item(unsigned long long *ctr) {
+  __shared__ int64_t item;
+  __syncthreads();
+  if (threadIdx.x == 0) item = (int64_t)atomicAdd(ctr, 1ull);
+  __syncthreads();
+  return item;
+}
+
 template <int BM, int BN>
 __global__ void __launch_bounds__(DmmaCfg<BM, BN>::THREADS)
     dmma_batch_kernel(const BatchDesc *descs, const int32_t *list, const int64_t *prefix, int n,
-                      int64_t total) {
+                      int64_t total, unsigned long long *ctr) {
   extern __shared__ __align__(16) unsigned char smem[];
-  for (int64_t w = blockIdx.x; w < total; w += gridDim.x) {
+  for (int64_t w = next_item(ctr); w < total; w = next_item(ctr)) {
     const int j = find_task(prefix, n, w);
     const BatchDesc &d = descs[list[j]];
     const GemmArgs a = d.a;
     const int local = (int)(w - prefix[j]);
     dmma_tile<BM, BN>((const double *)d.L, (const double *)d.R, (double *)d.D, a, local % a.tiles_m,
                       local / a.tiles_m, smem);
-    __syncthreads();  // the next tile rewrites the shared run tables
   }
 }
 
 template <typename T>
 __global__ void __launch_bounds__(kSThreads)
     simt_batch_kernel(const BatchDesc *descs, const int32_t *list, const int64_t *prefix, int n,
-                      int64_t total) {
-  for (int64_t w = blockIdx.x; w < total; w += gridDim.x) {
+                      int64_t total, unsigned long long *ctr) {
+  for (int64_t w = next_item(ctr); w < total; w = next_item(ctr)) {
     const int j = find_task(prefix, n, w);
     const BatchDesc &d = descs[list[j]];
     const GemmArgs a = d.a;
     const int local = (int)(w - prefix[j]);
     simt_tile<T>((const T *)d.L, (const T *)d.R, (T *)d.D, a, local % a.tiles_m, local / a.tiles_m);
-    __syncthreads();
   }
 }
 
@@ -901,7 +1060,8 @@ struct BatchPlan {
   std::vector<size_t> fb_off;
   std::vector<int32_t> list[kNumCfg];
   std::vector<int64_t> prefix[kNumCfg];
-  size_t off_desc = 0, off_list[kNumCfg] = {}, off_prefix[kNumCfg] = {}, off_tab = 0, off_fb = 0, total = 0;
+  size_t off_desc = 0, off_list[kNumCfg] = {}, off_prefix[kNumCfg] = {}, off_tab = 0, off_fb = 0, off_ctr = 0,
+         total = 0;
 };
 
 int batch_cfg_of(int kind, int64_t M, int64_t N) {
@@ -970,10 +1130,21 @@ int batch_plan(int ntasks, const tcContractTask *tasks, BatchPlan &bp) {
     bp.cfg[t] = c;
     bp.tab_off[t] = tab;
     tab += 2 * (T.M + T.N + T.K);
-    auto &pl = bp.prefix[c];
-    if (pl.empty()) pl.push_back(0);
     bp.list[c].push_back(t);
-    pl.push_back(pl.back() + tiles);
+    (void)tiles;
+  }
+  // Longest tiles (largest K) first, then the tile prefix sums.
+  for (int c = 0; c < kNumCfg; ++c) {
+    auto &l = bp.list[c];
+    std::stable_sort(l.begin(), l.end(), [&](int x, int y) { return bp.descs[x].a.K > bp.descs[y].a.K; });
+    auto &pl = bp.prefix[c];
+    if (l.empty()) continue;
+    pl.push_back(0);
+    for (int t : l) {
+      const GemmArgs &a = bp.descs[t].a;
+      const int bn = (c == kCfgD32) ? 32 : 64;
+      pl.push_back(pl.back() + (int64_t)a.tiles_m * ((a.N + bn - 1) / bn));
+    }
   }
   size_t off = 0;
   auto take = [&](size_t bytes) { const size_t o = off; off = (off + bytes + 255) & ~size_t(255); return o; };
@@ -983,6 +1154,7 @@ int batch_plan(int ntasks, const tcContractTask *tasks, BatchPlan &bp) {
     bp.off_prefix[c] = take(sizeof(int64_t) * bp.prefix[c].size());
   }
   bp.off_tab = take(sizeof(int64_t) * (size_t)tab);
+  bp.off_ctr = take(sizeof(unsigned long long) * kNumCfg);
   for (int t = 0; t < ntasks; ++t)
     if (bp.cfg[t] < 0) bp.fb_off[t] = take(bp.fb_scratch[t]);
   bp.total = off;
@@ -1006,7 +1178,8 @@ int launch_dmma_batch(const BatchPlan &bp, int c, char *base, cudaStream_t st) {
   const int64_t grid = std::min<int64_t>(total, (int64_t)sm_count_dev() * bps);
   dmma_batch_kernel<BM, BN><<<(unsigned)grid, C::THREADS, C::SMEM, st>>>(
       (const BatchDesc *)(base + bp.off_desc), (const int32_t *)(base + bp.off_list[c]),
-      (const int64_t *)(base + bp.off_prefix[c]), (int)bp.list[c].size(), total);
+      (const int64_t *)(base + bp.off_prefix[c]), (int)bp.list[c].size(), total,
+      (unsigned long long *)(base + bp.off_ctr) + c);
   note_launch();
   return check_launch("dmma_batch_kernel");
 }
@@ -1022,7 +1195,8 @@ int launch_simt_batch(const BatchPlan &bp, int c, char *base, cudaStream_t st) {
   const int64_t grid = std::min<int64_t>(total, (int64_t)sm_count_dev() * bps);
   simt_batch_kernel<T><<<(unsigned)grid, kSThreads, 0, st>>>(
       (const BatchDesc *)(base + bp.off_desc), (const int32_t *)(base + bp.off_list[c]),
-      (const int64_t *)(base + bp.off_prefix[c]), (int)bp.list[c].size(), total);
+      (const int64_t *)(base + bp.off_prefix[c]), (int)bp.list[c].size(), total,
+      (unsigned long long *)(base + bp.off_ctr) + c);
   note_launch();
   return check_launch("simt_batch_kernel");
 }
@@ -1066,6 +1240,7 @@ extern "C" int tcTensorContractBatch(int ntasks, const tcContractTask *tasks, vo
       e = cudaMemcpyAsync(base + bp.off_prefix[c], bp.prefix[c].data(), sizeof(int64_t) * bp.prefix[c].size(),
                           cudaMemcpyHostToDevice, st);
   }
+  if (e == cudaSuccess) e = cudaMemsetAsync(base + bp.off_ctr, 0, sizeof(unsigned long long) * kNumCfg, st);
   if (e != cudaSuccess) {
     note_cuda_error("batch descriptor upload", (int)e);
     return TALSH_FAILURE;
