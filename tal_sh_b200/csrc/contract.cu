@@ -235,10 +235,15 @@ __device__ __forceinline__ void dmma_tile(const double *__restrict__ L, const do
 // Complex-double tile on the FP64 tensor pipe: real and imaginary parts are
 // gathered into separate shared planes and C_re += A_re B_re - A_im B_im,
 // C_im += A_re B_im + A_im B_re run as four DMMA products.
+// Warp tiles are 32 x 16: two accumulator sets (real, imaginary) per fragment.
 template <int BM, int BN>
 struct ZmmaCfg {
-  using D = DmmaCfg<BM, BN>;
-  static constexpr size_t SMEM = 2 * (size_t)D::STAGES * D::BK * (D::AP + D::BP) * sizeof(double) +
+  static constexpr int WM = 32, WN = 16;
+  static constexpr int WARPS_M = BM / WM, WARPS_N = BN / WN;
+  static constexpr int THREADS = WARPS_M * WARPS_N * 32;
+  static constexpr int BK = 16, STAGES = 3;
+  static constexpr int AP = BM + 8, BP = BN + 8;
+  static constexpr size_t SMEM = 2 * (size_t)STAGES * BK * (AP + BP) * sizeof(double) +
                                  (size_t)(2 * BM + 2 * BN) * sizeof(int64_t);
 };
 
@@ -252,7 +257,7 @@ template <int BM, int BN>
 __device__ __forceinline__ void zmma_tile(const double2 *__restrict__ L, const double2 *__restrict__ R,
                                           double2 *D, const GemmArgs &a, int tile_m, int tile_n,
                                           unsigned char *smem) {
-  using C = DmmaCfg<BM, BN>;
+  using C = ZmmaCfg<BM, BN>;
   constexpr int BK = C::BK, ST = C::STAGES, AP = C::AP, BP = C::BP, NT = C::THREADS;
   double *Ar = reinterpret_cast<double *>(smem);
   double *Ai = Ar + ST * BK * AP;
@@ -372,11 +377,10 @@ __device__ __forceinline__ void zmma_tile(const double2 *__restrict__ L, const d
       }
     }
   }
-  __syncthreads();  // the next tile of a persistent caller rewrites the shared planes
 }
 
 template <int BM, int BN>
-__global__ void __launch_bounds__(DmmaCfg<BM, BN>::THREADS)
+__global__ void __launch_bounds__(ZmmaCfg<BM, BN>::THREADS)
     zgemm_gather_kernel(const double2 *__restrict__ L, const double2 *__restrict__ R, double2 *D,
                         const GemmArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
@@ -740,6 +744,23 @@ int launch_dmma(const double *L, const double *R, double *D, GemmArgs ga, cudaSt
   return check_launch("dgemm_gather_kernel");
 }
 
+template <int BM, int BN>
+int launch_zmma(const double2 *L, const double2 *R, double2 *D, GemmArgs ga, cudaStream_t st) {
+  using Z = ZmmaCfg<BM, BN>;
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaFuncSetAttribute(zgemm_gather_kernel<BM, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)Z::SMEM);
+    attr_set = true;
+  }
+  ga.tiles_m = (ga.M + BM - 1) / BM;
+  const int64_t tiles = (int64_t)ga.tiles_m * ((ga.N + BN - 1) / BN);
+  if (tiles > 0x7fffffffLL) return TALSH_LIMIT_EXCEEDED;
+  zgemm_gather_kernel<BM, BN><<<(unsigned)tiles, Z::THREADS, Z::SMEM, st>>>(L, R, D, ga);
+  note_launch();
+  return check_launch("zgemm_gather_kernel");
+}
+
 template <typename T>
 int launch_simt(const void *L, const void *R, void *D, GemmArgs ga, cudaStream_t st) {
   ga.tiles_m = (ga.M + kSBM - 1) / kSBM;
@@ -882,7 +903,7 @@ int contract_launch(int kind, const int *cptrn, int drank, const int *ddims, int
     }
     case R4: return launch_simt<float>(L, R, D, ga, st);
     case C4: return launch_simt<float2>(L, R, D, ga, st);
-    default: return launch_simt<double2>(L, R, D, ga, st);
+    default: return launch_zmma<64, 64>((const double2 *)L, (const double2 *)R, (double2 *)D, ga, st);
   }
 }
 
@@ -960,7 +981,9 @@ struct BatchDesc {
 
 // Tile configurations of the batch: 0 = DMMA 64x64, 1 = DMMA 32x32 (R8),
 // 2 = SIMT 64x64 (R4, C4, C8: one list per kind).
-enum : int { kCfgD64 = 0, kCfgD32 = 1, kCfgS4 = 2, kCfgS14 = 3, kCfgS18 = 4, kNumCfg = 5 };
+enum : int { kCfgD64 = 0, kCfgD32 = 1, kCfgZ64 = 2, kCfgZ32 = 3, kCfgS4 = 4, kCfgS14 = 5, kNumCfg = 6 };
+// Square tile edge of a configuration.
+inline int cfg_tile(int c) { return (c == kCfgD32 || c == kCfgZ32) ? 32 : 64; }
 
 __global__ void __launch_bounds__(256) batch_tables_kernel(const BatchDesc *descs) {
   const BatchDesc &d = descs[blockIdx.y];
@@ -1024,8 +1047,12 @@ __device__ __forceinline__ int64_t next_item(unsigned long long *ctr) {
   return item;
 }
 
+// Resident CTAs per SM asked of the compiler for the persistent batch kernels.
+template <int BM, int BN> struct BatchOcc { static constexpr int D = 1, Z = 1; };
+template <> struct BatchOcc<64, 64> { static constexpr int D = 1, Z = 2; };
+
 template <int BM, int BN>
-__global__ void __launch_bounds__(DmmaCfg<BM, BN>::THREADS)
+__global__ void __launch_bounds__(DmmaCfg<BM, BN>::THREADS, BatchOcc<BM, BN>::D)
     dmma_batch_kernel(const BatchDesc *descs, const int32_t *list, const int64_t *prefix, int n,
                       int64_t total, unsigned long long *ctr) {
   extern __shared__ __align__(16) unsigned char smem[];
@@ -1035,6 +1062,21 @@ __global__ void __launch_bounds__(DmmaCfg<BM, BN>::THREADS)
     const GemmArgs a = d.a;
     const int local = (int)(w - prefix[j]);
     dmma_tile<BM, BN>((const double *)d.L, (const double *)d.R, (double *)d.D, a, local % a.tiles_m,
+                      local / a.tiles_m, smem);
+  }
+}
+
+template <int BM, int BN>
+__global__ void __launch_bounds__(ZmmaCfg<BM, BN>::THREADS, BatchOcc<BM, BN>::Z)
+    zmma_batch_kernel(const BatchDesc *descs, const int32_t *list, const int64_t *prefix, int n,
+                      int64_t total, unsigned long long *ctr) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  for (int64_t w = next_item(ctr); w < total; w = next_item(ctr)) {
+    const int j = find_task(prefix, n, w);
+    const BatchDesc &d = descs[list[j]];
+    const GemmArgs a = d.a;
+    const int local = (int)(w - prefix[j]);
+    zmma_tile<BM, BN>((const double2 *)d.L, (const double2 *)d.R, (double2 *)d.D, a, local % a.tiles_m,
                       local / a.tiles_m, smem);
   }
 }
@@ -1067,9 +1109,9 @@ struct BatchPlan {
 int batch_cfg_of(int kind, int64_t M, int64_t N) {
   switch (kind) {
     case R8: return (M >= 48 && N >= 48) ? kCfgD64 : kCfgD32;
+    case C8: return (M >= 48 && N >= 48) ? kCfgZ64 : kCfgZ32;
     case R4: return kCfgS4;
-    case C4: return kCfgS14;
-    default: return kCfgS18;
+    default: return kCfgS14;
   }
 }
 
@@ -1124,7 +1166,7 @@ int batch_plan(int ntasks, const tcContractTask *tasks, BatchPlan &bp) {
     a.conj_l = cl; a.conj_r = cr;
     d.L = x.L; d.R = x.R; d.D = x.D;
     const int c = batch_cfg_of(x.data_kind, T.M, T.N);
-    const int bm = (c == kCfgD32) ? 32 : 64, bn = bm;
+    const int bm = cfg_tile(c), bn = bm;
     a.tiles_m = (int)((T.M + bm - 1) / bm);
     const int64_t tiles = (int64_t)a.tiles_m * ((T.N + bn - 1) / bn);
     bp.cfg[t] = c;
@@ -1142,7 +1184,7 @@ int batch_plan(int ntasks, const tcContractTask *tasks, BatchPlan &bp) {
     pl.push_back(0);
     for (int t : l) {
       const GemmArgs &a = bp.descs[t].a;
-      const int bn = (c == kCfgD32) ? 32 : 64;
+      const int bn = cfg_tile(c);
       pl.push_back(pl.back() + (int64_t)a.tiles_m * ((a.N + bn - 1) / bn));
     }
   }
@@ -1161,27 +1203,47 @@ int batch_plan(int ntasks, const tcContractTask *tasks, BatchPlan &bp) {
   return TALSH_SUCCESS;
 }
 
+using BatchKernel = void (*)(const BatchDesc *, const int32_t *, const int64_t *, int, int64_t,
+                             unsigned long long *);
+
+// Persistent launch of one tensor-pipe batch kernel: as many CTAs as fit at once.
+int launch_tc_batch(BatchKernel k, int threads, size_t smem, const char *name, const BatchPlan &bp, int c,
+                    char *base, cudaStream_t st) {
+  const int64_t total = bp.prefix[c].back();
+  int bps = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k, threads, smem) != cudaSuccess || bps < 1) bps = 1;
+  cudaGetLastError();
+  const int64_t grid = std::min<int64_t>(total, (int64_t)sm_count_dev() * bps);
+  k<<<(unsigned)grid, threads, smem, st>>>(
+      (const BatchDesc *)(base + bp.off_desc), (const int32_t *)(base + bp.off_list[c]),
+      (const int64_t *)(base + bp.off_prefix[c]), (int)bp.list[c].size(), total,
+      (unsigned long long *)(base + bp.off_ctr) + c);
+  note_launch();
+  return check_launch(name);
+}
+
 template <int BM, int BN>
 int launch_dmma_batch(const BatchPlan &bp, int c, char *base, cudaStream_t st) {
   using C = DmmaCfg<BM, BN>;
   static bool attr = false;
   if (!attr) {
     cudaFuncSetAttribute(dmma_batch_kernel<BM, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
+    cudaFuncSetAttribute(dmma_batch_kernel<BM, BN>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     attr = true;
   }
-  const int64_t total = bp.prefix[c].back();
-  int bps = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, dmma_batch_kernel<BM, BN>, C::THREADS, C::SMEM) !=
-          cudaSuccess || bps < 1)
-    bps = 1;
-  cudaGetLastError();
-  const int64_t grid = std::min<int64_t>(total, (int64_t)sm_count_dev() * bps);
-  dmma_batch_kernel<BM, BN><<<(unsigned)grid, C::THREADS, C::SMEM, st>>>(
-      (const BatchDesc *)(base + bp.off_desc), (const int32_t *)(base + bp.off_list[c]),
-      (const int64_t *)(base + bp.off_prefix[c]), (int)bp.list[c].size(), total,
-      (unsigned long long *)(base + bp.off_ctr) + c);
-  note_launch();
-  return check_launch("dmma_batch_kernel");
+  return launch_tc_batch(dmma_batch_kernel<BM, BN>, C::THREADS, C::SMEM, "dmma_batch_kernel", bp, c, base, st);
+}
+
+template <int BM, int BN>
+int launch_zmma_batch(const BatchPlan &bp, int c, char *base, cudaStream_t st) {
+  using Z = ZmmaCfg<BM, BN>;
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(zmma_batch_kernel<BM, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Z::SMEM);
+    cudaFuncSetAttribute(zmma_batch_kernel<BM, BN>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    attr = true;
+  }
+  return launch_tc_batch(zmma_batch_kernel<BM, BN>, Z::THREADS, Z::SMEM, "zmma_batch_kernel", bp, c, base, st);
 }
 
 template <typename T>
@@ -1255,7 +1317,8 @@ extern "C" int tcTensorContractBatch(int ntasks, const tcContractTask *tasks, vo
   if (!bp.list[kCfgD32].empty() && (rc = launch_dmma_batch<32, 32>(bp, kCfgD32, base, st)) != 0) return rc;
   if (!bp.list[kCfgS4].empty() && (rc = launch_simt_batch<float>(bp, kCfgS4, base, st)) != 0) return rc;
   if (!bp.list[kCfgS14].empty() && (rc = launch_simt_batch<float2>(bp, kCfgS14, base, st)) != 0) return rc;
-  if (!bp.list[kCfgS18].empty() && (rc = launch_simt_batch<double2>(bp, kCfgS18, base, st)) != 0) return rc;
+  if (!bp.list[kCfgZ64].empty() && (rc = launch_zmma_batch<64, 64>(bp, kCfgZ64, base, st)) != 0) return rc;
+  if (!bp.list[kCfgZ32].empty() && (rc = launch_zmma_batch<32, 32>(bp, kCfgZ32, base, st)) != 0) return rc;
   for (int t = 0; t < ntasks; ++t) {
     if (bp.cfg[t] >= 0) continue;
     const tcContractTask &x = tasks[t];

@@ -84,7 +84,8 @@ def test_batch_matches_single_and_oracle(talsh):
     assert lib.tcTensorContractBatch(len(specs), tasks, scratch.data_ptr(), need, s) == 0, lib.tcLastErrorString()
     torch.cuda.synchronize()
     batched_launches = lib.tcKernelLaunchCount() - launches
-    assert batched_launches <= 6 + 1  # tables + one launch per configuration + the scalar-by-tensor task
+    # tables + one launch per tile configuration (six) + the scalar-by-tensor task
+    assert batched_launches <= 1 + 6 + 1
     for sp, Lh, Rh, D0, acc, alpha, d, l, r, d1 in keep:
         kind = sp["kind"]
         args = (kind, T.ivec(sp["cptrn"]), len(sp["dd"]), T.ivec(sp["dd"]), len(sp["ld"]), T.ivec(sp["ld"]),
