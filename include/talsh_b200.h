@@ -19,6 +19,7 @@
 #define TALSH_B200_CORE_H_
 
 #include <stddef.h>
+#include <stdint.h>
 
 #ifdef __cplusplus
 extern "C" {
@@ -114,8 +115,9 @@ size_t tcTensorContractBatchScratch(int ntasks, const tcContractTask *tasks);
 
 /* Runs every task with tcTensorContract's semantics.  The tasks' offset
  * tables are built by one launch and the GEMM tiles of all tasks run in one
- * persistent launch per tile configuration (DMMA 64x64 or 32x32 for R8, SIMT
- * for R4/C4/C8), each CTA finding its task from a tile prefix sum (a full
+ * persistent launch per tile configuration (FP64 tensor-pipe 64x64 or 32x32
+ * tiles for R8 and C8, SIMT for R4/C4), each CTA finding its task from a tile
+ * prefix sum (a full
  * contraction is a 1 x 1 tile: its sum order differs from tcTensorContract's
  * two-pass dot product); scalar operands and hyper-indices take the
  * single-task path.
@@ -124,6 +126,66 @@ size_t tcTensorContractBatchScratch(int ntasks, const tcContractTask *tasks);
  * counterpart (the reference schedules one task per call). */
 int tcTensorContractBatch(int ntasks, const tcContractTask *tasks, void *scratch, size_t scratch_bytes,
                           void *stream);
+
+/* ---------------------------------------------------------------- serving
+ * A contraction server on the current GPU: tasks arrive one by one
+ * (tcServerSubmit), wait for admission under a device-memory budget, and run
+ * as soon as their inputs are ready.  Small tasks are gathered into
+ * continuous batches (one tcTensorContractBatch-style launch set per batch,
+ * a new batch whenever a batch slot is free); tasks at or above a flop
+ * threshold run alone on a second stream, R8 ones in split precision when
+ * r8_slices > 0.  A task may take an operand from an earlier task's output
+ * (l_from / r_from), which the server allocates and keeps on the device
+ * until its declared consumers have completed.  Results do not depend on what
+ * else is in flight: every tile is computed by the same code in the same order
+ * whichever batch carries it.  Single scheduling thread (as the reference's
+ * task scheduler, tensor_algebra_gpu_nvidia.cu:205).  The reference has no
+ * serving layer; its per-call scheduling is talshTensorContract +
+ * talshTaskComplete (talshc.cpp:5073, :2336-2561). */
+typedef struct tcServer tcServer;
+typedef struct {
+  size_t budget_bytes;  /* device bytes for server-held outputs and scratch (0: 90% of free memory) */
+  int r8_slices;        /* 0: plain FP64 for large R8 tasks, 2..7: split precision with that many slices */
+  int max_batch;        /* tasks per batch launch (0: 4096) */
+  int max_inflight;     /* batches in flight at once (0: 2) */
+  double large_flop;    /* tasks with at least this many flops run alone (0: 1e10) */
+} tcServeConfig;
+typedef struct {
+  tcContractTask op;    /* op.D == NULL: the server allocates the output and overwrites it */
+  uint64_t l_from;      /* nonzero: L is the output of that earlier submission (op.L ignored) */
+  uint64_t r_from;      /* nonzero: R is the output of that earlier submission (op.R ignored) */
+  int consumers;        /* later submissions that will read this task's output */
+  int keep_output;      /* 1: a server-allocated output stays until tcServerRelease */
+} tcServeTask;
+typedef struct {
+  unsigned long long submitted, completed, failed, batches, batched_tasks, large_tasks, admission_waits;
+  size_t bytes_in_use, bytes_peak, budget_bytes;
+} tcServeStats;
+
+int tcServerCreate(const tcServeConfig *cfg, tcServer **srv);
+int tcServerDestroy(tcServer *srv);  /* waits for work in flight, frees everything */
+/* Queues one task; *id (nonzero) names it from then on. */
+int tcServerSubmit(tcServer *srv, const tcServeTask *task, uint64_t *id);
+/* One scheduling step: retires finished batches, admits queued tasks,
+ * launches ready ones.  Returns the number of tasks not yet completed. */
+int tcServerProgress(tcServer *srv);
+/* Pops up to max completed tasks: ids, submit-to-completion seconds, status
+ * (TALSH_SUCCESS or an error code).  Returns how many were written. */
+int tcServerPoll(tcServer *srv, int max, uint64_t *ids, double *latency_s, int *status);
+/* Runs tcServerProgress until every submitted task has completed. */
+int tcServerDrain(tcServer *srv);
+/* Device address of a completed task's server-held output. */
+int tcServerOutput(tcServer *srv, uint64_t id, void **ptr);
+/* Gives up a kept output (freed once its consumers have completed). */
+int tcServerRelease(tcServer *srv, uint64_t id);
+int tcServerGetStats(tcServer *srv, tcServeStats *stats);
+/* Replays n tasks arriving at arrival_s[i] seconds after the call (ascending):
+ * submits each on time, runs the scheduling loop in between, returns when all
+ * have completed.  l_from / r_from in these tasks are 1-based indices into the
+ * array.  ids[i] and latency_s[i] (either may be NULL) receive each task's id
+ * and submit-to-completion time.  Returns TALSH_SUCCESS or the first error. */
+int tcServerReplay(tcServer *srv, int n, const tcServeTask *tasks, const double *arrival_s, uint64_t *ids,
+                   double *latency_s);
 
 /* Size of the fixed scratch array behind tcTensorContractNoAlloc: 8 MiB per GPU. */
 #define TC_CONTRACT_NOALLOC_SCRATCH_BYTES ((size_t)8 << 20)

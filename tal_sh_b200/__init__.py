@@ -95,6 +95,26 @@ class ContractTask(C.Structure):
                 ("conj_bits", C.c_int), ("accumulative", C.c_int)]
 
 
+class ServeConfig(C.Structure):
+    """tcServeConfig (talsh_b200.h)."""
+    _fields_ = [("budget_bytes", C.c_size_t), ("r8_slices", C.c_int), ("max_batch", C.c_int),
+                ("max_inflight", C.c_int), ("large_flop", C.c_double)]
+
+
+class ServeTask(C.Structure):
+    """tcServeTask (talsh_b200.h): a task for the contraction server."""
+    _fields_ = [("op", ContractTask), ("l_from", C.c_uint64), ("r_from", C.c_uint64),
+                ("consumers", C.c_int), ("keep_output", C.c_int)]
+
+
+class ServeStats(C.Structure):
+    """tcServeStats (talsh_b200.h)."""
+    _fields_ = [("submitted", C.c_ulonglong), ("completed", C.c_ulonglong), ("failed", C.c_ulonglong),
+                ("batches", C.c_ulonglong), ("batched_tasks", C.c_ulonglong), ("large_tasks", C.c_ulonglong),
+                ("admission_waits", C.c_ulonglong), ("bytes_in_use", C.c_size_t), ("bytes_peak", C.c_size_t),
+                ("budget_bytes", C.c_size_t)]
+
+
 _P = C.POINTER
 _I, _D, _V, _S, _Z = C.c_int, C.c_double, C.c_void_p, C.c_char_p, C.c_size_t
 _PROTOS = {
@@ -166,6 +186,16 @@ _PROTOS = {
     "tcTensorContractSplitScratch": (_Z, [_I, _P(_I), _I, _P(_I), _I, _P(_I), _I, _P(_I), _I]),
     "tcTensorContractBatchScratch": (_Z, [_I, _P(ContractTask)]),
     "tcTensorContractBatch": (_I, [_I, _P(ContractTask), _V, _Z, _V]),
+    "tcServerCreate": (_I, [_P(ServeConfig), _P(_V)]),
+    "tcServerDestroy": (_I, [_V]),
+    "tcServerSubmit": (_I, [_V, _P(ServeTask), _P(C.c_uint64)]),
+    "tcServerProgress": (_I, [_V]),
+    "tcServerPoll": (_I, [_V, _I, _P(C.c_uint64), _P(_D), _P(_I)]),
+    "tcServerDrain": (_I, [_V]),
+    "tcServerOutput": (_I, [_V, C.c_uint64, _P(_V)]),
+    "tcServerRelease": (_I, [_V, C.c_uint64]),
+    "tcServerGetStats": (_I, [_V, _P(ServeStats)]),
+    "tcServerReplay": (_I, [_V, _I, _P(ServeTask), _P(_D), _P(C.c_uint64), _P(_D)]),
     "tcTensorContractSplit": (_I, [_I, _P(_I), _I, _P(_I), _I, _P(_I), _I, _P(_I), _V, _V, _V, _D, _D,
                                    _I, _I, _I, _V, _Z, _V]),
     "tcPermutePlanInfo": (_I, [_I, _I, _P(_I), _P(_I), _P(_I)]),

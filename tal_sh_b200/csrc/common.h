@@ -32,4 +32,15 @@ void note_cuda_error(const char *what, int code);
 void note_error_text(const char *msg);  // sets the text tcLastErrorString returns
 int check_launch(const char *what);  // 0 or TALSH_FAILURE after a kernel launch
 
+// Batched contractions for host-side schedulers: `get` returns device scratch
+// of scratch_bytes and sets *stage to a pinned host block of stage_bytes that
+// stays untouched until the launch's upload has run (nullptr refuses: the
+// call returns TRY_LATER).
+using BatchScratchFn = void *(*)(void *ctx, size_t scratch_bytes, size_t stage_bytes, void **stage);
+int batch_launch_with(int ntasks, const tcContractTask *tasks, BatchScratchFn get, void *ctx, void *stream);
+// A batch's scratch is at most batch_fixed_scratch() plus the sum of
+// batch_task_scratch_bound over its tasks.
+size_t batch_task_scratch_bound(const tcContractTask &task);
+size_t batch_fixed_scratch();
+
 }  // namespace tb

@@ -822,6 +822,28 @@ size_t contract_scratch_bytes(int kind, const int *cptrn, int drank, const int *
   return b;
 }
 
+// The argument checks of contract_launch without launching anything.
+int contract_validate(int kind, const int *cptrn, int drank, const int *ddims, int lrank, const int *ldims,
+                      int rrank, const int *rdims) {
+  int rc = check_args(kind, cptrn, drank, ddims, lrank, ldims, rrank, rdims);
+  if (rc) return rc;
+  if (lrank == 0 && rrank == 0) return drank == 0 ? TALSH_SUCCESS : TALSH_INVALID_ARGS;
+  if (lrank == 0 || rrank == 0) {
+    const int trank = lrank ? lrank : rrank;
+    const int *tdims = lrank ? ldims : rdims;
+    const int *tptrn = lrank ? cptrn : cptrn + lrank;
+    if (trank != drank) return TALSH_INVALID_ARGS;
+    for (int i = 0; i < trank; ++i)
+      if (tptrn[i] < 1 || tptrn[i] > drank || ddims[tptrn[i] - 1] != tdims[i]) return TALSH_INVALID_ARGS;
+    return TALSH_SUCCESS;
+  }
+  Analysis an;
+  if ((rc = analyze(cptrn, drank, ddims, lrank, ldims, rrank, rdims, an)) != 0) return rc;
+  if (an.hyper) return TALSH_NOT_IMPLEMENTED;
+  if (an.T.M > 0x7fffffffLL || an.T.N > 0x7fffffffLL || an.T.K > 0x7fffffffLL) return TALSH_LIMIT_EXCEEDED;
+  return TALSH_SUCCESS;
+}
+
 int contract_launch(int kind, const int *cptrn, int drank, const int *ddims, int lrank,
                     const int *ldims, int rrank, const int *rdims, void *D, const void *L,
                     const void *R, double alpha_re, double alpha_im, int conj_bits,
@@ -1266,21 +1288,17 @@ int launch_simt_batch(const BatchPlan &bp, int c, char *base, cudaStream_t st) {
 }  // namespace
 }  // namespace tb
 
-extern "C" size_t tcTensorContractBatchScratch(int ntasks, const tcContractTask *tasks) {
-  tb::BatchPlan bp;
-  if (tb::batch_plan(ntasks, tasks, bp) != TALSH_SUCCESS) return 0;
-  return bp.total;
-}
+namespace tb {
+namespace {
 
-extern "C" int tcTensorContractBatch(int ntasks, const tcContractTask *tasks, void *scratch,
-                                     size_t scratch_bytes, void *stream) {
-  using namespace tb;
-  if (ntasks == 0) return TALSH_SUCCESS;
-  BatchPlan bp;
-  int rc = batch_plan(ntasks, tasks, bp);
-  if (rc) return rc;
+// Uploads the descriptors, work lists and prefix sums (the scratch bytes below
+// off_tab) as one copy, then launches the table build, one persistent kernel
+// per configuration and the single-task fallbacks.  `stage`, when given, is a
+// pinned host block of at least off_tab bytes that stays untouched until the
+// copy has run; otherwise the block is packed in pageable memory.
+int batch_run(int ntasks, const tcContractTask *tasks, BatchPlan &bp, void *scratch, size_t scratch_bytes,
+              void *stage, cudaStream_t st) {
   if (scratch == nullptr || scratch_bytes < bp.total) return TALSH_INVALID_ARGS;
-  cudaStream_t st = (cudaStream_t)stream;
   char *base = (char *)scratch;
   int64_t *tabs = (int64_t *)(base + bp.off_tab);
   int64_t max_entries = 0;
@@ -1291,22 +1309,25 @@ extern "C" int tcTensorContractBatch(int ntasks, const tcContractTask *tasks, vo
     a.mL = p; a.mD = p + a.M; a.nR = a.mD + a.M; a.nD = a.nR + a.N; a.kL = a.nD + a.N; a.kR = a.kL + a.K;
     max_entries = std::max<int64_t>(max_entries, (int64_t)a.M + a.N + a.K);
   }
-  // Descriptors and work lists (pageable source: the copy is staged before it returns).
-  cudaError_t e = cudaMemcpyAsync(base + bp.off_desc, bp.descs.data(), sizeof(BatchDesc) * ntasks,
-                                  cudaMemcpyHostToDevice, st);
-  for (int c = 0; c < kNumCfg && e == cudaSuccess; ++c) {
-    if (bp.list[c].empty()) continue;
-    e = cudaMemcpyAsync(base + bp.off_list[c], bp.list[c].data(), sizeof(int32_t) * bp.list[c].size(),
-                        cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess)
-      e = cudaMemcpyAsync(base + bp.off_prefix[c], bp.prefix[c].data(), sizeof(int64_t) * bp.prefix[c].size(),
-                          cudaMemcpyHostToDevice, st);
+  std::vector<char> pageable;
+  char *host = (char *)stage;
+  if (host == nullptr) {
+    pageable.assign(bp.off_tab, 0);
+    host = pageable.data();
   }
+  std::memcpy(host + bp.off_desc, bp.descs.data(), sizeof(BatchDesc) * ntasks);
+  for (int c = 0; c < kNumCfg; ++c) {
+    if (bp.list[c].empty()) continue;
+    std::memcpy(host + bp.off_list[c], bp.list[c].data(), sizeof(int32_t) * bp.list[c].size());
+    std::memcpy(host + bp.off_prefix[c], bp.prefix[c].data(), sizeof(int64_t) * bp.prefix[c].size());
+  }
+  cudaError_t e = cudaMemcpyAsync(base, host, bp.off_tab, cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess) e = cudaMemsetAsync(base + bp.off_ctr, 0, sizeof(unsigned long long) * kNumCfg, st);
   if (e != cudaSuccess) {
     note_cuda_error("batch descriptor upload", (int)e);
     return TALSH_FAILURE;
   }
+  int rc;
   if (max_entries > 0) {
     const int gx = (int)std::max<int64_t>(1, std::min<int64_t>((max_entries + 255) / 256, 64));
     batch_tables_kernel<<<dim3(gx, ntasks), 256, 0, st>>>((const BatchDesc *)(base + bp.off_desc));
@@ -1315,17 +1336,62 @@ extern "C" int tcTensorContractBatch(int ntasks, const tcContractTask *tasks, vo
   }
   if (!bp.list[kCfgD64].empty() && (rc = launch_dmma_batch<64, 64>(bp, kCfgD64, base, st)) != 0) return rc;
   if (!bp.list[kCfgD32].empty() && (rc = launch_dmma_batch<32, 32>(bp, kCfgD32, base, st)) != 0) return rc;
-  if (!bp.list[kCfgS4].empty() && (rc = launch_simt_batch<float>(bp, kCfgS4, base, st)) != 0) return rc;
-  if (!bp.list[kCfgS14].empty() && (rc = launch_simt_batch<float2>(bp, kCfgS14, base, st)) != 0) return rc;
   if (!bp.list[kCfgZ64].empty() && (rc = launch_zmma_batch<64, 64>(bp, kCfgZ64, base, st)) != 0) return rc;
   if (!bp.list[kCfgZ32].empty() && (rc = launch_zmma_batch<32, 32>(bp, kCfgZ32, base, st)) != 0) return rc;
+  if (!bp.list[kCfgS4].empty() && (rc = launch_simt_batch<float>(bp, kCfgS4, base, st)) != 0) return rc;
+  if (!bp.list[kCfgS14].empty() && (rc = launch_simt_batch<float2>(bp, kCfgS14, base, st)) != 0) return rc;
   for (int t = 0; t < ntasks; ++t) {
     if (bp.cfg[t] >= 0) continue;
     const tcContractTask &x = tasks[t];
     rc = contract_launch(x.data_kind, x.cptrn, x.drank, x.ddims, x.lrank, x.ldims, x.rrank, x.rdims, x.D, x.L,
                          x.R, x.alpha_re, x.alpha_im, x.conj_bits, x.accumulative,
-                         bp.fb_scratch[t] ? base + bp.fb_off[t] : nullptr, bp.fb_scratch[t], stream);
+                         bp.fb_scratch[t] ? base + bp.fb_off[t] : nullptr, bp.fb_scratch[t], (void *)st);
     if (rc) return rc;
   }
   return TALSH_SUCCESS;
+}
+
+}  // namespace
+
+// Upper bound of one task's share of a batch's scratch: its descriptor, work
+// list and prefix entries, and its offset tables or single-task fallback
+// scratch.  A batch needs the sum over its tasks plus batch_fixed_scratch().
+size_t batch_task_scratch_bound(const tcContractTask &x) {
+  const size_t fb = contract_scratch_bytes(x.data_kind, x.cptrn, x.drank, x.ddims, x.lrank, x.ldims, x.rrank,
+                                           x.rdims);
+  return sizeof(BatchDesc) + sizeof(int32_t) + sizeof(int64_t) + fb + 256;
+}
+
+size_t batch_fixed_scratch() { return (size_t)(2 * kNumCfg + 4) * 256 + sizeof(unsigned long long) * kNumCfg; }
+
+// Plans a batch, asks `get` for device scratch and a pinned staging block of
+// the sizes the plan needs (get returns nullptr to refuse: TRY_LATER), and
+// launches it on `stream`.
+int batch_launch_with(int ntasks, const tcContractTask *tasks, BatchScratchFn get, void *ctx, void *stream) {
+  cudaStream_t st = (cudaStream_t)stream;
+  if (ntasks == 0) return TALSH_SUCCESS;
+  BatchPlan bp;
+  int rc = batch_plan(ntasks, tasks, bp);
+  if (rc) return rc;
+  void *stage = nullptr;
+  void *scratch = get(ctx, bp.total, bp.off_tab, &stage);
+  if (scratch == nullptr) return TRY_LATER;
+  return batch_run(ntasks, tasks, bp, scratch, bp.total, stage, st);
+}
+
+}  // namespace tb
+
+extern "C" size_t tcTensorContractBatchScratch(int ntasks, const tcContractTask *tasks) {
+  tb::BatchPlan bp;
+  if (tb::batch_plan(ntasks, tasks, bp) != TALSH_SUCCESS) return 0;
+  return bp.total;
+}
+
+extern "C" int tcTensorContractBatch(int ntasks, const tcContractTask *tasks, void *scratch,
+                                     size_t scratch_bytes, void *stream) {
+  if (ntasks == 0) return TALSH_SUCCESS;
+  tb::BatchPlan bp;
+  const int rc = tb::batch_plan(ntasks, tasks, bp);
+  if (rc) return rc;
+  return tb::batch_run(ntasks, tasks, bp, scratch, scratch_bytes, nullptr, (cudaStream_t)stream);
 }

@@ -177,3 +177,29 @@ def test_host_runtime_without_gpu(built):
     finally:
         assert L.talshShutdown() == 0
     assert L.talshShutdown() == T.TALSH_NOT_INITIALIZED
+
+
+def test_batch_and_serve_struct_layouts_match_c(built, tmp_path):
+    """ctypes mirrors of tcContractTask / tcServe* agree with the C compiler's layout."""
+    import subprocess
+    fields = {"tcContractTask": (T.ContractTask, ["D", "L", "R", "alpha_re", "conj_bits", "accumulative"]),
+              "tcServeTask": (T.ServeTask, ["op", "l_from", "r_from", "consumers", "keep_output"]),
+              "tcServeConfig": (T.ServeConfig, ["budget_bytes", "r8_slices", "max_batch", "max_inflight",
+                                                "large_flop"]),
+              "tcServeStats": (T.ServeStats, ["submitted", "admission_waits", "bytes_in_use", "budget_bytes"])}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "talsh_b200.h"', "int main(void){"]
+    for name, (_, fs) in fields.items():
+        lines.append('printf("%%zu\\n", sizeof(%s));' % name)
+        for f in fs:
+            lines.append('printf("%%zu\\n", offsetof(%s, %s));' % (name, f))
+    lines.append("return 0;}")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    got = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
+    want = []
+    for name, (cls, fs) in fields.items():
+        want.append(C.sizeof(cls))
+        want += [getattr(cls, f).offset for f in fs]
+    assert got == want
