@@ -533,6 +533,7 @@ def main():
     if not args.no_contract:
         contract = bench_contractions(T, L, torch, dev)
         contract["C4_batch"] = bench_batch(T, L, torch, dev)
+        contract["C5_serve"] = bench_serve(T, L, torch, dev)
 
     del lbuf, dbuf
     peak, peak_kind = measured_peak()
@@ -776,11 +777,217 @@ def bench_batch(T, L, torch, dev):
     return res
 
 
+CC_PATTERN = "D(a,b,i,j)+=L(a,k,c,i)*R(c,b,k,j)"  # coupled-cluster shaped, v = 128 (a,b,c), o = 48 (i,j,k)
+
+
+def c5_tasks(n, rate, seed, cap=1 << 21, open_chains=16, cc_share=0.05):
+    """C5 arrivals: Poisson at `rate` tasks/s.  Each arrival is, with probability
+    cc_share, a CC-shaped R8 task (v=128, o=48), else the next task of one of
+    `open_chains` chains of 3-8 dependent contractions (R8 or C8 per chain):
+    the first reads two operands from the input pool, every later one
+    contracts the previous task's device-resident output with a pool operand.
+    Shapes as the C4 batch (extents log-uniform in [4, 48], operands <= 2^21
+    elements).  Returns (tasks, arrival seconds); each task is a dict."""
+    rng = np.random.default_rng(seed)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, n))
+    ext_of = lambda k: [int(round(x)) for x in np.exp(rng.uniform(np.log(4), np.log(48), k))]
+    vol = lambda d: int(np.prod(d)) if len(d) else 1
+    chains, tasks, next_chain = [], [], 0
+
+    def new_chain():
+        nonlocal next_chain
+        next_chain += 1
+        return {"id": next_chain, "kind": R8 if rng.integers(0, 2) == 0 else C8,
+                "left": int(rng.integers(3, 9)), "prev": None}
+
+    def first_task(kind):
+        while True:
+            nc = int(rng.integers(1, 4))
+            lu, ru = int(rng.integers(max(1, 2 - nc), 5 - nc)), int(rng.integers(max(1, 2 - nc), 5 - nc))
+            ext = ext_of(nc + lu + ru)
+            c, lo, ro = list(range(nc)), list(range(nc, nc + lu)), list(range(nc + lu, nc + lu + ru))
+            Li, Ri, Di = list(rng.permutation(c + lo)), list(rng.permutation(c + ro)), list(rng.permutation(lo + ro))
+            dims = lambda idx: [ext[i] for i in idx]
+            if max(vol(dims(Li)), vol(dims(Ri)), vol(dims(Di))) > cap:
+                continue
+            cp = [Di.index(i) + 1 if i not in c else -(Ri.index(i) + 1) for i in Li] + \
+                 [Di.index(i) + 1 if i not in c else -(Li.index(i) + 1) for i in Ri]
+            return cp, dims(Di), dims(Li), dims(Ri), vol(dims(lo)) * vol(dims(ro)) * vol(dims(c))
+
+    def next_task(pd):
+        r = len(pd)
+        while True:
+            nc = int(rng.integers(1, min(3, r) + 1))
+            cpos = [int(x) for x in rng.choice(r, nc, replace=False)]
+            lo = [p for p in range(r) if p not in cpos]
+            ru = int(rng.integers(0, 4))
+            if not lo and ru == 0:
+                ru = 1
+            ne = ext_of(ru)
+            new = list(range(r, r + ru))
+            ext = list(pd) + ne
+            Ri, Di = list(rng.permutation(cpos + new)), list(rng.permutation(lo + new))
+            dims = lambda idx: [ext[i] for i in idx]
+            if max(vol(dims(Ri)), vol(dims(Di))) > cap:
+                continue
+            cp = [Di.index(p) + 1 if p not in cpos else -(Ri.index(p) + 1) for p in range(r)] + \
+                 [Di.index(i) + 1 if i not in cpos else -(i + 1) for i in Ri]
+            return cp, dims(Di), list(pd), dims(Ri), vol(dims(lo)) * vol(ne) * vol(dims(cpos))
+
+    import tal_sh_b200 as T
+    cc_dig = T.parse_pattern(CC_PATTERN)[1]
+    v, o = 128, 48
+    for _ in range(n):
+        if rng.uniform() < cc_share:
+            tasks.append({"kind": R8, "cptrn": list(cc_dig), "dd": [v, v, o, o], "ld": [v, o, v, o],
+                          "rd": [v, v, o, o], "flop": 2.0 * v ** 3 * o ** 3, "l_from": 0, "consumers": 0,
+                          "cc": True, "chain": 0})
+            continue
+        while len(chains) < open_chains:
+            chains.append(new_chain())
+        ch = chains[int(rng.integers(0, len(chains)))]
+        if ch["prev"] is None:
+            cp, dd, ld, rd, mnk = first_task(ch["kind"])
+            l_from = 0
+        else:
+            cp, dd, ld, rd, mnk = next_task(tasks[ch["prev"]]["dd"])
+            l_from = ch["prev"] + 1
+        ch["left"] -= 1
+        last = ch["left"] == 0
+        tasks.append({"kind": ch["kind"], "cptrn": cp, "dd": dd, "ld": ld, "rd": rd,
+                      "flop": (2.0 if ch["kind"] == R8 else 8.0) * mnk, "l_from": l_from,
+                      "consumers": 0 if last else 1, "cc": False, "chain": ch["id"]})
+        ch["prev"] = len(tasks) - 1
+        if last:
+            chains.remove(ch)
+    return tasks, arrivals
+
+
+def bench_serve(T, L, torch, dev, slices=6):
+    """C5: Poisson arrivals at 100, 1000 and 10000 tasks/s through the contraction
+    server (tcServerReplay): chains of dependent tasks on device-resident
+    intermediates, 5% CC-shaped R8 tasks in split precision, admission under a
+    150 GB budget.  Latency = scheduled arrival to observed completion."""
+    es = {R8: 8, C8: 16}
+    half = (1 << 21) * 16
+    pool = torch.empty(2 * half // 8, dtype=torch.float64, device=dev).uniform_(-1.0, 1.0)
+    ccn = 128 * 128 * 48 * 48
+    ccL = torch.empty(ccn, dtype=torch.float64, device=dev).normal_().mul_((128 * 48) ** -0.5)
+    ccR = torch.empty(ccn, dtype=torch.float64, device=dev).normal_().mul_((128 * 48) ** -0.5)
+    torch.cuda.synchronize(dev)
+    free, _ = torch.cuda.mem_get_info(dev)
+    budget = int(min(150e9, 0.85 * free))
+
+    def to_ctypes(tasks, keep=()):
+        arr = (T.ServeTask * len(tasks))()
+        for st, x in zip(arr, tasks):
+            t = st.op
+            t.data_kind, t.drank, t.lrank, t.rrank = x["kind"], len(x["dd"]), len(x["ld"]), len(x["rd"])
+            for i, v in enumerate(x["cptrn"]):
+                t.cptrn[i] = v
+            for i, v in enumerate(x["dd"]):
+                t.ddims[i] = v
+            for i, v in enumerate(x["ld"]):
+                t.ldims[i] = v
+            for i, v in enumerate(x["rd"]):
+                t.rdims[i] = v
+            t.D = None
+            t.L = ccL.data_ptr() if x["cc"] else (None if x["l_from"] else pool.data_ptr())
+            t.R = ccR.data_ptr() if x["cc"] else pool.data_ptr() + half
+            t.alpha_re, t.alpha_im, t.conj_bits, t.accumulative = 1.0, 0.0, 0, 0
+            st.l_from, st.r_from, st.consumers, st.keep_output = x["l_from"], 0, x["consumers"], 0
+        for i in keep:
+            arr[i].keep_output = 1
+        return arr
+
+    def server():
+        cfg = T.ServeConfig(budget_bytes=budget, r8_slices=slices, max_batch=4096, max_inflight=2, large_flop=1e10)
+        h = C.c_void_p()
+        assert L.tcServerCreate(C.byref(cfg), C.byref(h)) == 0
+        return h
+
+    def replay(h, tasks, arrivals, keep=()):
+        n = len(tasks)
+        arr = to_ctypes(tasks, keep)
+        ids, lat = (C.c_uint64 * n)(), (C.c_double * n)()
+        rc = L.tcServerReplay(h, n, arr, (C.c_double * n)(*arrivals), ids, lat)
+        if rc:
+            raise RuntimeError("replay failed %d: %s" % (rc, L.tcLastErrorString()))
+        return list(ids), np.array(lat[:n])
+
+    def fetch(h, i, x):
+        p = C.c_void_p()
+        assert L.tcServerOutput(h, i, C.byref(p)) == 0
+        n = int(np.prod(x["dd"])) if x["dd"] else 1
+        ts = "<f8" if x["kind"] == R8 else "<c16"
+        arr = _DevArray(p.value, n, ts)
+        out = torch.as_tensor(arr, device=dev).clone()
+        assert L.tcServerRelease(h, i) == 0
+        return out
+
+    # One server for every rate; warm-up (kernel attributes, the server's memory
+    # pool, pinned staging) not reported.
+    h = server()
+    wt, wa = c5_tasks(300, 2000.0, seed=99)
+    replay(h, wt, wa)
+    out = {"config": "Poisson arrivals (seeded), chains of 3-8 dependent tasks (C4 shapes, R8/C8 per chain, "
+                     "operands <= 2^21 elements) on device-resident intermediates, 5%% CC-shaped R8 tasks "
+                     "(D(a,b,i,j)+=L(a,k,c,i)*R(c,b,k,j), v=128, o=48, %d-slice split precision), "
+                     "admission budget %.0f GB; latency = scheduled arrival to observed completion" %
+                     (slices, budget / 1e9)}
+    for rate, n in ((100, 200), (1000, 2000), (10000, 10000)):
+        tasks, arrivals = c5_tasks(n, float(rate), seed=rate)
+        keep = []
+        if rate == 1000:  # sampled results for the alone-versus-mix comparison
+            ends = [i for i, x in enumerate(tasks) if not x["cc"] and x["consumers"] == 0]
+            keep = [i for i in ends if tasks[i]["kind"] == R8][:2] + [i for i in ends if tasks[i]["kind"] == C8][:2]
+            keep += [i for i, x in enumerate(tasks) if x["cc"]][:2]
+        assert L.tcServerResetStats(h) == 0
+        ids, lat = replay(h, tasks, arrivals, keep)
+        st = T.ServeStats()
+        L.tcServerGetStats(h, C.byref(st))
+        mixed = {i: fetch(h, ids[i], tasks[i]) for i in keep}
+        done = arrivals + lat
+        span = float(done.max() - arrivals[0])
+        flop = sum(x["flop"] for x in tasks)
+        cc = np.array([x["cc"] for x in tasks])
+        pct = lambda a, q: float(np.percentile(a, q) * 1e3) if len(a) else None
+        r = {"offered_tasks_per_s": rate, "tasks": n, "cc_tasks": int(cc.sum()),
+             "chains": len({x["chain"] for x in tasks if x["chain"]}),
+             "makespan_s": span, "tasks_per_s": n / span, "tflops": flop / span / 1e12,
+             "p50_ms": pct(lat, 50), "p99_ms": pct(lat, 99), "max_ms": float(lat.max() * 1e3),
+             "small_p50_ms": pct(lat[~cc], 50), "small_p99_ms": pct(lat[~cc], 99),
+             "cc_p50_ms": pct(lat[cc], 50), "cc_p99_ms": pct(lat[cc], 99),
+             "batches": st.batches, "mean_batch": st.batched_tasks / max(st.batches, 1),
+             "large_tasks": st.large_tasks, "admission_waits": st.admission_waits,
+             "bytes_peak_gb": st.bytes_peak / 1e9, "failed": st.failed}
+        if keep:
+            worst, same = 0.0, True
+            for i in keep:
+                members = [i]
+                while tasks[members[0]]["l_from"]:
+                    members.insert(0, tasks[members[0]]["l_from"] - 1)
+                local = {g: j for j, g in enumerate(members)}
+                sub = [dict(tasks[g], l_from=(local[tasks[g]["l_from"] - 1] + 1) if tasks[g]["l_from"] else 0)
+                       for g in members]
+                sids, _ = replay(h, sub, [0.0] * len(sub), [len(sub) - 1])  # the idle server, this chain only
+                alone = fetch(h, sids[-1], sub[-1])
+                m = mixed[i]
+                same = same and bool(torch.equal(alone, m))
+                worst = max(worst, float((alone - m).abs().max() / m.abs().max().clamp_min(1e-300)))
+            r["alone_vs_mix"] = {"sampled": len(keep), "bit_identical": same, "max_rel_diff": worst,
+                                 "tolerance": 1e-10}
+        out["rate_%d" % rate] = r
+    assert L.tcServerDestroy(h) == 0
+    del pool, ccL, ccR
+    return out
+
+
 class _DevArray:
     """__cuda_array_interface__ wrapper for a device body owned by TAL-SH."""
 
-    def __init__(self, ptr, n):
-        self.__cuda_array_interface__ = {"shape": (n,), "typestr": "<f8", "data": (ptr, False), "version": 3}
+    def __init__(self, ptr, n, typestr="<f8"):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": typestr, "data": (ptr, False), "version": 3}
 
 
 if __name__ == "__main__":

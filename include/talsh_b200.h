@@ -144,7 +144,8 @@ int tcTensorContractBatch(int ntasks, const tcContractTask *tasks, void *scratch
  * talshTaskComplete (talshc.cpp:5073, :2336-2561). */
 typedef struct tcServer tcServer;
 typedef struct {
-  size_t budget_bytes;  /* device bytes for server-held outputs and scratch (0: 90% of free memory) */
+  size_t budget_bytes;  /* device bytes for server-held outputs and scratch (0: 90% of free memory);
+                           the server's memory pool keeps up to this much mapped between tasks */
   int r8_slices;        /* 0: plain FP64 for large R8 tasks, 2..7: split precision with that many slices */
   int max_batch;        /* tasks per batch launch (0: 4096) */
   int max_inflight;     /* batches in flight at once (0: 2) */
@@ -179,6 +180,8 @@ int tcServerOutput(tcServer *srv, uint64_t id, void **ptr);
 /* Gives up a kept output (freed once its consumers have completed). */
 int tcServerRelease(tcServer *srv, uint64_t id);
 int tcServerGetStats(tcServer *srv, tcServeStats *stats);
+/* Zeroes the counters; the peak restarts from the bytes in use. */
+int tcServerResetStats(tcServer *srv);
 /* Replays n tasks arriving at arrival_s[i] seconds after the call (ascending):
  * submits each on time, runs the scheduling loop in between, returns when all
  * have completed.  l_from / r_from in these tasks are 1-based indices into the

@@ -195,6 +195,7 @@ _PROTOS = {
     "tcServerOutput": (_I, [_V, C.c_uint64, _P(_V)]),
     "tcServerRelease": (_I, [_V, C.c_uint64]),
     "tcServerGetStats": (_I, [_V, _P(ServeStats)]),
+    "tcServerResetStats": (_I, [_V]),
     "tcServerReplay": (_I, [_V, _I, _P(ServeTask), _P(_D), _P(C.c_uint64), _P(_D)]),
     "tcTensorContractSplit": (_I, [_I, _P(_I), _I, _P(_I), _I, _P(_I), _I, _P(_I), _V, _V, _V, _D, _D,
                                    _I, _I, _I, _V, _Z, _V]),

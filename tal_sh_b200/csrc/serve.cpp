@@ -1,10 +1,12 @@
 // Contraction server (tcServer*, declared in talsh_b200.h).
 //
 // A single scheduling thread drives three queues:
-//  * admission: submitted tasks in arrival order; the head is admitted when
-//    its server-held output (and, for a large task, its scratch) fits the
-//    device-memory budget; a task that alone exceeds the budget fails with
-//    TALSH_LIMIT_EXCEEDED;
+//  * admission: submitted tasks in arrival order, one queue for small and one
+//    for large tasks (a large task waiting for memory never holds up small
+//    ones); a head is admitted when its server-held output (and, for a large
+//    task, its scratch) fits the device-memory budget, and large tasks only
+//    while fewer than max_inflight + 1 of them are admitted and unfinished; a
+//    task that alone exceeds the budget fails with TALSH_LIMIT_EXCEEDED;
 //  * waiting: admitted tasks whose producers have not been launched yet;
 //  * in flight: launched batches, each with one event.
 // Small tasks are gathered into continuous batches on stream 0 (one
@@ -69,6 +71,7 @@ struct STask {
   bool waited = false;     // held at admission at least once
   bool released = false;   // tcServerRelease called
   bool split = false;      // large R8 task in split precision
+  bool counted = false;    // large task counted in large_active
   void *out = nullptr;     // D used by the launch
   size_t out_bytes = 0;    // server-held output bytes (0: caller's D)
   void *scratch = nullptr; // large tasks: scratch allocated at admission
@@ -118,13 +121,15 @@ double task_flops(const tcContractTask &t) {
 struct tcServer {
   int dev = 0;
   cudaStream_t st[2] = {nullptr, nullptr};
+  cudaMemPool_t pool = nullptr;  // the server's own stream-ordered pool; it keeps freed memory
   tcServeConfig cfg{};
   size_t used = 0, peak = 0;
   size_t reserved = 0;  // batch scratch promised to admitted, unlaunched small tasks
   uint64_t next_id = 1;
   size_t pending = 0;  // submitted, not completed
   std::unordered_map<uint64_t, STask> tasks;
-  std::deque<uint64_t> admit_q;
+  std::deque<uint64_t> admit_q[2];  // per stream: small, large
+  int large_active = 0;              // large tasks admitted and not completed
   std::vector<uint64_t> waiting;
   std::deque<Inflight> inflight;
   std::deque<DoneRec> done;
@@ -138,7 +143,7 @@ namespace {
 int dalloc(tcServer *s, size_t bytes, int stream, void **p) {
   bytes = round_bytes(bytes);
   if (s->used + s->reserved + bytes > s->cfg.budget_bytes) return TRY_LATER;
-  if (cudaMallocAsync(p, bytes, s->st[stream]) != cudaSuccess) {
+  if (cudaMallocFromPoolAsync(p, bytes, s->pool, s->st[stream]) != cudaSuccess) {
     cudaGetLastError();
     *p = nullptr;
     return TRY_LATER;
@@ -202,6 +207,8 @@ void complete(tcServer *s, uint64_t id, int status, double t_now) {
   s->done.push_back(DoneRec{id, t_now - t.t_submit, status});
   s->reserved -= t.reserve;
   t.reserve = 0;
+  if (t.counted) s->large_active--;
+  t.counted = false;
   s->pending--;
   if (status == TALSH_SUCCESS) s->stats.completed++; else s->stats.failed++;
   for (uint64_t p : {t.spec.l_from, t.spec.r_from}) {
@@ -254,9 +261,11 @@ size_t large_scratch(const STask &t, int slices) {
   return tb::contract_scratch_bytes(x.data_kind, x.cptrn, x.drank, x.ddims, x.lrank, x.ldims, x.rrank, x.rdims);
 }
 
-void admit(tcServer *s) {
-  while (!s->admit_q.empty()) {
-    const uint64_t id = s->admit_q.front();
+void admit(tcServer *s, int cls) {
+  std::deque<uint64_t> &q = s->admit_q[cls];
+  while (!q.empty()) {
+    if (cls == 1 && s->large_active >= s->cfg.max_inflight + 1) return;
+    const uint64_t id = q.front();
     STask &t = s->tasks[id];
     if (t.large) {
       t.split = t.spec.op.data_kind == R8 && s->cfg.r8_slices > 0 && t.spec.op.drank > 0;
@@ -270,7 +279,7 @@ void admit(tcServer *s) {
     const size_t need = (t.own_out ? round_bytes(t.out_bytes) : 0) +
                         (t.scratch_bytes ? round_bytes(t.scratch_bytes) : 0) + resv + tb::batch_fixed_scratch();
     if (need > s->cfg.budget_bytes) {
-      s->admit_q.pop_front();
+      q.pop_front();
       tb::note_error_text("served task needs more device memory than the server budget");
       complete(s, id, TALSH_LIMIT_EXCEEDED, now_s());
       continue;
@@ -298,7 +307,11 @@ void admit(tcServer *s) {
     t.reserve = resv;
     s->reserved += resv;
     t.state = kAdmitted;
-    s->admit_q.pop_front();
+    if (t.large) {
+      t.counted = true;
+      s->large_active++;
+    }
+    q.pop_front();
     s->waiting.push_back(id);
   }
 }
@@ -502,16 +515,20 @@ void launch_large(tcServer *s) {
 
 int progress(tcServer *s) {
   retire(s);
-  admit(s);
+  admit(s, 1);
+  admit(s, 0);
   launch_large(s);
   launch_batches(s);
-  if (s->inflight.empty() && s->waiting.empty() && !s->admit_q.empty()) {
-    // Nothing running can free memory for the head of the queue: the budget
-    // is held by kept outputs.
-    const uint64_t id = s->admit_q.front();
-    s->admit_q.pop_front();
-    tb::note_error_text("served task cannot be admitted: the budget is held by kept outputs");
-    complete(s, id, TALSH_LIMIT_EXCEEDED, now_s());
+  if (s->inflight.empty()) {
+    // Nothing could be launched and nothing running can free memory for the
+    // heads of the queues: the budget is held by kept outputs.
+    for (auto &q : s->admit_q) {
+      if (q.empty()) continue;
+      const uint64_t id = q.front();
+      q.pop_front();
+      tb::note_error_text("served task cannot be admitted: the budget is held by kept outputs");
+      complete(s, id, TALSH_LIMIT_EXCEEDED, now_s());
+    }
   }
   return (int)std::min<size_t>(s->pending, 0x7fffffff);
 }
@@ -555,7 +572,7 @@ int submit_at(tcServer *s, const tcServeTask *task, double t_submit, uint64_t *i
   for (int o = 0; o < 2; ++o)
     if (from[o]) s->tasks[from[o]].readers++;
   s->tasks.emplace(nid, t);
-  s->admit_q.push_back(nid);
+  s->admit_q[t.stream].push_back(nid);
   s->pending++;
   s->stats.submitted++;
   *id = nid;
@@ -591,10 +608,27 @@ extern "C" int tcServerCreate(const tcServeConfig *cfg, tcServer **srv) {
     c.budget_bytes = (size_t)(0.9 * (double)fr);
   }
   s->cfg = c;
+  // A pool of its own whose freed blocks stay mapped (release threshold =
+  // budget): admissions after a burst reuse memory instead of mapping new
+  // pages on the scheduling thread.
+  cudaMemPoolProps props;
+  std::memset(&props, 0, sizeof(props));
+  props.allocType = cudaMemAllocationTypePinned;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = s->dev;
+  uint64_t keep = (uint64_t)c.budget_bytes;
+  if (cudaMemPoolCreate(&s->pool, &props) != cudaSuccess ||
+      cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep) != cudaSuccess) {
+    cudaGetLastError();
+    if (s->pool) cudaMemPoolDestroy(s->pool);
+    delete s;
+    return TALSH_FAILURE;
+  }
   for (int i = 0; i < 2; ++i) {
     if (cudaStreamCreateWithFlags(&s->st[i], cudaStreamNonBlocking) != cudaSuccess) {
       cudaGetLastError();
       if (s->st[0]) cudaStreamDestroy(s->st[0]);
+      cudaMemPoolDestroy(s->pool);
       delete s;
       return TALSH_FAILURE;
     }
@@ -673,6 +707,13 @@ extern "C" int tcServerGetStats(tcServer *srv, tcServeStats *stats) {
   return TALSH_SUCCESS;
 }
 
+extern "C" int tcServerResetStats(tcServer *srv) {
+  if (srv == nullptr) return TALSH_INVALID_ARGS;
+  srv->stats = tcServeStats{};
+  srv->peak = srv->used;
+  return TALSH_SUCCESS;
+}
+
 extern "C" int tcServerReplay(tcServer *srv, int n, const tcServeTask *tasks, const double *arrival_s,
                               uint64_t *ids, double *latency_s) {
   if (srv == nullptr || n < 0 || (n > 0 && (tasks == nullptr || arrival_s == nullptr))) return TALSH_INVALID_ARGS;
@@ -748,6 +789,7 @@ extern "C" int tcServerDestroy(tcServer *srv) {
   for (auto &p : srv->stages) cudaFreeHost(p.first);
   for (auto e : srv->events) cudaEventDestroy(e);
   for (int i = 0; i < 2; ++i) cudaStreamDestroy(srv->st[i]);
+  cudaMemPoolDestroy(srv->pool);
   cudaGetLastError();
   delete srv;
   return TALSH_SUCCESS;
