@@ -901,7 +901,8 @@ def bench_serve(T, L, torch, dev, slices=6):
         return arr
 
     def server():
-        cfg = T.ServeConfig(budget_bytes=budget, r8_slices=slices, max_batch=4096, max_inflight=2, large_flop=1e10)
+        cfg = T.ServeConfig(budget_bytes=budget, r8_slices=slices, max_batch=4096, max_inflight=2, large_flop=1e10,
+                            prealloc_bytes=16 << 30)
         h = C.c_void_p()
         assert L.tcServerCreate(C.byref(cfg), C.byref(h)) == 0
         return h
@@ -960,7 +961,8 @@ def bench_serve(T, L, torch, dev, slices=6):
              "cc_p50_ms": pct(lat[cc], 50), "cc_p99_ms": pct(lat[cc], 99),
              "batches": st.batches, "mean_batch": st.batched_tasks / max(st.batches, 1),
              "large_tasks": st.large_tasks, "admission_waits": st.admission_waits,
-             "bytes_peak_gb": st.bytes_peak / 1e9, "failed": st.failed}
+             "bytes_peak_gb": st.bytes_peak / 1e9, "failed": st.failed,
+             "sched_host_s": st.sched_s, "max_sched_step_ms": st.max_step_s * 1e3}
         if keep:
             worst, same = 0.0, True
             for i in keep:

@@ -150,6 +150,8 @@ typedef struct {
   int max_batch;        /* tasks per batch launch (0: 4096) */
   int max_inflight;     /* batches in flight at once (0: 2) */
   double large_flop;    /* tasks with at least this many flops run alone (0: 1e10) */
+  size_t prealloc_bytes;/* device memory mapped into the server's pool at creation, so that
+                           admissions up to that much never map pages on the scheduling thread */
 } tcServeConfig;
 typedef struct {
   tcContractTask op;    /* op.D == NULL: the server allocates the output and overwrites it */
@@ -161,6 +163,8 @@ typedef struct {
 typedef struct {
   unsigned long long submitted, completed, failed, batches, batched_tasks, large_tasks, admission_waits;
   size_t bytes_in_use, bytes_peak, budget_bytes;
+  double sched_s;       /* host seconds spent in scheduling steps */
+  double max_step_s;    /* longest single scheduling step */
 } tcServeStats;
 
 int tcServerCreate(const tcServeConfig *cfg, tcServer **srv);

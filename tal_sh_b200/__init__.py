@@ -98,7 +98,7 @@ class ContractTask(C.Structure):
 class ServeConfig(C.Structure):
     """tcServeConfig (talsh_b200.h)."""
     _fields_ = [("budget_bytes", C.c_size_t), ("r8_slices", C.c_int), ("max_batch", C.c_int),
-                ("max_inflight", C.c_int), ("large_flop", C.c_double)]
+                ("max_inflight", C.c_int), ("large_flop", C.c_double), ("prealloc_bytes", C.c_size_t)]
 
 
 class ServeTask(C.Structure):
@@ -112,7 +112,7 @@ class ServeStats(C.Structure):
     _fields_ = [("submitted", C.c_ulonglong), ("completed", C.c_ulonglong), ("failed", C.c_ulonglong),
                 ("batches", C.c_ulonglong), ("batched_tasks", C.c_ulonglong), ("large_tasks", C.c_ulonglong),
                 ("admission_waits", C.c_ulonglong), ("bytes_in_use", C.c_size_t), ("bytes_peak", C.c_size_t),
-                ("budget_bytes", C.c_size_t)]
+                ("budget_bytes", C.c_size_t), ("sched_s", C.c_double), ("max_step_s", C.c_double)]
 
 
 _P = C.POINTER

@@ -513,7 +513,18 @@ void launch_large(tcServer *s) {
   }
 }
 
+int progress_step(tcServer *s);
+
 int progress(tcServer *s) {
+  const double t0 = now_s();
+  const int r = progress_step(s);
+  const double dt = now_s() - t0;
+  s->stats.sched_s += dt;
+  s->stats.max_step_s = std::max(s->stats.max_step_s, dt);
+  return r;
+}
+
+int progress_step(tcServer *s) {
   retire(s);
   admit(s, 1);
   admit(s, 0);
@@ -624,14 +635,33 @@ extern "C" int tcServerCreate(const tcServeConfig *cfg, tcServer **srv) {
     delete s;
     return TALSH_FAILURE;
   }
+  // The batch stream outranks the large-task stream: CTAs of a small batch are
+  // dispatched ahead of the remaining CTAs of a long contraction.
+  int prio_low = 0, prio_high = 0;
+  if (cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high) != cudaSuccess) {
+    cudaGetLastError();
+    prio_low = prio_high = 0;
+  }
   for (int i = 0; i < 2; ++i) {
-    if (cudaStreamCreateWithFlags(&s->st[i], cudaStreamNonBlocking) != cudaSuccess) {
+    if (cudaStreamCreateWithPriority(&s->st[i], cudaStreamNonBlocking, i == 0 ? prio_high : prio_low) !=
+        cudaSuccess) {
       cudaGetLastError();
       if (s->st[0]) cudaStreamDestroy(s->st[0]);
       cudaMemPoolDestroy(s->pool);
       delete s;
       return TALSH_FAILURE;
     }
+  }
+  if (c.prealloc_bytes > 0) {
+    // Map the pool's first pages now: one allocation, freed at once, stays in
+    // the pool (release threshold = budget).
+    void *p = nullptr;
+    const size_t b = std::min(c.prealloc_bytes, c.budget_bytes);
+    if (cudaMallocFromPoolAsync(&p, b, s->pool, s->st[0]) == cudaSuccess) {
+      cudaFreeAsync(p, s->st[0]);
+      cudaStreamSynchronize(s->st[0]);
+    }
+    cudaGetLastError();
   }
   *srv = s;
   return TALSH_SUCCESS;

@@ -185,8 +185,9 @@ def test_batch_and_serve_struct_layouts_match_c(built, tmp_path):
     fields = {"tcContractTask": (T.ContractTask, ["D", "L", "R", "alpha_re", "conj_bits", "accumulative"]),
               "tcServeTask": (T.ServeTask, ["op", "l_from", "r_from", "consumers", "keep_output"]),
               "tcServeConfig": (T.ServeConfig, ["budget_bytes", "r8_slices", "max_batch", "max_inflight",
-                                                "large_flop"]),
-              "tcServeStats": (T.ServeStats, ["submitted", "admission_waits", "bytes_in_use", "budget_bytes"])}
+                                                "large_flop", "prealloc_bytes"]),
+              "tcServeStats": (T.ServeStats, ["submitted", "admission_waits", "bytes_in_use", "budget_bytes",
+                                               "max_step_s"])}
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "talsh_b200.h"', "int main(void){"]
     for name, (_, fs) in fields.items():
         lines.append('printf("%%zu\\n", sizeof(%s));' % name)
