@@ -37,19 +37,35 @@ namespace {
 constexpr int kMaxGR = 24;  // max indices per group (m, n or k)
 
 struct TableParams {
-  int nm, nn, nk;
-  int64_t M, N, K;
+  int nm, nn, nk, nh;
+  int64_t M, N, K, H;
   int64_t mext[kMaxGR], mstrL[kMaxGR], mstrD[kMaxGR];
   int64_t next[kMaxGR], nstrR[kMaxGR], nstrD[kMaxGR];
   int64_t kext[kMaxGR], kstrL[kMaxGR], kstrR[kMaxGR];
+  // hyper-indices (in D, L and R): one independent GEMM per combination
+  int64_t hext[kMaxGR], hstrL[kMaxGR], hstrR[kMaxGR], hstrD[kMaxGR];
   int64_t *mL, *mD, *nR, *nD, *kL, *kR;
+  int64_t *hL, *hR, *hD;  // used when nh > 0
 };
 
 __global__ void build_tables_kernel(const TableParams T) {
-  const int64_t total = T.M + T.N + T.K;
+  const int64_t mnk = T.M + T.N + T.K;
+  const int64_t total = mnk + (T.nh > 0 ? T.H : 0);
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
-    if (i < T.M) {
+    if (i >= mnk) {
+      int64_t r = i - mnk, a = 0, b = 0, c = 0;
+      for (int d = 0; d < T.nh; ++d) {
+        const int64_t x = r % T.hext[d];
+        r /= T.hext[d];
+        a += x * T.hstrL[d];
+        b += x * T.hstrR[d];
+        c += x * T.hstrD[d];
+      }
+      T.hL[i - mnk] = a;
+      T.hR[i - mnk] = b;
+      T.hD[i - mnk] = c;
+    } else if (i < T.M) {
       int64_t r = i, a = 0, b = 0;
       for (int d = 0; d < T.nm; ++d) {
         const int64_t c = r % T.mext[d];
@@ -86,6 +102,9 @@ __global__ void build_tables_kernel(const TableParams T) {
 struct GemmArgs {
   int M, N, K;
   int tiles_m;
+  int tiles_mn;                      // tiles of one GEMM (hyper-index launches)
+  int H;                             // hyper combinations (1 without hyper-indices)
+  const int64_t *hL, *hR, *hD;       // per hyper combination offsets, or null
   const int64_t *mL, *mD, *nR, *nD, *kL, *kR;
   double alpha_re, alpha_im;
   int beta;       // 1: D += ..., 0: D = ...
@@ -93,6 +112,21 @@ struct GemmArgs {
   int b_along_n;  // B tile loads: lanes along n (else along k)
   int conj_l, conj_r;
 };
+
+// Hyper-index launches: block b runs tile b mod tiles_mn of the GEMM for
+// hyper combination b / tiles_mn, whose operands start at the table offsets.
+template <typename T>
+__device__ __forceinline__ int hyper_offsets(const GemmArgs &a, const T *&L, const T *&R, T *&D) {
+  int local = (int)blockIdx.x;
+  if (a.hL != nullptr) {
+    const int h = local / a.tiles_mn;
+    local -= h * a.tiles_mn;
+    L += a.hL[h];
+    R += a.hR[h];
+    D += a.hD[h];
+  }
+  return local;
+}
 
 // ---------------------------------------------------------------- R8: DMMA
 __device__ __forceinline__ void cp_async8(void *smem_ptr, const void *gptr, bool valid) {
@@ -384,7 +418,10 @@ __global__ void __launch_bounds__(ZmmaCfg<BM, BN>::THREADS)
     zgemm_gather_kernel(const double2 *__restrict__ L, const double2 *__restrict__ R, double2 *D,
                         const GemmArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
-  zmma_tile<BM, BN>(L, R, D, a, blockIdx.x % a.tiles_m, blockIdx.x / a.tiles_m, smem);
+  const double2 *Lp = L, *Rp = R;
+  double2 *Dp = D;
+  const int local = hyper_offsets(a, Lp, Rp, Dp);
+  zmma_tile<BM, BN>(Lp, Rp, Dp, a, local % a.tiles_m, local / a.tiles_m, smem);
 }
 
 template <int BM, int BN>
@@ -392,7 +429,10 @@ __global__ void __launch_bounds__(DmmaCfg<BM, BN>::THREADS)
     dgemm_gather_kernel(const double *__restrict__ L, const double *__restrict__ R, double *D,
                         const GemmArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
-  dmma_tile<BM, BN>(L, R, D, a, blockIdx.x % a.tiles_m, blockIdx.x / a.tiles_m, smem);
+  const double *Lp = L, *Rp = R;
+  double *Dp = D;
+  const int local = hyper_offsets(a, Lp, Rp, Dp);
+  dmma_tile<BM, BN>(Lp, Rp, Dp, a, local % a.tiles_m, local / a.tiles_m, smem);
 }
 
 // ------------------------------------------------- R4 / C4 / C8: SIMT FMA
@@ -520,7 +560,10 @@ __device__ __forceinline__ void simt_tile(const T *__restrict__ L, const T *__re
 template <typename T>
 __global__ void __launch_bounds__(kSThreads)
     gemm_gather_simt_kernel(const T *__restrict__ L, const T *__restrict__ R, T *D, const GemmArgs a) {
-  simt_tile<T>(L, R, D, a, blockIdx.x % a.tiles_m, blockIdx.x / a.tiles_m);
+  const T *Lp = L, *Rp = R;
+  T *Dp = D;
+  const int local = hyper_offsets(a, Lp, Rp, Dp);
+  simt_tile<T>(Lp, Rp, Dp, a, local % a.tiles_m, local / a.tiles_m);
 }
 
 // ------------------------------------------------------ full contraction
@@ -662,21 +705,33 @@ int analyze(const int *cptrn, int drank, const int *ddims, int lrank, const int 
     if (dseen[i] == 2) an.hyper++;
     else if (dseen[i] != 1) return TALSH_INVALID_ARGS;
   }
-  if (an.hyper) return TALSH_SUCCESS;
+  // h: indices in D, L and R, in L order (reference nhu groups,
+  // tensor_algebra_cpu.F90:5829-5839).
+  T.H = 1;
+  for (int i = 0; i < lrank; ++i) {
+    const int j = cptrn[i];
+    if (j <= 0 || dseen[j - 1] != 2 || ldims[i] == 1) continue;
+    int r = 0;
+    while (r < rrank && cptrn[lrank + r] != j) ++r;
+    if (r == rrank) return TALSH_INVALID_ARGS;
+    if (T.nh >= kMaxGR) return TALSH_LIMIT_EXCEEDED;
+    T.hext[T.nh] = ldims[i]; T.hstrL[T.nh] = lstr[i]; T.hstrR[T.nh] = rstr[r]; T.hstrD[T.nh] = dstr[j - 1];
+    T.H *= ldims[i]; T.nh++;
+  }
   int64_t lvol = 1, rvol = 1;
   for (int i = 0; i < lrank; ++i) lvol *= ldims[i];
   for (int i = 0; i < rrank; ++i) rvol *= rdims[i];
   // m: L uncontracted in L order; n: R uncontracted in R order.
   T.M = T.N = T.K = 1;
   for (int i = 0; i < lrank; ++i) {
-    if (cptrn[i] > 0 && ldims[i] > 1) {
+    if (cptrn[i] > 0 && dseen[cptrn[i] - 1] == 1 && ldims[i] > 1) {
       if (T.nm >= kMaxGR) return TALSH_LIMIT_EXCEEDED;
       T.mext[T.nm] = ldims[i]; T.mstrL[T.nm] = lstr[i]; T.mstrD[T.nm] = dstr[cptrn[i] - 1];
       T.M *= ldims[i]; T.nm++;
     }
   }
   for (int i = 0; i < rrank; ++i) {
-    if (cptrn[lrank + i] > 0 && rdims[i] > 1) {
+    if (cptrn[lrank + i] > 0 && dseen[cptrn[lrank + i] - 1] == 1 && rdims[i] > 1) {
       if (T.nn >= kMaxGR) return TALSH_LIMIT_EXCEEDED;
       T.next[T.nn] = rdims[i]; T.nstrR[T.nn] = rstr[i]; T.nstrD[T.nn] = dstr[cptrn[lrank + i] - 1];
       T.N *= rdims[i]; T.nn++;
@@ -713,7 +768,18 @@ int analyze(const int *cptrn, int drank, const int *ddims, int lrank, const int 
 }
 
 size_t table_bytes(const TableParams &T) {
-  return (size_t)align_up(8 * (2 * T.M + 2 * T.N + 2 * T.K), 256);
+  return (size_t)align_up(8 * (2 * T.M + 2 * T.N + 2 * T.K + (T.nh > 0 ? 3 * T.H : 0)), 256);
+}
+
+// Grid of a gather-GEMM launch: tiles of one GEMM times hyper combinations.
+int gemm_grid(GemmArgs &ga, int bm, int bn, int64_t *blocks) {
+  ga.tiles_m = (ga.M + bm - 1) / bm;
+  const int64_t per = (int64_t)ga.tiles_m * ((ga.N + bn - 1) / bn);
+  const int64_t all = per * std::max(ga.H, 1);
+  if (per > 0x7fffffffLL || all > 0x7fffffffLL) return TALSH_LIMIT_EXCEEDED;
+  ga.tiles_mn = (int)per;
+  *blocks = all;
+  return TALSH_SUCCESS;
 }
 
 int sm_count_dev() {
@@ -736,9 +802,8 @@ int launch_dmma(const double *L, const double *R, double *D, GemmArgs ga, cudaSt
                          (int)C::SMEM);
     attr_set = true;
   }
-  ga.tiles_m = (ga.M + BM - 1) / BM;
-  const int64_t tiles = (int64_t)ga.tiles_m * ((ga.N + BN - 1) / BN);
-  if (tiles > 0x7fffffffLL) return TALSH_LIMIT_EXCEEDED;
+  int64_t tiles = 0;
+  if (gemm_grid(ga, BM, BN, &tiles)) return TALSH_LIMIT_EXCEEDED;
   dgemm_gather_kernel<BM, BN><<<(unsigned)tiles, C::THREADS, C::SMEM, st>>>(L, R, D, ga);
   note_launch();
   return check_launch("dgemm_gather_kernel");
@@ -753,9 +818,8 @@ int launch_zmma(const double2 *L, const double2 *R, double2 *D, GemmArgs ga, cud
                          (int)Z::SMEM);
     attr_set = true;
   }
-  ga.tiles_m = (ga.M + BM - 1) / BM;
-  const int64_t tiles = (int64_t)ga.tiles_m * ((ga.N + BN - 1) / BN);
-  if (tiles > 0x7fffffffLL) return TALSH_LIMIT_EXCEEDED;
+  int64_t tiles = 0;
+  if (gemm_grid(ga, BM, BN, &tiles)) return TALSH_LIMIT_EXCEEDED;
   zgemm_gather_kernel<BM, BN><<<(unsigned)tiles, Z::THREADS, Z::SMEM, st>>>(L, R, D, ga);
   note_launch();
   return check_launch("zgemm_gather_kernel");
@@ -763,9 +827,8 @@ int launch_zmma(const double2 *L, const double2 *R, double2 *D, GemmArgs ga, cud
 
 template <typename T>
 int launch_simt(const void *L, const void *R, void *D, GemmArgs ga, cudaStream_t st) {
-  ga.tiles_m = (ga.M + kSBM - 1) / kSBM;
-  const int64_t tiles = (int64_t)ga.tiles_m * ((ga.N + kSBN - 1) / kSBN);
-  if (tiles > 0x7fffffffLL) return TALSH_LIMIT_EXCEEDED;
+  int64_t tiles = 0;
+  if (gemm_grid(ga, kSBM, kSBN, &tiles)) return TALSH_LIMIT_EXCEEDED;
   gemm_gather_simt_kernel<T><<<(unsigned)tiles, kSThreads, 0, st>>>((const T *)L, (const T *)R,
                                                                      (T *)D, ga);
   note_launch();
@@ -816,7 +879,7 @@ size_t contract_scratch_bytes(int kind, const int *cptrn, int drank, const int *
   if (check_args(kind, cptrn, drank, ddims, lrank, ldims, rrank, rdims)) return 0;
   if (lrank == 0 || rrank == 0) return 0;
   Analysis an;
-  if (analyze(cptrn, drank, ddims, lrank, ldims, rrank, rdims, an) || an.hyper) return 0;
+  if (analyze(cptrn, drank, ddims, lrank, ldims, rrank, rdims, an)) return 0;
   size_t b = table_bytes(an.T);
   if (drank == 0) b += (size_t)dot_blocks(an.T.K) * sizeof(double2);
   return b;
@@ -839,8 +902,8 @@ int contract_validate(int kind, const int *cptrn, int drank, const int *ddims, i
   }
   Analysis an;
   if ((rc = analyze(cptrn, drank, ddims, lrank, ldims, rrank, rdims, an)) != 0) return rc;
-  if (an.hyper) return TALSH_NOT_IMPLEMENTED;
-  if (an.T.M > 0x7fffffffLL || an.T.N > 0x7fffffffLL || an.T.K > 0x7fffffffLL) return TALSH_LIMIT_EXCEEDED;
+  if (an.T.M > 0x7fffffffLL || an.T.N > 0x7fffffffLL || an.T.K > 0x7fffffffLL || an.T.H > 0x7fffffffLL)
+    return TALSH_LIMIT_EXCEEDED;
   return TALSH_SUCCESS;
 }
 
@@ -885,15 +948,18 @@ int contract_launch(int kind, const int *cptrn, int drank, const int *ddims, int
   }
   Analysis an;
   if ((rc = analyze(cptrn, drank, ddims, lrank, ldims, rrank, rdims, an)) != 0) return rc;
-  if (an.hyper) return TALSH_NOT_IMPLEMENTED;
   TableParams T = an.T;
   const size_t need = table_bytes(T) + (drank == 0 ? (size_t)dot_blocks(T.K) * sizeof(double2) : 0);
   if (scratch == nullptr || scratch_bytes < need) return TALSH_INVALID_ARGS;
-  if (T.M > 0x7fffffffLL || T.N > 0x7fffffffLL || T.K > 0x7fffffffLL) return TALSH_LIMIT_EXCEEDED;
+  if (T.M > 0x7fffffffLL || T.N > 0x7fffffffLL || T.K > 0x7fffffffLL || T.H > 0x7fffffffLL)
+    return TALSH_LIMIT_EXCEEDED;
   int64_t *base = (int64_t *)scratch;
   T.mL = base; T.mD = T.mL + T.M; T.nR = T.mD + T.M; T.nD = T.nR + T.N; T.kL = T.nD + T.N; T.kR = T.kL + T.K;
+  if (T.nh > 0) {
+    T.hL = T.kR + T.K; T.hR = T.hL + T.H; T.hD = T.hR + T.H;
+  }
   {
-    const int64_t total = T.M + T.N + T.K;
+    const int64_t total = T.M + T.N + T.K + (T.nh > 0 ? T.H : 0);
     const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((total + 255) / 256, 4096));
     build_tables_kernel<<<grid, 256, 0, st>>>(T);
     note_launch();
@@ -916,9 +982,13 @@ int contract_launch(int kind, const int *cptrn, int drank, const int *ddims, int
   ga.a_along_m = an.a_along_m ? 1 : 0;
   ga.b_along_n = an.b_along_n ? 1 : 0;
   ga.conj_l = cl; ga.conj_r = cr;
+  ga.H = (int)T.H;
+  if (T.nh > 0) {
+    ga.hL = T.hL; ga.hR = T.hR; ga.hD = T.hD;
+  }
   switch (kind) {
     case R8: {
-      const int64_t big_tiles = ((T.M + 127) / 128) * ((T.N + 127) / 128);
+      const int64_t big_tiles = ((T.M + 127) / 128) * ((T.N + 127) / 128) * T.H;
       if (big_tiles >= 2 * sm_count_dev())
         return launch_dmma<128, 128>((const double *)L, (const double *)R, (double *)D, ga, st);
       return launch_dmma<64, 64>((const double *)L, (const double *)R, (double *)D, ga, st);

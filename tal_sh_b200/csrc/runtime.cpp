@@ -655,10 +655,6 @@ int parse_and_check(const char *cptrn, OpSpec &op, int want_inputs) {
   if (op.t[1] && talshTensorRank(op.t[1]) != lr) return TALSH_INVALID_ARGS;
   if (want_inputs == 2) {
     if (op.t[2] && talshTensorRank(op.t[2]) != rr) return TALSH_INVALID_ARGS;
-    // Indices shared by D, L and R (hyper-contractions) have no GPU kernel here.
-    for (int i = 0; i < lr; ++i)
-      for (int j = 0; j < rr; ++j)
-        if (op.dig[i] > 0 && op.dig[i] == op.dig[lr + j]) return TALSH_NOT_IMPLEMENTED;
   } else if (rr != 0) {
     return TALSH_INVALID_ARGS;
   }

@@ -133,7 +133,59 @@ def test_known_answer_nwchem(talsh):
     assert np.abs(D).sum() <= 1e-12 * np.abs(np.einsum("cd,dabc->ab", L, R)).sum()
 
 
-def test_hyper_indices_not_supported(talsh):
+HYPER_CASES = [  # indices in D, L and R: one GEMM per hyper combination
+    ("D(a,b,c)+=L(c,a)*R(b,c)", dict(a=3, b=4, c=5)),                       # no contracted index
+    ("D(i,j,k)+=L(k,a,i,b)*R(b,k,a,j)", dict(i=12, j=10, k=7, a=6, b=5)),   # the reference's hyper test shape
+    ("D(x,h,g)+=L(x,h,k,g)*R(g,k,h)", dict(h=4, g=3, x=33, k=17)),          # two hyper indices, R without free index
+    ("D(h)+=L(k,h)*R(h,k)", dict(h=9, k=40)),                                # D only hyper: a dot per h
+    ("D(a,h,b)+=L(a,k,h)*R(h,k,b)", dict(a=70, b=66, h=1, k=20)),            # extent-1 hyper index
+]
+
+
+@pytest.mark.parametrize("kind", [T.R8, T.C8, T.R4, T.C4])
+@pytest.mark.parametrize("pattern,ext", HYPER_CASES)
+def test_hyper_contractions_match_oracle(talsh, pattern, ext, kind):
+    """Hyper-contractions (reference nhu path, tensor_algebra_cpu.F90:5829-5839,
+    tensor_block_pcontract_batch_dlf :11256) against the oracle."""
+    import re
     rng = np.random.default_rng(8)
-    D, L, R = fort(np.zeros((3, 4, 5))), rand((5, 3), T.R8, rng), rand((4, 5), T.R8, rng)
-    assert gpu_contract("D(a,b,c)+=L(c,a)*R(b,c)", D, L, R) == T.TALSH_NOT_IMPLEMENTED
+    groups = [[x for x in g.split(",") if x] for g in re.findall(r"\(([^)]*)\)", pattern)]
+    dd, ld, rd = ([ext[x] for x in g] for g in groups)
+    D, L, R = rand(dd, kind, rng), rand(ld, kind, rng), rand(rd, kind, rng)
+    ref = D.copy(order="F")
+    e, dig, *_ = T.parse_pattern(pattern)
+    alpha = (0.5, -0.25) if kind in (T.C4, T.C8) else (0.5, 0.0)
+    assert O.tensor_contract(ref, L, R, dig, alpha[0], alpha[1], 0, True) == 0
+    got = D.copy(order="F")
+    assert gpu_contract(pattern, got, L, R, alpha[0], alpha[1]) == 0
+    tol = 1e-12 if kind in (T.R8, T.C8) else 2e-5
+    assert np.linalg.norm(got - ref) <= tol * np.linalg.norm(ref - D), (pattern, kind)
+
+
+def test_hyper_indices_anywhere_in_d(talsh):
+    """Hyper indices ahead of simple ones in D.  The reference's CPU matricization
+    assumes they trail D (get_contraction_permutations, tensor_algebra_cpu.F90:5878,
+    puts them at D's end unpermuted) and the oracle follows it, so this placement is
+    checked against an FP64 einsum instead."""
+    rng = np.random.default_rng(12)
+    for pattern, spec, dims in (("D(h,g,x)+=L(x,h,k,g)*R(g,k,h)", "xhkg,gkh->hgx", ((4, 3, 33), (33, 4, 17, 3), (3, 17, 4))),
+                                ("D(b,h,a)+=L(a,k,h)*R(h,b,k)", "akh,hbk->bha", ((21, 5, 19), (19, 23, 5), (5, 21, 23)))):
+        for kind in (T.R8, T.C8):
+            D, L, R = (rand(d, kind, rng) for d in dims)
+            got = D.copy(order="F")
+            assert gpu_contract(pattern, got, L, R, 0.5, 0.0) == 0
+            want = D + 0.5 * np.einsum(spec, L, R)
+            assert np.linalg.norm(got - want) <= 1e-12 * np.linalg.norm(want - D), (pattern, kind)
+
+
+def test_hyper_contraction_reference_known_answer(talsh):
+    """test.cpp:377-430 (test_talsh_hyper): C4 D(i,j,k)+=L(k,a,i,b)*R(b,k,a,j) with
+    constant L = (0.001,-0.0001), R = (0.002,-0.0002), alpha 0.5; the 1-norm of D is
+    |l r| * 48*24 * vol(D) * 0.5."""
+    l, r = np.complex64(0.001 - 0.0001j), np.complex64(0.002 - 0.0002j)
+    D = fort(np.zeros((48, 24, 32), dtype=np.complex64))
+    L = fort(np.full((32, 48, 48, 24), l, dtype=np.complex64))
+    R = fort(np.full((24, 32, 48, 24), r, dtype=np.complex64))
+    assert gpu_contract("D(i,j,k)+=L(k,a,i,b)*R(b,k,a,j)", D, L, R, 0.5, 0.0) == 0
+    want = abs(48.0 * 24.0) * abs(complex(l) * complex(r)) * (48.0 * 24.0 * 32.0) * 0.5
+    assert abs(np.abs(D).sum() - want) <= 1e-5 * want

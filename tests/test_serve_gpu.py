@@ -316,12 +316,13 @@ def test_error_paths(talsh):
     rc, c = srv.submit(_task(T.R8, "D(a,c)+=L(a,b)*R(b,c)", dict(a=600, b=600, c=1), R=buf.data_ptr(), l_from=big,
                              D=buf.data_ptr()))
     assert rc == 0
-    # shape mismatch with the producer, unknown producer, hyper-index pattern: refused at submit
+    # shape mismatch with the producer, unknown producer, inconsistent extents: refused at submit
     assert srv.submit(_task(T.R8, "D(a,c)+=L(a,b)*R(b,c)", dict(a=5, b=600, c=1), R=buf.data_ptr(), l_from=big,
                             D=buf.data_ptr()))[0] == T.TALSH_INVALID_ARGS
     assert srv.submit(_task(T.R8, p, dict(a=4, k=4, b=4), R=buf.data_ptr(), l_from=987654))[0] == T.TALSH_INVALID_ARGS
-    assert srv.submit(_task(T.R8, "D(a,b)+=L(a,b)*R(b)", dict(a=4, b=4), L=buf.data_ptr(), R=buf.data_ptr(),
-                            D=buf.data_ptr()))[0] == T.TALSH_NOT_IMPLEMENTED
+    bad = _task(T.R8, p, dict(a=4, k=4, b=4), L=buf.data_ptr(), R=buf.data_ptr(), D=buf.data_ptr())
+    bad.op.rdims[0] = 5  # contracted extents differ
+    assert srv.submit(bad)[0] == T.TALSH_INVALID_ARGS
     srv.drain()
     done = srv.poll()
     assert done[big][1] == T.TALSH_LIMIT_EXCEEDED
