@@ -96,6 +96,19 @@ int tcTensorContractSplit(int data_kind, const int *cptrn, int drank, const int 
                           int accumulative, int slices, void *scratch, size_t scratch_bytes,
                           void *stream);
 
+/* Slicing: slice (+)= full[offsets : offsets + slice_dims] (0-based offsets, both
+ * tensors dense column-major of the same rank and kind).  Replaces
+ * gpu_tensor_block_slice (tensor_algebra_gpu_nvidia.cu:4788, a stub there) with
+ * the semantics of the CPU path tensor_block_slice_dlf_* (tensor_algebra_cpu.F90:6900);
+ * accumulative = 0 overwrites the slice. */
+int tcTensorSlice(int data_kind, int rank, const int *full_dims, const int *slice_dims, const int *offsets,
+                  const void *full, void *slice, int accumulative, void *stream);
+/* Insertion: full[offsets : offsets + slice_dims] (+)= slice.  Replaces
+ * gpu_tensor_block_insert (tensor_algebra_gpu_nvidia.cu:4798, a stub there);
+ * semantics of tensor_block_insert_dlf_* (tensor_algebra_cpu.F90:7216). */
+int tcTensorInsert(int data_kind, int rank, const int *full_dims, const int *slice_dims, const int *offsets,
+                   const void *slice, void *full, int accumulative, void *stream);
+
 /* Batched contractions (many small tasks, one launch per tile configuration). */
 #define TC_BATCH_MAX_RANK 8
 typedef struct {

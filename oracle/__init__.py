@@ -52,6 +52,8 @@ def lib():
         L.orc_cmplx8_to_real8.argtypes = [D, D]
         L.orc_cmplx8_to_real8.restype = D
         L.orc_fill_uniform.argtypes = [I, Z, V, C.c_ulonglong]
+        L.orc_tensor_slice.argtypes = [I, I, P(I), P(I), P(I), V, V, I]
+        L.orc_tensor_insert.argtypes = [I, I, P(I), P(I), P(I), V, V, I]
         _lib = L
     return _lib
 
@@ -151,6 +153,22 @@ def tensor_contract(d, l, r, cptrn, sr=1.0, si=0.0, conj_bits=0, accumulative=Tr
     return lib().orc_tensor_contract(KIND_OF[d.dtype], _iv(cptrn), d.ndim, _iv(d.shape), l.ndim, _iv(l.shape),
                                      r.ndim, _iv(r.shape), _ptr(d), _ptr(l), _ptr(r), sr, si, conj_bits,
                                      1 if accumulative else 0)
+
+
+def tensor_slice(slice_, full, offsets, accumulative=False):
+    """In place on slice_ (Fortran-ordered): reference tensor_block_slice. Returns ierr."""
+    full = _fort(full)
+    assert slice_.flags["F_CONTIGUOUS"] and slice_.ndim == full.ndim
+    return lib().orc_tensor_slice(KIND_OF[full.dtype], full.ndim, _iv(full.shape), _iv(slice_.shape), _iv(offsets),
+                                  _ptr(full), _ptr(slice_), 1 if accumulative else 0)
+
+
+def tensor_insert(full, slice_, offsets, accumulative=False):
+    """In place on full (Fortran-ordered): reference tensor_block_insert. Returns ierr."""
+    slice_ = _fort(slice_)
+    assert full.flags["F_CONTIGUOUS"] and slice_.ndim == full.ndim
+    return lib().orc_tensor_insert(KIND_OF[full.dtype], full.ndim, _iv(full.shape), _iv(slice_.shape),
+                                   _iv(offsets), _ptr(slice_), _ptr(full), 1 if accumulative else 0)
 
 
 def cmplx8_to_real8(re, im):

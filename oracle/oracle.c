@@ -936,6 +936,66 @@ int orc_tensor_contract(int kind, const int *cptrn, int drank, const int *ddims,
 }
 
 /* ------------------------------------------------------------------------- */
+/* Slicing / insertion (tensor_algebra_cpu.F90:6900-6974, :7216-7290)          */
+/* ------------------------------------------------------------------------- */
+/* One element: d = d*beta + s*alpha in the element's own precision, complex
+ * products written out as the Fortran complex multiply does them. */
+#define ORC_SLICE_MOVE_REAL(T)                                                   \
+  {                                                                              \
+    T *dp = (T *)dst + di;                                                       \
+    const T sv = ((const T *)src)[si];                                           \
+    *dp = *dp * (T)bet + sv * (T)1;                                              \
+  }
+#define ORC_SLICE_MOVE_CPLX(CT, T)                                               \
+  {                                                                              \
+    CT *dp = (CT *)dst + di;                                                     \
+    const CT sv = ((const CT *)src)[si];                                         \
+    const T bre = (T)bet, one = (T)1, zero = (T)0;                               \
+    const T pre = dp->re * bre - dp->im * zero, pim = dp->re * zero + dp->im * bre; \
+    const T qre = sv.re * one - sv.im * zero, qim = sv.re * zero + sv.im * one; \
+    dp->re = pre + qre;                                                          \
+    dp->im = pim + qim;                                                          \
+  }
+
+static int orc_slice_move(int insert, int kind, int rank, const int *full_dims, const int *slice_dims,
+                          const int *offsets, const void *src, void *dst, int accumulative) {
+  if (kind_size(kind) == 0 || rank < 1 || rank > ORC_MAX_RANK) return 1;
+  for (int i = 0; i < rank; ++i)
+    if (full_dims[i] <= 0 || slice_dims[i] <= 0 || offsets[i] < 0 || offsets[i] + slice_dims[i] > full_dims[i])
+      return 1;
+  const double bet = accumulative ? 1.0 : 0.0;
+  size_t fstr[ORC_MAX_RANK], svol = 1, s = 1;
+  for (int i = 0; i < rank; ++i) { fstr[i] = s; s *= (size_t)full_dims[i]; svol *= (size_t)slice_dims[i]; }
+  int im[ORC_MAX_RANK] = {0};
+  for (size_t e = 0; e < svol; ++e) {
+    size_t f = 0;
+    for (int i = 0; i < rank; ++i) f += (size_t)(offsets[i] + im[i]) * fstr[i];
+    const size_t si = insert ? e : f, di = insert ? f : e;
+    switch (kind) {
+      case 4: ORC_SLICE_MOVE_REAL(float) break;
+      case 8: ORC_SLICE_MOVE_REAL(double) break;
+      case 14: ORC_SLICE_MOVE_CPLX(c4_t, float) break;
+      default: ORC_SLICE_MOVE_CPLX(c8_t, double) break;
+    }
+    for (int i = 0; i < rank; ++i) {
+      if (++im[i] < slice_dims[i]) break;
+      im[i] = 0;
+    }
+  }
+  return 0;
+}
+
+int orc_tensor_slice(int kind, int rank, const int *full_dims, const int *slice_dims, const int *offsets,
+                     const void *full, void *slice, int accumulative) {
+  return orc_slice_move(0, kind, rank, full_dims, slice_dims, offsets, full, slice, accumulative);
+}
+
+int orc_tensor_insert(int kind, int rank, const int *full_dims, const int *slice_dims, const int *offsets,
+                      const void *slice, void *full, int accumulative) {
+  return orc_slice_move(1, kind, rank, full_dims, slice_dims, offsets, slice, full, accumulative);
+}
+
+/* ------------------------------------------------------------------------- */
 /* Generator: mt19937_64                                                     */
 /* ------------------------------------------------------------------------- */
 typedef struct { uint64_t mt[312]; int mti; } orc_mt64_t;

@@ -60,6 +60,14 @@ int orc_tensor_contract(int kind, const int *cptrn, int drank, const int *ddims,
 /* cmplx8_to_real8 (tensor_algebra_cpu.F90:430-445). */
 double orc_cmplx8_to_real8(double re, double im);
 
+/* Slicing / insertion (tensor_block_slice_dlf_* tensor_algebra_cpu.F90:6900-6974,
+ * tensor_block_insert_dlf_* :7216-7290): dst = dst*beta + src*alpha with alpha = 1,
+ * beta = 1 when accumulative else 0, over the sub-block at 0-based offsets. */
+int orc_tensor_slice(int kind, int rank, const int *full_dims, const int *slice_dims, const int *offsets,
+                     const void *full, void *slice, int accumulative);
+int orc_tensor_insert(int kind, int rank, const int *full_dims, const int *slice_dims, const int *offsets,
+                      const void *slice, void *full, int accumulative);
+
 /* Seeded generator: mt19937_64 stream, uniform[-1,1] = 2*(x>>11)*2^-53 - 1. */
 void orc_fill_uniform(int kind, size_t vol, void *out, unsigned long long seed);
 

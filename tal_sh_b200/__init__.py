@@ -154,6 +154,8 @@ _PROTOS = {
     "talshTensorDiscardOther": (_I, [_P(Tens), _I, _I]),
     "talshTensorInit": (_I, [_P(Tens), _D, _D, _I, _I, _I, _P(Task)]),
     "talshTensorScale": (_I, [_P(Tens), _D, _D, _I, _I, _I, _P(Task)]),
+    "talshTensorSlice": (_I, [_P(Tens), _P(Tens), _P(_I), _I, _I, _I, _I, _P(Task)]),
+    "talshTensorInsert": (_I, [_P(Tens), _P(Tens), _P(_I), _I, _I, _I, _I, _P(Task)]),
     "talshTensorCopy": (_I, [_S, _P(Tens), _P(Tens), _I, _I, _I, _P(Task)]),
     "talshTensorAdd": (_I, [_S, _P(Tens), _P(Tens), _D, _D, _I, _I, _I, _P(Task)]),
     "talshTensorContract": (_I, [_S, _P(Tens), _P(Tens), _P(Tens), _D, _D, _I, _I, _I, _I, _P(Task)]),
@@ -186,6 +188,8 @@ _PROTOS = {
     "tcTensorContractSplitScratch": (_Z, [_I, _P(_I), _I, _P(_I), _I, _P(_I), _I, _P(_I), _I]),
     "tcTensorContractBatchScratch": (_Z, [_I, _P(ContractTask)]),
     "tcTensorContractBatch": (_I, [_I, _P(ContractTask), _V, _Z, _V]),
+    "tcTensorSlice": (_I, [_I, _I, _P(_I), _P(_I), _P(_I), _V, _V, _I, _V]),
+    "tcTensorInsert": (_I, [_I, _I, _P(_I), _P(_I), _P(_I), _V, _V, _I, _V]),
     "tcServerCreate": (_I, [_P(ServeConfig), _P(_V)]),
     "tcServerDestroy": (_I, [_V]),
     "tcServerSubmit": (_I, [_V, _P(ServeTask), _P(C.c_uint64)]),

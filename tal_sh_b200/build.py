@@ -17,7 +17,7 @@ LIB = os.path.join(HERE, "libtalsh.so")
 BUILD_DIR = os.path.join(ROOT, "_build", "talsh")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-CUDA_SOURCES = ["permute.cu", "elementwise.cu", "contract.cu", "diag.cu", "noalloc.cu", "ozaki.cu"]
+CUDA_SOURCES = ["permute.cu", "elementwise.cu", "contract.cu", "diag.cu", "noalloc.cu", "ozaki.cu", "slice.cu"]
 CXX_SOURCES = ["pattern.cpp", "runtime.cpp", "serve.cpp"]
 COMMON = ["-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-I" + INCLUDE, "-I" + CSRC]
 

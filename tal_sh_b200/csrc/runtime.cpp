@@ -374,7 +374,7 @@ int task_progress(talsh_task_t *task, bool wait) {
 }
 
 // ------------------------------------------------------- operation driver
-enum OpKind { kOpInit, kOpScale, kOpCopy, kOpAdd, kOpContract, kOpNorm1, kOpPlace };
+enum OpKind { kOpInit, kOpScale, kOpCopy, kOpAdd, kOpContract, kOpNorm1, kOpPlace, kOpSlice, kOpInsert };
 
 struct OpSpec {
   OpKind kind;
@@ -386,6 +386,7 @@ struct OpSpec {
   double sr = 0.0, si = 0.0;
   int accumulative = YEP;
   double *norm_out = nullptr;        // host result of kOpNorm1
+  int offsets[MAX_TENSOR_RANK];      // kOpSlice / kOpInsert base offsets (0-based)
 };
 
 // Resolves the execution GPU: returns its ordinal or a negative TAL-SH error.
@@ -478,7 +479,7 @@ int schedule(OpSpec &op, int dev_id, int dev_kind, talsh_task_t *user_task) {
     a.bytes = shape_volume(t->shape_p) * esz;
     a.output = (k == 0) && op.kind != kOpNorm1 && op.kind != kOpPlace;
     a.need_input = !(k == 0 && (op.kind == kOpInit || op.kind == kOpCopy ||
-                               (op.kind == kOpContract && op.accumulative == NOPE)));
+                               ((op.kind == kOpContract || op.kind == kOpSlice) && op.accumulative == NOPE)));
     if (a.src_dev == exec_dev) {
       a.dptr = a.src_ptr;
     } else {
@@ -615,6 +616,14 @@ int schedule(OpSpec &op, int dev_id, int dev_kind, talsh_task_t *user_task) {
         break;
       }
       case kOpPlace:
+        break;
+      case kOpSlice:   // D = slice of L
+        rc = tcTensorSlice(dkind, op.drank, op.t[1]->shape_p->dims, op.t[0]->shape_p->dims, op.offsets,
+                           tr->a[1].dptr, tr->a[0].dptr, op.accumulative == YEP ? 1 : 0, st);
+        break;
+      case kOpInsert:  // L inserted into D
+        rc = tcTensorInsert(dkind, op.drank, op.t[0]->shape_p->dims, op.t[1]->shape_p->dims, op.offsets,
+                            tr->a[1].dptr, tr->a[0].dptr, op.accumulative == YEP ? 1 : 0, st);
         break;
     }
   }
@@ -1653,11 +1662,46 @@ int talshTensorScale(talsh_tens_t *d, double vr, double vi, int dev_id, int dev_
 }
 int talshTensorScale_(talsh_tens_t *d, double a, double b, int c, int e, int f, talsh_task_t *g) { return talshTensorScale(d, a, b, c, e, f, g); }
 
-int talshTensorSlice(talsh_tens_t *, talsh_tens_t *, const int *, int, int, int, int, talsh_task_t *) { return TALSH_NOT_IMPLEMENTED; }
+// Slicing and insertion (reference talshc.cpp:4008-4268, :4269-4528): the
+// slice's extents plus the offsets must lie inside the full tensor; the
+// reference runs them on the CPU only (its GPU entry points are stubs).
+static int slice_or_insert(OpKind kind, talsh_tens_t *d, talsh_tens_t *l, const int *offsets, int dev_id,
+                           int dev_kind, int copy_ctrl, int accumulative, talsh_task_t *task) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (!R.on) return TALSH_NOT_INITIALIZED;
+  if (d == nullptr || l == nullptr || offsets == nullptr) return TALSH_INVALID_ARGS;
+  if (talshTensorIsEmpty(d) != NOPE || talshTensorIsEmpty(l) != NOPE) return TALSH_OBJECT_IS_EMPTY;
+  if (copy_ctrl < 0 || copy_ctrl > 15) return TALSH_INVALID_ARGS;
+  const int rank = d->shape_p->num_dim;
+  if (rank < 1 || l->shape_p->num_dim != rank) return TALSH_INVALID_ARGS;
+  const talsh_tens_shape_t *full = (kind == kOpSlice) ? l->shape_p : d->shape_p;
+  const talsh_tens_shape_t *part = (kind == kOpSlice) ? d->shape_p : l->shape_p;
+  OpSpec op;
+  op.kind = kind;
+  op.nt = 2;
+  op.t[0] = d;
+  op.t[1] = l;
+  op.coh_ctrl = (unsigned)copy_ctrl;
+  op.accumulative = accumulative == YEP ? YEP : NOPE;
+  op.drank = op.lrank = rank;
+  for (int i = 0; i < rank; ++i) {
+    if (offsets[i] < 0 || (int64_t)offsets[i] + part->dims[i] > full->dims[i]) return TALSH_INVALID_ARGS;
+    op.offsets[i] = offsets[i];
+  }
+  return schedule(op, dev_id, dev_kind, task);
+}
+
+int talshTensorSlice(talsh_tens_t *d, talsh_tens_t *l, const int *offsets, int dev_id, int dev_kind, int copy_ctrl,
+                     int accumulative, talsh_task_t *task) {
+  return slice_or_insert(kOpSlice, d, l, offsets, dev_id, dev_kind, copy_ctrl, accumulative, task);
+}
 int talshTensorSlice_(talsh_tens_t *a, talsh_tens_t *b, const int *c, int d, int e, int f, int g, talsh_task_t *h) {
   return talshTensorSlice(a, b, c, d, e, f, g, h);
 }
-int talshTensorInsert(talsh_tens_t *, talsh_tens_t *, const int *, int, int, int, int, talsh_task_t *) { return TALSH_NOT_IMPLEMENTED; }
+int talshTensorInsert(talsh_tens_t *d, talsh_tens_t *l, const int *offsets, int dev_id, int dev_kind, int copy_ctrl,
+                      int accumulative, talsh_task_t *task) {
+  return slice_or_insert(kOpInsert, d, l, offsets, dev_id, dev_kind, copy_ctrl, accumulative, task);
+}
 int talshTensorInsert_(talsh_tens_t *a, talsh_tens_t *b, const int *c, int d, int e, int f, int g, talsh_task_t *h) {
   return talshTensorInsert(a, b, c, d, e, f, g, h);
 }

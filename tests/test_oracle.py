@@ -196,3 +196,31 @@ def test_generator_is_deterministic():
     a = O.uniform((5, 7), O.R8, 0)
     b = O.uniform((5, 7), O.R8, 0)
     assert np.array_equal(a, b) and a.min() >= -1 and a.max() <= 1 and a.std() > 0.3
+
+
+def test_slice_insert_match_numpy():
+    """tensor_block_slice / tensor_block_insert restated: sub-block reads and writes
+    equal numpy slicing (accumulating and overwriting), every kind, ranks 1-6."""
+    rng = np.random.default_rng(0)
+    for _ in range(60):
+        r = int(rng.integers(1, 7))
+        full = [int(rng.integers(1, 9)) for _ in range(r)]
+        sl = [int(rng.integers(1, f + 1)) for f in full]
+        off = [int(rng.integers(0, f - s + 1)) for f, s in zip(full, sl)]
+        idx = tuple(slice(o, o + s) for o, s in zip(off, sl))
+        for dt in (np.float32, np.float64, np.complex64, np.complex128):
+            F = np.asfortranarray((rng.uniform(-1, 1, full) + 1j * rng.uniform(-1, 1, full)).astype(dt)
+                                  if np.dtype(dt).kind == "c" else rng.uniform(-1, 1, full).astype(dt))
+            S0 = np.asfortranarray(rng.uniform(-1, 1, sl).astype(dt))
+            S = S0.copy(order="F")
+            assert O.tensor_slice(S, F, off, False) == 0 and np.array_equal(S, F[idx])
+            S = S0.copy(order="F")
+            assert O.tensor_slice(S, F, off, True) == 0 and np.array_equal(S, S0 + F[idx])
+            G, W = F.copy(order="F"), F.copy()
+            W[idx] = S0
+            assert O.tensor_insert(G, S0, off, False) == 0 and np.array_equal(G, W)
+            G, W = F.copy(order="F"), F.copy()
+            W[idx] += S0
+            assert O.tensor_insert(G, S0, off, True) == 0 and np.array_equal(G, W)
+    bad = np.asfortranarray(np.zeros((3, 3)))
+    assert O.tensor_slice(bad, np.zeros((4, 4), order="F"), [2, 0], False) != 0  # 2 + 3 > 4
