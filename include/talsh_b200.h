@@ -236,6 +236,8 @@ size_t tcTensorContractNoAllocMaxScratch(void);
  * width, [9] shared bytes, [10] tile count, [11] per-element tables in use. */
 int tcPermutePlanInfo(int data_kind, int rank, const int *dims_in, const int *o2n, int *info);
 
+/* Sub-contractions the last talshTensorContractXL call ran (diagnostics). */
+size_t tcContractXLLastOps(void);
 /* Number of kernels this library launched since load (diagnostics). */
 unsigned long long tcKernelLaunchCount(void);
 /* Last CUDA error text seen by the library (diagnostics). */

@@ -86,6 +86,8 @@ std::recursive_mutex g_mu;
 // precision with that many int8 slices (TALSH_B200_R8_SLICES or
 // talshContractSlicesSet).
 std::atomic<int> g_r8_slices{0};
+// Sub-contractions of the last talshTensorContractXL call (diagnostics).
+size_t g_xl_last_ops = 0;
 
 int node_gpu_count() {
   int n = 0;
@@ -1777,11 +1779,269 @@ int talshTensorContract_(const char *p, talsh_tens_t *d, talsh_tens_t *l, talsh_
   return talshTensorContract(p, d, l, r, a, b, c, e, f, g, t);
 }
 
+// ------------------------------------------------- out-of-core contraction
+namespace tb {
+namespace {
+
+// A sub-contraction: offsets and extents of its D, L and R blocks.
+struct XLBlock {
+  int off[3][MAX_TENSOR_RANK];
+  int dims[3][MAX_TENSOR_RANK];
+};
+
+size_t xl_bytes(const XLBlock &b, int a, int rank, int es) {
+  size_t v = (size_t)es;
+  for (int i = 0; i < rank; ++i) v *= (size_t)b.dims[a][i];
+  return v;
+}
+
+// Halves one dimension of a sub-contraction, chosen as the reference's
+// talshTensorOpDecompose2 does (talshc.cpp:3150-3294): the largest batch
+// (hyper) dimension if any, else the largest dimension of the biggest of the
+// right, left and contracted groups.  Returns false when nothing can be split.
+bool xl_split(const XLBlock &p, const int *dig, int drank, int lrank, int rrank, XLBlock &c1, XLBlock &c2) {
+  size_t lc = 1, ll = 1, lr = 1, lb = 1, sc = 0, sl = 0, sr = 0, sb = 0;
+  int mc = -1, ml = -1, mr = -1, mb = -1;
+  int dst[MAX_TENSOR_RANK] = {0};
+  for (int i = 0; i < lrank; ++i) {
+    const size_t cd = (size_t)p.dims[1][i];
+    if (dig[i] < 0) {
+      lc *= cd;
+      if (cd >= sc) { sc = cd; mc = i; }
+    } else if (dig[i] > 0) {
+      dst[dig[i] - 1] = i + 1;
+      ll *= cd;
+      if (cd >= sl) { sl = cd; ml = i; }
+    }
+  }
+  for (int i = 0; i < rrank; ++i) {
+    const size_t cd = (size_t)p.dims[2][i];
+    const int j = dig[lrank + i];
+    if (j <= 0) continue;
+    if (dst[j - 1] == 0) {
+      lr *= cd;
+      if (cd >= sr) { sr = cd; mr = lrank + i; }
+    } else {  // batch (hyper) index
+      ll /= cd;
+      lb *= cd;
+      if (cd >= sb) { sb = cd; mb = lrank + i; }
+    }
+  }
+  if (lb <= 1 && lr <= 1 && ll <= 1 && lc <= 1) return false;
+  int d0 = -1, d1 = -1, d2 = -1;  // split positions in D, L, R (-1: not split)
+  if (lb > 1) {
+    d0 = dig[mb] - 1; d1 = dst[d0] - 1; d2 = mb - lrank;
+  } else if (lr >= ll && lr >= lc) {
+    d0 = dig[mr] - 1; d2 = mr - lrank;
+  } else if (ll >= lr && ll >= lc) {
+    d0 = dig[ml] - 1; d1 = ml;
+  } else {
+    d1 = mc; d2 = -dig[mc] - 1;
+  }
+  c1 = p;
+  c2 = p;
+  const int at[3] = {d0, d1, d2};
+  for (int a = 0; a < 3; ++a) {
+    const int x = at[a];
+    if (x < 0) continue;
+    const int h1 = (p.dims[a][x] + 1) / 2, h2 = p.dims[a][x] - h1;
+    if (h2 <= 0) return false;
+    c1.dims[a][x] = h1;
+    c2.dims[a][x] = h2;
+    c2.off[a][x] += h1;
+  }
+  (void)drank;
+  return true;
+}
+
+// Device address of a Host body: pinned bodies are mapped already; other
+// (caller) memory is registered for the duration of the call.
+void *xl_map(void *host, size_t bytes, bool &registered) {
+  registered = false;
+  cudaPointerAttributes at;
+  if (cudaPointerGetAttributes(&at, host) == cudaSuccess && at.type == cudaMemoryTypeHost && at.devicePointer)
+    return at.devicePointer;
+  cudaGetLastError();
+  const cudaError_t e = cudaHostRegister(host, bytes, cudaHostRegisterMapped | cudaHostRegisterPortable);
+  if (e == cudaErrorHostMemoryAlreadyRegistered) {
+    cudaGetLastError();  // registered by someone else: just map it
+  } else if (e != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  } else {
+    registered = true;
+  }
+  void *dp = nullptr;
+  if (cudaHostGetDevicePointer(&dp, host, 0) != cudaSuccess) {
+    cudaGetLastError();
+    cudaHostUnregister(host);
+    registered = false;
+    return nullptr;
+  }
+  return dp;
+}
+
+}  // namespace
+}  // namespace tb
+
+// Out-of-core contraction (reference talshTensorContractXL, talshc.cpp:5394-5648):
+// the operands are placed on the Host, the contraction is halved along its
+// largest dimension until the three blocks of every sub-contraction fit a
+// quarter of the GPU's free budget, and the sub-contractions run one after
+// another on the GPU's stream: gather the L, R and D blocks straight from
+// mapped Host memory (tcTensorSlice), contract into the D block, write it back
+// (tcTensorInsert).  Sub-contractions that split a contracted dimension add
+// into the same D block in stream order.  Blocking, like the reference.
 int talshTensorContractXL(const char *cptrn, talsh_tens_t *d, talsh_tens_t *l, talsh_tens_t *r, double sr, double si,
                           int dev_id, int dev_kind, int accumulative) {
-  // Without out-of-core decomposition yet: a blocking contraction on one GPU.
-  return talshTensorContract(cptrn, d, l, r, sr, si, dev_id, dev_kind, COPY_MTT, accumulative, nullptr);
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (!R.on) return TALSH_NOT_INITIALIZED;
+  if (cptrn == nullptr || d == nullptr || l == nullptr || r == nullptr) return TALSH_INVALID_ARGS;
+  if (talshTensorIsEmpty(d) != NOPE || talshTensorIsEmpty(l) != NOPE || talshTensorIsEmpty(r) != NOPE)
+    return TALSH_OBJECT_IS_EMPTY;
+  if (!healthy(d) || !healthy(l) || !healthy(r)) return TALSH_OBJECT_BROKEN;
+  OpSpec op;
+  op.kind = kOpContract;
+  op.nt = 3;
+  op.t[0] = d; op.t[1] = l; op.t[2] = r;
+  int rc = parse_and_check(cptrn, op, 2);
+  if (rc) return rc;
+  int err = 0;
+  talsh_tens_t *ts[3] = {d, l, r};
+  const int gpu = resolve_gpu(dev_id, dev_kind, ts, 3, err);
+  if (gpu < 0) return err;
+  // Operands on the Host; D keeps only its Host image.
+  for (talsh_tens_t *t : {r, l, d})
+    if ((rc = talshTensorPlace(t, 0, DEV_HOST, nullptr, COPY_K, nullptr)) != TALSH_SUCCESS) return rc;
+  if ((rc = talshTensorDiscardOther(d, 0, DEV_HOST)) != TALSH_SUCCESS) return rc;
+  void *hp[3];
+  int kind = NO_TYPE;
+  for (int a = 0; a < 3; ++a) {
+    const int i = choose_image(ts[a], DEV_HOST, 0);
+    if (i < 0) return TALSH_FAILURE;
+    hp[a] = ts[a]->dev_rsc[i].gmem_p;
+    if (a == 0) kind = ts[a]->data_kind[i];
+    else if (ts[a]->data_kind[i] != kind) return TALSH_INVALID_ARGS;
+  }
+  const int es = kind_size(kind);
+  if (es == 0) return TALSH_INVALID_ARGS;
+  const int rank[3] = {op.drank, op.lrank, op.rrank};
+  const int *full[3] = {d->shape_p->dims, l->shape_p->dims, r->shape_p->dims};
+  // Decomposition.
+  GpuCtx &G = R.gpu[gpu];
+  const size_t avail = G.budget > G.used ? G.budget - G.used : 0;
+  std::vector<XLBlock> ops(1), next;
+  std::memset(&ops[0], 0, sizeof(XLBlock));
+  for (int a = 0; a < 3; ++a)
+    for (int i = 0; i < rank[a]; ++i) ops[0].dims[a][i] = full[a][i];
+  const size_t kMaxOps = 1 << 16;
+  for (bool again = true; again;) {
+    again = false;
+    next.clear();
+    for (const XLBlock &b : ops) {
+      const size_t need = xl_bytes(b, 0, rank[0], es) + xl_bytes(b, 1, rank[1], es) + xl_bytes(b, 2, rank[2], es);
+      XLBlock c1, c2;
+      if (need * 4 > avail && xl_split(b, op.dig, op.drank, op.lrank, op.rrank, c1, c2)) {
+        next.push_back(c1);
+        next.push_back(c2);
+        again = true;
+      } else {
+        next.push_back(b);
+      }
+    }
+    ops.swap(next);
+    if (ops.size() > kMaxOps) return TALSH_LIMIT_EXCEEDED;
+  }
+  // Device buffers sized for the largest block of each argument, and scratch.
+  size_t bb[3] = {0, 0, 0}, scratch_bytes = 0;
+  const int sl = g_r8_slices.load();
+  bool hyper = false;
+  for (int i = 0; i < op.lrank && !hyper; ++i)
+    for (int j = 0; j < op.rrank; ++j)
+      if (op.dig[i] > 0 && op.dig[i] == op.dig[op.lrank + j]) { hyper = true; break; }
+  const bool split = sl > 0 && kind == R8 && op.conj == 0 && !hyper && op.drank > 0 && op.lrank > 0 && op.rrank > 0;
+  for (const XLBlock &b : ops) {
+    for (int a = 0; a < 3; ++a) bb[a] = std::max(bb[a], xl_bytes(b, a, rank[a], es));
+    const size_t sc = split ? contract_split_scratch(kind, op.dig, op.drank, b.dims[0], op.lrank, b.dims[1], op.rrank,
+                                                     b.dims[2], sl)
+                            : contract_scratch_bytes(kind, op.dig, op.drank, b.dims[0], op.lrank, b.dims[1],
+                                                     op.rrank, b.dims[2]);
+    scratch_bytes = std::max(scratch_bytes, sc);
+  }
+  void *db[3] = {nullptr, nullptr, nullptr}, *scr = nullptr;
+  bool reg[3] = {false, false, false};
+  void *mp[3] = {nullptr, nullptr, nullptr};
+  auto cleanup = [&]() {
+    cudaStreamSynchronize(G.stream);
+    cudaGetLastError();
+    for (int a = 0; a < 3; ++a) {
+      if (db[a]) mem_free(db[a]);
+      if (reg[a]) cudaHostUnregister(hp[a]);
+    }
+    if (scr) mem_free(scr);
+  };
+  cudaSetDevice(gpu);
+  for (int a = 0; a < 3 && rc == TALSH_SUCCESS; ++a) rc = dev_alloc(gpu, bb[a], &db[a]);
+  if (rc == TALSH_SUCCESS && scratch_bytes) rc = dev_alloc(gpu, scratch_bytes, &scr);
+  for (int a = 0; a < 3 && rc == TALSH_SUCCESS; ++a) {
+    const size_t whole = shape_volume(ts[a]->shape_p) * (size_t)es;
+    mp[a] = xl_map(hp[a], whole, reg[a]);
+    if (mp[a] == nullptr) rc = TALSH_FAILURE;
+  }
+  if (rc != TALSH_SUCCESS) {
+    cleanup();
+    return rc;
+  }
+  if (accumulative == NOPE) std::memset(hp[0], 0, shape_volume(d->shape_p) * (size_t)es);
+  cudaStream_t st = G.stream;
+  double flops = 0.0;
+  for (const XLBlock &b : ops) {
+    // gather the blocks (rank-0 arguments are single elements)
+    for (int a = 0; a < 3 && rc == TALSH_SUCCESS; ++a) {
+      if (rank[a] == 0) {
+        const cudaError_t e = cudaMemcpyAsync(db[a], mp[a], (size_t)es, cudaMemcpyDefault, st);
+        if (e != cudaSuccess) { note_cuda_error("XL scalar gather", (int)e); rc = TALSH_FAILURE; }
+      } else {
+        rc = tcTensorSlice(kind, rank[a], full[a], b.dims[a], b.off[a], mp[a], db[a], 0, st);
+      }
+    }
+    if (rc != TALSH_SUCCESS) break;
+    if (split)
+      rc = contract_split_launch(kind, op.dig, op.drank, b.dims[0], op.lrank, b.dims[1], op.rrank, b.dims[2], db[0],
+                                 db[1], db[2], sr, YEP, sl, scr, scratch_bytes, st);
+    else
+      rc = contract_launch(kind, op.dig, op.drank, b.dims[0], op.lrank, b.dims[1], op.rrank, b.dims[2], db[0], db[1],
+                           db[2], sr, si, op.conj, 1, scr, scratch_bytes, st);
+    if (rc != TALSH_SUCCESS) break;
+    if (rank[0] == 0) {
+      const cudaError_t e = cudaMemcpyAsync(mp[0], db[0], (size_t)es, cudaMemcpyDefault, st);
+      if (e != cudaSuccess) { note_cuda_error("XL scalar store", (int)e); rc = TALSH_FAILURE; }
+    } else {
+      rc = tcTensorInsert(kind, rank[0], full[0], b.dims[0], b.off[0], db[0], mp[0], 0, st);
+    }
+    if (rc != TALSH_SUCCESS) break;
+    double m = 1.0, n = 1.0, k = 1.0;
+    for (int i = 0; i < op.lrank; ++i) (op.dig[i] > 0 ? m : k) *= (double)b.dims[1][i];
+    for (int i = 0; i < op.rrank; ++i) if (op.dig[op.lrank + i] > 0) n *= (double)b.dims[2][i];
+    flops += (kind_is_complex(kind) ? 8.0 : 2.0) * m * n * k;
+  }
+  const cudaError_t se = cudaStreamSynchronize(st);
+  if (rc == TALSH_SUCCESS && se != cudaSuccess) {
+    note_cuda_error("XL contraction", (int)se);
+    rc = TALSH_FAILURE;
+  }
+  cleanup();
+  if (rc == TALSH_SUCCESS) {
+    G.flops += flops;
+    G.tasks_ok++;
+    g_xl_last_ops = ops.size();
+  } else {
+    G.tasks_failed++;
+  }
+  return rc;
 }
+size_t tcContractXLLastOps(void) { return g_xl_last_ops; }
+
 int talshTensorContractXL_(const char *p, talsh_tens_t *d, talsh_tens_t *l, talsh_tens_t *r, double a, double b, int c,
                            int e, int f) {
   return talshTensorContractXL(p, d, l, r, a, b, c, e, f);
