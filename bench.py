@@ -714,6 +714,7 @@ def bench_batch(T, L, torch, dev):
     flops = sum((2.0 if k == R8 else 8.0) * mnk for k, _, _, _, _, mnk in tasks)
     # inputs: one random pool shared read-only by all tasks; outputs: one region per task
     maxin = max(max(int(np.prod(ld)), int(np.prod(rd))) * es[k] for k, _, _, ld, rd, _ in tasks)
+    maxin = (maxin + 255) // 256 * 256  # operands aligned to their element size
     pool = torch.empty(2 * maxin + 256, dtype=torch.uint8, device=dev)
     pool.view(torch.float64).uniform_(-1.0, 1.0)
     douts, off = [], 0

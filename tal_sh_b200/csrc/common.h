@@ -21,6 +21,12 @@ inline int kind_size(int kind) {
   }
 }
 inline bool kind_is_complex(int kind) { return kind == C4 || kind == C8; }
+// True when p is aligned to the element size of kind (the kernels move whole
+// elements with vector accesses; a complex(8) body must be 16-byte aligned).
+inline bool elem_aligned(int kind, const void *p) {
+  const int es = kind_size(kind);
+  return es > 0 && (reinterpret_cast<uintptr_t>(p) % (uintptr_t)es) == 0;
+}
 
 // Real approximant of a complex scale factor that keeps the modulus and the
 // sign of the real part (reference cmplx8_to_real8, tensor_algebra_cpu.F90:430-445).

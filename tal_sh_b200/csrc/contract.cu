@@ -146,14 +146,43 @@ __device__ __forceinline__ void dmma_8x8x4(double &c0, double &c1, double a, dou
 
 template <int BM, int BN>
 struct DmmaCfg {
-  static constexpr int WM = 32, WN = 32;            // warp tile
+  // warp tile: 32x32, or 16x16 in 32x32 CTA tiles (four warps per small tile)
+  static constexpr int WM = BM <= 32 ? 16 : 32, WN = BN <= 32 ? 16 : 32;
   static constexpr int WARPS_M = BM / WM, WARPS_N = BN / WN;
   static constexpr int THREADS = WARPS_M * WARPS_N * 32;
   static constexpr int BK = 16, STAGES = 3;
   static constexpr int AP = BM + 8, BP = BN + 8;    // pitches: 2-wavefront fragment loads
   static constexpr size_t SMEM = (size_t)STAGES * BK * (AP + BP) * sizeof(double) +
-                                 (size_t)(2 * BM + 2 * BN) * sizeof(int64_t);
+                                 (size_t)(2 * BM + 2 * BN + 2 * STAGES * BK) * sizeof(int64_t);
 };
+
+// k-offset tables of the tiles in flight live in a shared ring (slot t % ST
+// holds tile t's BK entries of kL and kR).  The tables of tiles 0..ST-1 are
+// written before the main loop; afterwards warp 0 fetches tile t+ST's entries
+// from global memory during iteration t and stores them at its end, so the
+// address of a cp.async never waits for a global load.
+template <int BK, int ST>
+__device__ __forceinline__ void kring_init(const GemmArgs &a, int64_t *kLs, int64_t *kRs, int tid, int nt,
+                                           int64_t &pf) {
+  for (int i = tid; i < ST * BK; i += nt) {
+    kLs[i] = i < a.K ? a.kL[i] : 0;
+    kRs[i] = i < a.K ? a.kR[i] : 0;
+  }
+  if (tid < 2 * BK) {
+    const int k = ST * BK + (tid % BK);
+    pf = k < a.K ? (tid < BK ? a.kL[k] : a.kR[k]) : 0;
+  }
+}
+template <int BK, int ST>
+__device__ __forceinline__ void kring_step(const GemmArgs &a, int64_t *kLs, int64_t *kRs, int tid, int kt,
+                                           int64_t &pf) {
+  if (tid < 2 * BK) {
+    const int j = tid % BK;
+    (tid < BK ? kLs : kRs)[(kt % ST) * BK + j] = pf;
+    const int64_t k = (int64_t)(kt + ST + 1) * BK + j;
+    pf = k < a.K ? (tid < BK ? a.kL[k] : a.kR[k]) : 0;
+  }
+}
 
 // One BM x BN tile of a gather-GEMM (shared by the single-contraction kernel and
 // the batched one).
@@ -169,6 +198,9 @@ __device__ __forceinline__ void dmma_tile(const double *__restrict__ L, const do
   int64_t *mDs = mLs + BM;
   int64_t *nRs = mDs + BM;
   int64_t *nDs = nRs + BN;
+  int64_t *kLs = nDs + BN;
+  int64_t *kRs = kLs + ST * BK;
+  int64_t pf = 0;
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int m0 = tile_m * BM, n0 = tile_n * BN;
@@ -182,6 +214,7 @@ __device__ __forceinline__ void dmma_tile(const double *__restrict__ L, const do
     nRs[i] = n < a.N ? a.nR[n] : 0;
     nDs[i] = n < a.N ? a.nD[n] : 0;
   }
+  kring_init<BK, ST>(a, kLs, kRs, tid, NT, pf);
   __syncthreads();
 
   const int numK = (a.K + BK - 1) / BK;
@@ -195,7 +228,7 @@ __device__ __forceinline__ void dmma_tile(const double *__restrict__ L, const do
       const int kl = a.a_along_m ? (idx / BM) : (idx % BK);
       const int m = m0 + ml, k = kt * BK + kl;
       const bool v = (m < a.M) && (k < a.K);
-      const double *src = v ? (L + mLs[ml] + a.kL[k]) : L;
+      const double *src = v ? (L + mLs[ml] + kLs[s * BK + kl]) : L;
       cp_async8(as + kl * AP + ml, src, v);
     }
 #pragma unroll
@@ -205,7 +238,7 @@ __device__ __forceinline__ void dmma_tile(const double *__restrict__ L, const do
       const int kl = a.b_along_n ? (idx / BN) : (idx % BK);
       const int n = n0 + nl, k = kt * BK + kl;
       const bool v = (n < a.N) && (k < a.K);
-      const double *src = v ? (R + nRs[nl] + a.kR[k]) : R;
+      const double *src = v ? (R + nRs[nl] + kRs[s * BK + kl]) : R;
       cp_async8(bs + kl * BP + nl, src, v);
     }
   };
@@ -245,6 +278,7 @@ __device__ __forceinline__ void dmma_tile(const double *__restrict__ L, const do
 #pragma unroll
         for (int j = 0; j < FN; ++j) dmma_8x8x4(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
     }
+    kring_step<BK, ST>(a, kLs, kRs, tid, kt, pf);
   }
   cp_async_wait<0>();
 
@@ -266,26 +300,31 @@ __device__ __forceinline__ void dmma_tile(const double *__restrict__ L, const do
   }
 }
 
-// Complex-double tile on the FP64 tensor pipe: real and imaginary parts are
-// gathered into separate shared planes and C_re += A_re B_re - A_im B_im,
-// C_im += A_re B_im + A_im B_re run as four DMMA products.
-// Warp tiles are 32 x 16: two accumulator sets (real, imaginary) per fragment.
+// Complex-double tile on the FP64 tensor pipe: complex elements stay
+// interleaved in shared memory (one 16-byte cp.async per element, one 128-bit
+// load per fragment element), and
+// C_re += A_re B_re - A_im B_im, C_im += A_re B_im + A_im B_re run as four
+// DMMA products.  Row pitches of BM + 2 elements put the four k-rows of a
+// fragment load in different bank groups.
+// Warp tiles are 32 x 16 (16 x 16 in 32x32 CTA tiles): two accumulator sets
+// (real, imaginary) per fragment.
 template <int BM, int BN>
 struct ZmmaCfg {
-  static constexpr int WM = 32, WN = 16;
+  static constexpr int WM = BM <= 32 ? 16 : 32, WN = 16;
   static constexpr int WARPS_M = BM / WM, WARPS_N = BN / WN;
   static constexpr int THREADS = WARPS_M * WARPS_N * 32;
-  static constexpr int BK = 16, STAGES = 3;
-  static constexpr int AP = BM + 8, BP = BN + 8;
-  static constexpr size_t SMEM = 2 * (size_t)STAGES * BK * (AP + BP) * sizeof(double) +
-                                 (size_t)(2 * BM + 2 * BN) * sizeof(int64_t);
+  static constexpr int BK = 16, STAGES = BM <= 32 ? 2 : 3;  // two stages keep five small CTAs per SM
+  static constexpr int AP = BM + 2, BP = BN + 2;           // in complex elements
+  static constexpr size_t SMEM = (size_t)STAGES * BK * (AP + BP) * sizeof(double2) +
+                                 (size_t)(2 * BM + 2 * BN + 2 * STAGES * BK) * sizeof(int64_t);
 };
 
-__device__ __forceinline__ void cp_async16(void *smem_lo, void *smem_hi, const void *gptr, bool valid) {
-  // one double2 element: real part to one plane, imaginary part to the other
-  cp_async8(smem_lo, gptr, valid);
-  cp_async8(smem_hi, (const char *)gptr + 8, valid);
+__device__ __forceinline__ void cp_async16(void *smem_ptr, const void *gptr, bool valid) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem_ptr);
+  const int n = valid ? 16 : 0;
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gptr), "r"(n));
 }
+
 
 template <int BM, int BN>
 __device__ __forceinline__ void zmma_tile(const double2 *__restrict__ L, const double2 *__restrict__ R,
@@ -293,14 +332,15 @@ __device__ __forceinline__ void zmma_tile(const double2 *__restrict__ L, const d
                                           unsigned char *smem) {
   using C = ZmmaCfg<BM, BN>;
   constexpr int BK = C::BK, ST = C::STAGES, AP = C::AP, BP = C::BP, NT = C::THREADS;
-  double *Ar = reinterpret_cast<double *>(smem);
-  double *Ai = Ar + ST * BK * AP;
-  double *Br = Ai + ST * BK * AP;
-  double *Bi = Br + ST * BK * BP;
-  int64_t *mLs = reinterpret_cast<int64_t *>(Bi + ST * BK * BP);
+  double2 *As = reinterpret_cast<double2 *>(smem);
+  double2 *Bs = As + ST * BK * AP;
+  int64_t *mLs = reinterpret_cast<int64_t *>(Bs + ST * BK * BP);
   int64_t *mDs = mLs + BM;
   int64_t *nRs = mDs + BM;
   int64_t *nDs = nRs + BN;
+  int64_t *kLs = nDs + BN;
+  int64_t *kRs = kLs + ST * BK;
+  int64_t pf = 0;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int m0 = tile_m * BM, n0 = tile_n * BN;
   for (int i = tid; i < BM; i += NT) {
@@ -313,6 +353,7 @@ __device__ __forceinline__ void zmma_tile(const double2 *__restrict__ L, const d
     nRs[i] = n < a.N ? a.nR[n] : 0;
     nDs[i] = n < a.N ? a.nD[n] : 0;
   }
+  kring_init<BK, ST>(a, kLs, kRs, tid, NT, pf);
   __syncthreads();
   const int numK = (a.K + BK - 1) / BK;
   auto load_tile = [&](int kt, int s) {
@@ -323,9 +364,8 @@ __device__ __forceinline__ void zmma_tile(const double2 *__restrict__ L, const d
       const int kl = a.a_along_m ? (idx / BM) : (idx % BK);
       const int m = m0 + ml, k = kt * BK + kl;
       const bool v = (m < a.M) && (k < a.K);
-      const double2 *src = v ? (L + mLs[ml] + a.kL[k]) : L;
-      const int o = s * BK * AP + kl * AP + ml;
-      cp_async16(Ar + o, Ai + o, src, v);
+      const double2 *src = v ? (L + mLs[ml] + kLs[s * BK + kl]) : L;
+      cp_async16(As + (s * BK + kl) * AP + ml, src, v);
     }
 #pragma unroll
     for (int i = 0; i < (BN * BK) / NT; ++i) {
@@ -334,9 +374,8 @@ __device__ __forceinline__ void zmma_tile(const double2 *__restrict__ L, const d
       const int kl = a.b_along_n ? (idx / BN) : (idx % BK);
       const int n = n0 + nl, k = kt * BK + kl;
       const bool v = (n < a.N) && (k < a.K);
-      const double2 *src = v ? (R + nRs[nl] + a.kR[k]) : R;
-      const int o = s * BK * BP + kl * BP + nl;
-      cp_async16(Br + o, Bi + o, src, v);
+      const double2 *src = v ? (R + nRs[nl] + kRs[s * BK + kl]) : R;
+      cp_async16(Bs + (s * BK + kl) * BP + nl, src, v);
     }
   };
   constexpr int FM = C::WM / 8, FN = C::WN / 8;
@@ -365,16 +404,16 @@ __device__ __forceinline__ void zmma_tile(const double2 *__restrict__ L, const d
       double ar[FM], ai[FM], nai[FM], br[FN], bi[FN];
 #pragma unroll
       for (int i = 0; i < FM; ++i) {
-        const int o = so * BK * AP + (ks * 4 + fc) * AP + wm0 + i * 8 + fr;
-        ar[i] = Ar[o];
-        ai[i] = sl * Ai[o];
+        const double2 v = As[(so * BK + ks * 4 + fc) * AP + wm0 + i * 8 + fr];
+        ar[i] = v.x;
+        ai[i] = sl * v.y;
         nai[i] = -ai[i];
       }
 #pragma unroll
       for (int j = 0; j < FN; ++j) {
-        const int o = so * BK * BP + (ks * 4 + fc) * BP + wn0 + j * 8 + fr;
-        br[j] = Br[o];
-        bi[j] = sr * Bi[o];
+        const double2 v = Bs[(so * BK + ks * 4 + fc) * BP + wn0 + j * 8 + fr];
+        br[j] = v.x;
+        bi[j] = sr * v.y;
       }
 #pragma unroll
       for (int i = 0; i < FM; ++i)
@@ -386,6 +425,7 @@ __device__ __forceinline__ void zmma_tile(const double2 *__restrict__ L, const d
           dmma_8x8x4(ci[i][j][0], ci[i][j][1], ai[i], br[j]);
         }
     }
+    kring_step<BK, ST>(a, kLs, kRs, tid, kt, pf);
   }
   cp_async_wait<0>();
   const double alr = a.alpha_re, ali = a.alpha_im;
@@ -856,6 +896,13 @@ int launch_scalar(const void *L, const void *R, void *D, double ar, double ai, i
   return check_launch("scalar_mul_kernel");
 }
 
+// Operands must be aligned to their element size (16 bytes for C8): the
+// kernels move whole elements with vector loads and stores.
+bool elements_aligned(int kind, const void *D, const void *L, const void *R) {
+  const uintptr_t m = (uintptr_t)kind_size(kind) - 1;
+  return ((reinterpret_cast<uintptr_t>(D) | reinterpret_cast<uintptr_t>(L) | reinterpret_cast<uintptr_t>(R)) & m) == 0;
+}
+
 // Shape / kind checks shared by the scratch query and the launch.
 int check_args(int kind, const int *cptrn, int drank, const int *ddims, int lrank, const int *ldims,
                int rrank, const int *rdims) {
@@ -914,6 +961,7 @@ int contract_launch(int kind, const int *cptrn, int drank, const int *ddims, int
   int rc = check_args(kind, cptrn, drank, ddims, lrank, ldims, rrank, rdims);
   if (rc) return rc;
   if (D == nullptr || L == nullptr || R == nullptr) return TALSH_INVALID_ARGS;
+  if (!elements_aligned(kind, D, L, R)) return TALSH_INVALID_ARGS;
   const bool cplx = kind_is_complex(kind);
   int cl = 0, cr = 0;
   if (cplx) {
@@ -1141,7 +1189,8 @@ __device__ __forceinline__ int64_t next_item(unsigned long long *ctr) {
 
 // Resident CTAs per SM asked of the compiler for the persistent batch kernels.
 template <int BM, int BN> struct BatchOcc { static constexpr int D = 1, Z = 1; };
-template <> struct BatchOcc<64, 64> { static constexpr int D = 1, Z = 2; };
+template <> struct BatchOcc<64, 64> { static constexpr int D = 3, Z = 2; };
+template <> struct BatchOcc<32, 32> { static constexpr int D = 6, Z = 5; };
 
 template <int BM, int BN>
 __global__ void __launch_bounds__(DmmaCfg<BM, BN>::THREADS, BatchOcc<BM, BN>::D)
@@ -1222,6 +1271,7 @@ int batch_plan(int ntasks, const tcContractTask *tasks, BatchPlan &bp) {
     int rc = check_args(x.data_kind, x.cptrn, x.drank, x.ddims, x.lrank, x.ldims, x.rrank, x.rdims);
     if (rc) return rc;
     if (x.D == nullptr || x.L == nullptr || x.R == nullptr) return TALSH_INVALID_ARGS;
+    if (!elements_aligned(x.data_kind, x.D, x.L, x.R)) return TALSH_INVALID_ARGS;
     Analysis an;
     bool batchable = x.lrank > 0 && x.rrank > 0;  // a full contraction (D of rank 0) is a 1 x 1 GEMM
     if (batchable) {

@@ -126,6 +126,7 @@ using namespace tb;
 extern "C" int tcTensorInit(int data_kind, size_t vol, void *dst, double val_re, double val_im,
                             void *stream) {
   if (kind_size(data_kind) == 0 || (dst == nullptr && vol > 0)) return TALSH_INVALID_ARGS;
+  if (vol > 0 && !elem_aligned(data_kind, dst)) return TALSH_INVALID_ARGS;
   if (vol == 0) return TALSH_SUCCESS;
   cudaStream_t st = (cudaStream_t)stream;
   const int grid = grid_for((int64_t)vol);
@@ -147,6 +148,7 @@ extern "C" int tcTensorInit(int data_kind, size_t vol, void *dst, double val_re,
 extern "C" int tcTensorScale(int data_kind, size_t vol, void *dst, double alpha_re,
                              double alpha_im, void *stream) {
   if (kind_size(data_kind) == 0 || (dst == nullptr && vol > 0)) return TALSH_INVALID_ARGS;
+  if (vol > 0 && !elem_aligned(data_kind, dst)) return TALSH_INVALID_ARGS;
   if (vol == 0) return TALSH_SUCCESS;
   cudaStream_t st = (cudaStream_t)stream;
   const int grid = grid_for((int64_t)vol);
@@ -186,6 +188,7 @@ int norm1_launch(int data_kind, size_t vol, const void *src, double *result_dev,
 
 extern "C" int tcTensorNorm1(int data_kind, size_t vol, const void *src, double *result_dev,
                              void *scratch, size_t scratch_bytes, void *stream) {
+  if (vol > 0 && src != nullptr && !elem_aligned(data_kind, src)) return TALSH_INVALID_ARGS;
   if (kind_size(data_kind) == 0 || result_dev == nullptr || (src == nullptr && vol > 0))
     return TALSH_INVALID_ARGS;
   if (vol == 0) return TALSH_INVALID_ARGS;

@@ -664,6 +664,7 @@ int contract_split_launch(int kind, const int *cptrn, int drank, const int *ddim
   if (slices <= 0) slices = 6;
   if (slices < 2 || slices > kOzMaxSlices) return TALSH_INVALID_ARGS;
   if (D == nullptr || L == nullptr || R == nullptr || cptrn == nullptr) return TALSH_INVALID_ARGS;
+  if (!elem_aligned(R8, D) || !elem_aligned(R8, L) || !elem_aligned(R8, R)) return TALSH_INVALID_ARGS;
   const size_t need = contract_split_scratch(kind, cptrn, drank, ddims, lrank, ldims, rrank, rdims, slices);
   if (need == 0 || scratch == nullptr || scratch_bytes < need) return TALSH_INVALID_ARGS;
   cudaStream_t st = (cudaStream_t)stream;

@@ -1196,6 +1196,7 @@ int permute_entry(int kind, int rank, const int *dims, const int *o2n, const voi
   int rc = validate(kind, rank, dims, o2n);
   if (rc) return rc;
   if (src == nullptr || dst == nullptr) return TALSH_INVALID_ARGS;
+  if (!elem_aligned(kind, src) || !elem_aligned(kind, dst)) return TALSH_INVALID_ARGS;
   if (!kind_is_complex(kind)) conj = 0;
   Fused F;
   if (rank == 0) { F.n = 0; F.vol = 1; }

@@ -120,6 +120,7 @@ int slice_op(bool insert, int kind, int rank, const int *full_dims, const int *s
   if (kind_size(kind) == 0 || rank < 1 || rank > kMaxRank || full_dims == nullptr || slice_dims == nullptr ||
       offsets == nullptr || src == nullptr || dst == nullptr)
     return TALSH_INVALID_ARGS;
+  if (!elem_aligned(kind, src) || !elem_aligned(kind, dst)) return TALSH_INVALID_ARGS;
   for (int i = 0; i < rank; ++i)
     if (full_dims[i] <= 0 || slice_dims[i] <= 0 || offsets[i] < 0 || offsets[i] + (int64_t)slice_dims[i] > full_dims[i])
       return TALSH_INVALID_ARGS;

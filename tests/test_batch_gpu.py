@@ -110,3 +110,33 @@ def test_batch_rejects_bad_tasks(talsh):
     assert lib.tcTensorContractBatchScratch(1, tasks) == 0
     assert lib.tcTensorContractBatch(1, tasks, None, 0, None) == T.TALSH_INVALID_ARGS
     assert lib.tcTensorContractBatch(0, tasks, None, 0, None) == 0
+
+
+def test_operands_must_be_element_aligned(talsh):
+    """Device operands aligned to less than their element size (an 8-byte
+    aligned complex(8) tensor) are refused before any launch, alone and batched."""
+    torch = pytest.importorskip("torch")
+    lib = T.lib()
+    rng = np.random.default_rng(21)
+    sp = random_task(rng, T.C8)
+    buf = torch.zeros(1 << 16, dtype=torch.float64, device="cuda")
+    args = (T.C8, T.ivec(sp["cptrn"]), len(sp["dd"]), T.ivec(sp["dd"]), len(sp["ld"]), T.ivec(sp["ld"]),
+            len(sp["rd"]), T.ivec(sp["rd"]))
+    ns = lib.tcTensorContractScratch(*args)
+    sc = torch.empty(max(ns, 1), dtype=torch.uint8, device="cuda")
+    base = buf.data_ptr()
+    for dp, lp, rp in ((base + 8, base + 4096, base + 8192), (base, base + 4104, base + 8192),
+                       (base, base + 4096, base + 8200)):
+        assert lib.tcTensorContract(*args, dp, lp, rp, 1.0, 0.0, 0, 0, sc.data_ptr(), ns, None) == \
+            T.TALSH_INVALID_ARGS
+        t = (T.ContractTask * 1)()
+        x = t[0]
+        x.data_kind, x.drank, x.lrank, x.rrank = T.C8, len(sp["dd"]), len(sp["ld"]), len(sp["rd"])
+        for i, v in enumerate(sp["cptrn"]):
+            x.cptrn[i] = v
+        for arr, name in ((sp["dd"], "ddims"), (sp["ld"], "ldims"), (sp["rd"], "rdims")):
+            for i, v in enumerate(arr):
+                getattr(x, name)[i] = v
+        x.D, x.L, x.R = dp, lp, rp
+        assert lib.tcTensorContractBatchScratch(1, t) == 0
+        assert lib.tcTensorContractBatch(1, t, sc.data_ptr(), 1 << 20, None) == T.TALSH_INVALID_ARGS
