@@ -314,12 +314,17 @@ def main():
     ap.add_argument("--profile-contract", default=None,
                     help="C3a|C3b:v:o[:slices] -- run one FP64 contraction (plain, or split with slices) "
                          "four times (for ncu) and exit")
+    ap.add_argument("--profile-batch", action="store_true",
+                    help="run the C4 batch (4096 small contractions) four times (for ncu) and exit")
     args = ap.parse_args()
     if args.profile_case:
         profile_case(args.profile_case, args.profile_op)
         return
     if args.profile_contract:
         profile_contract(args.profile_contract)
+        return
+    if args.profile_batch:
+        profile_batch()
         return
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -707,12 +712,10 @@ def c4_tasks(seed=4096, ntasks=4096, cap=1 << 21):
     return out
 
 
-def bench_batch(T, L, torch, dev):
-    """C4: 4096 small contractions, batched (tcTensorContractBatch) vs one call per task."""
-    tasks = c4_tasks()
+def c4_prepare(T, L, torch, dev, tasks):
+    """Device buffers and tcContractTask records for the C4 tasks: one random input
+    pool shared read-only by all tasks, one output region per task (256-byte aligned)."""
     es = {R8: 8, C8: 16}
-    flops = sum((2.0 if k == R8 else 8.0) * mnk for k, _, _, _, _, mnk in tasks)
-    # inputs: one random pool shared read-only by all tasks; outputs: one region per task
     maxin = max(max(int(np.prod(ld)), int(np.prod(rd))) * es[k] for k, _, _, ld, rd, _ in tasks)
     maxin = (maxin + 255) // 256 * 256  # operands aligned to their element size
     pool = torch.empty(2 * maxin + 256, dtype=torch.uint8, device=dev)
@@ -737,9 +740,36 @@ def bench_batch(T, L, torch, dev):
         t.L = pool.data_ptr()
         t.R = pool.data_ptr() + maxin
         t.alpha_re, t.alpha_im, t.conj_bits, t.accumulative = 1.0, 0.0, 0, 1
-    s = torch.cuda.current_stream(dev).cuda_stream
     need = L.tcTensorContractBatchScratch(len(tasks), arr)
     scratch = torch.empty(need, dtype=torch.uint8, device=dev)
+    return arr, scratch, need, (pool, dbuf)
+
+
+def profile_batch():
+    """The C4 batch through tcTensorContractBatch, four calls, for profilers."""
+    import torch
+    import tal_sh_b200 as T
+    L = T.lib()
+    dev = torch.device("cuda", 0)
+    tasks = c4_tasks()
+    arr, scratch, need, keep = c4_prepare(T, L, torch, dev, tasks)
+    s = torch.cuda.current_stream(dev).cuda_stream
+    for rep in range(4):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        rc = L.tcTensorContractBatch(len(tasks), arr, scratch.data_ptr(), need, s)
+        e1.record()
+        torch.cuda.synchronize(dev)
+        assert rc == 0, (rc, L.tcLastErrorString())
+        print("C4 batch rep %d: %.3f ms" % (rep, e0.elapsed_time(e1)))
+
+
+def bench_batch(T, L, torch, dev):
+    """C4: 4096 small contractions, batched (tcTensorContractBatch) vs one call per task."""
+    tasks = c4_tasks()
+    flops = sum((2.0 if k == R8 else 8.0) * mnk for k, _, _, _, _, mnk in tasks)
+    arr, scratch, need, keep = c4_prepare(T, L, torch, dev, tasks)
+    s = torch.cuda.current_stream(dev).cuda_stream
 
     def batched():
         rc = L.tcTensorContractBatch(len(tasks), arr, scratch.data_ptr(), need, s)
