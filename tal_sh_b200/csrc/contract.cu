@@ -184,6 +184,13 @@ __device__ __forceinline__ void kring_step(const GemmArgs &a, int64_t *kLs, int6
   }
 }
 
+// Column swizzle of the FP64 tiles: row k stores column c at c ^ ((k >> 1) & 7)
+// (a permutation inside each aligned group of 8 columns).  Tile loads whose
+// lanes run along k (the operand's stride-1 index is contracted) then hit 16
+// different bank pairs per half-warp instead of 2; fragment loads, which read
+// 8 consecutive columns of one row, are unaffected.
+__device__ __forceinline__ int kswz(int k) { return (k >> 1) & 7; }
+
 // One BM x BN tile of a gather-GEMM (shared by the single-contraction kernel and
 // the batched one).
 template <int BM, int BN>
@@ -229,7 +236,7 @@ __device__ __forceinline__ void dmma_tile(const double *__restrict__ L, const do
       const int m = m0 + ml, k = kt * BK + kl;
       const bool v = (m < a.M) && (k < a.K);
       const double *src = v ? (L + mLs[ml] + kLs[s * BK + kl]) : L;
-      cp_async8(as + kl * AP + ml, src, v);
+      cp_async8(as + kl * AP + (ml ^ kswz(kl)), src, v);
     }
 #pragma unroll
     for (int i = 0; i < (BN * BK) / NT; ++i) {
@@ -239,7 +246,7 @@ __device__ __forceinline__ void dmma_tile(const double *__restrict__ L, const do
       const int n = n0 + nl, k = kt * BK + kl;
       const bool v = (n < a.N) && (k < a.K);
       const double *src = v ? (R + nRs[nl] + kRs[s * BK + kl]) : R;
-      cp_async8(bs + kl * BP + nl, src, v);
+      cp_async8(bs + kl * BP + (nl ^ kswz(kl)), src, v);
     }
   };
 
@@ -269,10 +276,11 @@ __device__ __forceinline__ void dmma_tile(const double *__restrict__ L, const do
 #pragma unroll
     for (int ks = 0; ks < BK / 4; ++ks) {
       double af[FM], bf[FN];
+      const int sw = kswz(ks * 4 + fc);
 #pragma unroll
-      for (int i = 0; i < FM; ++i) af[i] = as[(ks * 4 + fc) * AP + wm0 + i * 8 + fr];
+      for (int i = 0; i < FM; ++i) af[i] = as[(ks * 4 + fc) * AP + wm0 + i * 8 + (fr ^ sw)];
 #pragma unroll
-      for (int j = 0; j < FN; ++j) bf[j] = bs[(ks * 4 + fc) * BP + wn0 + j * 8 + fr];
+      for (int j = 0; j < FN; ++j) bf[j] = bs[(ks * 4 + fc) * BP + wn0 + j * 8 + (fr ^ sw)];
 #pragma unroll
       for (int i = 0; i < FM; ++i)
 #pragma unroll
