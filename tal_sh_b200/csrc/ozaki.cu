@@ -67,6 +67,14 @@ __device__ __forceinline__ uint64_t make_desc_sw32(uint32_t saddr) {
   return (uint64_t)((saddr >> 4) & 0x3FFFu) | (1ull << 16) | ((uint64_t)(256 >> 4) << 32) | (1ull << 46) |
          (6ull << 61);
 }
+// The same for CU_TENSOR_MAP_SWIZZLE_64B tiles (64-byte rows, 8-row groups
+// 512 bytes apart).  A K step inside the 64-byte row starts 32 bytes further:
+// the swizzle is a function of the absolute shared address, so advancing the
+// start address selects the second half of every row.
+__device__ __forceinline__ uint64_t make_desc_sw64(uint32_t saddr) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | (1ull << 16) | ((uint64_t)(512 >> 4) << 32) | (1ull << 46) |
+         (4ull << 61);
+}
 
 // Instruction descriptor of kind::i8: int32 accumulator, signed A and B, both
 // K-major, M = 128, N = 64.
@@ -300,15 +308,17 @@ __global__ void __launch_bounds__(kOzThreads, 1) oz_gemm_kernel(const OzArgs a) 
 
 // ---------------------------------------------------------------------------
 // Warp-specialised mainloop.  Warp 0: one thread issues the TMA tile copies of
-// each stage (2-D tensor maps over the slice matrices, boxes of 16 bytes x
-// rows, which land exactly in the canonical K-major layout).  Warp 1: one
+// each stage (2-D tensor maps over the slice matrices, 64-byte x rows boxes
+// with the 64-byte swizzle: two UMMA K steps per box, half the TMA requests of
+// 32-byte boxes).  Warp 1: one
 // thread issues the MMAs of a stage once its copies have landed and commits
 // them to the stage's "empty" barrier; warp 1 also owns the tensor memory.
 // Warps 2-5: epilogue, TMEM lane quadrant (warp % 4).
 // ---------------------------------------------------------------------------
 constexpr int kOzWsThreads = 192;
-constexpr int kWsBK = 32;                    // K bytes per stage: one UMMA K step
-constexpr int kWsATile = kOzBM * kWsBK;      // 4 KB
+constexpr int kWsBK = 32;                    // K bytes of one UMMA K step
+constexpr int kWsBox = 64;                   // K bytes per TMA box row: two UMMA K steps
+constexpr int kWsATile = kOzBM * kWsBox;     // 8 KB
 constexpr int kWsGroupM = 8;                 // m tiles per raster group (L2 reuse of A and B)
 
 __device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
@@ -343,7 +353,7 @@ struct OzWsArgs {
 };
 
 constexpr int kWsBN = 128;                    // tile columns of the pass kernel (UMMA N)
-constexpr int kWsBTile128 = kWsBN * kWsBK;    // 4 KB
+constexpr int kWsBTile128 = kWsBN * kWsBox;   // 8 KB
 constexpr int kWsDiagPerPass = 3;             // accumulators per pass: 3 x 128 TMEM columns
 constexpr uint32_t kIdescI8N128 = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kWsBN >> 3) << 17) |
                                   ((uint32_t)(kOzBM >> 4) << 24);
@@ -388,7 +398,8 @@ __global__ void __launch_bounds__(kOzWsThreads, 1)
     tm = first_m + r % gm;
     tn = r / gm;
   }
-  const int64_t nkb = a.kb1 - a.kb0;
+  const int64_t nkb = a.kb1 - a.kb0;      // UMMA K steps of this launch
+  const int64_t nbox = (nkb + 1) / 2;      // 64-byte TMA boxes covering them
   auto pass_g0 = [&](int p) { return 2 + p * kWsDiagPerPass; };
   auto pass_g1 = [&](int p) { return min(S + 1, pass_g0(p) + kWsDiagPerPass - 1); };
 
@@ -421,22 +432,25 @@ __global__ void __launch_bounds__(kOzWsThreads, 1)
       int64_t itg = 0;  // stage-ring iteration across passes
       for (int p = 0; p < npass && !*(volatile int *)&abort_sh; ++p) {
         const int smax = pass_g1(p) - 1;
-        const uint32_t bytes = (uint32_t)(smax * (kWsATile + kWsBTile128));
-        for (int64_t it = 0; it < nkb; ++it, ++itg) {
+        const int kper = max(1, S / smax);  // boxes per slice and stage: early passes need fewer slices
+        for (int64_t it = 0; it < nbox; it += kper, ++itg) {
+          const int nk = (int)min((int64_t)kper, nbox - it);
           const int st = (int)(itg % nst);
           if (itg >= nst && !mbar_wait(&empty[st], (uint32_t)(((itg / nst) - 1) & 1), a.err)) {
             atomicExch(&abort_sh, 1);
             break;
           }
           if (*(volatile int *)&abort_sh) break;
-          mbar_expect_tx(&full[st], bytes);
+          mbar_expect_tx(&full[st], (uint32_t)(nk * smax * (kWsATile + kWsBTile128)));
           const uint32_t sst = sbase + (uint32_t)(st * slot_bytes);
-          const int kx = (int)((a.kb0 + it) * kWsBK);
-          for (int s = 0; s < smax; ++s) {
-            const uint32_t sa = sst + (uint32_t)(s * kWsATile);
-            const uint32_t sb = sst + (uint32_t)(S * kWsATile + s * kWsBTile128);
-            tma_load_2d(sa, &mapA, kx, (int)(s * a.Mp + tm * kOzBM), &full[st]);
-            tma_load_2d(sb, &mapB, kx, (int)(s * a.Np + tn * kWsBN), &full[st]);
+          for (int j = 0; j < nk; ++j) {
+            const int kx = (int)((a.kb0 + 2 * (it + j)) * kWsBK);
+            for (int s = 0; s < smax; ++s) {
+              const uint32_t sa = sst + (uint32_t)((j * smax + s) * kWsATile);
+              const uint32_t sb = sst + (uint32_t)(S * kWsATile + (j * smax + s) * kWsBTile128);
+              tma_load_2d(sa, &mapA, kx, (int)(s * a.Mp + tm * kOzBM), &full[st]);
+              tma_load_2d(sb, &mapB, kx, (int)(s * a.Np + tn * kWsBN), &full[st]);
+            }
           }
         }
       }
@@ -452,7 +466,10 @@ __global__ void __launch_bounds__(kOzWsThreads, 1)
         }
         asm volatile("tcgen05.fence::after_thread_sync;" ::);
         const int g0 = pass_g0(p), g1 = pass_g1(p);
-        for (int64_t it = 0; it < nkb; ++it, ++itg) {
+        const int smax = g1 - 1;
+        const int kper = max(1, S / smax);
+        for (int64_t it = 0; it < nbox; it += kper, ++itg) {
+          const int nk = (int)min((int64_t)kper, nbox - it);
           const int st = (int)(itg % nst);
           if (!mbar_wait(&full[st], (uint32_t)((itg / nst) & 1), a.err)) {
             atomicExch(&abort_sh, 1);
@@ -460,12 +477,21 @@ __global__ void __launch_bounds__(kOzWsThreads, 1)
           }
           asm volatile("tcgen05.fence::after_thread_sync;" ::);
           const uint32_t sst = sbase + (uint32_t)(st * slot_bytes);
-          for (int g = g0; g <= g1; ++g) {
-            const uint32_t dcol = tmem + (uint32_t)((g - g0) * kWsBN);
-            for (int s1 = 1; s1 < g; ++s1) {
-              const uint32_t sa = sst + (uint32_t)((s1 - 1) * kWsATile);
-              const uint32_t sb = sst + (uint32_t)(S * kWsATile + (g - s1 - 1) * kWsBTile128);
-              mma_i8_n128(dcol, make_desc_sw32(sa), make_desc_sw32(sb), (it > 0 || s1 > 1) ? 1u : 0u);
+          for (int j = 0; j < nk; ++j) {
+            // the two K steps of the box; the second lies past this launch's
+            // K range when the range has an odd number of steps
+            const int nsteps = (2 * (it + j) + 1 < nkb) ? 2 : 1;
+            for (int kk = 0; kk < nsteps; ++kk) {
+              for (int g = g0; g <= g1; ++g) {
+                const uint32_t dcol = tmem + (uint32_t)((g - g0) * kWsBN);
+                for (int s1 = 1; s1 < g; ++s1) {
+                  const uint32_t sa = sst + (uint32_t)((j * smax + s1 - 1) * kWsATile + kk * kWsBK);
+                  const uint32_t sb =
+                      sst + (uint32_t)(S * kWsATile + (j * smax + g - s1 - 1) * kWsBTile128 + kk * kWsBK);
+                  mma_i8_n128(dcol, make_desc_sw64(sa), make_desc_sw64(sb),
+                              (it > 0 || j > 0 || kk > 0 || s1 > 1) ? 1u : 0u);
+                }
+              }
             }
           }
           mma_commit(&empty[st]);
@@ -548,16 +574,16 @@ EncodeTiledFn encode_fn() {
 }
 
 // 2-D map over a [rows][Kp] int8 matrix, box 32 bytes (one UMMA K step) x
-// box_rows, 32-byte swizzle (the layout make_desc_sw32 describes).
+// box_rows, 64-byte swizzle (the layout make_desc_sw64 describes).
 bool make_slice_map(CUtensorMap *map, const void *base, int64_t Kp, int64_t rows, int box_rows) {
   EncodeTiledFn fn = encode_fn();
   if (fn == nullptr) return false;
   const cuuint64_t dims[2] = {(cuuint64_t)Kp, (cuuint64_t)rows};
   const cuuint64_t strides[1] = {(cuuint64_t)Kp};
-  const cuuint32_t box[2] = {(cuuint32_t)kWsBK, (cuuint32_t)box_rows};
+  const cuuint32_t box[2] = {(cuuint32_t)kWsBox, (cuuint32_t)box_rows};
   const cuuint32_t estr[2] = {1u, 1u};
   return fn(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<void *>(base), dims, strides, box, estr,
-            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_32B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
