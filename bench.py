@@ -299,6 +299,23 @@ def profile_contract(spec):
         print(json.dumps({"case": spec, "rep": rep, "tflops": flop / (e0.elapsed_time(e1) * 1e-3) / 1e12}))
 
 
+def slowest_rank(seconds, world, device):
+    """Max over ranks of a per-rank time (every rank calls it, in the same order)."""
+    if world <= 1:
+        return seconds
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(seconds)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(units_per_rank, world, slowest_seconds):
+    """Replicas: every rank processes the same units; the job rate is all ranks'
+    units over the slowest rank's time."""
+    return units_per_rank * world / slowest_seconds
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -460,11 +477,8 @@ def main():
     sampler.stop()
     elapsed = t0.elapsed_time(t1) * 1e-3
     gpu_launches = len(ops) * args.steps if graph is not None else int(L.tcKernelLaunchCount() - launches_before)
-    if world > 1:
-        tt = torch.tensor([elapsed], device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        elapsed = float(tt.item())
-    value = step_bytes * args.steps * world / elapsed / 1e9
+    elapsed = slowest_rank(elapsed, world, dev)
+    value = whole_job_rate(step_bytes * args.steps, world, elapsed) / 1e9
     ms_per_step = elapsed / args.steps * 1e3
 
     # Bit-exact spot check of one case against the oracle (small, outside timing).
@@ -522,13 +536,10 @@ def main():
             e2e_step()
         torch.cuda.synchronize(dev)
         e2e_s = time.perf_counter() - t
-        if world > 1:
-            tt = torch.tensor([e2e_s], device=dev)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            e2e_s = float(tt.item())
+        e2e_s = slowest_rank(e2e_s, world, dev)
         for lt, dt_, _, _ in tens:
             L.talshTensorDestruct(C.byref(lt)); L.talshTensorDestruct(C.byref(dt_))
-        e2e = {"value": step_bytes * args.e2e_steps * world / e2e_s / 1e9, "unit": "GB/s",
+        e2e = {"value": whole_job_rate(step_bytes * args.e2e_steps, world, e2e_s) / 1e9, "unit": "GB/s",
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                "path": "talshTensorCopy + talshTensorAdd, pinned Host tensors, COPY_TT, blocking calls",
                "steps": args.e2e_steps}
