@@ -787,6 +787,12 @@ def bench_batch(T, L, torch, dev):
         if rc:
             raise RuntimeError("batch failed %d: %s" % (rc, L.tcLastErrorString()))
 
+    # Autotune the tile per task class on this batch (untimed; the choice stays for later batches).
+    assert L.tcTensorContractBatchTune(len(tasks), arr, scratch.data_ptr(), need, s, 2) == 0
+    tuned = {"%s M%d N%d" % ("R8" if k == R8 else "C8", mb, nb): L.tcTensorContractBatchTuned(k, mb, nb)
+             for k in (R8, C8) for mb in range(4) for nb in range(4)}
+    need = L.tcTensorContractBatchScratch(len(tasks), arr)  # depends on the tiles chosen
+    scratch = torch.empty(need, dtype=torch.uint8, device=dev)
     single_need = max(L.tcTensorContractScratch(k, T.ivec(cp), len(dd), T.ivec(dd), len(ld), T.ivec(ld),
                                                 len(rd), T.ivec(rd)) for k, cp, dd, ld, rd, _ in tasks)
     sscr = torch.empty(max(single_need, 1), dtype=torch.uint8, device=dev)
@@ -816,6 +822,8 @@ def bench_batch(T, L, torch, dev):
                      "R8/C8 alternating, operands <= 2^21 elements (seed 4096); timed host call to completion, "
                      "descriptor upload included")
     res["flop"] = flops
+    res["autotuned_tile_edge"] = {k: v for k, v in tuned.items() if v}
+    res["autotune_buckets"] = "M and N buckets 0..3: < 16, < 48, < 128, >= 128"
     return res
 
 
@@ -942,9 +950,9 @@ def bench_serve(T, L, torch, dev, slices=6):
             arr[i].keep_output = 1
         return arr
 
-    def server():
-        cfg = T.ServeConfig(budget_bytes=budget, r8_slices=slices, max_batch=4096, max_inflight=2, large_flop=1e10,
-                            prealloc_bytes=16 << 30)
+    def server(r8_slices=slices):
+        cfg = T.ServeConfig(budget_bytes=budget, r8_slices=r8_slices, max_batch=4096, max_inflight=2,
+                            large_flop=1e10, prealloc_bytes=16 << 30)
         h = C.c_void_p()
         assert L.tcServerCreate(C.byref(cfg), C.byref(h)) == 0
         return h
@@ -978,10 +986,10 @@ def bench_serve(T, L, torch, dev, slices=6):
                      "(D(a,b,i,j)+=L(a,k,c,i)*R(c,b,k,j), v=128, o=48, %d-slice split precision), "
                      "admission budget %.0f GB; latency = scheduled arrival to observed completion" %
                      (slices, budget / 1e9)}
-    for rate, n in ((100, 200), (1000, 2000), (10000, 10000)):
+    def run_rate(h, rate, n, check):
         tasks, arrivals = c5_tasks(n, float(rate), seed=rate)
         keep = []
-        if rate == 1000:  # sampled results for the alone-versus-mix comparison
+        if check:  # sampled results for the alone-versus-mix comparison
             ends = [i for i, x in enumerate(tasks) if not x["cc"] and x["consumers"] == 0]
             keep = [i for i in ends if tasks[i]["kind"] == R8][:2] + [i for i in ends if tasks[i]["kind"] == C8][:2]
             keep += [i for i, x in enumerate(tasks) if x["cc"]][:2]
@@ -1021,7 +1029,15 @@ def bench_serve(T, L, torch, dev, slices=6):
                 worst = max(worst, float((alone - m).abs().max() / m.abs().max().clamp_min(1e-300)))
             r["alone_vs_mix"] = {"sampled": len(keep), "bit_identical": same, "max_rel_diff": worst,
                                  "tolerance": 1e-10}
-        out["rate_%d" % rate] = r
+        return r
+
+    for rate, n in ((100, 200), (1000, 2000), (10000, 10000)):
+        out["rate_%d" % rate] = run_rate(h, rate, n, rate == 1000)
+    assert L.tcServerDestroy(h) == 0
+    # The same 1000 tasks/s load with the CC-shaped tasks in plain FP64 (the drop-in path).
+    h = server(0)
+    replay(h, wt, wa)
+    out["rate_1000_plain_fp64"] = run_rate(h, 1000, 2000, False)
     assert L.tcServerDestroy(h) == 0
     del pool, ccL, ccR
     return out

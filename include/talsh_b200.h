@@ -207,6 +207,24 @@ int tcServerResetStats(tcServer *srv);
 int tcServerReplay(tcServer *srv, int n, const tcServeTask *tasks, const double *arrival_s, uint64_t *ids,
                    double *latency_s);
 
+/* Autotuner of the batched form: tasks fall in classes by kind (R8, C8) and
+ * the buckets of their GEMM sizes M and N (< 16, < 48, < 128, >= 128).  For
+ * each class present among `tasks`, runs that class's tasks as one batch with
+ * 32x32 and with 64x64 tiles (`reps` timed runs each after one warm-up, CUDA
+ * events on `stream`) and keeps the faster tile for the class; later batches
+ * (tcTensorContractBatch, the contraction server) use it, so query
+ * tcTensorContractBatchScratch again afterwards (the scratch size depends on
+ * the tiles).  The tasks are executed several times, so their D contents are
+ * unspecified afterwards.
+ * scratch: at least tcTensorContractBatchScratch(ntasks, tasks) bytes.  Not to
+ * run concurrently with other batch launches. */
+int tcTensorContractBatchTune(int ntasks, const tcContractTask *tasks, void *scratch, size_t scratch_bytes,
+                              void *stream, int reps);
+/* Tile edge chosen for a class (0: not tuned, the shape rule applies; -1: bad class). */
+int tcTensorContractBatchTuned(int data_kind, int m_bucket, int n_bucket);
+/* Forgets every tuned choice. */
+void tcTensorContractBatchTuneReset(void);
+
 /* Size of the fixed scratch array behind tcTensorContractNoAlloc: 8 MiB per GPU. */
 #define TC_CONTRACT_NOALLOC_SCRATCH_BYTES ((size_t)8 << 20)
 

@@ -188,6 +188,9 @@ _PROTOS = {
     "tcTensorContractSplitScratch": (_Z, [_I, _P(_I), _I, _P(_I), _I, _P(_I), _I, _P(_I), _I]),
     "tcTensorContractBatchScratch": (_Z, [_I, _P(ContractTask)]),
     "tcTensorContractBatch": (_I, [_I, _P(ContractTask), _V, _Z, _V]),
+    "tcTensorContractBatchTune": (_I, [_I, _P(ContractTask), _V, _Z, _V, _I]),
+    "tcTensorContractBatchTuned": (_I, [_I, _I, _I]),
+    "tcTensorContractBatchTuneReset": (None, []),
     "tcContractXLLastOps": (_Z, []),
     "tcTensorSlice": (_I, [_I, _I, _P(_I), _P(_I), _P(_I), _V, _V, _I, _V]),
     "tcTensorInsert": (_I, [_I, _I, _P(_I), _P(_I), _P(_I), _V, _V, _I, _V]),

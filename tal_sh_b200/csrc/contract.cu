@@ -22,6 +22,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <vector>
 
@@ -1255,7 +1256,20 @@ struct BatchPlan {
          total = 0;
 };
 
+// Tile choices of the autotuner (tcTensorContractBatchTune) per task class:
+// kind (R8, C8) x bucket of M x bucket of N, buckets < 16, < 48, < 128, >= 128.
+// 0 = not tuned (the shape rule below applies), else the tile edge (32 or 64).
+constexpr int kTuneBuckets = 4;
+std::atomic<int> g_tune[2][kTuneBuckets][kTuneBuckets];
+
+int tune_bucket(int64_t x) { return x < 16 ? 0 : x < 48 ? 1 : x < 128 ? 2 : 3; }
+
 int batch_cfg_of(int kind, int64_t M, int64_t N) {
+  if (kind == R8 || kind == C8) {
+    const int t = g_tune[kind == C8][tune_bucket(M)][tune_bucket(N)].load(std::memory_order_relaxed);
+    if (t == 32) return kind == R8 ? kCfgD32 : kCfgZ32;
+    if (t == 64) return kind == R8 ? kCfgD64 : kCfgZ64;
+  }
   switch (kind) {
     case R8: return (M >= 48 && N >= 48) ? kCfgD64 : kCfgD32;
     case C8: return (M >= 48 && N >= 48) ? kCfgZ64 : kCfgZ32;
@@ -1522,4 +1536,78 @@ extern "C" int tcTensorContractBatch(int ntasks, const tcContractTask *tasks, vo
   const int rc = tb::batch_plan(ntasks, tasks, bp);
   if (rc) return rc;
   return tb::batch_run(ntasks, tasks, bp, scratch, scratch_bytes, nullptr, (cudaStream_t)stream);
+}
+
+// Autotuner: for every class present among the tasks, runs that class's tasks
+// as one batch with each candidate tile (32x32, 64x64), `reps` times each,
+// timed with events on `stream`, and keeps the faster tile for the class.
+extern "C" int tcTensorContractBatchTune(int ntasks, const tcContractTask *tasks, void *scratch,
+                                         size_t scratch_bytes, void *stream, int reps) {
+  using namespace tb;
+  if (ntasks < 0 || (ntasks > 0 && tasks == nullptr) || reps < 1) return TALSH_INVALID_ARGS;
+  if (scratch_bytes < tcTensorContractBatchScratch(ntasks, tasks)) return TALSH_INVALID_ARGS;
+  std::vector<int> cls[2][kTuneBuckets][kTuneBuckets];
+  for (int t = 0; t < ntasks; ++t) {
+    const tcContractTask &x = tasks[t];
+    if (x.data_kind != R8 && x.data_kind != C8) continue;
+    if (x.lrank == 0 || x.rrank == 0) continue;
+    Analysis an;
+    if (analyze(x.cptrn, x.drank, x.ddims, x.lrank, x.ldims, x.rrank, x.rdims, an) != 0 || an.hyper) continue;
+    cls[x.data_kind == C8][tune_bucket(an.T.M)][tune_bucket(an.T.N)].push_back(t);
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+    cudaGetLastError();
+    if (e0) cudaEventDestroy(e0);
+    return TALSH_FAILURE;
+  }
+  int rc = TALSH_SUCCESS;
+  std::vector<tcContractTask> sub;
+  for (int k = 0; k < 2 && rc == TALSH_SUCCESS; ++k)
+    for (int mb = 0; mb < kTuneBuckets && rc == TALSH_SUCCESS; ++mb)
+      for (int nb = 0; nb < kTuneBuckets && rc == TALSH_SUCCESS; ++nb) {
+        const std::vector<int> &ids = cls[k][mb][nb];
+        if (ids.empty()) continue;
+        sub.clear();
+        for (int t : ids) sub.push_back(tasks[t]);
+        float best_ms = 0.0f;
+        int best = 0;
+        for (int edge : {32, 64}) {
+          g_tune[k][mb][nb].store(edge);
+          float ms = 0.0f;
+          for (int r = 0; r <= reps && rc == TALSH_SUCCESS; ++r) {  // the first run warms up
+            cudaEventRecord(e0, st);
+            rc = tcTensorContractBatch((int)sub.size(), sub.data(), scratch, scratch_bytes, stream);
+            cudaEventRecord(e1, st);
+            if (rc == TALSH_SUCCESS && cudaEventSynchronize(e1) != cudaSuccess) rc = TALSH_FAILURE;
+            float dt = 0.0f;
+            if (rc == TALSH_SUCCESS && r > 0 && cudaEventElapsedTime(&dt, e0, e1) == cudaSuccess) ms += dt;
+          }
+          if (rc != TALSH_SUCCESS) break;
+          if (best == 0 || ms < best_ms) { best_ms = ms; best = edge; }
+        }
+        g_tune[k][mb][nb].store(rc == TALSH_SUCCESS ? best : 0);
+      }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaGetLastError();
+  return rc;
+}
+
+// Tile edge the autotuner chose for a class (0: not tuned), or -1 for a bad class.
+extern "C" int tcTensorContractBatchTuned(int data_kind, int m_bucket, int n_bucket) {
+  using namespace tb;
+  if ((data_kind != R8 && data_kind != C8) || m_bucket < 0 || m_bucket >= kTuneBuckets || n_bucket < 0 ||
+      n_bucket >= kTuneBuckets)
+    return -1;
+  return g_tune[data_kind == C8][m_bucket][n_bucket].load();
+}
+
+// Forgets every tuned choice (the shape rule applies again).
+extern "C" void tcTensorContractBatchTuneReset(void) {
+  using namespace tb;
+  for (auto &a : g_tune)
+    for (auto &b : a)
+      for (auto &c : b) c.store(0);
 }

@@ -140,3 +140,70 @@ def test_operands_must_be_element_aligned(talsh):
         x.D, x.L, x.R = dp, lp, rp
         assert lib.tcTensorContractBatchScratch(1, t) == 0
         assert lib.tcTensorContractBatch(1, t, sc.data_ptr(), 1 << 20, None) == T.TALSH_INVALID_ARGS
+
+
+def test_autotune_chooses_tiles_and_keeps_results(talsh):
+    """tcTensorContractBatchTune records a tile per class present; batches run
+    afterwards still match tcTensorContract bit for bit (the tile does not change
+    any element's summation order)."""
+    torch = pytest.importorskip("torch")
+    lib = T.lib()
+    rng = np.random.default_rng(33)
+    specs = [random_task(rng, T.R8 if i % 2 == 0 else T.C8, emax=40, vmax=1 << 15) for i in range(48)]
+    s = torch.cuda.current_stream().cuda_stream
+
+    def build(specs, seed):
+        r = np.random.default_rng(seed)
+        tasks = (T.ContractTask * len(specs))()
+        keep = []
+        for t, sp in zip(tasks, specs):
+            kind = sp["kind"]
+            def mk(d):
+                x = r.uniform(-1, 1, d)
+                if kind == T.C8:
+                    x = x + 1j * r.uniform(-1, 1, d)
+                return torch.from_numpy(fort(x.astype(NPT[kind])).ravel(order="F").copy()).cuda()
+            l, rr, d = mk(sp["ld"]), mk(sp["rd"]), mk(sp["dd"] if sp["dd"] else [1])
+            keep.append((sp, l, rr, d))
+            t.data_kind, t.drank, t.lrank, t.rrank = kind, len(sp["dd"]), len(sp["ld"]), len(sp["rd"])
+            for i, v in enumerate(sp["cptrn"]):
+                t.cptrn[i] = v
+            for arr, name in ((sp["dd"], "ddims"), (sp["ld"], "ldims"), (sp["rd"], "rdims")):
+                for i, v in enumerate(arr):
+                    getattr(t, name)[i] = v
+            t.D, t.L, t.R = d.data_ptr(), l.data_ptr(), rr.data_ptr()
+            t.alpha_re, t.alpha_im, t.conj_bits, t.accumulative = 0.5, 0.0, 0, 0
+        return tasks, keep
+
+    lib.tcTensorContractBatchTuneReset()
+    try:
+        tasks, keep = build(specs, 1)
+        need = lib.tcTensorContractBatchScratch(len(specs), tasks)
+        sc = torch.empty(need, dtype=torch.uint8, device="cuda")
+        assert lib.tcTensorContractBatchTune(len(specs), tasks, sc.data_ptr(), need, s, 1) == 0
+        tuned = [lib.tcTensorContractBatchTuned(k, mb, nb) for k in (T.R8, T.C8) for mb in range(4) for nb in range(4)]
+        assert set(tuned) <= {0, 32, 64} and any(t in (32, 64) for t in tuned), tuned
+        assert lib.tcTensorContractBatchTuned(T.R4, 0, 0) == -1
+        # a fresh batch after tuning equals one tcTensorContract per task (the
+        # scratch size depends on the tiles chosen: query it again)
+        tasks, keep = build(specs, 2)
+        need = lib.tcTensorContractBatchScratch(len(specs), tasks)
+        sc = torch.empty(need, dtype=torch.uint8, device="cuda")
+        assert lib.tcTensorContractBatch(len(specs), tasks, sc.data_ptr(), need, s) == 0
+        torch.cuda.synchronize()
+        for sp, l, r, d in keep:
+            if not sp["dd"]:
+                continue
+            args = (sp["kind"], T.ivec(sp["cptrn"]), len(sp["dd"]), T.ivec(sp["dd"]), len(sp["ld"]),
+                    T.ivec(sp["ld"]), len(sp["rd"]), T.ivec(sp["rd"]))
+            d1 = torch.empty_like(d)
+            ns = lib.tcTensorContractScratch(*args)
+            s1 = torch.empty(max(ns, 1), dtype=torch.uint8, device="cuda")
+            assert lib.tcTensorContract(*args, d1.data_ptr(), l.data_ptr(), r.data_ptr(), 0.5, 0.0, 0, 0,
+                                        s1.data_ptr(), ns, s) == 0
+            torch.cuda.synchronize()
+            assert torch.equal(d1, d), sp
+    finally:
+        lib.tcTensorContractBatchTuneReset()
+    assert all(lib.tcTensorContractBatchTuned(k, mb, nb) == 0 for k in (T.R8, T.C8) for mb in range(4)
+               for nb in range(4))
