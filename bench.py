@@ -550,6 +550,7 @@ def main():
         contract = bench_contractions(T, L, torch, dev)
         contract["C4_batch"] = bench_batch(T, L, torch, dev)
         contract["C5_serve"] = bench_serve(T, L, torch, dev)
+        contract["transpose_batch"] = bench_transpose_batch(T, L, torch, dev)
 
     del lbuf, dbuf
     peak, peak_kind = measured_peak()
@@ -1041,6 +1042,65 @@ def bench_serve(T, L, torch, dev, slices=6):
     assert L.tcServerDestroy(h) == 0
     del pool, ccL, ccR
     return out
+
+
+def bench_transpose_batch(T, L, torch, dev, ntasks=2048, seed=2048):
+    """Many small transposes (ranks 2-6, volumes 2^10-2^16 elements, R4/R8, seeded
+    random permutations): one tcTensorPermute call per task versus one replay of
+    a graph-captured batch (tcPermuteBatch, 16 concurrent branches)."""
+    rng = np.random.default_rng(seed)
+    specs, off = [], 0
+    for _ in range(ntasks):
+        kind = R8 if rng.integers(0, 2) else R4
+        r = int(rng.integers(2, 7))
+        vol = float(np.exp(rng.uniform(np.log(1 << 10), np.log(1 << 16))))
+        dims = [max(1, int(round(vol ** (1.0 / r) * rng.uniform(0.6, 1.6)))) for _ in range(r)]
+        o2n = [int(x) + 1 for x in rng.permutation(r)]
+        nbytes = int(np.prod(dims)) * ESIZE[kind]
+        specs.append((kind, dims, o2n, off, nbytes))
+        off += (nbytes + 255) // 256 * 256
+    src = torch.empty(off, dtype=torch.uint8, device=dev)
+    src.view(torch.float32).uniform_(-1.0, 1.0)
+    dst = torch.empty(off, dtype=torch.uint8, device=dev)
+    arr = (T.PermuteTask * ntasks)()
+    for t, (kind, dims, o2n, o, nb) in zip(arr, specs):
+        t.data_kind, t.rank = kind, len(dims)
+        for i, v in enumerate(dims):
+            t.dims[i] = v
+        for i, v in enumerate(o2n):
+            t.o2n[i] = v
+        t.src, t.dst = src.data_ptr() + o, dst.data_ptr() + o
+        t.add, t.alpha_re, t.alpha_im, t.conj = 0, 1.0, 0.0, 0
+    s = torch.cuda.current_stream(dev).cuda_stream
+    calls = [(k, len(d), T.ivec(d), T.ivec(p), src.data_ptr() + o, dst.data_ptr() + o) for k, d, p, o, _ in specs]
+    h = C.c_void_p()
+    assert L.tcPermuteBatchCreate(ntasks, arr, 16, C.byref(h)) == 0
+    nbytes = 2.0 * sum(nb for *_, nb in specs)
+
+    def per_call():
+        for k, r, d, p, a, b in calls:
+            assert L.tcTensorPermute(k, r, d, p, a, b, 0, s) == 0
+
+    def batched():
+        assert L.tcPermuteBatchLaunch(h, s) == 0
+
+    res = {}
+    for name, fn in (("per_call", per_call), ("batched_graph", batched)):
+        fn()
+        torch.cuda.synchronize(dev)
+        reps = 5
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            fn()
+        torch.cuda.synchronize(dev)
+        dt = (time.perf_counter() - t0) / reps
+        res[name] = {"ms": dt * 1e3, "gbs": nbytes / dt / 1e9}
+    assert L.tcPermuteBatchDestroy(h) == 0
+    res["speedup"] = res["per_call"]["ms"] / res["batched_graph"]["ms"]
+    res["config"] = ("%d transposes, ranks 2-6, volumes 2^10-2^16 elements, R4/R8, random permutations (seed %d); "
+                     "timed host call to completion" % (ntasks, seed))
+    res["bytes"] = nbytes
+    return res
 
 
 class _DevArray:

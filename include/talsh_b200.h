@@ -109,8 +109,31 @@ int tcTensorSlice(int data_kind, int rank, const int *full_dims, const int *slic
 int tcTensorInsert(int data_kind, int rank, const int *full_dims, const int *slice_dims, const int *offsets,
                    const void *slice, void *full, int accumulative, void *stream);
 
-/* Batched contractions (many small tasks, one launch per tile configuration). */
 #define TC_BATCH_MAX_RANK 8
+
+/* Batched transposes: many independent transposes / transpose-adds recorded
+ * once into a CUDA graph whose `branches` (1..32) run concurrently, then
+ * replayed with one launch per tcPermuteBatchLaunch.  Each task keeps the tile
+ * plan a single tcTensorPermute(Add) call would use.  The graph holds the
+ * tasks' pointers: replays read and write the same buffers.  Tasks must not
+ * write overlapping destinations.  No reference counterpart (the reference
+ * issues one gpu_tensor_block_copy / _add per call). */
+typedef struct {
+  int data_kind, rank;
+  int dims[TC_BATCH_MAX_RANK];        /* input extents */
+  int o2n[TC_BATCH_MAX_RANK];         /* 1-based output position of each input index */
+  const void *src;
+  void *dst;
+  int add;                            /* 0: dst = permute(src); 1: dst += alpha * permute(src) */
+  double alpha_re, alpha_im;
+  int conj;                           /* complex kinds: conjugate the source */
+} tcPermuteTask;
+typedef struct tcPermuteBatch tcPermuteBatch;
+int tcPermuteBatchCreate(int ntasks, const tcPermuteTask *tasks, int branches, tcPermuteBatch **batch);
+int tcPermuteBatchLaunch(tcPermuteBatch *batch, void *stream);
+int tcPermuteBatchDestroy(tcPermuteBatch *batch);
+
+/* Batched contractions (many small tasks, one launch per tile configuration). */
 typedef struct {
   int data_kind;                      /* R4, R8, C4, C8 */
   int drank, lrank, rrank;            /* each at most TC_BATCH_MAX_RANK */

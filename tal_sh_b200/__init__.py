@@ -95,6 +95,13 @@ class ContractTask(C.Structure):
                 ("conj_bits", C.c_int), ("accumulative", C.c_int)]
 
 
+class PermuteTask(C.Structure):
+    """tcPermuteTask (talsh_b200.h): one transpose of a graph-captured batch."""
+    _fields_ = [("data_kind", C.c_int), ("rank", C.c_int), ("dims", C.c_int * TC_BATCH_MAX_RANK),
+                ("o2n", C.c_int * TC_BATCH_MAX_RANK), ("src", C.c_void_p), ("dst", C.c_void_p),
+                ("add", C.c_int), ("alpha_re", C.c_double), ("alpha_im", C.c_double), ("conj", C.c_int)]
+
+
 class ServeConfig(C.Structure):
     """tcServeConfig (talsh_b200.h)."""
     _fields_ = [("budget_bytes", C.c_size_t), ("r8_slices", C.c_int), ("max_batch", C.c_int),
@@ -188,6 +195,9 @@ _PROTOS = {
     "tcTensorContractSplitScratch": (_Z, [_I, _P(_I), _I, _P(_I), _I, _P(_I), _I, _P(_I), _I]),
     "tcTensorContractBatchScratch": (_Z, [_I, _P(ContractTask)]),
     "tcTensorContractBatch": (_I, [_I, _P(ContractTask), _V, _Z, _V]),
+    "tcPermuteBatchCreate": (_I, [_I, _P(PermuteTask), _I, _P(_V)]),
+    "tcPermuteBatchLaunch": (_I, [_V, _V]),
+    "tcPermuteBatchDestroy": (_I, [_V]),
     "tcTensorContractBatchTune": (_I, [_I, _P(ContractTask), _V, _Z, _V, _I]),
     "tcTensorContractBatchTuned": (_I, [_I, _I, _I]),
     "tcTensorContractBatchTuneReset": (None, []),

@@ -1280,3 +1280,93 @@ extern "C" int tcPermutePlanInfo(int data_kind, int rank, const int *dims_in, co
   }
   return 0;
 }
+
+// ---------------------------------------------------------------------------
+// Batched transposes (tcPermuteBatch*): many independent transposes and
+// transpose-adds recorded once into a CUDA graph whose branches run
+// concurrently, replayed with one launch.  Each task keeps its own tile plan
+// and kernel instantiation (the plan is chosen per permutation and extents as
+// for a single call); the graph removes the per-call host cost and lets small
+// tasks overlap on the SMs.  No reference counterpart: the reference issues one
+// gpu_tensor_block_copy / _add per call.
+// ---------------------------------------------------------------------------
+struct tcPermuteBatch {
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int ntasks = 0;
+};
+
+extern "C" int tcPermuteBatchCreate(int ntasks, const tcPermuteTask *tasks, int branches, tcPermuteBatch **out) {
+  if (out == nullptr) return TALSH_INVALID_ARGS;
+  *out = nullptr;
+  if (ntasks < 1 || tasks == nullptr || branches < 1 || branches > 32) return TALSH_INVALID_ARGS;
+  branches = std::min(branches, ntasks);
+  std::vector<cudaStream_t> st(branches, nullptr);
+  std::vector<cudaEvent_t> ev(branches + 1, nullptr);
+  int rc = TALSH_SUCCESS;
+  for (int i = 0; i < branches && rc == TALSH_SUCCESS; ++i)
+    if (cudaStreamCreateWithFlags(&st[i], cudaStreamNonBlocking) != cudaSuccess) rc = TALSH_FAILURE;
+  for (int i = 0; i <= branches && rc == TALSH_SUCCESS; ++i)
+    if (cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming) != cudaSuccess) rc = TALSH_FAILURE;
+  cudaGraph_t graph = nullptr;
+  if (rc == TALSH_SUCCESS) {
+    // Capture: fork every branch off stream 0, tasks round-robin over the
+    // branches, join back into stream 0.
+    if (cudaStreamBeginCapture(st[0], cudaStreamCaptureModeThreadLocal) != cudaSuccess) rc = TALSH_FAILURE;
+    if (rc == TALSH_SUCCESS) {
+      cudaEventRecord(ev[branches], st[0]);
+      for (int i = 1; i < branches; ++i) cudaStreamWaitEvent(st[i], ev[branches], 0);
+      for (int t = 0; t < ntasks && rc == TALSH_SUCCESS; ++t) {
+        const tcPermuteTask &x = tasks[t];
+        cudaStream_t s = st[t % branches];
+        rc = x.add ? tcTensorPermuteAdd(x.data_kind, x.rank, x.dims, x.o2n, x.src, x.dst, x.alpha_re, x.alpha_im,
+                                        x.conj, s)
+                   : tcTensorPermute(x.data_kind, x.rank, x.dims, x.o2n, x.src, x.dst, x.conj, s);
+      }
+      for (int i = 1; i < branches; ++i) {
+        cudaEventRecord(ev[i], st[i]);
+        cudaStreamWaitEvent(st[0], ev[i], 0);
+      }
+      const cudaError_t e = cudaStreamEndCapture(st[0], &graph);
+      if (e != cudaSuccess && rc == TALSH_SUCCESS) {
+        tb::note_cuda_error("tcPermuteBatchCreate capture", (int)e);
+        rc = TALSH_FAILURE;
+      }
+    }
+  }
+  cudaGraphExec_t exec = nullptr;
+  if (rc == TALSH_SUCCESS && cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess) rc = TALSH_FAILURE;
+  cudaGetLastError();
+  for (auto e : ev) if (e) cudaEventDestroy(e);
+  for (auto s : st) if (s) cudaStreamDestroy(s);
+  if (rc != TALSH_SUCCESS) {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    return rc;
+  }
+  tcPermuteBatch *b = new tcPermuteBatch();
+  b->graph = graph;
+  b->exec = exec;
+  b->ntasks = ntasks;
+  *out = b;
+  return TALSH_SUCCESS;
+}
+
+extern "C" int tcPermuteBatchLaunch(tcPermuteBatch *b, void *stream) {
+  if (b == nullptr) return TALSH_INVALID_ARGS;
+  const cudaError_t e = cudaGraphLaunch(b->exec, (cudaStream_t)stream);
+  if (e != cudaSuccess) {
+    tb::note_cuda_error("tcPermuteBatchLaunch", (int)e);
+    return TALSH_FAILURE;
+  }
+  tb::note_launch((unsigned)b->ntasks);
+  return TALSH_SUCCESS;
+}
+
+extern "C" int tcPermuteBatchDestroy(tcPermuteBatch *b) {
+  if (b == nullptr) return TALSH_INVALID_ARGS;
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  delete b;
+  return TALSH_SUCCESS;
+}

@@ -183,6 +183,7 @@ def test_batch_and_serve_struct_layouts_match_c(built, tmp_path):
     """ctypes mirrors of tcContractTask / tcServe* agree with the C compiler's layout."""
     import subprocess
     fields = {"tcContractTask": (T.ContractTask, ["D", "L", "R", "alpha_re", "conj_bits", "accumulative"]),
+              "tcPermuteTask": (T.PermuteTask, ["o2n", "src", "dst", "add", "alpha_re", "conj"]),
               "tcServeTask": (T.ServeTask, ["op", "l_from", "r_from", "consumers", "keep_output"]),
               "tcServeConfig": (T.ServeConfig, ["budget_bytes", "r8_slices", "max_batch", "max_inflight",
                                                 "large_flop", "prealloc_bytes"]),
