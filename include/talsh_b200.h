@@ -279,6 +279,17 @@ int tcPermutePlanInfo(int data_kind, int rank, const int *dims_in, const int *o2
 
 /* Sub-contractions the last talshTensorContractXL call ran (diagnostics). */
 size_t tcContractXLLastOps(void);
+/* The sub-contractions talshTensorContractXL forms for this shape when
+ * budget_bytes of device memory are free (host-side planning only, no GPU
+ * needed): the contraction is halved with the choice rule of the reference's
+ * talshTensorOpDecompose2 (talshc.cpp:3150-3294) until the D, L and R blocks of
+ * every piece take at most a quarter of the budget.  Writes, per piece, the
+ * block offsets and extents of D, L and R in that order (drank + lrank + rrank
+ * ints each; either array may be NULL) for up to max_ops pieces and returns the
+ * number of pieces, TALSH_LIMIT_EXCEEDED if there would be more than max_ops,
+ * or TALSH_INVALID_ARGS. */
+int tcContractXLPlan(int data_kind, const int *cptrn, int drank, const int *ddims, int lrank, const int *ldims,
+                     int rrank, const int *rdims, size_t budget_bytes, int max_ops, int *offsets, int *extents);
 /* Number of kernels this library launched since load (diagnostics). */
 unsigned long long tcKernelLaunchCount(void);
 /* Last CUDA error text seen by the library (diagnostics). */

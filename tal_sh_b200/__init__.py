@@ -202,6 +202,7 @@ _PROTOS = {
     "tcTensorContractBatchTuned": (_I, [_I, _I, _I]),
     "tcTensorContractBatchTuneReset": (None, []),
     "tcContractXLLastOps": (_Z, []),
+    "tcContractXLPlan": (_I, [_I, _P(_I), _I, _P(_I), _I, _P(_I), _I, _P(_I), _Z, _I, _P(_I), _P(_I)]),
     "tcTensorSlice": (_I, [_I, _I, _P(_I), _P(_I), _P(_I), _V, _V, _I, _V]),
     "tcTensorInsert": (_I, [_I, _I, _P(_I), _P(_I), _P(_I), _V, _V, _I, _V]),
     "tcServerCreate": (_I, [_P(ServeConfig), _P(_V)]),

@@ -88,6 +88,7 @@ std::recursive_mutex g_mu;
 std::atomic<int> g_r8_slices{0};
 // Sub-contractions of the last talshTensorContractXL call (diagnostics).
 size_t g_xl_last_ops = 0;
+constexpr size_t kXLMaxOps = 1 << 16;  // cap on the sub-contractions of one call
 
 int node_gpu_count() {
   int n = 0;
@@ -1854,6 +1855,36 @@ bool xl_split(const XLBlock &p, const int *dig, int drank, int lrank, int rrank,
   return true;
 }
 
+// Halves sub-contractions until the D, L and R blocks of each take at most a
+// quarter of `avail` bytes (or nothing is left to split).  Children replace
+// their parent in place, in order.
+int xl_decompose(const int *dig, const int rank[3], const int *const full[3], int es, size_t avail,
+                 size_t max_ops, std::vector<XLBlock> &ops) {
+  std::vector<XLBlock> next;
+  ops.assign(1, XLBlock());
+  std::memset(&ops[0], 0, sizeof(XLBlock));
+  for (int a = 0; a < 3; ++a)
+    for (int i = 0; i < rank[a]; ++i) ops[0].dims[a][i] = full[a][i];
+  for (bool again = true; again;) {
+    again = false;
+    next.clear();
+    for (const XLBlock &b : ops) {
+      const size_t need = xl_bytes(b, 0, rank[0], es) + xl_bytes(b, 1, rank[1], es) + xl_bytes(b, 2, rank[2], es);
+      XLBlock c1, c2;
+      if (need * 4 > avail && xl_split(b, dig, rank[0], rank[1], rank[2], c1, c2)) {
+        next.push_back(c1);
+        next.push_back(c2);
+        again = true;
+      } else {
+        next.push_back(b);
+      }
+    }
+    ops.swap(next);
+    if (ops.size() > max_ops) return TALSH_LIMIT_EXCEEDED;
+  }
+  return TALSH_SUCCESS;
+}
+
 // Device address of a Host body: pinned bodies are mapped already; other
 // (caller) memory is registered for the duration of the call.
 void *xl_map(void *host, size_t bytes, bool &registered) {
@@ -1930,28 +1961,8 @@ int talshTensorContractXL(const char *cptrn, talsh_tens_t *d, talsh_tens_t *l, t
   // Decomposition.
   GpuCtx &G = R.gpu[gpu];
   const size_t avail = G.budget > G.used ? G.budget - G.used : 0;
-  std::vector<XLBlock> ops(1), next;
-  std::memset(&ops[0], 0, sizeof(XLBlock));
-  for (int a = 0; a < 3; ++a)
-    for (int i = 0; i < rank[a]; ++i) ops[0].dims[a][i] = full[a][i];
-  const size_t kMaxOps = 1 << 16;
-  for (bool again = true; again;) {
-    again = false;
-    next.clear();
-    for (const XLBlock &b : ops) {
-      const size_t need = xl_bytes(b, 0, rank[0], es) + xl_bytes(b, 1, rank[1], es) + xl_bytes(b, 2, rank[2], es);
-      XLBlock c1, c2;
-      if (need * 4 > avail && xl_split(b, op.dig, op.drank, op.lrank, op.rrank, c1, c2)) {
-        next.push_back(c1);
-        next.push_back(c2);
-        again = true;
-      } else {
-        next.push_back(b);
-      }
-    }
-    ops.swap(next);
-    if (ops.size() > kMaxOps) return TALSH_LIMIT_EXCEEDED;
-  }
+  std::vector<XLBlock> ops;
+  if ((rc = xl_decompose(op.dig, rank, full, es, avail, kXLMaxOps, ops)) != TALSH_SUCCESS) return rc;
   // Device buffers sized for the largest block of each argument, and scratch.
   size_t bb[3] = {0, 0, 0}, scratch_bytes = 0;
   const int sl = g_r8_slices.load();
@@ -2041,6 +2052,33 @@ int talshTensorContractXL(const char *cptrn, talsh_tens_t *d, talsh_tens_t *l, t
   return rc;
 }
 size_t tcContractXLLastOps(void) { return g_xl_last_ops; }
+
+int tcContractXLPlan(int data_kind, const int *cptrn, int drank, const int *ddims, int lrank, const int *ldims,
+                     int rrank, const int *rdims, size_t budget_bytes, int max_ops, int *offsets, int *extents) {
+  const int es = kind_size(data_kind);
+  if (es == 0 || drank < 0 || lrank < 0 || rrank < 0 || drank > MAX_TENSOR_RANK || lrank > MAX_TENSOR_RANK ||
+      rrank > MAX_TENSOR_RANK || lrank + rrank == 0 || cptrn == nullptr || max_ops < 1 ||
+      (drank > 0 && ddims == nullptr) || (lrank > 0 && ldims == nullptr) || (rrank > 0 && rdims == nullptr))
+    return TALSH_INVALID_ARGS;
+  const int rank[3] = {drank, lrank, rrank};
+  const int *full[3] = {ddims, ldims, rdims};
+  for (int a = 0; a < 3; ++a)
+    for (int i = 0; i < rank[a]; ++i)
+      if (full[a][i] <= 0) return TALSH_INVALID_ARGS;
+  std::vector<XLBlock> ops;
+  const int rc = xl_decompose(cptrn, rank, full, es, budget_bytes, (size_t)max_ops, ops);
+  if (rc != TALSH_SUCCESS) return rc;
+  const int w = drank + lrank + rrank;
+  for (size_t o = 0; o < ops.size(); ++o) {
+    int j = 0;
+    for (int a = 0; a < 3; ++a)
+      for (int i = 0; i < rank[a]; ++i, ++j) {
+        if (offsets) offsets[o * w + j] = ops[o].off[a][i];
+        if (extents) extents[o * w + j] = ops[o].dims[a][i];
+      }
+  }
+  return (int)ops.size();
+}
 
 int talshTensorContractXL_(const char *p, talsh_tens_t *d, talsh_tens_t *l, talsh_tens_t *r, double a, double b, int c,
                            int e, int f) {
