@@ -319,7 +319,7 @@ constexpr int kOzWsThreads = 192;
 constexpr int kWsBK = 32;                    // K bytes of one UMMA K step
 constexpr int kWsBox = 64;                   // K bytes per TMA box row: two UMMA K steps
 constexpr int kWsATile = kOzBM * kWsBox;     // 8 KB
-constexpr int kWsGroupM = 8;                 // m tiles per raster group (L2 reuse of A and B)
+constexpr int kWsGroupM = 4;                 // m tiles per raster group (L2 reuse of A and B)
 
 __device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
@@ -340,6 +340,7 @@ __device__ __forceinline__ void tma_load_2d(uint32_t sdst, const CUtensorMap *ma
 struct OzWsArgs {
   int64_t Mp, Np;
   int tiles_m, tiles_n;
+  int group_m;  // m tiles per raster group
   int64_t kb0, kb1;
   int S, nst;
   const int32_t *ea, *eb;
@@ -390,10 +391,10 @@ __global__ void __launch_bounds__(kOzWsThreads, 1)
   int tm, tn;
   {
     const int id = blockIdx.x;
-    const int per_group = kWsGroupM * a.tiles_n;
+    const int per_group = a.group_m * a.tiles_n;
     const int grp = id / per_group;
-    const int first_m = grp * kWsGroupM;
-    const int gm = min(kWsGroupM, a.tiles_m - first_m);
+    const int first_m = grp * a.group_m;
+    const int gm = min(a.group_m, a.tiles_m - first_m);
     const int r = id - grp * per_group;
     tm = first_m + r % gm;
     tn = r / gm;
@@ -591,6 +592,17 @@ int64_t round_up(int64_t x, int64_t a) { return (x + a - 1) / a * a; }
 
 constexpr int kOzWsSmem = 208 * 1024;  // dynamic shared bytes for the stage ring (+1 KB alignment slack)
 
+// m tiles per raster group of the warp-specialised kernel: kWsGroupM, or
+// TALSH_B200_SPLIT_GROUP_M (1..64) for tuning.
+int ws_group_m() {
+  static const int v = [] {
+    const char *e = std::getenv("TALSH_B200_SPLIT_GROUP_M");
+    const int g = e ? std::atoi(e) : 0;
+    return (g >= 1 && g <= 64) ? g : kWsGroupM;
+  }();
+  return v;
+}
+
 // TALSH_B200_SPLIT_SIMPLE=1 selects the single-loop kernel (for tests).
 bool oz_force_simple() {
   static const bool v = [] {
@@ -767,6 +779,7 @@ int contract_split_launch(int kind, const int *cptrn, int drank, const int *ddim
     w.Mp = p.Mp; w.Np = p.Np; w.S = slices; w.nst = nst;
     w.tiles_m = (int)(p.Mp / kOzBM);
     w.tiles_n = (int)(p.Np / kWsBN);
+    w.group_m = ws_group_m();
     w.ea = ea; w.eb = eb; w.D = (double *)D; w.mD = mD; w.nD = nD; w.M = M; w.N = N;
     w.alpha = alpha_re; w.err = err;
     w.tmem_cols = 32;
