@@ -63,9 +63,20 @@ struct AllocRec {
   bool pinned;   // host only
 };
 
+// A copy back into memory outside the executing GPU (a Host image, or another
+// GPU's) still in flight: later reads of an overlapping range wait for it.
+struct PendingWrite {
+  const char *p;
+  size_t n;
+  cudaEvent_t ev;
+};
+
 struct GpuCtx {
   bool in_use = false;
-  cudaStream_t stream = nullptr;
+  cudaStream_t stream = nullptr;  // compute (and all work of operations without staging)
+  cudaStream_t h2d = nullptr;     // staging copies into the GPU
+  cudaStream_t d2h = nullptr;     // copies back out of the GPU
+  std::vector<PendingWrite> pending;
   size_t budget = 0, used = 0, peak = 0;
   double flops = 0.0, bytes = 0.0;
   unsigned long long tasks_ok = 0, tasks_failed = 0, try_later = 0;
@@ -171,6 +182,54 @@ cudaEvent_t event_get(int gpu) {
 }
 void event_put(int gpu, cudaEvent_t e) {
   if (e) R.gpu[gpu].event_pool.push_back(e);
+}
+
+// Drops the records of copies back that have completed.
+void prune_pending(int gpu) {
+  GpuCtx &G = R.gpu[gpu];
+  for (size_t i = 0; i < G.pending.size();) {
+    if (cudaEventQuery(G.pending[i].ev) == cudaSuccess) {
+      event_put(gpu, G.pending[i].ev);
+      G.pending[i] = G.pending.back();
+      G.pending.pop_back();
+    } else {
+      ++i;
+    }
+  }
+  cudaGetLastError();  // a not-ready query is not an error
+}
+
+// Makes stream s wait for every copy back in flight into [p, p + n).
+void wait_pending(int gpu, cudaStream_t s, const void *p, size_t n) {
+  prune_pending(gpu);
+  const char *a = (const char *)p;
+  for (const PendingWrite &w : R.gpu[gpu].pending)
+    if (a < w.p + w.n && w.p < a + n) cudaStreamWaitEvent(s, w.ev, 0);
+}
+
+// Blocks the host until every copy back into [p, p + n) on any GPU is done.
+void sync_pending(const void *p, size_t n) {
+  const char *a = (const char *)p;
+  for (int g = 0; g < MAX_GPUS_PER_NODE; ++g) {
+    if (!R.gpu[g].in_use) continue;
+    for (const PendingWrite &w : R.gpu[g].pending)
+      if (a < w.p + w.n && w.p < a + n) cudaEventSynchronize(w.ev);
+  }
+}
+
+// Waits for everything queued on the GPU's three streams.
+void sync_gpu_streams(int gpu) {
+  GpuCtx &G = R.gpu[gpu];
+  cudaStreamSynchronize(G.h2d);
+  cudaStreamSynchronize(G.stream);
+  cudaStreamSynchronize(G.d2h);
+}
+
+// Records a copy back into [p, p + n) just issued on stream s.
+void note_pending(int gpu, const void *p, size_t n, cudaStream_t s) {
+  cudaEvent_t e = event_get(gpu);
+  cudaEventRecord(e, s);
+  R.gpu[gpu].pending.push_back(PendingWrite{(const char *)p, n, e});
 }
 
 // ---------------------------------------------------------------- tensors
@@ -460,7 +519,13 @@ int schedule(OpSpec &op, int dev_id, int dev_kind, talsh_task_t *user_task) {
   int img[3] = {-1, -1, -1};
   for (int k = 0; k < op.nt; ++k) {
     img[k] = choose_image(op.t[k], DEV_NVIDIA_GPU, gpu);
-    if (img[k] < 0) return TALSH_FAILURE;
+    if (img[k] < 0) {
+      // Every image held by a task still in flight (its output, or a moved
+      // input): the operation can run once that task has completed.
+      bool held = false;
+      for (int i = 0; i < op.t[k]->ndev; ++i) held = held || op.t[k]->avail[i] != YEP;
+      return held ? TRY_LATER : TALSH_FAILURE;
+    }
   }
   const int dkind = op.t[0]->data_kind[img[0]];
   for (int k = 1; k < op.nt; ++k)
@@ -559,17 +624,35 @@ int schedule(OpSpec &op, int dev_id, int dev_kind, talsh_task_t *user_task) {
   }
   task->flops = 0.0;
 
-  // Enqueue: inputs, compute, outputs.
+  // Enqueue: inputs on the staging stream, compute on the GPU's stream,
+  // outputs on the copy-back stream, chained by the task's events, so the
+  // copies of consecutive asynchronous tasks overlap each other and the
+  // compute.  A staging read waits for copies back still in flight into the
+  // same Host (or peer) range.
   cudaSetDevice(gpu);
   cudaStream_t st = G.stream;
   for (auto &e : tr->ev) e = event_get(gpu);
   int rc = TALSH_SUCCESS;
-  cudaEventRecord(tr->ev[0], st);
-  for (int k = 0; k < op.nt && rc == TALSH_SUCCESS; ++k) {
-    ArgRec &a = tr->a[k];
-    if (a.dalloc && a.need_input) rc = copy_between(a.dptr, exec_dev, a.src_ptr, a.src_dev, a.bytes, st);
+  cudaEventRecord(tr->ev[0], st);  // after the staging buffers' stream-ordered allocation
+  bool any_in = false, any_out = false;
+  for (int k = 0; k < op.nt; ++k) {
+    any_in = any_in || (tr->a[k].dalloc && tr->a[k].need_input);
+    any_out = any_out || tr->a[k].copy_back;
   }
-  cudaEventRecord(tr->ev[1], st);
+  if (any_in) {
+    cudaStreamWaitEvent(G.h2d, tr->ev[0], 0);
+    // inputs first, the destination (most likely to wait for a copy back) last
+    for (int k = op.nt - 1; k >= 0 && rc == TALSH_SUCCESS; --k) {
+      ArgRec &a = tr->a[k];
+      if (!(a.dalloc && a.need_input)) continue;
+      wait_pending(gpu, G.h2d, a.src_ptr, a.bytes);
+      rc = copy_between(a.dptr, exec_dev, a.src_ptr, a.src_dev, a.bytes, G.h2d);
+    }
+    cudaEventRecord(tr->ev[1], G.h2d);
+    cudaStreamWaitEvent(st, tr->ev[1], 0);
+  } else {
+    cudaEventRecord(tr->ev[1], st);
+  }
   if (rc == TALSH_SUCCESS) {
     const size_t vol = shape_volume(op.t[0]->shape_p);
     switch (op.kind) {
@@ -631,14 +714,23 @@ int schedule(OpSpec &op, int dev_id, int dev_kind, talsh_task_t *user_task) {
     }
   }
   cudaEventRecord(tr->ev[2], st);
-  for (int k = 0; k < op.nt && rc == TALSH_SUCCESS; ++k) {
-    ArgRec &a = tr->a[k];
-    if (a.copy_back) rc = copy_between(a.src_ptr, a.src_dev, a.dptr, exec_dev, a.bytes, st);
+  if (any_out) {
+    cudaStreamWaitEvent(G.d2h, tr->ev[2], 0);
+    for (int k = 0; k < op.nt && rc == TALSH_SUCCESS; ++k) {
+      ArgRec &a = tr->a[k];
+      if (!a.copy_back) continue;
+      rc = copy_between(a.src_ptr, a.src_dev, a.dptr, exec_dev, a.bytes, G.d2h);
+      if (rc == TALSH_SUCCESS) note_pending(gpu, a.src_ptr, a.bytes, G.d2h);
+    }
+    cudaEventRecord(tr->ev[3], G.d2h);
+  } else {
+    cudaEventRecord(tr->ev[3], st);
   }
-  cudaEventRecord(tr->ev[3], st);
   if (rc != TALSH_SUCCESS) {
     // Scheduling failed after the task was recorded: the work already queued
     // must drain before its buffers can be released.
+    cudaStreamSynchronize(G.h2d);
+    cudaStreamSynchronize(G.d2h);
     cudaStreamSynchronize(st);
     cudaGetLastError();
     tr->failed = 20;
@@ -845,7 +937,10 @@ int talshInit(size_t *host_buf_size, int *host_arg_max, int ngpus, int gpu_list[
     const int g = gpu_list[i];
     GpuCtx &G = R.gpu[g];
     if (cudaSetDevice(g) != cudaSuccess) { cudaGetLastError(); return TALSH_FAILURE; }
-    if (cudaStreamCreateWithFlags(&G.stream, cudaStreamNonBlocking) != cudaSuccess) return TALSH_FAILURE;
+    if (cudaStreamCreateWithFlags(&G.stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&G.h2d, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&G.d2h, cudaStreamNonBlocking) != cudaSuccess)
+      return TALSH_FAILURE;
     cudaMemPool_t pool;
     if (cudaDeviceGetDefaultMemPool(&pool, g) == cudaSuccess) {
       uint64_t keep = UINT64_MAX;
@@ -871,7 +966,9 @@ int talshShutdown(void) {
     GpuCtx &G = R.gpu[g];
     if (!G.in_use) continue;
     cudaSetDevice(g);
+    cudaStreamSynchronize(G.h2d);
     cudaStreamSynchronize(G.stream);
+    cudaStreamSynchronize(G.d2h);
   }
   for (auto &kv : R.allocs) {
     if (kv.second.gpu < 0) { if (kv.second.pinned) cudaFreeHost(kv.first); else std::free(kv.first); }
@@ -883,9 +980,13 @@ int talshShutdown(void) {
     GpuCtx &G = R.gpu[g];
     if (!G.in_use) continue;
     cudaSetDevice(g);
+    for (const PendingWrite &w : G.pending) cudaEventDestroy(w.ev);
+    G.pending.clear();
     for (cudaEvent_t e : G.event_pool) cudaEventDestroy(e);
     G.event_pool.clear();
     cudaStreamDestroy(G.stream);
+    cudaStreamDestroy(G.h2d);
+    cudaStreamDestroy(G.d2h);
     G = GpuCtx();
   }
   cudaGetLastError();
@@ -1131,7 +1232,7 @@ int talshTensorImportData(talsh_tens_t *t, int data_kind, const void *ext_data) 
       std::memcpy(t->dev_rsc[i].gmem_p, ext_data, bytes);
     } else if (dk == DEV_NVIDIA_GPU) {
       cudaSetDevice(dn);
-      if (R.gpu[dn].in_use) cudaStreamSynchronize(R.gpu[dn].stream);
+      if (R.gpu[dn].in_use) sync_gpu_streams(dn);
       if (cudaMemcpy(t->dev_rsc[i].gmem_p, ext_data, bytes, cudaMemcpyDefault) != cudaSuccess) {
         cudaGetLastError();
         return TALSH_FAILURE;
@@ -1154,7 +1255,7 @@ int talshTensorDestruct(talsh_tens_t *t) {
       const int dn = decode_device_id(t->dev_rsc[i].dev_id, &dk);
       if (dk == DEV_NVIDIA_GPU && dn >= 0 && dn < MAX_GPUS_PER_NODE && R.gpu[dn].in_use) {
         cudaSetDevice(dn);
-        cudaStreamSynchronize(R.gpu[dn].stream);  // no queued task may still use the body
+        sync_gpu_streams(dn);  // no queued task may still use the body
       }
       if (rsc_release(&t->dev_rsc[i]) != TALSH_SUCCESS) rc = NOT_CLEAN;
     }
@@ -1259,7 +1360,7 @@ int talshTensorGetBodyAccess(talsh_tens_t *t, void **body_p, int data_kind, int 
       if (t->avail[i] != YEP) return TALSH_NOT_ALLOWED;
       int dk = DEV_NULL;
       const int dn = decode_device_id(flat, &dk);
-      if (dk == DEV_NVIDIA_GPU && R.gpu[dn].in_use) { cudaSetDevice(dn); cudaStreamSynchronize(R.gpu[dn].stream); }
+      if (dk == DEV_NVIDIA_GPU && R.gpu[dn].in_use) { cudaSetDevice(dn); sync_gpu_streams(dn); }
       *body_p = t->dev_rsc[i].gmem_p;
       return TALSH_SUCCESS;
     }
@@ -1290,7 +1391,7 @@ int talshTensorGetScalar(talsh_tens_t *t, double *sr, double *si) {
       std::memcpy(buf, t->dev_rsc[i].gmem_p, es);
     } else if (dk == DEV_NVIDIA_GPU && R.gpu[dn].in_use) {
       cudaSetDevice(dn);
-      cudaStreamSynchronize(R.gpu[dn].stream);
+      sync_gpu_streams(dn);
       if (cudaMemcpy(buf, t->dev_rsc[i].gmem_p, es, cudaMemcpyDeviceToHost) != cudaSuccess) {
         cudaGetLastError();
         return TALSH_FAILURE;
@@ -1558,6 +1659,7 @@ int talshTensorPlace(talsh_tens_t *t, int dev_id, int dev_kind, void *dev_mem, i
   for (auto &e : tr->ev) e = event_get(gpu);
   cudaEventRecord(tr->ev[0], G.stream);
   cudaEventRecord(tr->ev[1], G.stream);
+  wait_pending(gpu, G.stream, t->dev_rsc[src].gmem_p, bytes);
   int rc = copy_between(dst, flat, t->dev_rsc[src].gmem_p, t->dev_rsc[src].dev_id, bytes, G.stream);
   cudaEventRecord(tr->ev[2], G.stream);
   cudaEventRecord(tr->ev[3], G.stream);
@@ -1571,7 +1673,7 @@ int talshTensorPlace(talsh_tens_t *t, int dev_id, int dev_kind, void *dev_mem, i
   tk->tens_args[0].source_image = src;
   tk->data_vol = (double)bytes;
   if (rc != TALSH_SUCCESS) {
-    cudaStreamSynchronize(G.stream);
+    sync_gpu_streams(gpu);
     if (owned) mem_free(dst);
     tr->failed = 20;
     task_finalize(tk, false);
@@ -1589,7 +1691,7 @@ int talshTensorPlace(talsh_tens_t *t, int dev_id, int dev_kind, void *dev_mem, i
   t->data_kind[k] = t->data_kind[src];
   t->avail[k] = YEP;
   if (copy_ctrl == COPY_M) {
-    cudaStreamSynchronize(G.stream);
+    sync_gpu_streams(gpu);
     image_discard(t, src);
   }
   if (task == nullptr) {
@@ -1613,7 +1715,7 @@ int talshTensorDiscard(talsh_tens_t *t, int dev_id, int dev_kind) {
     if (t->dev_rsc[i].dev_id != flat) continue;
     int dk = DEV_NULL;
     const int dn = decode_device_id(flat, &dk);
-    if (dk == DEV_NVIDIA_GPU && R.gpu[dn].in_use) { cudaSetDevice(dn); cudaStreamSynchronize(R.gpu[dn].stream); }
+    if (dk == DEV_NVIDIA_GPU && R.gpu[dn].in_use) { cudaSetDevice(dn); sync_gpu_streams(dn); }
     return image_discard(t, i);
   }
   return TALSH_SUCCESS;
@@ -1629,7 +1731,7 @@ int talshTensorDiscardOther(talsh_tens_t *t, int dev_id, int dev_kind) {
   for (int i = 0; i < t->ndev; ++i) {
     if (t->dev_rsc[i].dev_id != flat) continue;
     for (int g = 0; g < MAX_GPUS_PER_NODE; ++g)
-      if (R.gpu[g].in_use) { cudaSetDevice(g); cudaStreamSynchronize(R.gpu[g].stream); }
+      if (R.gpu[g].in_use) { cudaSetDevice(g); sync_gpu_streams(g); }
     return image_discard_other(t, i);
   }
   return TALSH_NOT_FOUND;
@@ -1945,6 +2047,9 @@ int talshTensorContractXL(const char *cptrn, talsh_tens_t *d, talsh_tens_t *l, t
   for (talsh_tens_t *t : {r, l, d})
     if ((rc = talshTensorPlace(t, 0, DEV_HOST, nullptr, COPY_K, nullptr)) != TALSH_SUCCESS) return rc;
   if ((rc = talshTensorDiscardOther(d, 0, DEV_HOST)) != TALSH_SUCCESS) return rc;
+  // Earlier asynchronous tasks may still stage from or copy back into these
+  // Host bodies; the blocks below are read and written directly.
+  sync_gpu_streams(gpu);
   void *hp[3];
   int kind = NO_TYPE;
   for (int a = 0; a < 3; ++a) {
@@ -2100,6 +2205,12 @@ double talshTensorImageNorm1_cpu(const talsh_tens_t *t) {
     if (t->dev_rsc[i].dev_id != 0) continue;
     const size_t n = shape_volume(t->shape_p);
     const void *p = t->dev_rsc[i].gmem_p;
+    {
+      int es = 0;
+      tens_valid_data_kind(t->data_kind[i], &es);
+      std::lock_guard<std::recursive_mutex> lk(g_mu);
+      if (R.on) sync_pending(p, n * (size_t)es);  // copies back into this image still in flight
+    }
     double s = 0.0;
     switch (t->data_kind[i]) {
       case R4: for (size_t j = 0; j < n; ++j) s += (double)std::fabs(((const float *)p)[j]); break;
