@@ -11,8 +11,12 @@
 // T temporary, K keep).
 //
 // B200-specific design:
-//  * one in-order CUDA stream per GPU carries every task, so data
-//    dependencies between asynchronous tasks are honoured without tracking;
+//  * one in-order compute stream per GPU carries every task's kernels, so
+//    device-side dependencies between asynchronous tasks need no tracking;
+//    staging copies in and copies back out run on two more streams, chained
+//    to the compute stream by the task's events, so consecutive tasks overlap
+//    their transfers; Host ranges still being copied back are tracked and
+//    waited for before they are staged again;
 //  * each task records four events (start, inputs ready, compute done,
 //    finished) that give the TAL-SH task status ladder and timings;
 //  * device memory comes from the stream-ordered CUDA allocator with a byte
