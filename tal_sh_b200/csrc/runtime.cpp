@@ -231,6 +231,7 @@ void sync_gpu_streams(int gpu) {
 
 // Records a copy back into [p, p + n) just issued on stream s.
 void note_pending(int gpu, const void *p, size_t n, cudaStream_t s) {
+  if (R.gpu[gpu].pending.size() >= 64) prune_pending(gpu);  // keep the list short without staging reads
   cudaEvent_t e = event_get(gpu);
   cudaEventRecord(e, s);
   R.gpu[gpu].pending.push_back(PendingWrite{(const char *)p, n, e});
