@@ -205,3 +205,35 @@ def test_batch_and_serve_struct_layouts_match_c(built, tmp_path):
         want.append(C.sizeof(cls))
         want += [getattr(cls, f).offset for f in fs]
     assert got == want
+
+
+def test_batch_planner_on_the_host(built):
+    """tcTensorContractBatchScratch plans on the host (no GPU): the scratch grows
+    with the tasks, and bad tasks -- an invalid pattern, a pointer not aligned to
+    the element size -- make the whole batch unplannable (0 bytes)."""
+    L = T.lib()
+
+    def task(kind, pattern, dd, ld, rd, ptr=1 << 20):
+        e, dig, dr, lr, rr, _ = T.parse_pattern(pattern)
+        t = T.ContractTask()
+        t.data_kind, t.drank, t.lrank, t.rrank = kind, len(dd), len(ld), len(rd)
+        for i, v in enumerate(dig):
+            t.cptrn[i] = v
+        for arr, name in ((dd, "ddims"), (ld, "ldims"), (rd, "rdims")):
+            for i, v in enumerate(arr):
+                getattr(t, name)[i] = v
+        t.D, t.L, t.R = ptr, ptr + (1 << 20), ptr + (2 << 20)
+        t.alpha_re = 1.0
+        return t
+
+    a = task(T.R8, "D(a,b)+=L(a,k)*R(k,b)", [40, 30], [40, 20], [20, 30])
+    b = task(T.C8, "D(a,b,c)+=L(c,a)*R(b,c)", [4, 5, 6], [6, 4], [5, 6])  # hyper: single-task path inside
+    one = (T.ContractTask * 1)(a)
+    two = (T.ContractTask * 2)(a, b)
+    s1, s2 = L.tcTensorContractBatchScratch(1, one), L.tcTensorContractBatchScratch(2, two)
+    assert 0 < s1 < s2
+    assert s1 >= 8 * 2 * (40 + 30 + 20)  # the offset tables at least
+    bad = task(T.R8, "D(a,b)+=L(a,k)*R(k,b)", [40, 30], [40, 21], [20, 30])  # contracted extents differ
+    assert L.tcTensorContractBatchScratch(2, (T.ContractTask * 2)(a, bad)) == 0
+    mis = task(T.C8, "D(a,b)+=L(a,k)*R(k,b)", [4, 3], [4, 2], [2, 3], ptr=(1 << 20) + 8)  # 8-byte aligned complex
+    assert L.tcTensorContractBatchScratch(1, (T.ContractTask * 1)(mis)) == 0
