@@ -576,12 +576,22 @@ def main():
                "steps": args.e2e_steps}
 
     # Contractions (FP64) through talshTensorContract on GPU-resident tensors.
+    # A leg that fails records its error; the line is still printed.
     contract = None
     if not args.no_contract:
-        contract = bench_contractions(T, L, torch, dev)
-        contract["C4_batch"] = bench_batch(T, L, torch, dev)
-        contract["C5_serve"] = bench_serve(T, L, torch, dev)
-        contract["transpose_batch"] = bench_transpose_batch(T, L, torch, dev)
+        contract = {}
+        for name, leg in (("", bench_contractions), ("C4_batch", bench_batch), ("C5_serve", bench_serve),
+                          ("transpose_batch", bench_transpose_batch)):
+            try:
+                res = leg(T, L, torch, dev)
+            except Exception as exc:  # recorded, not hidden: the key carries the error
+                print("bench leg %s failed: %r" % (name or "contractions", exc), file=sys.stderr)
+                res = {"error": repr(exc)}
+                torch.cuda.synchronize(dev)
+            if name:
+                contract[name] = res
+            else:
+                contract.update(res if "error" not in res else {"contractions": res})
 
     del lbuf, dbuf
     peak, peak_kind = measured_peak()
