@@ -587,7 +587,10 @@ def main():
             except Exception as exc:  # recorded, not hidden: the key carries the error
                 print("bench leg %s failed: %r" % (name or "contractions", exc), file=sys.stderr)
                 res = {"error": repr(exc)}
-                torch.cuda.synchronize(dev)
+                try:
+                    torch.cuda.synchronize(dev)
+                except Exception:
+                    pass
             if name:
                 contract[name] = res
             else:
