@@ -224,3 +224,22 @@ def test_slice_insert_match_numpy():
             assert O.tensor_insert(G, S0, off, True) == 0 and np.array_equal(G, W)
     bad = np.asfortranarray(np.zeros((3, 3)))
     assert O.tensor_slice(bad, np.zeros((4, 4), order="F"), [2, 0], False) != 0  # 2 + 3 > 4
+
+
+def test_split_precision_model_error_bound():
+    """The split-precision arithmetic, modelled in numpy: the digits reconstruct
+    each scaled entry to 2^-42 (6 slices), and the product error against float64
+    stays below the 1e-10 bound stated for 6 slices, above it for 5."""
+    from oracle.ozaki import slice_rows, split_gemm
+    rng = np.random.default_rng(3)
+    A = rng.standard_normal((64, 768))
+    Bt = rng.standard_normal((48, 768))
+    e, d = slice_rows(A, 6)
+    rec = sum(np.ldexp(d[s].astype(np.float64), -7 * (s + 1)) for s in range(6))
+    assert np.abs(np.ldexp(A, -e[:, None]) - rec).max() < 2.0 ** -42
+    assert all(np.abs(x).max() <= 127 for x in d)
+    ref = A @ Bt.T
+    err = lambda S: np.linalg.norm(split_gemm(A, Bt, S) - ref) / np.linalg.norm(ref)
+    assert err(6) < 1e-10
+    assert err(5) > 1e-10
+    assert err(3) > err(4) > err(5) > err(6)
