@@ -28,6 +28,24 @@ inline bool elem_aligned(int kind, const void *p) {
   return es > 0 && (reinterpret_cast<uintptr_t>(p) % (uintptr_t)es) == 0;
 }
 
+// Flops of a contraction in digital form: 2 M N K H (real) or 8 M N K H
+// (complex), M and N the extents of the free indices of L and of R, K the
+// contracted extent, H the extent of the hyper indices (in D, L and R), counted
+// once.  Without hyper indices this is the reference's 2 ll lr lc
+// (tensor_algebra_cpu.F90:4096-4101).
+inline double contract_flops(int kind, const int *cptrn, int lrank, const int *ldims, int rrank,
+                             const int *rdims) {
+  double f = kind_is_complex(kind) ? 8.0 : 2.0;
+  for (int i = 0; i < lrank; ++i) f *= (double)ldims[i];
+  for (int j = 0; j < rrank; ++j) {
+    const int p = cptrn[lrank + j];
+    bool hyper = false;
+    for (int i = 0; p > 0 && i < lrank; ++i) hyper = hyper || cptrn[i] == p;
+    if (p > 0 && !hyper) f *= (double)rdims[j];
+  }
+  return f;
+}
+
 // Real approximant of a complex scale factor that keeps the modulus and the
 // sign of the real part (reference cmplx8_to_real8, tensor_algebra_cpu.F90:430-445).
 double cmplx8_to_real8(double re, double im);

@@ -691,10 +691,7 @@ int schedule(OpSpec &op, int dev_id, int dev_kind, talsh_task_t *user_task) {
           rc = contract_launch(dkind, op.dig, op.drank, dd, op.lrank, ld, op.rrank, rd, tr->a[0].dptr,
                                tr->a[1].dptr, tr->a[2].dptr, op.sr, op.si, op.conj, op.accumulative,
                                tr->scratch, scratch, st);
-        double m = 1.0, n = 1.0, kk = 1.0;
-        for (int i = 0; i < op.lrank; ++i) (op.dig[i] > 0 ? m : kk) *= (double)ld[i];
-        for (int i = 0; i < op.rrank; ++i) if (op.dig[op.lrank + i] > 0) n *= (double)rd[i];
-        task->flops = (kind_is_complex(dkind) ? 8.0 : 2.0) * m * n * kk;
+        task->flops = contract_flops(dkind, op.dig, op.lrank, ld, op.rrank, rd);
         break;
       }
       case kOpNorm1: {
@@ -2141,10 +2138,7 @@ int talshTensorContractXL(const char *cptrn, talsh_tens_t *d, talsh_tens_t *l, t
       rc = tcTensorInsert(kind, rank[0], full[0], b.dims[0], b.off[0], db[0], mp[0], 0, st);
     }
     if (rc != TALSH_SUCCESS) break;
-    double m = 1.0, n = 1.0, k = 1.0;
-    for (int i = 0; i < op.lrank; ++i) (op.dig[i] > 0 ? m : k) *= (double)b.dims[1][i];
-    for (int i = 0; i < op.rrank; ++i) if (op.dig[op.lrank + i] > 0) n *= (double)b.dims[2][i];
-    flops += (kind_is_complex(kind) ? 8.0 : 2.0) * m * n * k;
+    flops += contract_flops(kind, op.dig, op.lrank, b.dims[1], op.rrank, b.dims[2]);
   }
   const cudaError_t se = cudaStreamSynchronize(st);
   if (rc == TALSH_SUCCESS && se != cudaSuccess) {

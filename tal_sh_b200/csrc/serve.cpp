@@ -107,13 +107,8 @@ int64_t vol(const int *d, int n) {
   return v;
 }
 
-// 2 M N K (real) or 8 M N K (complex) of a contraction task.
 double task_flops(const tcContractTask &t) {
-  double m = 1, n = 1, k = 1;
-  for (int i = 0; i < t.lrank; ++i) (t.cptrn[i] > 0 ? m : k) *= t.ldims[i];
-  for (int i = 0; i < t.rrank; ++i)
-    if (t.cptrn[t.lrank + i] > 0) n *= t.rdims[i];
-  return (tb::kind_is_complex(t.data_kind) ? 8.0 : 2.0) * m * n * k;
+  return tb::contract_flops(t.data_kind, t.cptrn, t.lrank, t.ldims, t.rrank, t.rdims);
 }
 
 }  // namespace

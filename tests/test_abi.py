@@ -237,3 +237,39 @@ def test_batch_planner_on_the_host(built):
     assert L.tcTensorContractBatchScratch(2, (T.ContractTask * 2)(a, bad)) == 0
     mis = task(T.C8, "D(a,b)+=L(a,k)*R(k,b)", [4, 3], [4, 2], [2, 3], ptr=(1 << 20) + 8)  # 8-byte aligned complex
     assert L.tcTensorContractBatchScratch(1, (T.ContractTask * 1)(mis)) == 0
+
+
+def test_contract_flop_count(tmp_path):
+    """The core's flop count of a contraction (task flops, the server's large-task
+    threshold) is 2 (8 complex) times the product of the extents of the distinct
+    indices of L and R: a hyper index (in D, L and R) counts once."""
+    import subprocess
+    cases = [("D(a,b,i,j)+=L(a,k,c,i)*R(c,b,k,j)", dict(a=6, b=7, i=4, j=5, k=3, c=8), O.R8),
+             ("D(x,y,z)+=L(x,y,k)*R(k,z)", dict(x=64, y=48, z=40, k=32), O.C8),
+             ("D(a,b,c)+=L(c,a)*R(b,c)", dict(a=3, b=4, c=5), O.R8),
+             ("D(i,j,k)+=L(k,a,i,b)*R(b,k,a,j)", dict(i=12, j=10, k=7, a=6, b=5), O.C4),
+             ("D(x,h,g)+=L(x,h,k,g)*R(g,k,h)", dict(h=4, g=3, x=33, k=17), O.R4),
+             ("D(h)+=L(k,h)*R(h,k)", dict(h=9, k=40), O.R8),
+             ("D()+=L(a,b)*R(b,a)", dict(a=4, b=5), O.R8),
+             ("D(a,b)+=L(a)*R(b)", dict(a=4, b=5), O.R8),
+             ("D(b,a)+=L()*R(a,b)", dict(a=3, b=4), O.R8),
+             ("D()+=L()*R()", dict(), O.C8)]
+    body, want = [], []
+    for n, (pat, ext, kind) in enumerate(cases):
+        e, dig, dr, lr, rr, _ = O.str2dig(pat)
+        assert e == 0
+        groups = [[x for x in g.split(",") if x] for g in re.findall(r"\(([^)]*)\)", pat)]
+        ld, rd = [ext[x] for x in groups[1]], [ext[x] for x in groups[2]]
+        arr = lambda v: "{%s}" % ",".join(str(x) for x in (list(v) or [0]))
+        body.append("{ const int c[] = %s, l[] = %s, r[] = %s; std::printf(\"%%.17g\\n\", "
+                    "tb::contract_flops(%d, c, %d, l, %d, r)); }"
+                    % (arr(dig[:lr + rr]), arr(ld), arr(rd), kind, lr, rr))
+        labels = set(groups[1]) | set(groups[2])
+        want.append((8.0 if kind in (O.C4, O.C8) else 2.0) * float(np.prod([ext[x] for x in labels])))
+    src = tmp_path / "flops.cpp"
+    src.write_text('#include <cstdio>\n#include "common.h"\nint main() {\n%s\nreturn 0; }\n' % "\n".join(body))
+    exe = tmp_path / "flops"
+    subprocess.run(["g++", "-std=c++17", "-I", os.path.join(ROOT, "include"), "-I",
+                    os.path.join(ROOT, "tal_sh_b200", "csrc"), str(src), "-o", str(exe)], check=True)
+    got = [float(x) for x in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()]
+    assert got == want
