@@ -227,7 +227,8 @@ _lib = None
 
 
 def lib():
-    """Loads libtalsh.so (building it first if the sources are newer) and returns the CDLL."""
+    """Loads libtalsh.so and returns the CDLL; raises RuntimeError when it has not been built
+    (there is no fallback implementation)."""
     global _lib
     if _lib is not None:
         return _lib

@@ -273,3 +273,11 @@ def test_contract_flop_count(tmp_path):
                     os.path.join(ROOT, "tal_sh_b200", "csrc"), str(src), "-o", str(exe)], check=True)
     got = [float(x) for x in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()]
     assert got == want
+
+
+def test_missing_library_fails_loudly(monkeypatch, tmp_path):
+    """Without the built library the package raises instead of falling back."""
+    monkeypatch.setattr(T, "_lib", None)
+    monkeypatch.setattr(T, "LIB_PATH", str(tmp_path / "libtalsh.so"))
+    with pytest.raises(RuntimeError, match="missing"):
+        T.lib()
