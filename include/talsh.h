@@ -17,8 +17,9 @@
  *    completed by talshTaskComplete / talshTaskWait.
  *  - Scheduling is single-threaded: one host thread issues TAL-SH calls.
  *  - Entry points of the reference that this core does not provide (SVD,
- *    orthogonalization, tensor-operation objects, slicing) return
- *    TALSH_NOT_IMPLEMENTED.
+ *    orthogonalization, tensor-operation objects, slice descriptor objects)
+ *    return TALSH_NOT_IMPLEMENTED; talshTensorSlice / talshTensorInsert run on
+ *    the GPU.
  */
 #ifndef TALSH_B200_TALSH_H_
 #define TALSH_B200_TALSH_H_
@@ -237,7 +238,8 @@ void talshTensorPrint(const talsh_tens_t *tens_block);
 void talshTensorPrintInfo(const talsh_tens_t *tens_block);
 void talshTensorPrintBody(const talsh_tens_t *tens_block, double thresh);
 
-/* Tensor slice API (not provided by this core: TALSH_NOT_IMPLEMENTED) */
+/* Tensor slice descriptor objects (not provided by this core: TALSH_NOT_IMPLEMENTED;
+ * talshTensorSlice and talshTensorInsert themselves are provided) */
 int talshTensorSliceCreate(talsh_tens_slice_t **slice);
 int talshTensorSliceClean(talsh_tens_slice_t *slice);
 int talshTensorSliceConstruct(talsh_tens_slice_t *slice, const talsh_tens_t *tensor,

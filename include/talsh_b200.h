@@ -63,8 +63,9 @@ size_t tcTensorContractScratch(int data_kind, const int *cptrn, int drank, const
 
 /* D = beta*D + alpha * contraction(L, R) for a digital pattern cptrn[lrank+rrank]
  * (reference format: >0 position in D, <0 minus the position in the other
- * operand).  Indices present in D, L and R at once are not supported
- * (TALSH_NOT_IMPLEMENTED).  beta = 1 if accumulative else D is overwritten.
+ * operand).  Indices present in D, L and R at once (hyper-indices) run as one
+ * GEMM per combination of their values, all in the same launch.  beta = 1 if
+ * accumulative else D is overwritten.
  * conj_bits: bit0 D, bit1 L, bit2 R (complex kinds only).  Rank-0 operands are
  * single elements of the data kind, resident in device memory.  scratch:
  * device buffer of tcTensorContractScratch(...) bytes (may be NULL when that is 0).
@@ -88,7 +89,7 @@ size_t tcTensorContractSplitScratch(int data_kind, const int *cptrn, int drank, 
  * tcTensorContract; slices 2..7, 0 = 6 (relative error about sqrt(K)*2^-46 on
  * random data, below 1e-10 for contracted volumes up to ~10^8).  Indices
  * present in D, L and R at once return TALSH_NOT_IMPLEMENTED.  Inputs must be
- * finite.  The north-star's split-precision form of
+ * finite.  A split-precision form of
  * gpu_tensor_block_contract_dlf (reference :5847); no reference counterpart. */
 int tcTensorContractSplit(int data_kind, const int *cptrn, int drank, const int *ddims, int lrank,
                           const int *ldims, int rrank, const int *rdims, void *D, const void *L,
@@ -157,8 +158,8 @@ size_t tcTensorContractBatchScratch(int ntasks, const tcContractTask *tasks);
  * contraction is a 1 x 1 tile: its sum order differs from tcTensorContract's
  * two-pass dot product); scalar operands and hyper-indices take the
  * single-task path.
- * Tasks must not write overlapping D regions (they run concurrently).  The
- * north-star's batched form of gpu_tensor_block_contract_dlf; no reference
+ * Tasks must not write overlapping D regions (they run concurrently).  A
+ * batched form of gpu_tensor_block_contract_dlf; no reference
  * counterpart (the reference schedules one task per call). */
 int tcTensorContractBatch(int ntasks, const tcContractTask *tasks, void *scratch, size_t scratch_bytes,
                           void *stream);
