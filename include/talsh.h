@@ -402,13 +402,15 @@ double talshTensorNorm1(talsh_tens_t *tens, int dev_id TALSH_DEFAULT(DEV_DEFAULT
                         int dev_kind TALSH_DEFAULT(DEV_DEFAULT));
 double talshTensorNorm1_(talsh_tens_t *tens, int dev_id, int dev_kind);
 
-/* Extension of this core (no counterpart in the reference): the form R8
- * contractions run in.  0 (default) = plain FP64, the drop-in behaviour;
- * 2..7 = split precision on the tensor cores with that many int8 slices
- * (see tcTensorContractSplit in talsh_b200.h; 6 keeps the relative error
- * below 1e-10).  Also set by the environment variable TALSH_B200_R8_SLICES at
+/* Extension of this core (no counterpart in the reference): the form R8 and
+ * C8 contractions of talshTensorContract run in.  0 (default) = plain FP64,
+ * the drop-in behaviour; 2..7 = split precision on the tensor cores with that
+ * many int8 slices (see tcTensorContractSplit in talsh_b200.h; 6 keeps the
+ * relative error below 1e-10; C8 runs as one real contraction of twice the
+ * extents).  Also set by the environment variable TALSH_B200_R8_SLICES at
  * talshInit.  Contractions the split form cannot take (hyper-indices, rank-0
- * operands, conjugation) run plain.  Returns TALSH_INVALID_ARGS for other values. */
+ * operands, R8 with conjugation flags) run plain, and talshTensorContractXL
+ * uses the split form for R8 only.  Returns TALSH_INVALID_ARGS for other values. */
 int talshContractSlicesSet(int slices);
 int talshContractSlicesGet(void);
 #ifdef __cplusplus

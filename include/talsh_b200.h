@@ -76,7 +76,8 @@ int tcTensorContract(int data_kind, const int *cptrn, int drank, const int *ddim
                      int accumulative, void *scratch, size_t scratch_bytes, void *stream);
 
 /* Bytes of device scratch tcTensorContractSplit needs (0 when the form does
- * not apply: not R8, or an operand of rank 0). */
+ * not apply: not R8 or C8, an operand of rank 0, or a C8 contraction with
+ * hyper-indices). */
 size_t tcTensorContractSplitScratch(int data_kind, const int *cptrn, int drank, const int *ddims,
                                     int lrank, const int *ldims, int rrank, const int *rdims,
                                     int slices);
@@ -89,7 +90,11 @@ size_t tcTensorContractSplitScratch(int data_kind, const int *cptrn, int drank, 
  * tcTensorContract; slices 2..7, 0 = 6 (relative error about sqrt(K)*2^-46 on
  * random data, below 1e-10 for contracted volumes up to ~10^8).  Indices
  * present in D, L and R at once return TALSH_NOT_IMPLEMENTED.  Inputs must be
- * finite.  A split-precision form of
+ * finite.  C8: conj_bits and a complex alpha as in tcTensorContract; the
+ * contraction runs as one real contraction (L and D read as real tensors with
+ * a leading (re, im) index, R's conjugated and i-rotated copies, alpha folded
+ * in, stacked in the scratch), so the error bound is that of the real form with
+ * twice the contracted extent.  A split-precision form of
  * gpu_tensor_block_contract_dlf (reference :5847); no reference counterpart. */
 int tcTensorContractSplit(int data_kind, const int *cptrn, int drank, const int *ddims, int lrank,
                           const int *ldims, int rrank, const int *rdims, void *D, const void *L,

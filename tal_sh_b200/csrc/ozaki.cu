@@ -29,8 +29,11 @@
 #include <mutex>
 
 #include "common.h"
+#include "split_complex.h"
 
 namespace tb {
+int contract_validate(int kind, const int *cptrn, int drank, const int *ddims, int lrank, const int *ldims,
+                      int rrank, const int *rdims);
 int permute_launch_o2n(int kind, int rank, const int *dims, const int *o2n, const void *src, void *dst,
                        cudaStream_t st);
 size_t contract_tables_bytes(int64_t M, int64_t N, int64_t K);
@@ -805,11 +808,87 @@ int contract_split_launch(int kind, const int *cptrn, int drank, const int *ddim
   return TALSH_SUCCESS;
 }
 
+// ---------------------------------------------------------------------------
+// Complex(8) in split precision: the contraction is rewritten as one real(8)
+// contraction (split_complex.h).  Scratch layout: the stacked operand Rx
+// (2 x vol(R) complex elements, rounded up to 256 bytes), then the real form's
+// scratch.
+// ---------------------------------------------------------------------------
+
+namespace {
+
+bool has_hyper_index(const int *cptrn, int lrank, int rrank) {
+  for (int i = 0; i < lrank; ++i)
+    for (int j = 0; cptrn[i] > 0 && j < rrank; ++j)
+      if (cptrn[lrank + j] == cptrn[i]) return true;
+  return false;
+}
+
+size_t complex_rx_bytes(int rrank, const int *rdims) {
+  size_t v = 2;
+  for (int j = 0; j < rrank; ++j) v *= (size_t)rdims[j];
+  return (v * 16 + 255) & ~size_t(255);
+}
+
+}  // namespace
+
+size_t contract_split_complex_scratch(const int *cptrn, int drank, const int *ddims, int lrank, const int *ldims,
+                                      int rrank, const int *rdims, int slices) {
+  if (lrank == 0 || rrank == 0 || drank == 0) return 0;
+  if (contract_validate(C8, cptrn, drank, ddims, lrank, ldims, rrank, rdims) != TALSH_SUCCESS) return 0;
+  if (has_hyper_index(cptrn, lrank, rrank)) return 0;
+  ComplexSplitForm f;
+  if (complex_split_form(cptrn, drank, ddims, lrank, ldims, rrank, rdims, 0, f) != TALSH_SUCCESS) return 0;
+  const size_t need =
+      contract_split_scratch(R8, f.cptrn, f.drank, f.ddims, f.lrank, f.ldims, f.rrank, f.rdims, slices);
+  return need ? complex_rx_bytes(rrank, rdims) + need : 0;
+}
+
+int contract_split_complex_launch(const int *cptrn, int drank, const int *ddims, int lrank, const int *ldims,
+                                  int rrank, const int *rdims, void *D, const void *L, const void *R,
+                                  double alpha_re, double alpha_im, int conj_bits, int accumulative, int slices,
+                                  void *scratch, size_t scratch_bytes, void *stream) {
+  if (lrank == 0 || rrank == 0 || drank == 0) return TALSH_NOT_IMPLEMENTED;
+  if (slices <= 0) slices = 6;
+  if (slices < 2 || slices > kOzMaxSlices) return TALSH_INVALID_ARGS;
+  int rc = contract_validate(C8, cptrn, drank, ddims, lrank, ldims, rrank, rdims);
+  if (rc) return rc;
+  if (has_hyper_index(cptrn, lrank, rrank)) return TALSH_NOT_IMPLEMENTED;
+  if (D == nullptr || L == nullptr || R == nullptr || scratch == nullptr) return TALSH_INVALID_ARGS;
+  if (!elem_aligned(C8, D) || !elem_aligned(C8, L) || !elem_aligned(C8, R) || !elem_aligned(C8, scratch))
+    return TALSH_INVALID_ARGS;
+  ComplexSplitForm f;
+  if ((rc = complex_split_form(cptrn, drank, ddims, lrank, ldims, rrank, rdims, conj_bits, f)) != 0) return rc;
+  const size_t rx = complex_rx_bytes(rrank, rdims);
+  const size_t need =
+      contract_split_scratch(R8, f.cptrn, f.drank, f.ddims, f.lrank, f.ldims, f.rrank, f.rdims, slices);
+  if (need == 0 || scratch_bytes < rx + need) return TALSH_INVALID_ARGS;
+  // Rx = [Y s, Y (z i) s], Y = R or conj(R), s = alpha or conj(alpha); z i s is
+  // exact (a swap and a sign).
+  size_t half = 1;
+  for (int j = 0; j < rrank; ++j) half *= (size_t)rdims[j];
+  int id[kMaxRank];
+  for (int j = 0; j < rrank; ++j) id[j] = j + 1;
+  const double sr = alpha_re, si = f.alpha_conj ? -alpha_im : alpha_im;
+  const double zr = -f.z_im * si, zi = f.z_im * sr;
+  char *rxp = (char *)scratch;
+  if ((rc = tcTensorInit(C8, 2 * half, rxp, 0.0, 0.0, stream)) != TALSH_SUCCESS) return rc;
+  if ((rc = tcTensorPermuteAdd(C8, rrank, rdims, id, R, rxp, sr, si, f.y_conj, stream)) != TALSH_SUCCESS)
+    return rc;
+  if ((rc = tcTensorPermuteAdd(C8, rrank, rdims, id, R, rxp + half * 16, zr, zi, f.y_conj, stream)) !=
+      TALSH_SUCCESS)
+    return rc;
+  return contract_split_launch(R8, f.cptrn, f.drank, f.ddims, f.lrank, f.ldims, f.rrank, f.rdims, D, L, rxp, 1.0,
+                               accumulative, slices, rxp + rx, scratch_bytes - rx, stream);
+}
+
 }  // namespace tb
 
 extern "C" size_t tcTensorContractSplitScratch(int data_kind, const int *cptrn, int drank,
                                                const int *ddims, int lrank, const int *ldims,
                                                int rrank, const int *rdims, int slices) {
+  if (data_kind == C8)
+    return tb::contract_split_complex_scratch(cptrn, drank, ddims, lrank, ldims, rrank, rdims, slices);
   return tb::contract_split_scratch(data_kind, cptrn, drank, ddims, lrank, ldims, rrank, rdims, slices);
 }
 
@@ -818,8 +897,10 @@ extern "C" int tcTensorContractSplit(int data_kind, const int *cptrn, int drank,
                                      const void *L, const void *R, double alpha_re, double alpha_im,
                                      int conj_bits, int accumulative, int slices, void *scratch,
                                      size_t scratch_bytes, void *stream) {
-  (void)alpha_im;
-  (void)conj_bits;
+  if (data_kind == C8)
+    return tb::contract_split_complex_launch(cptrn, drank, ddims, lrank, ldims, rrank, rdims, D, L, R, alpha_re,
+                                             alpha_im, conj_bits, accumulative, slices, scratch, scratch_bytes,
+                                             stream);
   return tb::contract_split_launch(data_kind, cptrn, drank, ddims, lrank, ldims, rrank, rdims, D, L, R,
                                    alpha_re, accumulative, slices, scratch, scratch_bytes, stream);
 }

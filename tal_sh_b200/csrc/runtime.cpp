@@ -573,9 +573,13 @@ int schedule(OpSpec &op, int dev_id, int dev_kind, talsh_task_t *user_task) {
     for (int i = 0; i < op.lrank; ++i) ld[i] = op.t[1]->shape_p->dims[i];
     for (int i = 0; i < op.rrank; ++i) rd[i] = op.t[2]->shape_p->dims[i];
     const int sl = g_r8_slices.load();
-    const size_t split = (sl > 0 && dkind == R8 && op.conj == 0)
-                             ? contract_split_scratch(dkind, op.dig, op.drank, dd, op.lrank, ld, op.rrank, rd, sl)
-                             : 0;
+    // Split precision: R8 without conjugation flags, C8 with any (rewritten as
+    // one real contraction); 0 scratch where the form does not apply.
+    const bool split_kind = (dkind == R8 && op.conj == 0) || dkind == C8;
+    const size_t split =
+        (sl > 0 && split_kind)
+            ? tcTensorContractSplitScratch(dkind, op.dig, op.drank, dd, op.lrank, ld, op.rrank, rd, sl)
+            : 0;
     bool hyper = false;
     for (int i = 0; i < op.lrank && !hyper; ++i)
       for (int j = 0; j < op.rrank; ++j)
@@ -684,9 +688,9 @@ int schedule(OpSpec &op, int dev_id, int dev_kind, talsh_task_t *user_task) {
       case kOpContract: {
         const int *dd = op.t[0]->shape_p->dims, *ld = op.t[1]->shape_p->dims, *rd = op.t[2]->shape_p->dims;
         if (tr->split_slices > 0)
-          rc = contract_split_launch(dkind, op.dig, op.drank, dd, op.lrank, ld, op.rrank, rd, tr->a[0].dptr,
-                                     tr->a[1].dptr, tr->a[2].dptr, op.sr, op.accumulative, tr->split_slices,
-                                     tr->scratch, scratch, st);
+          rc = tcTensorContractSplit(dkind, op.dig, op.drank, dd, op.lrank, ld, op.rrank, rd, tr->a[0].dptr,
+                                     tr->a[1].dptr, tr->a[2].dptr, op.sr, op.si, op.conj, op.accumulative,
+                                     tr->split_slices, tr->scratch, scratch, st);
         else
           rc = contract_launch(dkind, op.dig, op.drank, dd, op.lrank, ld, op.rrank, rd, tr->a[0].dptr,
                                tr->a[1].dptr, tr->a[2].dptr, op.sr, op.si, op.conj, op.accumulative,

@@ -281,3 +281,103 @@ def test_missing_library_fails_loudly(monkeypatch, tmp_path):
     monkeypatch.setattr(T, "LIB_PATH", str(tmp_path / "libtalsh.so"))
     with pytest.raises(RuntimeError, match="missing"):
         T.lib()
+
+
+SPLIT_COMPLEX_CASES = [
+    ("D(a,b)+=L(a,k)*R(k,b)", dict(a=5, b=4, k=6)),
+    ("D(a,b,i,j)+=L(a,k,c,i)*R(c,b,k,j)", dict(a=3, b=4, c=2, i=3, j=2, k=5)),
+    ("D(i,a)+=L(k,a,j)*R(j,i,k)", dict(a=7, i=3, j=4, k=2)),
+    ("D(a,b,c)+=L(c,a)*R(b,c)", dict(a=3, b=4, c=5)),  # hyper index: the rewrite keeps it (the split form refuses it)
+]
+
+
+@pytest.mark.parametrize("pattern,ext", SPLIT_COMPLEX_CASES)
+def test_complex_split_rewrite_matches_oracle(tmp_path, pattern, ext):
+    """The real form of a complex contraction that the split-precision form runs
+    (split_complex.h): L and D read as real tensors with a leading (re, im) index,
+    R's conjugated and i-rotated copies (alpha folded in) stacked along a trailing
+    index.  The oracle's real contraction of the rewritten problem equals its
+    complex contraction of the original, for every conjugation flag."""
+    import subprocess
+    e, dig, dr, lr, rr, _ = O.str2dig(pattern)
+    assert e == 0
+    groups = [[x for x in g.split(",") if x] for g in re.findall(r"\(([^)]*)\)", pattern)]
+    dd, ld, rd = ([ext[x] for x in g] for g in groups)
+    arr = lambda v: "{%s}" % ",".join(str(x) for x in (list(v) or [0]))
+    body = []
+    for conj in range(8):
+        body.append("{ const int c[] = %s, d[] = %s, l[] = %s, r[] = %s; tb::ComplexSplitForm f;"
+                    " int rc = tb::complex_split_form(c, %d, d, %d, l, %d, r, %d, f);"
+                    " std::printf(\"%%d %%d %%d %%d %%d %%g %%d\", rc, f.drank, f.lrank, f.rrank, f.y_conj, f.z_im,"
+                    " f.alpha_conj);"
+                    " for (int i = 0; i < f.lrank + f.rrank; ++i) std::printf(\" %%d\", f.cptrn[i]);"
+                    " for (int i = 0; i < f.drank; ++i) std::printf(\" %%d\", f.ddims[i]);"
+                    " for (int i = 0; i < f.lrank; ++i) std::printf(\" %%d\", f.ldims[i]);"
+                    " for (int i = 0; i < f.rrank; ++i) std::printf(\" %%d\", f.rdims[i]);"
+                    " std::printf(\"\\n\"); }" % (arr(dig[:lr + rr]), arr(dd), arr(ld), arr(rd), dr, lr, rr, conj))
+    src = tmp_path / "cs.cpp"
+    src.write_text('#include <cstdio>\n#include "split_complex.h"\nint main() {\n%s\nreturn 0; }\n' % "\n".join(body))
+    exe = tmp_path / "cs"
+    subprocess.run(["g++", "-std=c++17", "-I", os.path.join(ROOT, "include"), "-I",
+                    os.path.join(ROOT, "tal_sh_b200", "csrc"), str(src), "-o", str(exe)], check=True)
+    lines = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.splitlines()
+    rng = np.random.default_rng(17)
+    cplx = lambda s: np.asfortranarray(rng.standard_normal(s) + 1j * rng.standard_normal(s))
+    L, R, D0 = cplx(ld), cplx(rd), cplx(dd)
+    alpha = (0.75, -0.5)
+    as_real = lambda X: np.frombuffer(np.asarray(X).tobytes(order="F"), dtype=np.float64).reshape(
+        [2] + list(X.shape), order="F")
+    for conj, line in enumerate(lines):
+        v = [float(x) for x in line.split()]
+        rc, fdr, flr, frr, yconj, zim, aconj = (int(v[0]), int(v[1]), int(v[2]), int(v[3]), int(v[4]), v[5],
+                                                int(v[6]))
+        assert rc == 0 and (fdr, flr, frr) == (dr + 1, lr + 1, rr + 2)
+        rest = [int(x) for x in v[7:]]
+        fdig, rest = rest[:flr + frr], rest[flr + frr:]
+        fdd, rest = rest[:fdr], rest[fdr:]
+        fld, frd = rest[:flr], rest[flr:]
+        assert fdd == [2] + dd and fld == [2] + ld and frd == [2] + rd + [2]
+        a = complex(*alpha).conjugate() if aconj else complex(*alpha)
+        Y = np.conj(R) if yconj else R
+        Rx = np.asfortranarray(np.stack([Y * a, Y * (1j * zim * a)], axis=-1))
+        Dr = np.asfortranarray(as_real(D0).copy(order="F"))
+        assert O.tensor_contract(Dr, as_real(L), as_real(Rx), fdig, 1.0, 0.0, 0, True) == 0
+        got = np.frombuffer(Dr.tobytes(order="F"), dtype=np.complex128).reshape(dd, order="F")
+        ref = D0.copy(order="F")
+        assert O.tensor_contract(ref, L, R, dig, alpha[0], alpha[1], conj, True) == 0
+        assert np.linalg.norm(got - ref) <= 1e-13 * np.linalg.norm(ref - D0), (pattern, conj)
+
+
+def test_complex_split_host_checks(built):
+    """Host side of the complex(8) split-precision form, without a GPU: its scratch
+    is the stacked operand (2 vol(R) complex elements, 256-byte rounded) plus the
+    scratch of the rewritten real contraction; hyper-indices, rank-0 operands and
+    complex(4) are refused before anything is launched."""
+    L = T.lib()
+    e, dig, dr, lr, rr, _ = T.parse_pattern("D(a,b,i,j)+=L(a,k,c,i)*R(c,b,k,j)")
+    dd, ld, rd = [3, 4, 3, 2], [3, 5, 2, 3], [2, 4, 5, 2]
+    args = (T.ivec(dig), dr, T.ivec(dd), lr, T.ivec(ld), rr, T.ivec(rd))
+    shift = lambda v: v + 1 if v > 0 else v - 1
+    fdig = [-1] + [shift(v) for v in dig[:lr]] + [-1] + [shift(v) for v in dig[lr:lr + rr]] + [1]
+    for slices in (3, 6):
+        real = L.tcTensorContractSplitScratch(T.R8, T.ivec(fdig), dr + 1, T.ivec([2] + dd), lr + 1,
+                                              T.ivec([2] + ld), rr + 2, T.ivec([2] + rd + [2]), slices)
+        rx = (2 * int(np.prod(rd)) * 16 + 255) // 256 * 256
+        assert real > 0 and L.tcTensorContractSplitScratch(T.C8, *args, slices) == real + rx
+    assert L.tcTensorContractSplit(T.C8, *args, None, None, None, 1.0, 0.0, 0, 1, 6, None, 0, None) == \
+        T.TALSH_INVALID_ARGS
+    assert L.tcTensorContractSplit(T.C8, *args, None, None, None, 1.0, 0.0, 0, 1, 9, None, 0, None) == \
+        T.TALSH_INVALID_ARGS
+    assert L.tcTensorContractSplitScratch(T.C4, *args, 6) == 0
+    assert L.tcTensorContractSplit(T.C4, *args, None, None, None, 1.0, 0.0, 0, 1, 6, None, 0, None) == \
+        T.TALSH_NOT_IMPLEMENTED
+    e, hd, hdr, hlr, hrr, _ = T.parse_pattern("D(a,b,c)+=L(c,a)*R(b,c)")
+    hargs = (T.ivec(hd), hdr, T.ivec([3, 4, 5]), hlr, T.ivec([5, 3]), hrr, T.ivec([4, 5]))
+    assert L.tcTensorContractSplitScratch(T.C8, *hargs, 6) == 0
+    assert L.tcTensorContractSplit(T.C8, *hargs, None, None, None, 1.0, 0.0, 0, 1, 6, None, 0, None) == \
+        T.TALSH_NOT_IMPLEMENTED
+    e, sd, sdr, slr, srr, _ = T.parse_pattern("D()+=L(a,b)*R(b,a)")
+    sargs = (T.ivec(sd), sdr, T.ivec([]), slr, T.ivec([4, 5]), srr, T.ivec([5, 4]))
+    assert L.tcTensorContractSplitScratch(T.C8, *sargs, 6) == 0
+    assert L.tcTensorContractSplit(T.C8, *sargs, None, None, None, 1.0, 0.0, 0, 1, 6, None, 0, None) == \
+        T.TALSH_NOT_IMPLEMENTED

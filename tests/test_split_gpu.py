@@ -1,5 +1,6 @@
-"""Split-precision R8 contraction (tcTensorContractSplit: int8 slices on the
-tensor cores, recombined in FP64) against the FP64 oracle, through the C ABI."""
+"""Split-precision R8 and C8 contractions (tcTensorContractSplit: int8 slices on
+the tensor cores, recombined in FP64; C8 rewritten as one real contraction)
+against the FP64 oracle, through the C ABI."""
 import ctypes as C
 import re
 
@@ -88,12 +89,66 @@ def test_split_long_contraction_chunks(talsh):
     assert err <= TOL_SPLIT6, err
 
 
+def _run_complex(torch, pattern, ext, slices, alpha, conj, acc=True, seed=0):
+    """Complex(8) through the split form (rewritten as one real contraction)
+    against the oracle's complex contraction; error relative to the term."""
+    e, dig, dr, lr, rr, _ = T.parse_pattern(pattern)
+    assert e == 0
+    dl, ll, rl = _labels(pattern)
+    dd, ld, rd = ([ext[x] for x in g] for g in (dl, ll, rl))
+    rng = np.random.default_rng(seed)
+    cplx = lambda sh: fort(rng.standard_normal(sh) + 1j * rng.standard_normal(sh))
+    Lh, Rh, D0 = cplx(ld), cplx(rd), cplx(dd)
+    L = T.lib()
+    args = (T.C8, T.ivec(dig), dr, T.ivec(dd), lr, T.ivec(ld), rr, T.ivec(rd))
+    need = L.tcTensorContractSplitScratch(*args, slices)
+    assert need > 0
+    dev = lambda a: torch.from_numpy(np.asarray(a).ravel(order="F").copy()).cuda()
+    d, l, r = dev(D0), dev(Lh), dev(Rh)
+    scratch = torch.empty(need, dtype=torch.uint8, device="cuda")
+    rc = L.tcTensorContractSplit(*args, d.data_ptr(), l.data_ptr(), r.data_ptr(), alpha[0], alpha[1], conj,
+                                 1 if acc else 0, slices, scratch.data_ptr(), need,
+                                 torch.cuda.current_stream().cuda_stream)
+    assert rc == 0, (rc, L.tcLastErrorString())
+    torch.cuda.synchronize()
+    got = d.cpu().numpy().reshape(dd, order="F")
+    ref = D0.copy(order="F")
+    assert O.tensor_contract(ref, Lh, Rh, dig, alpha[0], alpha[1], conj, acc) == 0
+    term = ref - (D0 if acc else 0)
+    return np.linalg.norm((got - ref).ravel()) / np.linalg.norm(term.ravel())
+
+
+COMPLEX_CASES = [
+    ("D(a,b)+=L(a,k)*R(k,b)", dict(a=130, b=70, k=200)),
+    ("D(a,b,i,j)+=L(a,k,c,i)*R(c,b,k,j)", dict(a=16, b=16, c=16, i=16, j=16, k=16)),
+    ("D(i,a)+=L(k,a,j)*R(j,i,k)", dict(a=77, i=33, j=19, k=5)),
+]
+
+
+@pytest.mark.parametrize("conj", range(8))
+def test_split_complex_conjugation_flags(talsh, conj):
+    """Complex(8) split precision for every conjugation flag, complex alpha."""
+    torch = pytest.importorskip("torch")
+    pattern, ext = COMPLEX_CASES[0]
+    err = _run_complex(torch, pattern, ext, 6, (0.75, -0.5), conj)
+    assert err <= TOL_SPLIT6, (conj, err)
+
+
+@pytest.mark.parametrize("pattern,ext", COMPLEX_CASES)
+def test_split_complex_accuracy(talsh, pattern, ext):
+    torch = pytest.importorskip("torch")
+    err = _run_complex(torch, pattern, ext, 6, (1.0, 0.0), 0)
+    assert err <= TOL_SPLIT6, (pattern, err)
+    err = _run_complex(torch, pattern, ext, 6, (-0.5, 0.25), 6, acc=False, seed=1)
+    assert err <= TOL_SPLIT6, (pattern, err)
+
+
 def test_split_rejects_other_forms(talsh):
     L = T.lib()
     e, dig, dr, lr, rr, _ = T.parse_pattern("D(a,b)+=L(a,k)*R(k,b)")
     args = (T.ivec(dig), dr, T.ivec([4, 4]), lr, T.ivec([4, 4]), rr, T.ivec([4, 4]))
-    assert L.tcTensorContractSplitScratch(T.C8, *args, 6) == 0
-    assert L.tcTensorContractSplit(T.C8, *args, None, None, None, 1.0, 0.0, 0, 1, 6, None, 0, None) == \
+    assert L.tcTensorContractSplitScratch(T.C4, *args, 6) == 0
+    assert L.tcTensorContractSplit(T.C4, *args, None, None, None, 1.0, 0.0, 0, 1, 6, None, 0, None) == \
         T.TALSH_NOT_IMPLEMENTED
     assert L.tcTensorContractSplit(T.R8, *args, None, None, None, 1.0, 0.0, 0, 1, 9, None, 0, None) == \
         T.TALSH_INVALID_ARGS
@@ -140,3 +195,22 @@ print("OK")
     p = subprocess.run([sys.executable, "-c", code], env=env, stdout=subprocess.PIPE, stderr=subprocess.STDOUT,
                        text=True, timeout=600)
     assert p.returncode == 0 and "OK" in p.stdout, p.stdout
+
+
+def test_split_complex_through_talsh_contract(talsh):
+    """talshContractSlicesSet also routes C8 talshTensorContract (with
+    conjugation flags) through the split form."""
+    from gpu_util import gpu_contract
+    L = talsh
+    rng = np.random.default_rng(12)
+    cplx = lambda sh: fort(rng.standard_normal(sh) + 1j * rng.standard_normal(sh))
+    A, B, D0 = cplx((40, 30, 20)), cplx((20, 30, 50)), cplx((40, 50))
+    ref = D0.copy(order="F")
+    assert O.tensor_contract(ref, A, B, [1, -2, -1, -3, -2, 2], 0.5, -0.25, 4, True) == 0
+    assert L.talshContractSlicesSet(6) == 0
+    try:
+        D = D0.copy(order="F")
+        assert gpu_contract("D(a,b)+=L(a,k,c)*R+(c,k,b)", D, A, B, 0.5, -0.25) == 0
+    finally:
+        assert L.talshContractSlicesSet(0) == 0
+    assert rel_err(D - D0, ref - D0) <= TOL_SPLIT6
