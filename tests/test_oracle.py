@@ -243,3 +243,22 @@ def test_split_precision_model_error_bound():
     assert err(6) < 1e-10
     assert err(5) > 1e-10
     assert err(3) > err(4) > err(5) > err(6)
+
+
+def test_split_precision_model_complex_form():
+    """The complex form's error, modelled: a complex product rewritten as the real
+    product [Lr Li] x [[Yr Zr], [Yi Zi]] (Y = conj(R), Z = i conj(R)) and run through
+    the slice model stays under 1e-10 with 6 slices at the complex test shapes."""
+    from oracle.ozaki import split_gemm
+    rng = np.random.default_rng(4)
+    for M, N, K in ((130, 70, 200), (256, 256, 256), (77, 33, 95)):
+        A = rng.standard_normal((M, K)) + 1j * rng.standard_normal((M, K))
+        B = rng.standard_normal((K, N)) + 1j * rng.standard_normal((K, N))
+        Ar = np.stack([A.real, A.imag], axis=-1).reshape(M, 2 * K)        # k' = (k, c), c fastest
+        Y, Z = np.conj(B).T, (1j * np.conj(B)).T                            # N x K each
+        Bt = np.concatenate([np.stack([Y.real, Y.imag], axis=-1).reshape(N, 2 * K),
+                             np.stack([Z.real, Z.imag], axis=-1).reshape(N, 2 * K)])
+        C = split_gemm(Ar, Bt, 6)
+        got = C[:, :N] + 1j * C[:, N:]
+        ref = A @ B
+        assert np.linalg.norm(got - ref) / np.linalg.norm(ref) < 1e-10
