@@ -18,7 +18,10 @@ D = TRN(L) and one transpose-add D += TRN(L)*alpha (alpha cycling through
   roofline   the sweep's kernel launches (permute_reg_kernel, linear_kernel for
              permutations that fuse to a straight copy) timed one by one with CUDA events.
   contract   C1 and C3 FP64 contractions through talshTensorContract on
-             GPU-resident tensors (TFLOP/s, error vs an FP64 reference).
+             GPU-resident tensors (TFLOP/s, error vs an FP64 reference), plain
+             and split precision; C3b's shape in complex(8) likewise
+             (contract.complex); the C4 batch, the C5 serving loop and the
+             batched small transposes.
   cpu_baseline  the reference's cache-blocked CPU transpose (restated in the
              oracle, OpenMP over all host cores) on a bounded sample of the sweep.
 
@@ -582,7 +585,7 @@ def main():
     if not args.no_contract:
         contract = {}
         for name, leg in (("", bench_contractions), ("C4_batch", bench_batch), ("C5_serve", bench_serve),
-                          ("transpose_batch", bench_transpose_batch)):
+                          ("transpose_batch", bench_transpose_batch), ("complex", bench_contract_c8)):
             try:
                 res = leg(T, L, torch, dev)
             except Exception as exc:  # recorded, not hidden: the key carries the error
@@ -744,6 +747,75 @@ def bench_contractions(T, L, torch, dev):
             L.talshTensorDestruct(C.byref(t))
         del views, ref, got, lv, rv
     return out
+
+
+def bench_contract_c8(T, L, torch, dev, slices=6, reps=1):
+    """C3b's pattern and extents in complex(8) through talshTensorContract, GPU-resident:
+    the plain four-product DMMA path, then the split form (one real contraction of twice
+    the extents); the error of each against a complex128 einsum on the GPU (cuBLAS)."""
+    hb, ha = C.c_size_t(0), C.c_int(0)
+    rc = L.talshInit(C.byref(hb), C.byref(ha), 1, T.ivec([dev.index or 0]), 0, None, 0, None)
+    assert rc in (0, T.TALSH_ALREADY_INITIALIZED)
+    gpu = 1 + (dev.index or 0)
+    pat = "D(a,b,i,j)+=L(a,k,c,i)*R(c,b,k,j)"
+    dd, ld, rd = [192, 192, 64, 64], [192, 64, 192, 64], [192, 192, 64, 64]
+    kvol = 64 * 192
+    flops = 8.0 * np.prod(dd) * kvol
+    tens, out = [], {}
+    try:
+        for dims in (dd, ld, rd):
+            t = T.Tens()
+            L.talshTensorClean(C.byref(t))
+            rc = L.talshTensorConstruct(C.byref(t), T.C8, 4, T.ivec(dims), gpu, None, -1, None, 0.0, 0.0)
+            if rc != 0:
+                return {"error": "construct %d" % rc}
+            tens.append(t)
+        views = []
+        for t, dims in zip(tens, (dd, ld, rd)):
+            p = C.c_void_p()
+            assert L.talshTensorGetBodyAccess(C.byref(t), C.byref(p), T.C8, gpu, T.DEV_NULL) == 0
+            views.append(torch.as_tensor(_DevArray(p.value, 2 * int(np.prod(dims))), device=dev))
+        gen = torch.Generator(device=dev)
+        gen.manual_seed(8)
+        views[1].normal_(generator=gen).mul_((2 * kvol) ** -0.5)
+        views[2].normal_(generator=gen).mul_((2 * kvol) ** -0.5)
+        torch.cuda.synchronize(dev)
+        cview = lambda v, dims: torch.view_as_complex(v.view(-1, 2)).view(*reversed(dims))
+        # column-major bodies seen as row-major tensors with reversed extents
+        ref = torch.einsum("dcfa,efbc->edba", cview(views[1], ld), cview(views[2], rd))
+        got = cview(views[0], dd)
+        run = lambda: L.talshTensorContract(pat.encode(), C.byref(tens[0]), C.byref(tens[1]), C.byref(tens[2]),
+                                           1.0, 0.0, gpu, T.DEV_NULL, T.COPY_MTT, T.NOPE, None)
+
+        def timed():
+            assert run() == 0
+            torch.cuda.synchronize(dev)
+            t0 = time.perf_counter()
+            for _ in range(reps):
+                assert run() == 0
+            torch.cuda.synchronize(dev)
+            return (time.perf_counter() - t0) / reps
+        dt = timed()
+        err = float(torch.linalg.norm(got - ref) / torch.linalg.norm(ref))
+        out["C3b_c8"] = {"pattern": pat, "tflops": flops / dt / 1e12, "ms": dt * 1e3, "flop": flops,
+                         "rel_err_vs_fp64": err, "dtype": "c128",
+                         "path": "talshTensorContract, GPU-resident, plain (four-product DMMA)"}
+        assert L.talshContractSlicesSet(slices) == 0
+        try:
+            dts = timed()
+        finally:
+            assert L.talshContractSlicesSet(0) == 0
+        errs = float(torch.linalg.norm(got - ref) / torch.linalg.norm(ref))
+        out["C3b_c8_split%d" % slices] = {
+            "tflops_fp64_equiv": flops / dts / 1e12, "speedup_vs_plain": dt / dts, "ms": dts * 1e3,
+            "rel_err_vs_fp64": errs,
+            "path": "talshTensorContract with talshContractSlicesSet(%d), one real contraction of twice "
+                    "the extents" % slices}
+        del views, ref, got
+        return out
+    finally:
+        for t in tens:
+            L.talshTensorDestruct(C.byref(t))
 
 
 def c4_tasks(seed=4096, ntasks=4096, cap=1 << 21):
