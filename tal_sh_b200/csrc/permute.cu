@@ -40,7 +40,7 @@ namespace {
 constexpr int kThreads = 256;
 constexpr int kMinBlocks = 3;      // resident CTAs per SM the register budget is sized for
 constexpr int kMaxFR = 40;         // max fused rank (every fused extent is >= 2)
-constexpr int kTileBytes = 32768;  // bytes of one tile buffer (two buffers per CTA)
+constexpr int kTileBytes = 32768;  // byte budget of one tile buffer (kStages buffers per CTA)
 constexpr int kMaxTabLo = 4096;    // output run length when B needs a table (more than 3 dims)
 constexpr int kMaxRuns = 1024;     // run count bound (run tables live in shared memory)
 constexpr int kStages = 3;              // tile buffers per CTA: loads run kStages - 1 tiles ahead

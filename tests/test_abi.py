@@ -381,3 +381,39 @@ def test_complex_split_host_checks(built):
     assert L.tcTensorContractSplitScratch(T.C8, *sargs, 6) == 0
     assert L.tcTensorContractSplit(T.C8, *sargs, None, None, None, 1.0, 0.0, 0, 1, 6, None, 0, None) == \
         T.TALSH_NOT_IMPLEMENTED
+
+
+def test_transpose_plan_invariants(built):
+    """The transpose planner (host only) over thousands of random shapes: every tile
+    fits the per-thread register tables (at most 8 elements per thread of a
+    256-thread CTA, 4 for complex(8)), the tile splits into whole input runs and whole
+    output runs, vector accesses are at most 16 bytes, the tiles cover the tensor,
+    and identity permutations become a straight copy."""
+    L = T.lib()
+    rng = np.random.default_rng(2024)
+    esize = {T.R4: 4, T.R8: 8, T.C4: 8, T.C8: 16}
+    info = (C.c_int * 12)()
+    n_tiled = 0
+    for it in range(3000):
+        kind = [T.R4, T.R8, T.C4, T.C8][it % 4]
+        rank = int(rng.integers(1, 7))
+        dims = [int(x) for x in rng.choice([1, 2, 3, 5, 7, 16, 17, 31, 32, 64, 97, 100, 128, 333], size=rank)]
+        while np.prod(dims, dtype=np.int64) > 1 << 31:
+            dims[int(np.argmax(dims))] //= 2
+        o2n = [int(x) + 1 for x in rng.permutation(rank)]
+        assert L.tcPermutePlanInfo(kind, rank, T.ivec(dims), T.ivec(o2n), info) == 0, (kind, dims, o2n)
+        vol = int(np.prod(dims, dtype=np.int64))
+        assert 0 <= info[0] <= rank
+        if o2n == list(range(1, rank + 1)):
+            assert info[1] == 1, (dims, o2n)
+        if info[1]:
+            continue
+        n_tiled += 1
+        V, Li, Lo, Ri, Ro, vin, vout, smem, ntiles = (info[i] for i in range(2, 11))
+        per_thread = 4 if kind == T.C8 else 8
+        assert 1 <= V <= 256 * per_thread, (kind, dims, o2n, V)
+        assert Li * Ri == V and Lo * Ro == V, (dims, o2n, V, Li, Ri, Lo, Ro)
+        assert vin >= 1 and vout >= 1 and vin * esize[kind] <= 16 and vout * esize[kind] <= 16
+        assert 0 < smem <= 227 * 1024
+        assert ntiles >= 1 and ntiles * V >= vol, (dims, o2n, ntiles, V)
+    assert n_tiled > 1000
