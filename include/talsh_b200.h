@@ -76,8 +76,8 @@ int tcTensorContract(int data_kind, const int *cptrn, int drank, const int *ddim
                      int accumulative, void *scratch, size_t scratch_bytes, void *stream);
 
 /* Bytes of device scratch tcTensorContractSplit needs (0 when the form does
- * not apply: not R8 or C8, an operand of rank 0, or a C8 contraction with
- * hyper-indices). */
+ * not apply: not R8 or C8, an operand of rank 0, hyper-indices, or an invalid
+ * pattern). */
 size_t tcTensorContractSplitScratch(int data_kind, const int *cptrn, int drank, const int *ddims,
                                     int lrank, const int *ldims, int rrank, const int *rdims,
                                     int slices);

@@ -683,9 +683,24 @@ void operand_o2n(const int *cptrn, int lrank, const int *ldims, int rrank, const
 
 }  // namespace
 
+namespace {
+
+bool has_hyper_index(const int *cptrn, int lrank, int rrank) {
+  for (int i = 0; i < lrank; ++i)
+    for (int j = 0; cptrn[i] > 0 && j < rrank; ++j)
+      if (cptrn[lrank + j] == cptrn[i]) return true;
+  return false;
+}
+
+}  // namespace
+
+// 0 when the form does not apply: not R8, an operand of rank 0, an invalid
+// pattern or hyper-indices.
 size_t contract_split_scratch(int kind, const int *cptrn, int drank, const int *ddims, int lrank,
                               const int *ldims, int rrank, const int *rdims, int slices) {
   if (kind != R8 || lrank == 0 || rrank == 0 || drank == 0) return 0;
+  if (contract_validate(R8, cptrn, drank, ddims, lrank, ldims, rrank, rdims) != TALSH_SUCCESS) return 0;
+  if (has_hyper_index(cptrn, lrank, rrank)) return 0;
   int64_t M = 1, N = 1, K = 1;
   for (int i = 0; i < lrank; ++i) (cptrn[i] > 0 ? M : K) *= ldims[i];
   for (int i = 0; i < rrank; ++i)
@@ -705,6 +720,7 @@ int contract_split_launch(int kind, const int *cptrn, int drank, const int *ddim
   if (slices <= 0) slices = 6;
   if (slices < 2 || slices > kOzMaxSlices) return TALSH_INVALID_ARGS;
   if (D == nullptr || L == nullptr || R == nullptr || cptrn == nullptr) return TALSH_INVALID_ARGS;
+  if (has_hyper_index(cptrn, lrank, rrank)) return TALSH_NOT_IMPLEMENTED;
   if (!elem_aligned(R8, D) || !elem_aligned(R8, L) || !elem_aligned(R8, R)) return TALSH_INVALID_ARGS;
   const size_t need = contract_split_scratch(kind, cptrn, drank, ddims, lrank, ldims, rrank, rdims, slices);
   if (need == 0 || scratch == nullptr || scratch_bytes < need) return TALSH_INVALID_ARGS;
@@ -816,13 +832,6 @@ int contract_split_launch(int kind, const int *cptrn, int drank, const int *ddim
 // ---------------------------------------------------------------------------
 
 namespace {
-
-bool has_hyper_index(const int *cptrn, int lrank, int rrank) {
-  for (int i = 0; i < lrank; ++i)
-    for (int j = 0; cptrn[i] > 0 && j < rrank; ++j)
-      if (cptrn[lrank + j] == cptrn[i]) return true;
-  return false;
-}
 
 size_t complex_rx_bytes(int rrank, const int *rdims) {
   size_t v = 2;

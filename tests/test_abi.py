@@ -417,3 +417,38 @@ def test_transpose_plan_invariants(built):
         assert 0 < smem <= 227 * 1024
         assert ntiles >= 1 and ntiles * V >= vol, (dims, o2n, ntiles, V)
     assert n_tiled > 1000
+
+
+def test_contraction_scratch_queries_on_malformed_and_valid_patterns(built):
+    """Host-side pattern analysis without a GPU: random (mostly malformed) digital
+    patterns are analysed without crashing; valid random contractions get
+    scratch for the plain and the split forms, except hyper-indices in the split form."""
+    L = T.lib()
+    rng = np.random.default_rng(0)
+    for it in range(5000):
+        kind = [T.R4, T.R8, T.C4, T.C8][it % 4]
+        lr, rr, dr = (int(x) for x in rng.integers(0, 5, size=3))
+        cp = [int(x) for x in rng.integers(-5, 6, size=lr + rr)]
+        args = (T.ivec(cp), dr, T.ivec(rng.integers(1, 5, size=dr)), lr, T.ivec(rng.integers(1, 5, size=lr)),
+                rr, T.ivec(rng.integers(1, 5, size=rr)))
+        L.tcTensorContractScratch(kind, *args)
+        L.tcTensorContractSplitScratch(kind, *args, 6)
+    for it in range(400):
+        nc, lu, ru = int(rng.integers(1, 3)), int(rng.integers(1, 3)), int(rng.integers(1, 3))
+        hyper = it % 4 == 3
+        names = "abcdefgh"[: nc + lu + ru + (1 if hyper else 0)]
+        c, lo, ro = list(names[:nc]), list(names[nc:nc + lu]), list(names[nc + lu:nc + lu + ru])
+        h = [names[-1]] if hyper else []
+        Li, Ri = list(rng.permutation(c + lo + h)), list(rng.permutation(c + ro + h))
+        Di = list(rng.permutation(lo + ro + h))
+        pat = "D(%s)+=L(%s)*R(%s)" % (",".join(Di), ",".join(Li), ",".join(Ri))
+        ext = {x: int(rng.integers(2, 9)) for x in names}
+        e, dig, dr, lr, rr, _ = T.parse_pattern(pat)
+        assert e == 0, pat
+        args = (T.ivec(dig), dr, T.ivec([ext[x] for x in Di]), lr, T.ivec([ext[x] for x in Li]), rr,
+                T.ivec([ext[x] for x in Ri]))
+        for kind in (T.R8, T.C8):
+            assert L.tcTensorContractScratch(kind, *args) > 0, pat
+            split = L.tcTensorContractSplitScratch(kind, *args, 6)
+            assert (split == 0) if hyper else (split > 0), (pat, kind)
+        assert L.tcTensorContractSplitScratch(T.R4, *args, 6) == 0
