@@ -27,6 +27,7 @@
 #include <vector>
 
 #include "common.h"
+#include "device_once.h"
 
 namespace tb {
 int permute_scaled_by_device_scalar(int kind, int rank, const int *dims, const int *o2n,
@@ -845,12 +846,11 @@ int sm_count_dev() {
 template <int BM, int BN>
 int launch_dmma(const double *L, const double *R, double *D, GemmArgs ga, cudaStream_t st) {
   using C = DmmaCfg<BM, BN>;
-  static bool attr_set = false;
-  if (!attr_set) {
+  static std::atomic<uint64_t> attr_set{0};
+  once_per_device(attr_set, [] {
     cudaFuncSetAttribute(dgemm_gather_kernel<BM, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)C::SMEM);
-    attr_set = true;
-  }
+  });
   int64_t tiles = 0;
   if (gemm_grid(ga, BM, BN, &tiles)) return TALSH_LIMIT_EXCEEDED;
   dgemm_gather_kernel<BM, BN><<<(unsigned)tiles, C::THREADS, C::SMEM, st>>>(L, R, D, ga);
@@ -861,12 +861,11 @@ int launch_dmma(const double *L, const double *R, double *D, GemmArgs ga, cudaSt
 template <int BM, int BN>
 int launch_zmma(const double2 *L, const double2 *R, double2 *D, GemmArgs ga, cudaStream_t st) {
   using Z = ZmmaCfg<BM, BN>;
-  static bool attr_set = false;
-  if (!attr_set) {
+  static std::atomic<uint64_t> attr_set{0};
+  once_per_device(attr_set, [] {
     cudaFuncSetAttribute(zgemm_gather_kernel<BM, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)Z::SMEM);
-    attr_set = true;
-  }
+  });
   int64_t tiles = 0;
   if (gemm_grid(ga, BM, BN, &tiles)) return TALSH_LIMIT_EXCEEDED;
   zgemm_gather_kernel<BM, BN><<<(unsigned)tiles, Z::THREADS, Z::SMEM, st>>>(L, R, D, ga);
@@ -1389,24 +1388,22 @@ int launch_tc_batch(BatchKernel k, int threads, size_t smem, const char *name, c
 template <int BM, int BN>
 int launch_dmma_batch(const BatchPlan &bp, int c, char *base, cudaStream_t st) {
   using C = DmmaCfg<BM, BN>;
-  static bool attr = false;
-  if (!attr) {
+  static std::atomic<uint64_t> attr{0};
+  once_per_device(attr, [] {
     cudaFuncSetAttribute(dmma_batch_kernel<BM, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
     cudaFuncSetAttribute(dmma_batch_kernel<BM, BN>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-    attr = true;
-  }
+  });
   return launch_tc_batch(dmma_batch_kernel<BM, BN>, C::THREADS, C::SMEM, "dmma_batch_kernel", bp, c, base, st);
 }
 
 template <int BM, int BN>
 int launch_zmma_batch(const BatchPlan &bp, int c, char *base, cudaStream_t st) {
   using Z = ZmmaCfg<BM, BN>;
-  static bool attr = false;
-  if (!attr) {
+  static std::atomic<uint64_t> attr{0};
+  once_per_device(attr, [] {
     cudaFuncSetAttribute(zmma_batch_kernel<BM, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Z::SMEM);
     cudaFuncSetAttribute(zmma_batch_kernel<BM, BN>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-    attr = true;
-  }
+  });
   return launch_tc_batch(zmma_batch_kernel<BM, BN>, Z::THREADS, Z::SMEM, "zmma_batch_kernel", bp, c, base, st);
 }
 

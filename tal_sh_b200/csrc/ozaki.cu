@@ -29,6 +29,7 @@
 #include <mutex>
 
 #include "common.h"
+#include "device_once.h"
 #include "split_complex.h"
 
 namespace tb {
@@ -763,12 +764,11 @@ int contract_split_launch(int kind, const int *cptrn, int drank, const int *ddim
   const int64_t kc_max = ((int64_t)0x7fffffff / ((int64_t)slices * 127 * 127)) / kOzBK;
   const int64_t nkb = p.Kp / kOzBK;
   const int smem = kOzStages * slices * (kATileBytes + kBTileBytes);
-  static bool attr_done = false;
-  if (!attr_done) {
+  static std::atomic<uint64_t> attr_done{0};
+  once_per_device(attr_done, [] {
     cudaFuncSetAttribute(oz_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          kOzStages * kOzMaxSlices * (kATileBytes + kBTileBytes));
-    attr_done = true;
-  }
+  });
   OzArgs a;
   a.A = As; a.B = Bs; a.Mp = p.Mp; a.Np = p.Np; a.Kp = p.Kp; a.S = slices;
   a.ea = ea; a.eb = eb; a.D = (double *)D; a.mD = mD; a.nD = nD; a.M = M; a.N = N;
@@ -789,11 +789,10 @@ int contract_split_launch(int kind, const int *cptrn, int drank, const int *ddim
     const int64_t nkb32 = p.Kp / kWsBK, kc32 = kc_max * (kOzBK / kWsBK);
     const int64_t tiles = (p.Mp / kOzBM) * (p.Np / kWsBN);
     if (tiles > 0x7fffffffLL) return TALSH_LIMIT_EXCEEDED;
-    static bool ws_attr = false;
-    if (!ws_attr) {
+    static std::atomic<uint64_t> ws_attr{0};
+    once_per_device(ws_attr, [] {
       cudaFuncSetAttribute(oz_gemm_ws_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kOzWsSmem + 1024);
-      ws_attr = true;
-    }
+    });
     OzWsArgs w;
     w.Mp = p.Mp; w.Np = p.Np; w.S = slices; w.nst = nst;
     w.tiles_m = (int)(p.Mp / kOzBM);

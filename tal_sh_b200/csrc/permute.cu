@@ -27,7 +27,9 @@
 #include <climits>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <mutex>
+#include <tuple>
 #include <type_traits>
 #include <unordered_map>
 #include <vector>
@@ -1077,12 +1079,15 @@ int sm_count(int dev) {
 // any size can share the same kernel function.
 int blocks_per_sm(const void *fn, size_t smem) {
   static std::mutex mu;
-  static std::unordered_map<uint64_t, int> cache;
-  static std::unordered_map<const void *, bool> raised;
+  static std::map<std::tuple<const void *, size_t, int>, int> cache;  // (function, dynamic smem, device)
+  static std::unordered_map<const void *, uint64_t> raised;  // per function: devices already set up
   std::lock_guard<std::mutex> lk(mu);
-  if (!raised[fn]) {
-    int dev = 0, optin = 0;
-    cudaGetDevice(&dev);
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) { cudaGetLastError(); dev = 0; }
+  const uint64_t dev_bit = (dev >= 0 && dev < 64) ? (uint64_t(1) << dev) : 0;
+  uint64_t &raised_on = raised[fn];
+  if (dev_bit == 0 || (raised_on & dev_bit) == 0) {
+    int optin = 0;
     if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) optin = 0;
     cudaFuncAttributes fa;
     const int static_bytes = (cudaFuncGetAttributes(&fa, fn) == cudaSuccess) ? (int)fa.sharedSizeBytes : 1024;
@@ -1090,9 +1095,9 @@ int blocks_per_sm(const void *fn, size_t smem) {
       cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - static_bytes);
     cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     cudaGetLastError();
-    raised[fn] = true;
+    raised_on |= dev_bit;
   }
-  const uint64_t key = (uint64_t)(uintptr_t)fn ^ ((uint64_t)smem << 44);
+  const auto key = std::make_tuple(fn, smem, dev);
   auto it = cache.find(key);
   if (it != cache.end()) return it->second;
   int nb = 0;
