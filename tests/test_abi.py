@@ -452,3 +452,17 @@ def test_contraction_scratch_queries_on_malformed_and_valid_patterns(built):
             split = L.tcTensorContractSplitScratch(kind, *args, 6)
             assert (split == 0) if hyper else (split > 0), (pat, kind)
         assert L.tcTensorContractSplitScratch(T.R4, *args, 6) == 0
+
+
+def test_complex_split_rank_limit(built):
+    """An R operand of rank 55 would need rank 57 in the complex form's real
+    contraction (MAX_TENSOR_RANK is 56): the split form does not apply (0 bytes),
+    the plain form and the R8 split form still do."""
+    L = T.lib()
+    rank_r = 55
+    dig = [rank_r, -1] + [-2] + list(range(1, rank_r))   # D(r1..r54, a) += L(a, k) * R(k, r1..r54)
+    dd, ld, rd = [1] * (rank_r - 1) + [3], [3, 2], [2] + [1] * (rank_r - 1)
+    args = (T.ivec(dig), rank_r, T.ivec(dd), 2, T.ivec(ld), rank_r, T.ivec(rd))
+    assert L.tcTensorContractScratch(T.C8, *args) > 0
+    assert L.tcTensorContractSplitScratch(T.C8, *args, 6) == 0
+    assert L.tcTensorContractSplitScratch(T.R8, *args, 6) > 0
