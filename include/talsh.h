@@ -26,10 +26,12 @@
 
 #include "tensor_algebra.h"
 
+#ifndef TALSH_DEFAULT
 #ifdef __cplusplus
 #define TALSH_DEFAULT(x) = x
 #else
 #define TALSH_DEFAULT(x)
+#endif
 #endif
 
 /* Parameters */

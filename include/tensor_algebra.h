@@ -202,6 +202,15 @@ typedef int (*talsh_tens_init_i)(const talsh_tens_data_t *tens_data,
                                  const talsh_tens_shape_t *tens_shape,
                                  const talsh_tens_signature_t *tens_signature);
 
+/* C++ default arguments, as in the reference headers (none in C). */
+#ifndef TALSH_DEFAULT
+#ifdef __cplusplus
+#define TALSH_DEFAULT(x) = x
+#else
+#define TALSH_DEFAULT(x)
+#endif
+#endif
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -209,10 +218,10 @@ extern "C" {
 int talsh_tens_no_init(const talsh_tens_data_t *, const talsh_tens_shape_t *,
                        const talsh_tens_signature_t *);
 /* YEP if datk is a valid data kind (NO_TYPE included); its byte size in *datk_size. */
-int tens_valid_data_kind(int datk, int *datk_size);
+int tens_valid_data_kind(int datk, int *datk_size TALSH_DEFAULT(NULL));
 int tens_valid_data_kind_(int datk, int *datk_size);
 /* YEP if perm[base..base+perm_len-1] is the identity (values 1-based). */
-int permutation_trivial(const int perm_len, const int *perm, const int base);
+int permutation_trivial(const int perm_len, const int *perm, const int base TALSH_DEFAULT(0));
 /* Two-bit coherence component of argument arg_num out of tot_args. */
 unsigned int argument_coherence_get_value(unsigned int coh_ctrl, unsigned int tot_args,
                                           unsigned int arg_num);
@@ -230,6 +239,10 @@ void get_contr_permutations(int gemm_tl, int gemm_tr, int lrank, int rrank, cons
 void get_contraction_permutations(int gemm_tl, int gemm_tr, int lrank, int rrank,
                                   const int *cptrn, int conj_bits, int *dprm, int *lprm,
                                   int *rprm, int *ncd, int *nlu, int *nru, int *nhu, int *ierr);
+/* Digital pattern -> symbolic pattern string (reference tensor_algebra.h:265,
+ * tensor_algebra_cpu.F90:5533-5611); *cpl = its length, *ierr = 0 on success. */
+void get_contr_pattern_sym(const int *rank_left, const int *rank_right, const int *conj_bits,
+                           const int *cptrn_dig, char *cptrn_sym, int *cpl, int *ierr);
 /* Symbolic pattern string -> digital pattern (0 = success). */
 int talsh_get_contr_ptrn_str2dig(const char *c_str, int *dig_ptrn, int *drank, int *lrank,
                                  int *rrank, int *conj_bits);

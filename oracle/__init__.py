@@ -82,6 +82,14 @@ def str2dig(pattern):
     return e, list(dig[:n]), dr.value, lr.value, rr.value, cj.value
 
 
+def pattern_sym(cptrn, lrank, rrank, conj_bits=0):
+    """Digital -> symbolic pattern: (ierr, string)."""
+    buf = C.create_string_buffer(16 + 4 * (max(lrank, 0) + max(rrank, 0)))
+    cpl = C.c_int()
+    e = lib().orc_pattern_sym(lrank, rrank, conj_bits, _iv(list(cptrn) or [0]), buf, C.byref(cpl))
+    return e, buf.raw[:cpl.value].decode("latin-1")
+
+
 def permutations(cptrn, lrank, rrank, conj=0, variant="cpu", gemm_tl=1, gemm_tr=0):
     """Matricization: (ierr, dprm[1:], lprm[1:], rprm[1:], ncd, nlu, nru, nhu)."""
     a = _iv(cptrn)

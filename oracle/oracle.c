@@ -189,6 +189,63 @@ int orc_str2dig(const char *s, int *dig, int *drank, int *lrank, int *rrank, int
   return 0;
 }
 
+/* get_contr_pattern_sym (tensor_algebra_cpu.F90:5533-5611): digital pattern ->
+ * symbolic pattern, written position by position as the Fortran does (the
+ * closing ')' replaces a trailing ',' or follows an empty '(').  Returns ierr:
+ * 1 for a negative rank; also for a rank above ORC_MAX_RANK or an R index whose
+ * partner is not a contracted L index (undefined in the reference). */
+static void put_head(char *out, int *n, char name, int conj) {
+  out[(*n)++] = name;
+  if (conj) out[(*n)++] = '+';
+  out[(*n)++] = '(';
+}
+
+static void put_close(char *out, int *n) {
+  if (out[*n - 1] == '(') ++*n;
+  out[*n - 1] = ')';
+}
+
+int orc_pattern_sym(int lrank, int rrank, int conj_bits, const int *dig, char *out, int *cpl) {
+  char left_lbl[ORC_MAX_RANK];
+  int n = 0, nu = 0, m;
+  *cpl = 0;
+  if (lrank < 0 || rrank < 0 || lrank > ORC_MAX_RANK || rrank > ORC_MAX_RANK) return 1;
+  for (int i = 0; i < lrank + rrank; ++i) if (dig[i] > 0) ++nu;
+  put_head(out, &n, 'D', conj_bits & 1);
+  m = 'a';
+  for (int i = 0; i < nu; ++i) { out[n++] = (char)m; out[n++] = ','; ++m; }
+  put_close(out, &n);
+  out[n++] = '+'; out[n++] = '=';
+  put_head(out, &n, 'L', conj_bits & 2);
+  for (int i = 0; i < lrank; ++i) {
+    if (dig[i] > 0) {
+      out[n++] = (char)('a' + dig[i] - 1);
+    } else {
+      left_lbl[i] = (char)m;
+      out[n++] = (char)m;
+      ++m;
+    }
+    out[n++] = ',';
+  }
+  put_close(out, &n);
+  out[n++] = '*';
+  put_head(out, &n, 'R', conj_bits & 4);
+  for (int i = 0; i < rrank; ++i) {
+    int v = dig[lrank + i];
+    if (v > 0) {
+      out[n++] = (char)('a' + v - 1);
+    } else {
+      if (-v < 1 || -v > lrank || dig[-v - 1] > 0) return 1;
+      out[n++] = left_lbl[-v - 1];
+    }
+    out[n++] = ',';
+  }
+  put_close(out, &n);
+  out[n] = '\0';
+  *cpl = n;
+  return 0;
+}
+
 /* ------------------------------------------------------------------------- */
 /* Permutation solvers                                                       */
 /* ------------------------------------------------------------------------- */

@@ -20,6 +20,10 @@
  * Returns 0 or the reference's error code. */
 int orc_str2dig(const char *s, int *dig, int *drank, int *lrank, int *rrank, int *conj_bits);
 
+/* Digital pattern -> symbolic pattern (tensor_algebra_cpu.F90:5533-5611); out
+ * holds at least 16 + 4 * (lrank + rrank) characters.  Returns ierr. */
+int orc_pattern_sym(int lrank, int rrank, int conj_bits, const int *dig, char *out, int *cpl);
+
 /* Matricization permutations for GEMM(T,N); CPU variant with hyper-indices
  * (tensor_algebra_cpu.F90:5757-5956). Returns ierr. */
 int orc_contraction_permutations(int gemm_tl, int gemm_tr, int lrank, int rrank, const int *cptrn,

@@ -172,6 +172,9 @@ _PROTOS = {
     "talshContractSlicesSet": (_I, [_I]),
     "talshContractSlicesGet": (_I, []),
     "talsh_get_contr_ptrn_str2dig": (_I, [_S, _P(_I), _P(_I), _P(_I), _P(_I), _P(_I)]),
+    "get_contr_pattern_sym": (None, [_P(_I), _P(_I), _P(_I), _P(_I), C.c_char_p, _P(_I), _P(_I)]),
+    "host_mem_register": (_I, [_V, _Z]),
+    "host_mem_unregister": (_I, [_V]),
     "get_contr_permutations": (None, [_I, _I, _I, _I, _P(_I), _I, _P(_I), _P(_I), _P(_I),
                                       _P(_I), _P(_I), _P(_I), _P(_I)]),
     "get_contraction_permutations": (None, [_I, _I, _I, _I, _P(_I), _I, _P(_I), _P(_I), _P(_I),
@@ -249,6 +252,15 @@ def ivec(seq):
     seq = list(seq)
     arr = (C.c_int * max(1, len(seq)))(*seq)
     return arr
+
+
+def pattern_sym(digital, lrank, rrank, conj_bits=0):
+    """get_contr_pattern_sym: returns (ierr, symbolic pattern string)."""
+    buf = C.create_string_buffer(16 + 4 * (max(lrank, 0) + max(rrank, 0)))
+    cpl, ierr = C.c_int(0), C.c_int(0)
+    lib().get_contr_pattern_sym(C.byref(C.c_int(lrank)), C.byref(C.c_int(rrank)), C.byref(C.c_int(conj_bits)),
+                                ivec(digital), buf, C.byref(cpl), C.byref(ierr))
+    return ierr.value, buf.raw[:cpl.value].decode("latin-1")
 
 
 def parse_pattern(pattern):

@@ -160,6 +160,71 @@ extern "C" int talsh_get_contr_ptrn_str2dig(const char *c_str, int *dig_ptrn, in
   return 0;
 }
 
+// Digital pattern -> symbolic pattern, the inverse direction (reference
+// get_contr_pattern_sym, tensor_algebra_cpu.F90:5533-5611, called by talshc.cpp
+// and talshxx.hpp): D's indices are named a, b, ... (one name per positive
+// entry of the pattern, so a hyper-index is named twice), every contracted
+// index of L takes the next free letter in order and its partner in R repeats
+// that letter; '+' after a tensor name marks conjugation (bit 0 D, bit 1 L,
+// bit 2 R).  The buffer must hold at most 15 + 4 * (rank_left + rank_right)
+// characters plus the NUL; *cpl is the length without the NUL.  *ierr = 1 for
+// a negative rank; also (the reference prints an undefined character or
+// overruns there) for a rank above MAX_TENSOR_RANK or a contracted index of R
+// whose partner position is not a contracted index of L.
+extern "C" void get_contr_pattern_sym(const int *rank_left, const int *rank_right, const int *conj_bits,
+                                      const int *cptrn_dig, char *cptrn_sym, int *cpl, int *ierr) {
+  *ierr = 0;
+  *cpl = 0;
+  const int lr = *rank_left, rr = *rank_right, cj = *conj_bits;
+  if (lr < 0 || rr < 0 || lr > MAX_TENSOR_RANK || rr > MAX_TENSOR_RANK) {
+    *ierr = 1;
+    return;
+  }
+  std::string s;
+  const auto open = [&](char name, int bit) {
+    s += name;
+    if (cj & bit) s += '+';
+    s += '(';
+  };
+  const auto close = [&] {
+    if (s.back() == ',') s.back() = ')';
+    else s += ')';
+  };
+  int nu = 0;
+  for (int i = 0; i < lr + rr; ++i) nu += cptrn_dig[i] > 0;
+  open('D', 1);
+  for (int i = 0; i < nu; ++i) (s += char('a' + i)) += ',';
+  close();
+  s += "+=";
+  open('L', 2);
+  char label[MAX_TENSOR_RANK];
+  int fresh = nu;
+  for (int i = 0; i < lr; ++i) {
+    const int v = cptrn_dig[i];
+    label[i] = v > 0 ? char('a' + v - 1) : char('a' + fresh++);
+    (s += label[i]) += ',';
+  }
+  close();
+  s += '*';
+  open('R', 4);
+  for (int j = 0; j < rr; ++j) {
+    const int v = cptrn_dig[lr + j];
+    if (v > 0) {
+      s += char('a' + v - 1);
+    } else {
+      if (-v < 1 || -v > lr || cptrn_dig[-v - 1] > 0) {
+        *ierr = 1;
+        return;
+      }
+      s += label[-v - 1];
+    }
+    s += ',';
+  }
+  close();
+  std::memcpy(cptrn_sym, s.c_str(), s.size() + 1);
+  *cpl = (int)s.size();
+}
+
 // ---------------------------------------------------------------------------
 // Matricization permutations (GEMM 'T','N' by default).  These are exported
 // for callers of the reference ABI; the GPU contraction of this core gathers

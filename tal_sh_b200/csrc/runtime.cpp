@@ -2255,3 +2255,27 @@ int talshContractSlicesSet(int slices) {
 int talshContractSlicesGet(void) { return g_r8_slices.load(); }
 
 }  // extern "C"
+
+// Pinning of caller memory (include/mem_manager.h), for the reference's C++
+// layer.  Portable: the pinned range serves every GPU of the process.
+#include "mem_manager.h"
+
+int host_mem_register(void *host_ptr, size_t tsize) {
+  const cudaError_t e = cudaHostRegister(host_ptr, tsize, cudaHostRegisterPortable);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    tb::note_cuda_error("host_mem_register", (int)e);
+    return 1;
+  }
+  return 0;
+}
+
+int host_mem_unregister(void *host_ptr) {
+  const cudaError_t e = cudaHostUnregister(host_ptr);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    tb::note_cuda_error("host_mem_unregister", (int)e);
+    return 1;
+  }
+  return 0;
+}

@@ -164,3 +164,18 @@ def test_device_abi_direct(talsh):
     assert L.tcTensorPermute(T.R8, 3, T.ivec([40, 30, 20]), T.ivec([1, 1, 2]), src.data_ptr(), dst.data_ptr(), 0,
                              stream) == T.TALSH_INVALID_ARGS
     assert L.tcKernelLaunchCount() == before
+
+
+def test_host_mem_register_pins_caller_memory(talsh):
+    """host_mem_register / host_mem_unregister (mem_manager.h; the reference C++
+    layer's pinHostMemory / unpinHostMemory): 0 on success, 1 for a second
+    registration or an unregistration of memory that is not pinned."""
+    L = talsh
+    buf = np.zeros(1 << 16)
+    p = C.c_void_p(buf.ctypes.data)
+    assert L.host_mem_register(p, buf.nbytes) == 0
+    try:
+        assert L.host_mem_register(p, buf.nbytes) == 1
+    finally:
+        assert L.host_mem_unregister(p) == 0
+    assert L.host_mem_unregister(p) == 1
