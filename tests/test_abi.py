@@ -545,3 +545,39 @@ def test_reference_cpp_layer_links_against_the_library(built, tmp_path):
         objs.append(str(obj))
     subprocess.run(["g++", "-shared", "-o", str(tmp_path / "libtalshxx.so"), *objs, "-L",
                     os.path.join(ROOT, "tal_sh_b200"), "-ltalsh", "-Wl,--no-undefined"], check=True)
+
+
+# Calls of the reference test driver's test_nvtal_c into the reference's internal
+# GPU layer (device_algebra.h, its argument buffers in mem_manager.h), which this
+# core replaces with the device ABI of talsh_b200.h instead of reproducing.
+NVTAL_INTERNAL = ["arg_buf_allocate", "arg_buf_deallocate", "cuda_task_create", "cuda_task_destroy",
+                  "cuda_task_print", "cuda_task_time", "cuda_task_wait", "gpu_print_stats",
+                  "gpu_tensor_block_contract_dlf", "tensBlck_attach_body", "tensBlck_construct", "tensBlck_create",
+                  "tensBlck_destroy", "tensBlck_init_host", "tensBlck_norm2_host", "tensBlck_volume"]
+
+
+def test_reference_test_driver_links_against_the_library(built, tmp_path):
+    """The reference's own test driver (test.cpp: test_talsh_c, _cxx, _xl, _hyper,
+    _svd, _qc, _nwchem, ...) with its C++ layer, compiled against include/, links
+    against libtalsh.so with nothing undefined except test_nvtal_c's internal-layer
+    calls (stubbed here).  Skipped where the reference sources are absent."""
+    import subprocess
+    ref = _reference_tree()
+    if ref is None or not os.path.exists(os.path.join(ref, "test.cpp")):
+        pytest.skip("reference sources not present")
+    cuda_inc = os.path.join(os.environ.get("CUDA_HOME", "/usr/local/cuda"), "include")
+    shim = tmp_path / "nvtal_decl.h"
+    shim.write_text('#include <stddef.h>\nextern "C" int arg_buf_allocate(size_t *, int *, int, int);\n'
+                    'extern "C" int arg_buf_deallocate(int, int);\n')
+    stub = tmp_path / "nvtal_stub.c"
+    stub.write_text("".join("int %s(void) { return -1; }\n" % n for n in NVTAL_INTERNAL))
+    objs = []
+    for name in ("test", "talshxx", "talsh_task"):
+        obj = tmp_path / (name + ".o")
+        subprocess.run(["g++", "-std=c++14", "-fPIC", "-w", "-c", "-include", str(shim), "-I",
+                        os.path.join(ROOT, "include"), "-I-", "-I", ref, "-I", cuda_inc,
+                        os.path.join(ref, name + ".cpp"), "-o", str(obj)], check=True)
+        objs.append(str(obj))
+    subprocess.run(["gcc", "-fPIC", "-c", str(stub), "-o", str(tmp_path / "stub.o")], check=True)
+    subprocess.run(["g++", "-shared", "-o", str(tmp_path / "libdriver.so"), *objs, str(tmp_path / "stub.o"), "-L",
+                    os.path.join(ROOT, "tal_sh_b200"), "-ltalsh", "-lm", "-Wl,--no-undefined"], check=True)
