@@ -404,6 +404,16 @@ double talshTensorNorm1(talsh_tens_t *tens, int dev_id TALSH_DEFAULT(DEV_DEFAULT
                         int dev_kind TALSH_DEFAULT(DEV_DEFAULT));
 double talshTensorNorm1_(talsh_tens_t *tens, int dev_id, int dev_kind);
 
+/* Entry points of the reference's C side that its Fortran module (talshf.F90:528-547)
+ * binds.  Body image information (reference talshc.cpp:245-267): TALSH_NOT_ALLOWED
+ * when the image is no longer available; *buf_entry is -1 for bodies the library
+ * allocates (no carved buffer here), the caller's value for external memory. */
+int talsh_tensor_image_info(const talsh_tens_t *talsh_tens, int image_id, int *dev_id, int *data_kind,
+                            void **gmem_p, int *buf_entry);
+/* GPU count (reference tensor_algebra_gpu_nvidia.cu:2728-2739): 0, or 1 with
+ * *dev_count = -1 when the CUDA runtime cannot tell. */
+int gpu_get_device_count(int *dev_count);
+
 /* Extension of this core (no counterpart in the reference): the form R8 and
  * C8 contractions of talshTensorContract run in.  0 (default) = plain FP64,
  * the drop-in behaviour; 2..7 = split precision on the tensor cores with that

@@ -175,6 +175,8 @@ _PROTOS = {
     "get_contr_pattern_sym": (None, [_P(_I), _P(_I), _P(_I), _P(_I), C.c_char_p, _P(_I), _P(_I)]),
     "host_mem_register": (_I, [_V, _Z]),
     "host_mem_unregister": (_I, [_V]),
+    "talsh_tensor_image_info": (_I, [_P(Tens), _I, _P(_I), _P(_I), _P(_V), _P(_I)]),
+    "gpu_get_device_count": (_I, [_P(_I)]),
     "get_contr_permutations": (None, [_I, _I, _I, _I, _P(_I), _I, _P(_I), _P(_I), _P(_I),
                                       _P(_I), _P(_I), _P(_I), _P(_I)]),
     "get_contraction_permutations": (None, [_I, _I, _I, _I, _P(_I), _I, _P(_I), _P(_I), _P(_I),

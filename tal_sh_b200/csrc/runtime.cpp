@@ -2279,3 +2279,43 @@ int host_mem_unregister(void *host_ptr) {
   }
   return 0;
 }
+
+// Entry points of the reference's C side that its Fortran module binds
+// (talshf.F90:528-547).
+
+// One body image of a tensor (reference talshc.cpp:245-267): its flat device
+// id, data kind, address and argument-buffer entry (-1 for bodies the library
+// allocates, which are not in a carved buffer; the caller's value for external
+// memory); TALSH_NOT_ALLOWED when the image is no longer available.
+int talsh_tensor_image_info(const talsh_tens_t *talsh_tens, int image_id, int *dev_id, int *data_kind,
+                            void **gmem_p, int *buf_entry) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (talsh_tens == nullptr || dev_id == nullptr || data_kind == nullptr || gmem_p == nullptr ||
+      buf_entry == nullptr)
+    return TALSH_INVALID_ARGS;
+  if (talshTensorIsEmpty(talsh_tens) != NOPE) return TALSH_OBJECT_IS_EMPTY;
+  if (!healthy(talsh_tens)) return TALSH_FAILURE;
+  if (image_id < 0 || image_id >= talsh_tens->ndev) return TALSH_INVALID_ARGS;
+  talsh_dev_rsc_t *r = &talsh_tens->dev_rsc[image_id];
+  if (tensDevRsc_is_empty(r) != NOPE) return TALSH_FAILURE;
+  if (talsh_tens->avail[image_id] != YEP) return TALSH_NOT_ALLOWED;
+  *dev_id = r->dev_id;
+  *data_kind = talsh_tens->data_kind[image_id];
+  *gmem_p = r->gmem_p;
+  *buf_entry = r->buf_entry;
+  return TALSH_SUCCESS;
+}
+
+// Number of NVIDIA GPUs on the node (reference tensor_algebra_gpu_nvidia.cu:2728-2739):
+// 0, or 1 with *dev_count = -1 when the CUDA runtime cannot tell.
+int gpu_get_device_count(int *dev_count) {
+  if (dev_count == nullptr) return 1;
+  const cudaError_t e = cudaGetDeviceCount(dev_count);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    tb::note_cuda_error("gpu_get_device_count", (int)e);
+    *dev_count = -1;
+    return 1;
+  }
+  return 0;
+}

@@ -581,3 +581,45 @@ def test_reference_test_driver_links_against_the_library(built, tmp_path):
     subprocess.run(["gcc", "-fPIC", "-c", str(stub), "-o", str(tmp_path / "stub.o")], check=True)
     subprocess.run(["g++", "-shared", "-o", str(tmp_path / "libdriver.so"), *objs, str(tmp_path / "stub.o"), "-L",
                     os.path.join(ROOT, "tal_sh_b200"), "-ltalsh", "-lm", "-Wl,--no-undefined"], check=True)
+
+
+def test_fortran_bound_entry_points_without_gpu(built):
+    """talsh_tensor_image_info and gpu_get_device_count, which the reference's
+    Fortran module binds: image information of a Host tensor, refusal of a
+    missing image, and a GPU count that reports failure without a device."""
+    L = T.lib()
+    hb, ha = C.c_size_t(0), C.c_int(0)
+    assert L.talshInit(C.byref(hb), C.byref(ha), 0, None, 0, None, 0, None) == 0
+    try:
+        ext = np.asfortranarray(np.arange(12.0).reshape(3, 4, order="F"))
+        t = T.Tensor([3, 4], T.R8, dev_id=0, ext=ext)
+        dev, kind, ptr, buf = C.c_int(), C.c_int(), C.c_void_p(), C.c_int()
+        args = (C.byref(dev), C.byref(kind), C.byref(ptr), C.byref(buf))
+        assert L.talsh_tensor_image_info(t.ref, 0, *args) == 0
+        assert (dev.value, kind.value, ptr.value) == (0, T.R8, ext.ctypes.data)
+        assert L.talsh_tensor_image_info(t.ref, 1, *args) == T.TALSH_INVALID_ARGS
+        assert t.destruct() == 0
+        assert L.talsh_tensor_image_info(t.ref, 0, *args) == T.TALSH_OBJECT_IS_EMPTY
+    finally:
+        assert L.talshShutdown() == 0
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        n = C.c_int(7)
+        assert L.gpu_get_device_count(C.byref(n)) == 1 and n.value == -1
+
+
+def test_fortran_module_imports_are_exported(built):
+    """Every C function the reference's Fortran module (talshf.F90) declares in its
+    interface blocks is exported by libtalsh.so, so the module links against it.
+    Skipped where the reference sources are absent."""
+    ref = _reference_tree()
+    if ref is None or not os.path.exists(os.path.join(ref, "talshf.F90")):
+        pytest.skip("reference sources not present")
+    text = open(os.path.join(ref, "talshf.F90")).read()
+    imports = set()
+    for block in re.findall(r"^\s*interface\s*$(.*?)^\s*end\s+interface", text, flags=re.M | re.S | re.I):
+        imports |= set(re.findall(r"bind\s*\(\s*c\s*,\s*name\s*=\s*'(\w+)'", block, flags=re.I))
+    assert len(imports) > 40
+    L = T.lib()
+    missing = sorted(n for n in imports if not hasattr(L, n))
+    assert not missing, missing
