@@ -259,6 +259,21 @@ int tensShape_rank(const talsh_tens_shape_t *tshape);
 int tensDevRsc_clean(talsh_dev_rsc_t *drsc);
 int tensDevRsc_is_empty(talsh_dev_rsc_t *drsc);
 int tensDevRsc_device_id(talsh_dev_rsc_t *drsc);
+/* Device-resource descriptors (reference tensor_algebra.h:283-295,
+ * tensor_algebra_gpu.cpp:278-555), with the reference's return codes.  Allocated
+ * memory comes from the library's allocators (Host: pinned when a GPU is in use;
+ * GPU: the stream-ordered pool under its budget, TRY_LATER above it); there is
+ * no argument buffer, so in_arg_buf is ignored. */
+int tensDevRsc_create(talsh_dev_rsc_t **drsc);
+int tensDevRsc_same(const talsh_dev_rsc_t *drsc0, const talsh_dev_rsc_t *drsc1);
+int tensDevRsc_clone(const talsh_dev_rsc_t *drsc_in, talsh_dev_rsc_t *drsc_out);
+int tensDevRsc_attach_mem(talsh_dev_rsc_t *drsc, int dev_id, void *mem_p, int buf_entry TALSH_DEFAULT(-1));
+int tensDevRsc_detach_mem(talsh_dev_rsc_t *drsc);
+int tensDevRsc_allocate_mem(talsh_dev_rsc_t *drsc, int dev_id, size_t mem_size, int in_arg_buf TALSH_DEFAULT(NOPE));
+int tensDevRsc_free_mem(talsh_dev_rsc_t *drsc);
+int tensDevRsc_get_gmem_ptr(talsh_dev_rsc_t *drsc, void **gmem_p);
+int tensDevRsc_release_all(talsh_dev_rsc_t *drsc);
+int tensDevRsc_destroy(talsh_dev_rsc_t *drsc);
 #ifdef __cplusplus
 }
 #endif

@@ -177,6 +177,19 @@ _PROTOS = {
     "host_mem_unregister": (_I, [_V]),
     "talsh_tensor_image_info": (_I, [_P(Tens), _I, _P(_I), _P(_I), _P(_V), _P(_I)]),
     "gpu_get_device_count": (_I, [_P(_I)]),
+    "tensDevRsc_create": (_I, [_P(_P(DevRsc))]),
+    "tensDevRsc_clean": (_I, [_P(DevRsc)]),
+    "tensDevRsc_is_empty": (_I, [_P(DevRsc)]),
+    "tensDevRsc_same": (_I, [_P(DevRsc), _P(DevRsc)]),
+    "tensDevRsc_clone": (_I, [_P(DevRsc), _P(DevRsc)]),
+    "tensDevRsc_attach_mem": (_I, [_P(DevRsc), _I, _V, _I]),
+    "tensDevRsc_detach_mem": (_I, [_P(DevRsc)]),
+    "tensDevRsc_allocate_mem": (_I, [_P(DevRsc), _I, _Z, _I]),
+    "tensDevRsc_free_mem": (_I, [_P(DevRsc)]),
+    "tensDevRsc_get_gmem_ptr": (_I, [_P(DevRsc), _P(_V)]),
+    "tensDevRsc_device_id": (_I, [_P(DevRsc)]),
+    "tensDevRsc_release_all": (_I, [_P(DevRsc)]),
+    "tensDevRsc_destroy": (_I, [_P(DevRsc)]),
     "get_contr_permutations": (None, [_I, _I, _I, _I, _P(_I), _I, _P(_I), _P(_I), _P(_I),
                                       _P(_I), _P(_I), _P(_I), _P(_I)]),
     "get_contraction_permutations": (None, [_I, _I, _I, _I, _P(_I), _I, _P(_I), _P(_I), _P(_I),

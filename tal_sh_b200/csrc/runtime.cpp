@@ -874,6 +874,118 @@ int tensDevRsc_is_empty(talsh_dev_rsc_t *drsc) {
 }
 int tensDevRsc_device_id(talsh_dev_rsc_t *drsc) { return drsc ? drsc->dev_id : DEV_NULL; }
 
+// The rest of the device-resource API (reference tensor_algebra_gpu.cpp:278-555),
+// with the reference's return codes.  Memory a descriptor allocates comes from
+// the same allocators as tensor bodies: Host memory pinned when a GPU is in use
+// (there is no Host argument buffer, so in_arg_buf is ignored), GPU memory from
+// that GPU's stream-ordered pool under its byte budget (TRY_LATER above it).
+int tensDevRsc_create(talsh_dev_rsc_t **drsc) {
+  if (drsc == nullptr) return TALSH_INVALID_ARGS;
+  *drsc = (talsh_dev_rsc_t *)std::malloc(sizeof(talsh_dev_rsc_t));
+  if (*drsc == nullptr) return TRY_LATER;
+  return tensDevRsc_clean(*drsc);
+}
+
+int tensDevRsc_same(const talsh_dev_rsc_t *drsc0, const talsh_dev_rsc_t *drsc1) {
+  if (drsc0 == nullptr) return -1;
+  if (drsc1 == nullptr) return -2;
+  return (drsc0->dev_id == drsc1->dev_id && drsc0->gmem_p == drsc1->gmem_p) ? YEP : NOPE;
+}
+
+int tensDevRsc_clone(const talsh_dev_rsc_t *drsc_in, talsh_dev_rsc_t *drsc_out) {
+  if (drsc_in == nullptr) return -1;
+  if (drsc_out == nullptr) return -2;
+  *drsc_out = *drsc_in;
+  return 0;
+}
+
+int tensDevRsc_attach_mem(talsh_dev_rsc_t *drsc, int dev_id, void *mem_p, int buf_entry) {
+  if (drsc == nullptr) return -1;
+  if (dev_id < 0 || dev_id >= DEV_MAX) return -2;
+  if (mem_p == nullptr) return -3;
+  if (drsc->dev_id >= 0 && drsc->dev_id != dev_id) return 1;  // bound to another device
+  if (drsc->gmem_p != nullptr || drsc->buf_entry >= 0) return 2;  // memory present already
+  drsc->dev_id = dev_id;
+  drsc->gmem_p = mem_p;
+  drsc->buf_entry = buf_entry;
+  drsc->mem_attached = 1;
+  return 0;
+}
+
+int tensDevRsc_detach_mem(talsh_dev_rsc_t *drsc) {
+  if (drsc == nullptr) return -1;
+  if (drsc->dev_id < 0 || drsc->dev_id >= DEV_MAX) return -2;
+  if (drsc->gmem_p == nullptr || drsc->mem_attached == 0) return 1;  // nothing attached
+  return tensDevRsc_clean(drsc);  // the memory itself is the caller's
+}
+
+int tensDevRsc_allocate_mem(talsh_dev_rsc_t *drsc, int dev_id, size_t mem_size, int in_arg_buf) {
+  (void)in_arg_buf;
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (drsc == nullptr) return -1;
+  if (dev_id < 0 || dev_id >= DEV_MAX) return -2;
+  if (mem_size == 0) return -3;
+  int kind = DEV_NULL;
+  const int num = decode_device_id(dev_id, &kind);
+  if (num < 0) return -4;
+  if (drsc->dev_id >= 0 && drsc->dev_id != dev_id) return 1;
+  if (drsc->gmem_p != nullptr || drsc->buf_entry >= 0) return 2;
+  void *p = nullptr;
+  if (kind == DEV_HOST) {
+    p = host_alloc(mem_size, any_gpu_in_use());
+    if (p == nullptr) return 3;
+  } else if (kind == DEV_NVIDIA_GPU) {
+    if (!R.on || num >= MAX_GPUS_PER_NODE || !R.gpu[num].in_use) return 5;
+    const int rc = dev_alloc(num, mem_size, &p);
+    if (rc != TALSH_SUCCESS) return rc;  // TRY_LATER: over the budget, not an error
+  } else {
+    return kind == DEV_INTEL_MIC ? -6 : kind == DEV_AMD_GPU ? -7 : -8;
+  }
+  drsc->dev_id = dev_id;
+  drsc->gmem_p = p;
+  drsc->buf_entry = -1;
+  drsc->mem_attached = 0;
+  return 0;
+}
+
+int tensDevRsc_free_mem(talsh_dev_rsc_t *drsc) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (drsc == nullptr) return -1;
+  if (drsc->dev_id < 0 || drsc->dev_id >= DEV_MAX) return -2;
+  if (drsc->gmem_p == nullptr) return -3;
+  int kind = DEV_NULL;
+  if (decode_device_id(drsc->dev_id, &kind) < 0) return -4;
+  if (drsc->mem_attached != 0) return 1;  // attached, not allocated: detach it instead
+  const int rc = mem_free(drsc->gmem_p) == TALSH_SUCCESS ? 0 : NOT_CLEAN;
+  tensDevRsc_clean(drsc);
+  return rc;
+}
+
+int tensDevRsc_get_gmem_ptr(talsh_dev_rsc_t *drsc, void **gmem_p) {
+  if (drsc == nullptr || gmem_p == nullptr) return -1;
+  if (tensDevRsc_is_empty(drsc) == YEP) return 1;
+  *gmem_p = drsc->gmem_p;
+  return 0;
+}
+
+int tensDevRsc_release_all(talsh_dev_rsc_t *drsc) {
+  if (drsc == nullptr) return -1;
+  int rc = 0;
+  if (drsc->dev_id >= 0 && drsc->dev_id < DEV_MAX && drsc->gmem_p != nullptr) {
+    const int e = drsc->mem_attached ? tensDevRsc_detach_mem(drsc) : tensDevRsc_free_mem(drsc);
+    if (e != 0) rc = NOT_CLEAN;
+  }
+  tensDevRsc_clean(drsc);
+  return rc;
+}
+
+int tensDevRsc_destroy(talsh_dev_rsc_t *drsc) {
+  if (drsc == nullptr) return -1;
+  const int rc = tensDevRsc_release_all(drsc) != 0 ? NOT_CLEAN : 0;
+  std::free(drsc);
+  return rc;
+}
+
 int tensShape_create(talsh_tens_shape_t **tshape) {
   if (tshape == nullptr) return TALSH_INVALID_ARGS;
   *tshape = (talsh_tens_shape_t *)std::malloc(sizeof(talsh_tens_shape_t));

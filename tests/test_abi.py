@@ -623,3 +623,41 @@ def test_fortran_module_imports_are_exported(built):
     L = T.lib()
     missing = sorted(n for n in imports if not hasattr(L, n))
     assert not missing, missing
+
+
+def test_device_resource_api_without_gpu(built):
+    """The device-resource descriptor API (reference tensor_algebra_gpu.cpp:278-555)
+    on the Host, with the reference's return codes: attach / compare / clone /
+    detach of caller memory, allocate / free of library memory, refusals."""
+    L = T.lib()
+    pp = C.POINTER(T.DevRsc)()
+    assert L.tensDevRsc_create(C.byref(pp)) == 0
+    d = pp
+    assert L.tensDevRsc_is_empty(d) == T.YEP and L.tensDevRsc_device_id(d) == T.DEV_NULL
+    buf = (C.c_double * 64)()
+    addr = C.cast(buf, C.c_void_p).value
+    assert L.tensDevRsc_attach_mem(d, -1, addr, -1) == -2
+    assert L.tensDevRsc_attach_mem(d, 0, None, -1) == -3
+    assert L.tensDevRsc_attach_mem(d, 0, addr, -1) == 0
+    assert L.tensDevRsc_is_empty(d) == T.NOPE and L.tensDevRsc_device_id(d) == 0
+    assert L.tensDevRsc_attach_mem(d, 0, addr, -1) == 2      # memory present already
+    assert L.tensDevRsc_attach_mem(d, 1, addr, -1) == 1      # bound to another device
+    g = C.c_void_p()
+    assert L.tensDevRsc_get_gmem_ptr(d, C.byref(g)) == 0 and g.value == addr
+    other = T.DevRsc()
+    assert L.tensDevRsc_clean(C.byref(other)) == 0 and L.tensDevRsc_same(d, C.byref(other)) == T.NOPE
+    assert L.tensDevRsc_clone(d, C.byref(other)) == 0 and L.tensDevRsc_same(d, C.byref(other)) == T.YEP
+    assert L.tensDevRsc_free_mem(d) == 1                     # attached, not allocated
+    assert L.tensDevRsc_detach_mem(d) == 0 and L.tensDevRsc_is_empty(d) == T.YEP
+    assert L.tensDevRsc_detach_mem(d) == -2
+    assert L.tensDevRsc_get_gmem_ptr(d, C.byref(g)) == 1
+    assert L.tensDevRsc_allocate_mem(d, 0, 0, T.NOPE) == -3
+    assert L.tensDevRsc_allocate_mem(d, 0, 4096, T.NOPE) == 0
+    assert L.tensDevRsc_get_gmem_ptr(d, C.byref(g)) == 0 and g.value
+    C.memset(g.value, 0, 4096)                                # the Host block is usable
+    assert L.tensDevRsc_allocate_mem(d, 0, 4096, T.NOPE) == 2
+    assert L.tensDevRsc_free_mem(d) == 0 and L.tensDevRsc_is_empty(d) == T.YEP
+    assert L.tensDevRsc_allocate_mem(d, 1, 4096, T.NOPE) == 5  # GPU 0 not in use: no runtime here
+    assert L.tensDevRsc_allocate_mem(d, 0, 4096, T.YEP) == 0
+    assert L.tensDevRsc_release_all(d) == 0 and L.tensDevRsc_is_empty(d) == T.YEP
+    assert L.tensDevRsc_destroy(d) == 0
