@@ -255,6 +255,24 @@ int tensShape_destruct(talsh_tens_shape_t *tshape);
 int tensShape_destroy(talsh_tens_shape_t *tshape);
 size_t tensShape_volume(const talsh_tens_shape_t *tshape);
 int tensShape_rank(const talsh_tens_shape_t *tshape);
+/* New extents of the same volume: 0, or -2 when the volume changed (the new
+ * shape stays), -3 / -4 for a shape without extents / extents for rank 0. */
+int tensShape_reshape(talsh_tens_shape_t *tshape, int rank, const int *dims TALSH_DEFAULT(NULL),
+                      const int *divs TALSH_DEFAULT(NULL), const int *grps TALSH_DEFAULT(NULL));
+/* Prints the extents as "[d1,d2,...]". */
+void tensShape_print(const talsh_tens_shape_t *tshape);
+/* Tensor signatures (reference tensor_algebra.h:298-304). */
+int tensSignature_create(talsh_tens_signature_t **tsigna);
+int tensSignature_clean(talsh_tens_signature_t *tsigna);
+int tensSignature_construct(talsh_tens_signature_t *tsigna, int rank, const size_t *offsets TALSH_DEFAULT(NULL));
+int tensSignature_destruct(talsh_tens_signature_t *tsigna);
+int tensSignature_destroy(talsh_tens_signature_t *tsigna);
+/* A C pointer as an integer, for Fortran callers. */
+size_t fortran_cptr_int(void *cptr);
+/* Column-major element offset <-> zero-based multi-index (reference
+ * tensor_algebra.h:274-275). */
+size_t tens_elem_offset_f(unsigned int num_dim, const unsigned int *dims, const unsigned int *mlndx);
+void tens_elem_mlndx_f(size_t offset, unsigned int num_dim, const unsigned int *dims, unsigned int *mlndx);
 /* Device resource helpers. */
 int tensDevRsc_clean(talsh_dev_rsc_t *drsc);
 int tensDevRsc_is_empty(talsh_dev_rsc_t *drsc);

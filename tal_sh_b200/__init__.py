@@ -190,6 +190,21 @@ _PROTOS = {
     "tensDevRsc_device_id": (_I, [_P(DevRsc)]),
     "tensDevRsc_release_all": (_I, [_P(DevRsc)]),
     "tensDevRsc_destroy": (_I, [_P(DevRsc)]),
+    "tensShape_create": (_I, [_P(_V)]),
+    "tensShape_construct": (_I, [_V, _I, _I, _P(_I), _P(_I), _P(_I)]),
+    "tensShape_volume": (_Z, [_V]),
+    "tensShape_rank": (_I, [_V]),
+    "tensShape_destroy": (_I, [_V]),
+    "tensShape_reshape": (_I, [_V, _I, _P(_I), _P(_I), _P(_I)]),
+    "tensShape_print": (None, [_V]),
+    "tensSignature_create": (_I, [_P(_V)]),
+    "tensSignature_clean": (_I, [_V]),
+    "tensSignature_construct": (_I, [_V, _I, _P(_Z)]),
+    "tensSignature_destruct": (_I, [_V]),
+    "tensSignature_destroy": (_I, [_V]),
+    "tens_elem_offset_f": (_Z, [C.c_uint, _P(C.c_uint), _P(C.c_uint)]),
+    "fortran_cptr_int": (_Z, [_V]),
+    "tens_elem_mlndx_f": (None, [_Z, C.c_uint, _P(C.c_uint), _P(C.c_uint)]),
     "get_contr_permutations": (None, [_I, _I, _I, _I, _P(_I), _I, _P(_I), _P(_I), _P(_I),
                                       _P(_I), _P(_I), _P(_I), _P(_I)]),
     "get_contraction_permutations": (None, [_I, _I, _I, _I, _P(_I), _I, _P(_I), _P(_I), _P(_I),

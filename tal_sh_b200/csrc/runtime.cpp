@@ -1033,6 +1033,92 @@ size_t tensShape_volume(const talsh_tens_shape_t *s) {
 }
 int tensShape_rank(const talsh_tens_shape_t *s) { return s ? s->num_dim : -1; }
 
+// New extents of the same volume (reference tensor_algebra_gpu.cpp): -2 when the
+// volume changed (the new shape stays), -3 for a ranked shape without extents,
+// -4 for extents given to a rank-0 or empty shape.
+int tensShape_reshape(talsh_tens_shape_t *tshape, int rank, const int *dims, const int *divs, const int *grps) {
+  if (tshape == nullptr) return -1;
+  if (tensShape_rank(tshape) <= 0) return (dims != nullptr || divs != nullptr || grps != nullptr) ? -4 : 0;
+  if (tshape->dims == nullptr) return -3;
+  const size_t vol = tensShape_volume(tshape);
+  int rc = tensShape_destruct(tshape);
+  if (rc == 0) rc = tensShape_construct(tshape, NOPE, rank, dims, divs, grps);
+  if (rc == 0 && tensShape_volume(tshape) != vol) rc = -2;
+  return rc;
+}
+
+// Prints the extents as "[d1,d2,...]" (reference tensShape_print).
+void tensShape_print(const talsh_tens_shape_t *tshape) {
+  if (tshape == nullptr) return;
+  std::printf("[");
+  for (int i = 0; i < tshape->num_dim; ++i) std::printf(i + 1 < tshape->num_dim ? "%d," : "%d", tshape->dims[i]);
+  std::printf("]");
+}
+
+// Tensor signatures: a rank and one offset per dimension (reference
+// tensor_algebra_gpu.cpp tensSignature_*), with its return codes.
+int tensSignature_create(talsh_tens_signature_t **tsigna) {
+  if (tsigna == nullptr) return -1;
+  *tsigna = (talsh_tens_signature_t *)std::malloc(sizeof(talsh_tens_signature_t));
+  if (*tsigna == nullptr) return TRY_LATER;
+  return tensSignature_clean(*tsigna);
+}
+
+int tensSignature_clean(talsh_tens_signature_t *tsigna) {
+  if (tsigna == nullptr) return -1;
+  tsigna->num_dim = -1;
+  tsigna->offsets = nullptr;
+  return 0;
+}
+
+int tensSignature_construct(talsh_tens_signature_t *tsigna, int rank, const size_t *offsets) {
+  if (tsigna == nullptr) return -1;
+  if (tsigna->num_dim >= 0) {
+    const int rc = tensSignature_destruct(tsigna);
+    if (rc != 0) return rc;
+  }
+  if (rank < 0) return -2;
+  if (rank > 0) {
+    if (offsets == nullptr) return -3;
+    tsigna->offsets = (size_t *)std::malloc(sizeof(size_t) * (size_t)rank);
+    if (tsigna->offsets == nullptr) return TRY_LATER;
+    std::memcpy(tsigna->offsets, offsets, sizeof(size_t) * (size_t)rank);
+  }
+  tsigna->num_dim = rank;
+  return 0;
+}
+
+int tensSignature_destruct(talsh_tens_signature_t *tsigna) {
+  if (tsigna == nullptr) return -1;
+  std::free(tsigna->offsets);
+  return tensSignature_clean(tsigna);
+}
+
+int tensSignature_destroy(talsh_tens_signature_t *tsigna) {
+  if (tsigna == nullptr) return -1;
+  const int rc = tensSignature_destruct(tsigna);
+  std::free(tsigna);
+  return rc;
+}
+
+// A C pointer as an integer, for Fortran callers (reference tensor_algebra.h:261).
+size_t fortran_cptr_int(void *cptr) { return (size_t)(uintptr_t)cptr; }
+
+// Column-major element offset <-> zero-based multi-index (reference
+// tensor_algebra_gpu.cpp:172-193; rank 0 is the single element at offset 0).
+size_t tens_elem_offset_f(unsigned int num_dim, const unsigned int *dims, const unsigned int *mlndx) {
+  size_t offset = 0;
+  for (unsigned int i = num_dim; i-- > 0;) offset = offset * dims[i] + mlndx[i];
+  return offset;
+}
+
+void tens_elem_mlndx_f(size_t offset, unsigned int num_dim, const unsigned int *dims, unsigned int *mlndx) {
+  for (unsigned int i = 0; i < num_dim; ++i) {
+    mlndx[i] = (unsigned int)(offset % dims[i]);
+    offset /= dims[i];
+  }
+}
+
 // ------------------------------------------------------------ control API
 int talshInit(size_t *host_buf_size, int *host_arg_max, int ngpus, int gpu_list[], int nmics,
               int mic_list[], int namds, int amd_list[]) {

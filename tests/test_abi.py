@@ -661,3 +661,59 @@ def test_device_resource_api_without_gpu(built):
     assert L.tensDevRsc_allocate_mem(d, 0, 4096, T.YEP) == 0
     assert L.tensDevRsc_release_all(d) == 0 and L.tensDevRsc_is_empty(d) == T.YEP
     assert L.tensDevRsc_destroy(d) == 0
+
+
+def test_shape_signature_and_offset_helpers(built, capfd):
+    """tensShape_reshape / _print, the tensor-signature API and the column-major
+    offset <-> multi-index helpers of the reference's tensor_algebra.h."""
+    L = T.lib()
+    sh = C.c_void_p()
+    assert L.tensShape_create(C.byref(sh)) == 0
+    assert L.tensShape_construct(sh, T.NOPE, 3, T.ivec([4, 6, 5]), None, None) == 0
+    assert L.tensShape_reshape(sh, 2, T.ivec([12, 10]), None, None) == 0
+    assert (L.tensShape_rank(sh), L.tensShape_volume(sh)) == (2, 120)
+    assert L.tensShape_reshape(sh, 2, T.ivec([12, 11]), None, None) == -2   # volume changed: flagged
+    assert L.tensShape_volume(sh) == 132
+    L.tensShape_print(sh)
+    C.CDLL(None).fflush(None)
+    assert capfd.readouterr().out.endswith("[12,11]")
+    assert L.tensShape_destroy(sh) == 0
+    sg = C.c_void_p()
+    assert L.tensSignature_create(C.byref(sg)) == 0
+    offs = (C.c_size_t * 3)(7, 0, 3)
+    assert L.tensSignature_construct(sg, 3, offs) == 0
+    rank = C.cast(sg, C.POINTER(C.c_int))[0]
+    assert rank == 3
+    assert L.tensSignature_construct(sg, 2, None) == -3
+    assert L.tensSignature_construct(sg, 0, None) == 0
+    assert L.tensSignature_construct(sg, -1, None) == -2
+    assert L.tensSignature_destroy(sg) == 0
+    rng = np.random.default_rng(5)
+    for _ in range(200):
+        dims = [int(x) for x in rng.integers(1, 9, size=int(rng.integers(0, 6)))]
+        idx = [int(rng.integers(0, d)) for d in dims]
+        off = L.tens_elem_offset_f(len(dims), (C.c_uint * max(1, len(dims)))(*dims),
+                                   (C.c_uint * max(1, len(dims)))(*idx))
+        assert off == (int(np.ravel_multi_index(idx, dims, order="F")) if dims else 0)
+        back = (C.c_uint * max(1, len(dims)))()
+        L.tens_elem_mlndx_f(off, len(dims), (C.c_uint * max(1, len(dims)))(*dims), back)
+        assert list(back[:len(dims)]) == idx
+
+
+def test_every_reference_header_function_is_exported(built):
+    """Every function the reference's talsh.h and tensor_algebra.h declare is
+    exported by libtalsh.so, except get_contr_pattern_cutensor (cuTENSOR builds
+    only; this core does not use cuTENSOR).  Skipped where the reference sources
+    are absent."""
+    ref = _reference_tree()
+    if ref is None:
+        pytest.skip("reference sources not present")
+    L = T.lib()
+    names = set()
+    for h in ("talsh.h", "tensor_algebra.h"):
+        names |= declared_functions(os.path.join(ref, h))
+    assert len(names) > 150
+    missing = sorted(n for n in names - {"get_contr_pattern_cutensor"} if not hasattr(L, n))
+    assert not missing, missing
+    buf = (C.c_char * 8)()
+    assert L.fortran_cptr_int(C.cast(buf, C.c_void_p)) == C.cast(buf, C.c_void_p).value
