@@ -17,9 +17,9 @@
  *    completed by talshTaskComplete / talshTaskWait.
  *  - Scheduling is single-threaded: one host thread issues TAL-SH calls.
  *  - Entry points of the reference that this core does not provide (SVD,
- *    orthogonalization, tensor-operation objects, slice descriptor objects)
- *    return TALSH_NOT_IMPLEMENTED; talshTensorSlice / talshTensorInsert run on
- *    the GPU.
+ *    orthogonalization, tensor-operation objects) return
+ *    TALSH_NOT_IMPLEMENTED; talshTensorSlice / talshTensorInsert run on the
+ *    GPU, and slice descriptor objects are host-side views.
  */
 #ifndef TALSH_B200_TALSH_H_
 #define TALSH_B200_TALSH_H_
@@ -240,8 +240,10 @@ void talshTensorPrint(const talsh_tens_t *tens_block);
 void talshTensorPrintInfo(const talsh_tens_t *tens_block);
 void talshTensorPrintBody(const talsh_tens_t *tens_block, double thresh);
 
-/* Tensor slice descriptor objects (not provided by this core: TALSH_NOT_IMPLEMENTED;
- * talshTensorSlice and talshTensorInsert themselves are provided) */
+/* Tensor slice descriptor objects: a non-owning pointer to a tensor, the base
+ * offsets of a window inside it and the window's extents (reference
+ * talshc.cpp:1857-1932; host-side only).  Construct refuses a window that leaves
+ * the tensor (TALSH_INVALID_ARGS) and releases a previous window's extents. */
 int talshTensorSliceCreate(talsh_tens_slice_t **slice);
 int talshTensorSliceClean(talsh_tens_slice_t *slice);
 int talshTensorSliceConstruct(talsh_tens_slice_t *slice, const talsh_tens_t *tensor,

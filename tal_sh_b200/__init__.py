@@ -204,6 +204,12 @@ _PROTOS = {
     "tensSignature_destroy": (_I, [_V]),
     "tens_elem_offset_f": (_Z, [C.c_uint, _P(C.c_uint), _P(C.c_uint)]),
     "fortran_cptr_int": (_Z, [_V]),
+    "talshTensorSliceCreate": (_I, [_P(_V)]),
+    "talshTensorSliceClean": (_I, [_V]),
+    "talshTensorSliceConstruct": (_I, [_V, _P(Tens), _P(_Z), _P(_I), _P(_I), _P(_I)]),
+    "talshTensorSliceVolume": (_Z, [_V]),
+    "talshTensorSliceDestruct": (_I, [_V]),
+    "talshTensorSliceDestroy": (_I, [_V]),
     "tens_elem_mlndx_f": (None, [_Z, C.c_uint, _P(C.c_uint), _P(C.c_uint)]),
     "get_contr_permutations": (None, [_I, _I, _I, _I, _P(_I), _I, _P(_I), _P(_I), _P(_I),
                                       _P(_I), _P(_I), _P(_I), _P(_I)]),

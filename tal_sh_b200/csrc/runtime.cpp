@@ -1648,14 +1648,62 @@ void talshTensorPrintBody(const talsh_tens_t *t, double thresh) {
 }
 
 // ------------------------------------------------------------- slices
-int talshTensorSliceCreate(talsh_tens_slice_t **) { return TALSH_NOT_IMPLEMENTED; }
-int talshTensorSliceClean(talsh_tens_slice_t *) { return TALSH_NOT_IMPLEMENTED; }
-int talshTensorSliceConstruct(talsh_tens_slice_t *, const talsh_tens_t *, const size_t *, const int *, const int *, const int *) {
-  return TALSH_NOT_IMPLEMENTED;
+// Slice views: a non-owning pointer to a tensor, the base offsets of the slice
+// inside it and the slice's extents (reference talshc.cpp:1857-1932), with the
+// reference's return codes.  Constructing an already constructed view releases
+// its previous extents first.
+int talshTensorSliceCreate(talsh_tens_slice_t **slice) {
+  if (slice == nullptr) return TALSH_INVALID_ARGS;
+  *slice = (talsh_tens_slice_t *)std::malloc(sizeof(talsh_tens_slice_t));
+  if (*slice == nullptr) return TRY_LATER;
+  return talshTensorSliceClean(*slice);
 }
-size_t talshTensorSliceVolume(const talsh_tens_slice_t *) { return 0; }
-int talshTensorSliceDestruct(talsh_tens_slice_t *) { return TALSH_NOT_IMPLEMENTED; }
-int talshTensorSliceDestroy(talsh_tens_slice_t *) { return TALSH_NOT_IMPLEMENTED; }
+
+int talshTensorSliceClean(talsh_tens_slice_t *slice) {
+  if (slice == nullptr) return TALSH_INVALID_ARGS;
+  slice->tensor = nullptr;
+  int rc = tensSignature_clean(&slice->bases);
+  if (rc == 0) rc = tensShape_clean(&slice->shape);
+  return rc;
+}
+
+int talshTensorSliceConstruct(talsh_tens_slice_t *slice, const talsh_tens_t *tensor, const size_t *offsets,
+                              const int *dims, const int *divs, const int *grps) {
+  if (slice == nullptr || tensor == nullptr) return TALSH_INVALID_ARGS;
+  int rank = -1;
+  const int *ext = talshTensorDimExtents(tensor, &rank);
+  if (rank < 0 || (rank > 0 && (offsets == nullptr || dims == nullptr || ext == nullptr))) return TALSH_INVALID_ARGS;
+  for (int i = 0; i < rank; ++i)
+    if (dims[i] <= 0 || offsets[i] + (size_t)dims[i] > (size_t)ext[i]) return TALSH_INVALID_ARGS;
+  if (slice->shape.num_dim >= 0) tensShape_destruct(&slice->shape);
+  int rc = tensSignature_construct(&slice->bases, rank, offsets);
+  if (rc == 0) rc = tensShape_construct(&slice->shape, NOPE, rank, dims, divs, grps);
+  if (rc != 0) {
+    talshTensorSliceDestruct(slice);
+    return rc;
+  }
+  slice->tensor = const_cast<talsh_tens_t *>(tensor);
+  return TALSH_SUCCESS;
+}
+
+size_t talshTensorSliceVolume(const talsh_tens_slice_t *slice) {
+  return slice != nullptr ? tensShape_volume(&slice->shape) : 0;
+}
+
+int talshTensorSliceDestruct(talsh_tens_slice_t *slice) {
+  if (slice == nullptr) return TALSH_INVALID_ARGS;
+  int rc = tensShape_destruct(&slice->shape);
+  if (rc == 0) rc = tensSignature_destruct(&slice->bases);
+  const int rc2 = talshTensorSliceClean(slice);
+  return rc != 0 ? rc : rc2;
+}
+
+int talshTensorSliceDestroy(talsh_tens_slice_t *slice) {
+  if (slice == nullptr) return TALSH_INVALID_ARGS;
+  const int rc = talshTensorSliceDestruct(slice);
+  std::free(slice);
+  return rc;
+}
 
 // ------------------------------------------------------------- tasks
 int talshTaskCreate(talsh_task_t **task) {

@@ -717,3 +717,37 @@ def test_every_reference_header_function_is_exported(built):
     assert not missing, missing
     buf = (C.c_char * 8)()
     assert L.fortran_cptr_int(C.cast(buf, C.c_void_p)) == C.cast(buf, C.c_void_p).value
+
+
+def test_slice_views_without_gpu(built):
+    """Slice descriptor objects (talshTensorSliceCreate / Construct / Volume /
+    Destruct / Destroy, reference talshc.cpp:1857-1932): a view of a window of a
+    tensor, refused when the window leaves the tensor, reconstructible, also for a
+    rank-0 tensor."""
+    L = T.lib()
+    hb, ha = C.c_size_t(0), C.c_int(0)
+    assert L.talshInit(C.byref(hb), C.byref(ha), 0, None, 0, None, 0, None) == 0
+    try:
+        t = T.Tensor([6, 5, 4], T.R8, dev_id=0, init=0.0)
+        sv = C.c_void_p()
+        assert L.talshTensorSliceCreate(C.byref(sv)) == 0 and L.talshTensorSliceVolume(sv) == 0
+        offs = (C.c_size_t * 3)(1, 0, 2)
+        assert L.talshTensorSliceConstruct(sv, t.ref, offs, T.ivec([5, 5, 2]), None, None) == 0
+        assert L.talshTensorSliceVolume(sv) == 50
+        assert L.talshTensorSliceConstruct(sv, t.ref, offs, T.ivec([2, 2, 2]), None, None) == 0
+        assert L.talshTensorSliceVolume(sv) == 8
+        assert L.talshTensorSliceConstruct(sv, t.ref, (C.c_size_t * 3)(2, 0, 0), T.ivec([5, 5, 4]), None,
+                                           None) == T.TALSH_INVALID_ARGS
+        assert L.talshTensorSliceConstruct(sv, t.ref, offs, T.ivec([2, 0, 2]), None, None) == T.TALSH_INVALID_ARGS
+        assert L.talshTensorSliceVolume(sv) == 8                  # a refused construct leaves the view as it was
+        assert L.talshTensorSliceDestruct(sv) == 0 and L.talshTensorSliceVolume(sv) == 0
+        s0 = T.Tensor([], T.R8, dev_id=0, init=1.0)
+        for _ in range(2):
+            assert L.talshTensorSliceConstruct(sv, s0.ref, None, None, None, None) == 0
+            assert L.talshTensorSliceVolume(sv) == 1
+        assert L.talshTensorSliceDestroy(sv) == 0
+        assert L.talshTensorSliceDestroy(None) == T.TALSH_INVALID_ARGS
+        for x in (t, s0):
+            assert x.destruct() == 0
+    finally:
+        assert L.talshShutdown() == 0
