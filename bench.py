@@ -170,54 +170,93 @@ def profile_traffic_ratio():
 
 
 # ----------------------------------------------------------------- CPU side
-def cpu_sample_cases(cases, budget_elems=1 << 25):
-    """A bounded sample of the sweep for the host cores: every 4th case, volume capped."""
-    out = []
-    for i, (kind, dims, o2n) in enumerate(cases):
-        if i % 4:
-            continue
-        dims = list(dims)
-        while np.prod(dims, dtype=np.int64) > budget_elems:
-            dims[int(np.argmax(dims))] //= 2
-        out.append((kind, dims, o2n))
+def sweep_slice(ncases, k, j):
+    """Case indices of slice j when the sweep is cut into k interleaved slices
+    (case i belongs to slice i mod k): k consecutive slices cover every case once."""
+    return [i for i in range(ncases) if i % k == j % k]
+
+
+class CpuSweep:
+    """The reference's CPU transpose and add, restated in the oracle, on all host
+    cores at the sweep's full sizes: the copy is the cache-blocked OpenMP transpose
+    (tensor_block_copy_dlf, tensor_algebra_cpu.F90:7699-7940); the add permutes L
+    into a temporary block with it and then adds in one OpenMP loop, as
+    cpu_tensor_block_add does (talshf.F90:1857-1904).  Wall-clock time per call."""
+
+    def __init__(self, cases, nthreads=None):
+        import oracle as O
+        self.lib = O.lib()
+        self.cases = cases
+        self.nt = nthreads or os.cpu_count() or 1
+        vmax = max(int(np.prod(d, dtype=np.int64)) for _, d, _ in cases)
+        rng = np.random.default_rng(0)
+        self.src = {R4: rng.random(vmax, dtype=np.float32) * 2 - 1, R8: rng.random(vmax) * 2 - 1}
+        self.dst = {R4: np.zeros(vmax, dtype=np.float32), R8: np.zeros(vmax)}  # touched outside timing
+
+    def run(self, idx):
+        """Copy then add for each case index; returns (algorithmic bytes, seconds)."""
+        iv = lambda s: (C.c_int * len(s))(*s)
+        nbytes = secs = 0.0
+        for i in idx:
+            kind, dims, o2n = self.cases[i]
+            vol = int(np.prod(dims, dtype=np.int64))
+            a, d = self.src[kind][:vol], self.dst[kind][:vol]
+            pa, pd = C.c_void_p(a.ctypes.data), C.c_void_p(d.ctypes.data)
+            t0 = time.perf_counter()
+            rc = self.lib.orc_permute_blocked(kind, len(dims), iv(dims), iv(o2n), pa, pd, self.nt)
+            t1 = time.perf_counter()
+            sr = ALPHAS[i % len(ALPHAS)][0]
+            rc |= self.lib.orc_tensor_add_blocked(kind, len(dims), iv(dims), iv(o2n), pa, pd, sr, 0.0, self.nt)
+            t2 = time.perf_counter()
+            if rc:
+                raise RuntimeError("oracle transpose/add failed for case %d" % i)
+            nbytes += 5.0 * vol * ESIZE[kind]
+            secs += t2 - t0
+        return nbytes, secs
+
+
+def cpu_contract_rates(names=("C1", "C3b"), nthreads=None):
+    """The reference's CPU contraction on the host cores for C1 and C3b: TTGT with
+    the CPU matricization, the cache-blocked transpose and one DGEMM from the BLAS
+    scipy links (OpenBLAS), restated in oracle.contract_ttgt_blas.  Seeded normal
+    operands scaled by 1/sqrt(contracted volume); TFLOP/s by wall clock."""
+    import oracle as O
+    out = {}
+    for name in names:
+        if name == "C1":
+            pat, dd, ld, rd, reps = C1_PATTERN, [32] * 4, [32] * 4, [32] * 4, 5
+        else:
+            dd, ld, rd = c3_dims(name, 192, 64)
+            pat, reps = C3_PATTERNS[name], 1
+        e, dig, _, _, _, _ = O.str2dig(pat)
+        rng = np.random.default_rng(11)
+        kvol = np.sqrt(float(np.prod(ld)) * float(np.prod(rd)) / float(np.prod(dd)))
+        Lh = np.asfortranarray(rng.standard_normal(ld) / np.sqrt(kvol))
+        Rh = np.asfortranarray(rng.standard_normal(rd) / np.sqrt(kvol))
+        Dh = np.zeros(dd, order="F")
+        O.contract_ttgt_blas(Dh, Lh, Rh, dig, nthreads=nthreads)  # warm-up (BLAS threads, pages)
+        ts = [O.contract_ttgt_blas(Dh, Lh, Rh, dig, nthreads=nthreads) for _ in range(reps)]
+        flop = 2.0 * float(np.prod(dd)) * kvol
+        out[name] = {"tflops": flop / statistics.median(ts) / 1e12, "s": statistics.median(ts)}
+        del Lh, Rh, Dh
     return out
 
 
-def run_cpu_baseline(cases, seconds_budget=20.0):
-    import oracle as O
-    O.lib()
-    threads = os.cpu_count() or 1
-    sample = cpu_sample_cases(cases)
-    total_bytes, total_time = 0.0, 0.0
-    rng = np.random.default_rng(0)
-    cap = max(int(np.prod(d, dtype=np.int64)) for _, d, _ in sample)
-    # inputs uniform in [-1,1] and outputs allocated and touched once, outside the timing
-    srcs = {R4: rng.uniform(-1.0, 1.0, cap).astype(np.float32), R8: rng.uniform(-1.0, 1.0, cap)}
-    dsts = {R4: np.zeros(cap, dtype=np.float32), R8: np.zeros(cap, dtype=np.float64)}
-    t_start = time.time()
-    n_done = 0
-    # cycle over the sample until about seconds_budget of transpose time is measured
-    order = [sample[j % len(sample)] for j in range(40 * len(sample))]
-    for i, (kind, dims, o2n) in enumerate(order):
-        vol = int(np.prod(dims, dtype=np.int64))
-        a = srcs[kind][:vol]
-        out = dsts[kind][:vol]
-        L = O.lib()
-        iv = lambda s: (C.c_int * max(1, len(s)))(*s)
-        t0 = time.perf_counter()
-        L.orc_permute_blocked(kind, len(dims), iv(dims), iv(o2n), C.c_void_p(a.ctypes.data),
-                              C.c_void_p(out.ctypes.data), threads)
-        dt_s = time.perf_counter() - t0
-        total_bytes += 2.0 * vol * ESIZE[kind]
-        total_time += dt_s
-        n_done += 1
-        if total_time > seconds_budget or time.time() - t_start > 3 * seconds_budget:
-            break
-    gbs = total_bytes / total_time / 1e9 if total_time > 0 else 0.0
-    return {"value": gbs, "unit": "GB/s", "cores": threads, "kind": "port",
-            "sample": "%d transposes cycling over every 4th of the %d sweep cases (volume capped at 2^25 elements), "
-                      "cache-blocked OpenMP transpose restating tensor_block_copy_dlf_r8, %.1f GB moved in %.2f s"
-                      % (n_done, len(cases), total_bytes / 1e9, total_time)}, total_time
+def run_cpu_baseline(cases, slices=4):
+    """cpu_baseline of the GPU line: one of `slices` interleaved slices of the sweep at
+    full size (copies and adds), plus the C1 and C3b contractions."""
+    cs = CpuSweep(cases)
+    idx = sweep_slice(len(cases), slices, 0)
+    cs.run(idx[:2])  # warm-up: OpenMP threads, first pages
+    nbytes, secs = cs.run(idx)
+    del cs
+    con = cpu_contract_rates()
+    return {"value": nbytes / secs / 1e9, "unit": "GB/s", "cores": os.cpu_count() or 1, "kind": "port",
+            "sample": "%d of the %d sweep cases at full size (every %dth), each a transpose and a "
+                      "transpose-add: the oracle's cache-blocked OpenMP transpose and blocked add restating "
+                      "the reference CPU path, %.1f GB in %.2f s" % (len(idx), len(cases), slices, nbytes / 1e9, secs),
+            "contract_tflops": {k: round(v["tflops"], 4) for k, v in con.items()},
+            "contract_path": "TTGT: blocked transposes + OpenBLAS DGEMM (scipy) on all cores"}
 
 
 # ----------------------------------------------------------------- GPU side
@@ -255,6 +294,7 @@ def profile_case(spec, op):
                           "gbs": moved / (e0.elapsed_time(e1) * 1e-3) / 1e9}))
 
 
+C1_PATTERN = "D(a,b,i,j)+=L(a,k,c,i)*R(c,b,k,j)"
 C3_PATTERNS = {"C3a": "D(a,b,i,j)+=L(a,b,c,d)*R(c,d,i,j)", "C3b": "D(a,b,i,j)+=L(a,k,c,i)*R(c,b,k,j)"}
 
 
@@ -319,6 +359,96 @@ def whole_job_rate(units_per_rank, world, slowest_seconds):
     return units_per_rank * world / slowest_seconds
 
 
+def sig(x, n=3):
+    """Rounds a number to n significant digits for the compact summary."""
+    if x is None or not isinstance(x, (int, float)) or x != x:
+        return x
+    if x == 0:
+        return 0.0
+    return float("%.*g" % (n, x))
+
+
+def contract_summary(con):
+    """Compact per-config numbers (TFLOP/s, error, ratios, latencies) for the end of
+    the JSON line; the full detail goes to the detail file."""
+    if not con:
+        return None
+    out = {}
+    for name in ("C1", "C3a", "C3b"):
+        p, q = con.get(name), con.get(name + "_split6")
+        if isinstance(p, dict) and "tflops" in p:
+            e = {"plain_tflops": sig(p["tflops"]), "plain_err": sig(p["rel_err_vs_fp64"], 2)}
+            if isinstance(q, dict) and "tflops_fp64_equiv" in q:
+                e.update({"split_tflops": sig(q["tflops_fp64_equiv"]), "split_err": sig(q["rel_err_vs_fp64"], 2),
+                          "split_x": sig(q["speedup_vs_plain"])})
+            for form in ("bf16x3", "tf32x3", "fp8"):
+                f = con.get(name + "_" + form)
+                if isinstance(f, dict) and "tflops_fp64_equiv" in f:
+                    e[form] = [sig(f["tflops_fp64_equiv"]), sig(f["rel_err_vs_fp64"], 2)]
+            out[name] = e
+    cx = con.get("complex") or {}
+    if isinstance(cx.get("C3b_c8"), dict) and "tflops" in cx["C3b_c8"]:
+        e = {"plain_tflops": sig(cx["C3b_c8"]["tflops"]), "plain_err": sig(cx["C3b_c8"]["rel_err_vs_fp64"], 2)}
+        q = cx.get("C3b_c8_split6")
+        if isinstance(q, dict) and "tflops_fp64_equiv" in q:
+            e.update({"split_tflops": sig(q["tflops_fp64_equiv"]), "split_err": sig(q["rel_err_vs_fp64"], 2),
+                      "split_x": sig(q["speedup_vs_plain"])})
+        out["C3b_c8"] = e
+    if isinstance(con.get("fp64_peak"), dict):
+        out["dgemm_tflops"] = sig(con["fp64_peak"].get("tflops"))
+    b = con.get("C4_batch") or {}
+    if "batched_tuned" in b or "batched" in b:
+        bt = b.get("batched_tuned") or b.get("batched")
+        out["C4"] = {"ms": sig(bt.get("ms")), "tasks_per_s": sig(bt.get("tasks_per_s")),
+                     "tflops": sig(bt.get("tflops")), "x_per_task": sig(b.get("speedup_tuned", b.get("speedup")))}
+    sv = con.get("C5_serve") or {}
+    c5 = {}
+    for k, v in sv.items():
+        if k.startswith("rate_") and isinstance(v, dict) and "p50_ms" in v:
+            c5[k[5:]] = {"tps": sig(v.get("tasks_per_s")), "small_p50": sig(v.get("small_p50_ms"), 2),
+                         "small_p99": sig(v.get("small_p99_ms"), 2), "cc_p50": sig(v.get("cc_p50_ms"), 2),
+                         "cc_p99": sig(v.get("cc_p99_ms"), 2)}
+    if c5:
+        out["C5_ms"] = c5
+        mix = [v.get("alone_vs_mix", {}).get("bit_identical") for v in sv.values()
+               if isinstance(v, dict) and "alone_vs_mix" in v]
+        if mix:
+            out["C5_alone_vs_mix_identical"] = all(mix)
+    tb = con.get("transpose_batch") or {}
+    if "batched_graph" in tb:
+        out["tr_batch"] = {"ms": sig(tb["batched_graph"]["ms"]), "x": sig(tb.get("speedup"))}
+    errs = {k: v["error"] for k, v in con.items() if isinstance(v, dict) and "error" in v}
+    if errs:
+        out["errors"] = {k: str(v)[:80] for k, v in errs.items()}
+    return out
+
+
+def bit_exact_cases(cases, n=32):
+    """n sweep cases spread over kinds and ranks 2-6 (every rank of each kind, then
+    evenly over the rest), for the full-size byte comparison after the timing."""
+    by = {}
+    for i, (kind, dims, o2n) in enumerate(cases):
+        by.setdefault((kind, len(dims)), []).append(i)
+    keys = sorted(by)
+    per = max(1, n // len(keys))
+    pick = []
+    for k in keys:
+        lst = by[k]
+        pick += [lst[int(j * len(lst) / per)] for j in range(min(per, len(lst)))]
+    rest = [i for i in range(len(cases)) if i not in set(pick)]
+    while len(pick) < n and rest:
+        pick.append(rest.pop(len(rest) // 2))
+    return sorted(pick[:n])
+
+
+def write_detail(obj, path):
+    try:
+        with open(path, "w") as f:
+            json.dump(obj, f)
+    except OSError as exc:
+        print("detail file not written: %s" % exc, file=sys.stderr)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -328,6 +458,10 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--no-contract", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--check-cases", type=int, default=32,
+                    help="full-size sweep cases byte-compared with the oracle after the timing (0: none)")
+    ap.add_argument("--detail", default=None,
+                    help="file for the full results (default: gpurun_out/bench_detail.json when that folder exists)")
     ap.add_argument("--profile-case", default=None,
                     help="KIND:d1,d2,..:p1,p2,.. -- run one transpose four times (for ncu) and exit")
     ap.add_argument("--profile-op", default="copy", choices=["copy", "add"])
@@ -346,6 +480,10 @@ def main():
     if args.profile_batch:
         profile_batch()
         return
+    detail_path = args.detail
+    if detail_path is None and os.path.isdir(os.path.join(ROOT, "gpurun_out")):
+        detail_path = os.path.join(ROOT, "gpurun_out", "bench_detail%s.json" % ("_ref" if args.impl == "reference"
+                                                                                 else ""))
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -357,20 +495,35 @@ def main():
               "parallelism": "replicas" if world > 1 else "single GPU"}
 
     if args.impl == "reference":
+        # The reference's CPU path on all host cores.  Step j runs slice j of the
+        # sweep cut into K interleaved slices (full-size cases, each a transpose and
+        # a transpose-add), so the K timed steps together run every case once.
         if rank != 0:
             return
-        for _ in range(args.warmup):
-            pass
-        vals = []
-        base = None
-        for _ in range(max(1, args.steps)):
-            base, _t = run_cpu_baseline(cases, seconds_budget=max(5.0, 60.0 / max(1, args.steps)))
-            vals.append(base["value"])
-        v = statistics.median(vals)
-        base["value"] = v
+        k = max(1, args.steps)
+        cs = CpuSweep(cases)
+        for w in range(args.warmup):  # untimed
+            cs.run(sweep_slice(len(cases), k, w)[:4])
+        tot_b = tot_s = 0.0
+        per_step = []
+        for j in range(k):
+            b, s_ = cs.run(sweep_slice(len(cases), k, j))
+            tot_b += b
+            tot_s += s_
+            per_step.append(s_)
+        del cs
+        v = tot_b / tot_s / 1e9
+        con = cpu_contract_rates()
+        base = {"value": v, "unit": "GB/s", "cores": os.cpu_count() or 1, "kind": "port",
+                "sample": "the whole sweep once: %d steps, step j = cases i with i mod %d == j, full size, each a "
+                          "transpose and a transpose-add (oracle's blocked OpenMP transpose and add restating the "
+                          "reference CPU path), %.1f GB in %.2f s" % (k, k, tot_b / 1e9, tot_s),
+                "contract_tflops": {n: sig(x["tflops"]) for n, x in con.items()},
+                "contract_path": "TTGT: blocked transposes + OpenBLAS DGEMM (scipy) on all cores"}
         line = {"metric": METRIC, "value": v, "unit": "GB/s", "n_gpus": args.gpus, "steps": args.steps,
-                "warmup": args.warmup, "higher_is_better": True, "impl": "reference", "dtype": "f32/f64",
-                "data": "synthetic", "config": config, "cpu_baseline": base, "vs_baseline": None,
+                "warmup": args.warmup, "ms_per_step": tot_s / k * 1e3, "higher_is_better": True,
+                "impl": "reference", "dtype": "f32/f64", "data": "synthetic", "config": config,
+                "cpu_baseline": base, "vs_baseline": None,
                 "e2e": {"value": v, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
         return
@@ -442,8 +595,14 @@ def main():
     add_t = sum(d for d, op in zip(durs, ops) if op[5])
     copy_b = sum(op[7] for op in ops if not op[5])
     add_b = sum(op[7] for op in ops if op[5])
+    r4_t = sum(d for d, op in zip(durs, ops) if op[0] == R4)
+    r4_b = sum(op[7] for op in ops if op[0] == R4)
+    r8_t = sum(d for d, op in zip(durs, ops) if op[0] == R8)
+    r8_b = sum(op[7] for op in ops if op[0] == R8)
     launch_avg_bytes = step_bytes / len(ops)
     launch_avg_s = sum(durs) / len(ops)
+    per_case = [{"i": i // 2, "op": "add" if op[5] else "copy", "kind": op[0], "dims": op[1], "o2n": op[2],
+                 "gbs": op[7] / d / 1e9} for i, (op, d) in enumerate(zip(ops, durs))]
 
     # CUDA graph of the whole sweep (falls back to eager launches).
     graph = None
@@ -483,23 +642,45 @@ def main():
     elapsed = slowest_rank(elapsed, world, dev)
     value = whole_job_rate(step_bytes * args.steps, world, elapsed) / 1e9
     ms_per_step = elapsed / args.steps * 1e3
+    del graph
 
-    # Bit-exact spot check of one case against numpy's transpose (a pure move:
-    # byte equality), small and outside timing.
+    # Full-size byte comparison with the oracle, outside the timing: for each
+    # checked case the GPU transpose, then the GPU transpose-add on top of it,
+    # against the oracle's blocked transpose and blocked add of the same bytes.
     check = None
-    if rank == 0:
-        kind, dims, o2n, src, dst, add, a, _ = ops[0]
-        vol = int(np.prod(dims))
-        nb = vol * ESIZE[kind]
-        dt = np.float32 if kind == R4 else np.float64
-        launch(ops[0])
-        torch.cuda.synchronize(dev)
-        lin = lbuf[(src - base_l):(src - base_l) + nb].cpu().numpy().view(dt).reshape(dims, order="F")
-        out = dbuf[(dst - base_d):(dst - base_d) + nb].cpu().numpy().view(dt)
-        n2o = [list(o2n).index(k + 1) for k in range(len(dims))]
-        check = bool(out.tobytes() == np.transpose(lin, n2o).tobytes(order="F"))
+    if rank == 0 and args.check_cases > 0:
+        import oracle as O
+        nt = os.cpu_count() or 1
+        picked = bit_exact_cases(cases, args.check_cases)
+        bad = []
+        for i in picked:
+            kind, dims, o2n, src, dst, _, _, _ = ops[2 * i]
+            a = ALPHAS[i % len(ALPHAS)]
+            vol = int(np.prod(dims, dtype=np.int64))
+            nb = vol * ESIZE[kind]
+            dt = np.float32 if kind == R4 else np.float64
+            launch(ops[2 * i])
+            torch.cuda.synchronize(dev)
+            lin = lbuf[(src - base_l):(src - base_l) + nb].cpu().numpy().view(dt).reshape(dims, order="F")
+            dcopy = dbuf[(dst - base_d):(dst - base_d) + nb].cpu().numpy().view(dt)
+            ref = O.permute(lin, o2n, blocked=True, nthreads=nt)
+            ok_copy = dcopy.tobytes() == ref.tobytes(order="F")
+            launch(ops[2 * i + 1])
+            torch.cuda.synchronize(dev)
+            dadd = dbuf[(dst - base_d):(dst - base_d) + nb].cpu().numpy().view(dt)
+            O.tensor_add_blocked(ref, lin, o2n, a[0], a[1], nthreads=nt)
+            ok_add = dadd.tobytes() == ref.tobytes(order="F")
+            if not (ok_copy and ok_add):
+                bad.append(i)
+            del lin, dcopy, dadd, ref
+        check = {"cases": len(picked), "bit_exact": not bad, "failed": bad[:8],
+                 "ranks": sorted({len(cases[i][1]) for i in picked}),
+                 "gb_checked": sig(sum(5 * case_bytes(cases[i][0], cases[i][1]) for i in picked) / 1e9)}
 
-    # End to end through the public API with pinned Host buffers.
+    # End to end through the public API with pinned Host buffers.  Each case is a
+    # talshTensorCopy with COPY_TK (D copied back, L's device image kept) and a
+    # talshTensorAdd with COPY_TD (D staged and copied back, L's kept device image
+    # used and then discarded): L crosses the link once per case.
     e2e = None
     if args.e2e_steps > 0:
         hl = torch.empty(2 * SLOT, dtype=torch.uint8, pin_memory=True)
@@ -522,8 +703,8 @@ def main():
         h2d = d2h = 0
         for (kind, dims, o2n) in cases:
             b = case_bytes(kind, dims)
-            h2d += b + 2 * b  # copy: L; add: L and D
-            d2h += b + b
+            h2d += b + b  # copy: L; add: D (L's device image is kept from the copy)
+            d2h += b + b  # D after the copy and after the add
         gdev = dev.index or 0
 
         import collections
@@ -558,9 +739,9 @@ def main():
             for i, (lt, dt_, pc, pa) in enumerate(tens):
                 a = ALPHAS[i % len(ALPHAS)]
                 submit(lambda tk: L.talshTensorCopy(pc, C.byref(dt_), C.byref(lt), gdev, T.DEV_NVIDIA_GPU,
-                                                    T.COPY_TT, C.byref(tk)))
+                                                    T.COPY_TK, C.byref(tk)))
                 submit(lambda tk: L.talshTensorAdd(pa, C.byref(dt_), C.byref(lt), a[0], a[1], gdev,
-                                                   T.DEV_NVIDIA_GPU, T.COPY_TT, C.byref(tk)))
+                                                   T.DEV_NVIDIA_GPU, T.COPY_TD, C.byref(tk)))
             while inflight:
                 finish_oldest()
         e2e_step()  # warm-up
@@ -573,11 +754,29 @@ def main():
         e2e_s = slowest_rank(e2e_s, world, dev)
         for lt, dt_, _, _ in tens:
             L.talshTensorDestruct(C.byref(lt)); L.talshTensorDestruct(C.byref(dt_))
+        # the host link's own rates, for the bound: pinned 1 GiB copies each way and both at once
+        link = {}
+        dbl = torch.empty(SLOT, dtype=torch.uint8, device=dev)
+        s1, s2 = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
+        for name in ("h2d", "d2h", "both"):
+            torch.cuda.synchronize(dev)
+            t_ = time.perf_counter()
+            for _ in range(2):
+                if name != "d2h":
+                    with torch.cuda.stream(s1):
+                        dbl.copy_(hl[:SLOT], non_blocking=True)
+                if name != "h2d":
+                    with torch.cuda.stream(s2):
+                        hd[:SLOT].copy_(lbuf[:SLOT], non_blocking=True)
+            torch.cuda.synchronize(dev)
+            link[name] = sig(2 * SLOT * (2 if name == "both" else 1) / (time.perf_counter() - t_) / 1e9)
+        del dbl
+        bound = step_bytes / max(h2d / link["h2d"], d2h / link["d2h"], (h2d + d2h) / link["both"]) / 1e9
         e2e = {"value": whole_job_rate(step_bytes * args.e2e_steps, world, e2e_s) / 1e9, "unit": "GB/s",
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-               "path": "talshTensorCopy + talshTensorAdd, pinned Host tensors, COPY_TT, asynchronous "
+               "path": "talshTensorCopy (COPY_TK) + talshTensorAdd (COPY_TD), pinned Host tensors, asynchronous "
                        "TAL-SH tasks (up to 5 in flight)",
-               "steps": args.e2e_steps}
+               "link_gbs": link, "link_bound_gbs": sig(bound), "steps": args.e2e_steps}
 
     # Contractions (FP64) through talshTensorContract on GPU-resident tensors.
     # A leg that fails records its error; the line is still printed.
@@ -606,21 +805,25 @@ def main():
     ratio = profile_traffic_ratio()
     roofline = {"kernel": "permute_reg_kernel (transpose and transpose-add)", "bound": "hbm",
                 "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)",
+                "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs, burst copy)",
                 "traffic": (ratio * launch_avg_bytes) if ratio else None,
                 "launches": len(ops), "avg_launch_bytes": launch_avg_bytes, "avg_launch_us": launch_avg_s * 1e6,
-                "transpose_gbs": copy_b / copy_t / 1e9, "add_gbs": add_b / add_t / 1e9}
+                "transpose_gbs": sig(copy_b / copy_t / 1e9), "add_gbs": sig(add_b / add_t / 1e9),
+                "r4_gbs": sig(r4_b / r4_t / 1e9), "r8_gbs": sig(r8_b / r8_t / 1e9)}
 
     if rank == 0:
         cpu = None
         if not args.no_cpu and world == 1:
-            cpu, _ = run_cpu_baseline(cases)
+            cpu = run_cpu_baseline(cases)
+        if detail_path:
+            write_detail({"contract": contract, "per_case": per_case, "e2e": e2e, "cpu_baseline": cpu,
+                          "check": check, "roofline": roofline}, detail_path)
         line = {"metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32/f64 (R4/R8)", "data": "synthetic", "config": config,
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": gpu_launches,
-                "clocks": sampler.summary(), "contract": contract, "check_bit_exact": check,
-                "graph": graph is not None}
+                "clocks": sampler.summary(), "check_bit_exact": check, "graph": True,
+                "contract": contract_summary(contract)}
         print(json.dumps(line))
     if world > 1:
         dist.destroy_process_group()

@@ -267,7 +267,9 @@ void tcTensorContractBatchTuneReset(void);
  * exit.  Shapes whose tcTensorContractScratch(...) exceeds that size are
  * rejected with TALSH_LIMIT_EXCEEDED (tcLastErrorString says why).  The first
  * call on a device looks up the array's device address, so make that first
- * call before any stream capture.  All calls share the one array: calls that
+ * call before any stream capture; the address is kept for the life of the
+ * process, so a device reset (cudaDeviceReset) after that first call is not
+ * supported.  All calls share the one array: calls that
  * may overlap on the GPU (other streams, other host threads) race and must be
  * serialised by the caller.  No counterpart in the reference. */
 int tcTensorContractNoAlloc(int data_kind, const int *cptrn, int drank, const int *ddims,

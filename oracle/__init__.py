@@ -44,6 +44,7 @@ def lib():
         L.orc_permute_blocked.argtypes = [I, I, P(I), P(I), V, V, I]
         L.orc_tensor_copy.argtypes = [I, P(I), I, P(I), V, V, I]
         L.orc_tensor_add.argtypes = [I, P(I), I, P(I), V, V, D, D, I]
+        L.orc_tensor_add_blocked.argtypes = [I, I, P(I), P(I), V, V, D, D, I]
         L.orc_tensor_scale.argtypes = [I, Z, V, D, D, I]
         L.orc_tensor_init.argtypes = [I, Z, V, D, D, I]
         L.orc_norm1.argtypes = [I, Z, V]
@@ -133,6 +134,59 @@ def tensor_add(d, l, cptrn, sr=1.0, si=0.0, conj_bits=0):
     e = lib().orc_tensor_add(KIND_OF[d.dtype], _iv(cptrn), l.ndim, _iv(l.shape), _ptr(l), _ptr(d), sr, si, conj_bits)
     assert e == 0, e
     return d
+
+
+def tensor_add_blocked(d, l, o2n, sr=1.0, si=0.0, nthreads=None):
+    """In place: d += permute(l) * s through the reference's multi-threaded flow
+    (blocked transpose into a temporary, then an OpenMP add); bit-identical to tensor_add."""
+    l = _fort(l)
+    assert d.flags["F_CONTIGUOUS"] and d.dtype == l.dtype
+    e = lib().orc_tensor_add_blocked(KIND_OF[l.dtype], l.ndim, _iv(l.shape), _iv(o2n), _ptr(l), _ptr(d), sr, si,
+                                     nthreads or os.cpu_count() or 1)
+    assert e == 0, e
+
+
+def contract_ttgt_blas(d, l, r, cptrn, sr=1.0, si=0.0, accumulative=True, nthreads=None):
+    """In place on d: the reference CPU contraction as it runs with a BLAS library
+    (tensor_block_contract, tensor_algebra_cpu.F90:3675-4358): L and R permuted by the
+    CPU matricization (get_contraction_permutations, :5757-5956) with the cache-blocked
+    transpose, D permuted unless its order is already the matrix order, one
+    ?GEMM('T','N', ll, lr, lc, alpha, L, lc, R, lc, beta=1, D, ll) (:3987-4044, the call at
+    :4005) from the BLAS scipy links (OpenBLAS, the reference's default BLASLIB), and the
+    back-transpose.  No hyper-indices and no conjugation flags.  Returns seconds spent."""
+    import time
+    from scipy.linalg import blas
+    nt = nthreads or os.cpu_count() or 1
+    l, r = _fort(l), _fort(r)
+    assert d.flags["F_CONTIGUOUS"] and d.dtype == l.dtype == r.dtype
+    t0 = time.perf_counter()
+    e, dprm, lprm, rprm, ncd, nlu, nru, nhu = permutations(cptrn, l.ndim, r.ndim, 0, "cpu")
+    assert e == 0 and nhu == 0, (e, nhu)
+    ident = lambda p: all(x == i + 1 for i, x in enumerate(p))
+    lt = l if ident(lprm) else permute(l, lprm, blocked=True, nthreads=nt)
+    rt = r if ident(rprm) else permute(r, rprm, blocked=True, nthreads=nt)
+    lc = int(np.prod(lt.shape[:ncd], dtype=np.int64))
+    ll = lt.size // max(1, lc)
+    lr = rt.size // max(1, lc)
+    if not accumulative:
+        d[...] = 0
+    dinv = [0] * len(dprm)
+    for k, p in enumerate(dprm):
+        dinv[p - 1] = k + 1
+    dt = d if ident(dinv) else permute(d, dinv, blocked=True, nthreads=nt)
+    A = lt.reshape((lc, ll), order="F")
+    B = rt.reshape((lc, lr), order="F")
+    Dm = dt.reshape((ll, lr), order="F")
+    gemm = {np.dtype(np.float32): blas.sgemm, np.dtype(np.float64): blas.dgemm,
+            np.dtype(np.complex64): blas.cgemm, np.dtype(np.complex128): blas.zgemm}[d.dtype]
+    alpha = complex(sr, si) if np.iscomplexobj(d) else sr
+    out = gemm(alpha, A, B, beta=1.0, c=Dm, trans_a=1, overwrite_c=1)
+    if out is not Dm and not np.shares_memory(out, Dm):
+        Dm[...] = out
+    if dt is not d:
+        e = lib().orc_permute_blocked(KIND_OF[d.dtype], dt.ndim, _iv(dt.shape), _iv(dprm), _ptr(dt), _ptr(d), nt)
+        assert e == 0, e
+    return time.perf_counter() - t0
 
 
 def tensor_copy(d, l, cptrn, conj_bits=0):

@@ -10,7 +10,7 @@ def build_oracle(force=False):
     src = os.path.join(HERE, "oracle.c")
     hdr = os.path.join(HERE, "oracle.h")
     if force or not os.path.exists(LIB) or max(os.path.getmtime(src), os.path.getmtime(hdr)) > os.path.getmtime(LIB):
-        subprocess.run(["gcc", "-O2", "-std=c11", "-fopenmp", "-fPIC", "-shared", "-Wall",
+        subprocess.run(["gcc", "-O2", "-std=c11", "-ffp-contract=off", "-fopenmp", "-fPIC", "-shared", "-Wall",
                         "-o", LIB, src, "-lm"], check=True)
     return LIB
 

@@ -769,6 +769,63 @@ int orc_tensor_add(int kind, const int *cptrn, int rank, const int *ldims, const
   return 0;
 }
 
+/* The reference's multi-threaded add, as timed on the host cores: a
+ * non-identity pattern first permutes L into a freshly allocated block with the
+ * cache-blocked OpenMP transpose (cpu_tensor_block_add, talshf.F90:1857-1904,
+ * calls tensor_block_copy and later destroys the block), then tensor_block_add
+ * (tensor_algebra_cpu.F90:3312-3673) runs one OpenMP loop d = d + l*s, each
+ * operation rounded on its own (the reference's GNU build has no FMA
+ * contraction; this file is compiled with -ffp-contract=off).  Real kinds use
+ * s = cmplx8_to_real8(alpha).  Result bit-identical to orc_tensor_add. */
+int orc_tensor_add_blocked(int kind, int rank, const int *dims_in, const int *o2n, const void *L,
+                           void *D, double sr, double si, int nthreads) {
+  int es = kind_size(kind);
+  if (es == 0 || rank < 1 || rank > ORC_MAX_RANK || !perm_ok(rank, o2n)) return 1;
+  if (nthreads < 1) nthreads = 1;
+  size_t vol = 1;
+  for (int i = 0; i < rank; ++i) vol *= (size_t)dims_in[i];
+  int permute = 0;
+  for (int i = 0; i < rank; ++i) if (o2n[i] != i + 1) { permute = 1; break; }
+  const void *src = L;
+  void *tmp = NULL;
+  if (permute) {
+    tmp = malloc(vol * (size_t)es);
+    if (!tmp) return 2;
+    int rc = orc_permute_blocked(kind, rank, dims_in, o2n, L, tmp, nthreads);
+    if (rc) { free(tmp); return rc; }
+    src = tmp;
+  }
+  const long long n = (long long)vol;
+  if (kind == 4) {
+    const float s = (float)orc_cmplx8_to_real8(sr, si);
+    float *d = (float *)D; const float *l = (const float *)src;
+#pragma omp parallel for schedule(static) num_threads(nthreads)
+    for (long long i = 0; i < n; ++i) d[i] = d[i] + l[i] * s;
+  } else if (kind == 8) {
+    const double s = orc_cmplx8_to_real8(sr, si);
+    double *d = (double *)D; const double *l = (const double *)src;
+#pragma omp parallel for schedule(static) num_threads(nthreads)
+    for (long long i = 0; i < n; ++i) d[i] = d[i] + l[i] * s;
+  } else if (kind == 14) {
+    const float ar = (float)sr, ai = (float)si;
+    c4_t *d = (c4_t *)D; const c4_t *l = (const c4_t *)src;
+#pragma omp parallel for schedule(static) num_threads(nthreads)
+    for (long long i = 0; i < n; ++i) {
+      const float pr = l[i].re * ar - l[i].im * ai, pi = l[i].re * ai + l[i].im * ar;
+      d[i].re = d[i].re + pr; d[i].im = d[i].im + pi;
+    }
+  } else {
+    c8_t *d = (c8_t *)D; const c8_t *l = (const c8_t *)src;
+#pragma omp parallel for schedule(static) num_threads(nthreads)
+    for (long long i = 0; i < n; ++i) {
+      const double pr = l[i].re * sr - l[i].im * si, pi = l[i].re * si + l[i].im * sr;
+      d[i].re = d[i].re + pr; d[i].im = d[i].im + pi;
+    }
+  }
+  free(tmp);
+  return 0;
+}
+
 int orc_tensor_scale(int kind, size_t vol, void *D, double sr, double si, int conj_bits) {
   if (conj_bits & 1) si = -si;
   if (kind == 4) {

@@ -49,6 +49,12 @@ int orc_tensor_copy(int kind, const int *cptrn, int rank, const int *ldims, cons
 /* cpu_tensor_block_add (talshf.F90:1857-1904) -> tensor_block_add (:3312-3673). */
 int orc_tensor_add(int kind, const int *cptrn, int rank, const int *ldims, const void *L, void *D,
                    double sr, double si, int conj_bits);
+/* The same add as the reference runs it on the host cores: permute into a
+ * temporary block with the cache-blocked OpenMP transpose, then one OpenMP add
+ * loop (talshf.F90:1857-1904, tensor_algebra_cpu.F90:3312-3673); used as the
+ * timed CPU baseline and for fast checks.  Bit-identical to orc_tensor_add. */
+int orc_tensor_add_blocked(int kind, int rank, const int *dims_in, const int *o2n, const void *L,
+                           void *D, double sr, double si, int nthreads);
 /* tensor_block_scale (tensor_algebra_cpu.F90:1821-1890) via cpu_tensor_block_scale. */
 int orc_tensor_scale(int kind, size_t vol, void *D, double sr, double si, int conj_bits);
 /* tensor_block_init with a value (cpu_tensor_block_init, talshf.F90:1720-1749). */

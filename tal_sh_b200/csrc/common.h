@@ -55,6 +55,8 @@ void note_launch(unsigned n = 1);
 void note_cuda_error(const char *what, int code);
 void note_error_text(const char *msg);  // sets the text tcLastErrorString returns
 int check_launch(const char *what);  // 0 or TALSH_FAILURE after a kernel launch
+// SM count of the current device, cached per device (thread-safe).
+int current_sm_count();
 
 // Batched contractions for host-side schedulers: `get` returns device scratch
 // of scratch_bytes and sets *stage to a pinned host block of stage_bytes that

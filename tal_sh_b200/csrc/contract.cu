@@ -832,16 +832,7 @@ int gemm_grid(GemmArgs &ga, int bm, int bn, int64_t *blocks) {
   return TALSH_SUCCESS;
 }
 
-int sm_count_dev() {
-  static int cache = 0;
-  if (cache == 0) {
-    int dev = 0, v = 0;
-    cudaGetDevice(&dev);
-    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0) v = 148;
-    cache = v;
-  }
-  return cache;
-}
+int sm_count_dev() { return current_sm_count(); }
 
 template <int BM, int BN>
 int launch_dmma(const double *L, const double *R, double *D, GemmArgs ga, cudaStream_t st) {

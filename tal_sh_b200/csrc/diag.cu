@@ -28,6 +28,22 @@ void note_error_text(const char *msg) {
   std::snprintf(g_last_err, sizeof(g_last_err), "%s", msg);
 }
 
+int current_sm_count() {
+  static std::atomic<int> cache[64];  // zero-initialised: 0 = not probed yet
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) { cudaGetLastError(); dev = 0; }
+  if (dev < 0 || dev >= 64) return 148;
+  int v = cache[dev].load(std::memory_order_relaxed);
+  if (v == 0) {
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0) {
+      cudaGetLastError();
+      v = 148;
+    }
+    cache[dev].store(v, std::memory_order_relaxed);
+  }
+  return v;
+}
+
 int check_launch(const char *what) {
   const cudaError_t e = cudaGetLastError();
   if (e == cudaSuccess) return TALSH_SUCCESS;

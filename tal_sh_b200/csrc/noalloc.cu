@@ -38,7 +38,9 @@ std::mutex g_scratch_mu;
 void *g_scratch_dev[kMaxDevices] = {};  // device address of g_contract_scratch, per device
 
 // Device address of the scratch array on the current device, looked up once
-// per device (the first call on a device does the lookup).
+// per device (the first call on a device does the lookup) and kept for the
+// life of the process: a device reset after that first call is not supported,
+// since the module would be reloaded at another address.
 int scratch_address(void **out) {
   int dev = -1;
   cudaError_t e = cudaGetDevice(&dev);

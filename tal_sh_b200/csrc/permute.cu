@@ -45,7 +45,32 @@ constexpr int kMaxFR = 40;         // max fused rank (every fused extent is >= 2
 constexpr int kTileBytes = 32768;  // byte budget of one tile buffer (kStages buffers per CTA)
 constexpr int kMaxTabLo = 4096;    // output run length when B needs a table (more than 3 dims)
 constexpr int kMaxRuns = 1024;     // run count bound (run tables live in shared memory)
-constexpr int kStages = 3;              // tile buffers per CTA: loads run kStages - 1 tiles ahead
+constexpr int kStages = 3;              // tile buffers per CTA of permute_tiled_kernel: loads run 2 tiles ahead
+
+// Tile buffers per CTA of permute_reg_kernel, by element size and operation:
+// loads run S - 1 tiles ahead of the write phase.  Adds also prefetch the D
+// vectors each thread will update into a private shared slot of the same stage
+// (kAddPrefetch), so the write phase waits on no global load.
+#ifndef TB_STAGES_COPY4
+#define TB_STAGES_COPY4 3
+#endif
+#ifndef TB_STAGES_COPY8
+#define TB_STAGES_COPY8 3
+#endif
+#ifndef TB_STAGES_ADD4
+#define TB_STAGES_ADD4 3
+#endif
+#ifndef TB_STAGES_ADD8
+#define TB_STAGES_ADD8 3
+#endif
+#ifndef TB_ADD_PREFETCH
+#define TB_ADD_PREFETCH 0
+#endif
+constexpr bool kAddPrefetch = TB_ADD_PREFETCH != 0;
+__host__ __device__ constexpr int reg_stages(int esize, int op) {
+  return op == 1 ? (esize <= 4 ? TB_STAGES_ADD4 : TB_STAGES_ADD8)
+                 : (esize <= 4 ? TB_STAGES_COPY4 : TB_STAGES_COPY8);
+}
 
 // Mixed-radix decomposition of an index over up to 3 tile dimensions with
 // precomputed magic divisors; groups of more dimensions use shared tables.
@@ -398,6 +423,9 @@ template <typename T, int K, int VOUT, int OP, bool SWZ>
 __global__ void __launch_bounds__(kThreads, K <= 4 ? 4 : 3)
     permute_reg_kernel(const T *__restrict__ src, T *dst, const PermParams P) {
   constexpr int KW = K / VOUT;  // write vectors per thread
+  constexpr int S = reg_stages((int)sizeof(T), OP);
+  constexpr bool DPF = OP == kOpAdd && kAddPrefetch;  // D vectors prefetched into shared slots
+  using V = Pack<T, VOUT>;
   extern __shared__ __align__(16) unsigned char smem[];
   T *buf0 = reinterpret_cast<T *>(smem);
   __shared__ TileSetup setup[kRing];
@@ -491,34 +519,47 @@ __global__ void __launch_bounds__(kThreads, K <= 4 ? 4 : 3)
   effective_scale<T>(P.sdev, P.sdev_kind, P.sdev_conj, sr, si);
   const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(buf0);
   const uint32_t stage_bytes = (uint32_t)P.buf_elems * (uint32_t)sizeof(T);
+  // Prefetched D vectors: slot (stage, k) of thread tid, after the S tile buffers.
+  constexpr uint32_t kSlotStage = (uint32_t)(KW * kThreads * sizeof(V));
+  const uint32_t dbase = sbase + (uint32_t)S * stage_bytes + (uint32_t)tid * (uint32_t)sizeof(V);
+  const unsigned char *dslots = smem + (size_t)S * stage_bytes + (size_t)tid * sizeof(V);
 
-  auto issue_loads = [&](const TileSetup &S, int stage) {
-    const T *g = src + S.in_base;
+  auto issue_loads = [&](const TileSetup &St, int stage) {
+    const T *g = src + St.in_base;
     const uint32_t sb = sbase + (uint32_t)stage * stage_bytes;
-    const uint32_t m = (uint32_t)S.type | 4u;
+    const uint32_t m = (uint32_t)St.type | 4u;
 #pragma unroll
     for (int k = 0; k < K; ++k)
       if (((rcls >> (3 * k)) & m) == 0) cp_async_s<sizeof(T)>(sb + half(rs2, k), g + rg[k]);
+    if constexpr (DPF) {
+      const T *gd = dst + St.out_base;
+      const uint32_t db = dbase + (uint32_t)stage * kSlotStage;
+#pragma unroll
+      for (int k = 0; k < KW; ++k)
+        if (((wcls >> (3 * k)) & m) == 0)
+          cp_async_s<sizeof(V)>(db + (uint32_t)(k * kThreads) * (uint32_t)sizeof(V), gd + wg[k]);
+    }
   };
 
   int64_t t = blockIdx.x;
 #pragma unroll
-  for (int k = 0; k < kStages - 1; ++k) {
+  for (int k = 0; k < S - 1; ++k) {
     if (t + k * G < P.num_tiles) issue_loads(setup[k], k);
     cp_async_commit();
   }
   for (int iter = 0; t < P.num_tiles; t += G, ++iter) {
-    const int64_t tn = t + (kStages - 1) * G;
+    const int64_t tn = t + (S - 1) * G;
     if (tn < P.num_tiles)
-      issue_loads(setup[(iter + kStages - 1) % kRing], (iter + kStages - 1) % kStages);
+      issue_loads(setup[(iter + S - 1) % kRing], (iter + S - 1) % S);
     cp_async_commit();
     if ((iter & 31) == 0 && iter > 0) fill_setups(P, dimS, iter + 32, setup);
-    cp_async_wait<kStages - 1>();
+    cp_async_wait<S - 1>();
     __syncthreads();
-    const TileSetup S = setup[iter % kRing];
-    const char *sbytes = reinterpret_cast<const char *>(smem) + (size_t)(iter % kStages) * stage_bytes;
-    T *g = dst + S.out_base;
-    const uint32_t m = (uint32_t)S.type | 4u;
+    const TileSetup St = setup[iter % kRing];
+    const char *sbytes = reinterpret_cast<const char *>(smem) + (size_t)(iter % S) * stage_bytes;
+    T *g = dst + St.out_base;
+    const uint32_t m = (uint32_t)St.type | 4u;
+    const unsigned char *ds = dslots + (size_t)(iter % S) * kSlotStage;
     // Batches of up to 4 vectors bound the live registers.
     constexpr int WB = KW < 4 ? KW : 4;
 #pragma unroll
@@ -539,7 +580,18 @@ __global__ void __launch_bounds__(kThreads, K <= 4 ? 4 : 3)
           }
         }
       }
-      emit_masked<T, VOUT, OP, WB>(gp, v, ok, sr, si);
+      if constexpr (DPF) {
+#pragma unroll
+        for (int u = 0; u < WB; ++u) {
+          if (!ok[u]) continue;
+          V d = *reinterpret_cast<const V *>(ds + (size_t)((c0 + u) * kThreads) * sizeof(V));
+#pragma unroll
+          for (int j = 0; j < VOUT; ++j) d.v[j] = Arith<T>::axpy(d.v[j], v[u].v[j], sr, si);
+          st_pack<T, VOUT>(gp[u], d);
+        }
+      } else {
+        emit_masked<T, VOUT, OP, WB>(gp, v, ok, sr, si);
+      }
     }
     __syncthreads();
   }
@@ -790,7 +842,8 @@ int64_t balanced_grow(int64_t ext, int64_t cur) {
 
 // out_major: tile index order follows the output's dimensions (copies), else
 // the input's (adds, whose output sectors are read before they are written).
-int build_plan(int esize, const Fused &F, Plan &plan, bool out_major = true) {
+int build_plan(int esize, const Fused &F, Plan &plan, int op = kOpCopy) {
+  const bool out_major = op != kOpAdd;
   plan.vol = F.vol;
   if (F.n <= 1) { plan.linear = true; return TALSH_SUCCESS; }
   PermParams &P = plan.P;
@@ -1022,13 +1075,13 @@ int build_plan(int esize, const Fused &F, Plan &plan, bool out_major = true) {
     }
     if (ok) plan.vout = vec;
   }
-  // Shared memory: kStages tile buffers and the run tables.  Each buffer is
+  // Shared memory: the stage buffers and the run tables.  Each buffer is
   // rounded up to whole 128-byte rows: the swizzle permutes within rows.  The
   // register-table kernel reads the run tables only before its first tile, so
-  // they overlay the buffers when they fit there.
+  // they overlay the buffers when they fit there; its adds also hold the
+  // prefetched D vectors of every stage (K per thread).
   const size_t buf_elems = (((size_t)P.Ri * P.Li_pad * esize + 127) / 128) * 128 / esize;
   P.buf_elems = (int)buf_elems;
-  const size_t bufs = (size_t)kStages * buf_elems * esize;
   P.ytab = (P.Lo <= kMaxTabLo || P.ymap.n < 0) ? 1 : 0;
   const size_t run_tabs = (size_t)P.Ri * 12 + (size_t)P.Ro * 16 + (P.ytab ? (size_t)P.Lo * 4 : 0) + 16;
   int64_t span_in = 0, span_out = 0;
@@ -1042,6 +1095,12 @@ int build_plan(int esize, const Fused &F, Plan &plan, bool out_major = true) {
     return e && std::atoi(e) == 1;
   }();
   P.reg = (!force_generic && span_in < INT_MAX && span_out < INT_MAX && P.V <= kThreads * reg_k(esize)) ? 1 : 0;
+  const int stages = P.reg ? reg_stages(esize, op) : kStages;
+  size_t bufs = (size_t)stages * buf_elems * esize;
+  if (P.reg && op == kOpAdd && kAddPrefetch) {
+    const int kreg = (P.V <= kThreads * 4) ? 4 : 8;  // the K permute_reg_kernel is launched with
+    bufs += (size_t)stages * kreg * kThreads * esize;
+  }
   size_t off = (P.reg && run_tabs <= bufs) ? 0 : ((bufs + 15) & ~size_t(15));
   P.off_rin = (int)off; off += (size_t)P.Ri * 8;
   P.off_wout = (int)off; off += (size_t)P.Ro * 8;
@@ -1061,17 +1120,6 @@ int build_plan(int esize, const Fused &F, Plan &plan, bool out_major = true) {
   }
   plan.smem = off;
   return TALSH_SUCCESS;
-}
-
-int sm_count(int dev) {
-  static int cache[64] = {0};
-  if (dev < 0 || dev >= 64) return 148;
-  if (cache[dev] == 0) {
-    int v = 0;
-    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0) v = 148;
-    cache[dev] = v;
-  }
-  return cache[dev];
 }
 
 // Resident CTAs per SM for a kernel with `smem` dynamic bytes.  The kernel's
@@ -1118,9 +1166,7 @@ struct ScaleArgs {
 template <typename T, int OP>
 int launch_typed(const Plan &plan, const void *src, void *dst, int conj, const ScaleArgs &sc,
                  cudaStream_t st) {
-  int dev = 0;
-  cudaGetDevice(&dev);
-  const int sms = sm_count(dev);
+  const int sms = current_sm_count();
   if (plan.linear) {
     constexpr int VEC = 16 / sizeof(T) > 0 ? 16 / sizeof(T) : 1;
     const bool aligned = ((uintptr_t)src % 16 == 0) && ((uintptr_t)dst % 16 == 0);
@@ -1207,7 +1253,7 @@ int permute_entry(int kind, int rank, const int *dims, const int *o2n, const voi
   if (rank == 0) { F.n = 0; F.vol = 1; }
   else if ((rc = fuse_dims(rank, dims, o2n, F)) != 0) return rc;
   Plan plan;
-  if ((rc = build_plan(kind_size(kind), F, plan, OP != kOpAdd)) != 0) return rc;
+  if ((rc = build_plan(kind_size(kind), F, plan, OP)) != 0) return rc;
   cudaStream_t st = (cudaStream_t)stream;
   switch (kind) {
     case R4: return launch_typed<float, OP>(plan, src, dst, conj, sc, st);

@@ -938,6 +938,14 @@ int tensDevRsc_allocate_mem(talsh_dev_rsc_t *drsc, int dev_id, size_t mem_size, 
     if (!R.on || num >= MAX_GPUS_PER_NODE || !R.gpu[num].in_use) return 5;
     const int rc = dev_alloc(num, mem_size, &p);
     if (rc != TALSH_SUCCESS) return rc;  // TRY_LATER: over the budget, not an error
+    // The block comes from the library's stream-ordered pool; the caller may use
+    // it on any stream (the reference's gpu_mem_alloc is synchronous), so the
+    // allocation is complete before the pointer is handed out.
+    if (cudaStreamSynchronize(R.gpu[num].stream) != cudaSuccess) {
+      note_cuda_error("tensDevRsc_allocate_mem", (int)cudaGetLastError());
+      mem_free(p);
+      return TALSH_FAILURE;
+    }
   } else {
     return kind == DEV_INTEL_MIC ? -6 : kind == DEV_AMD_GPU ? -7 : -8;
   }
@@ -956,6 +964,20 @@ int tensDevRsc_free_mem(talsh_dev_rsc_t *drsc) {
   int kind = DEV_NULL;
   if (decode_device_id(drsc->dev_id, &kind) < 0) return -4;
   if (drsc->mem_attached != 0) return 1;  // attached, not allocated: detach it instead
+  if (kind == DEV_NVIDIA_GPU) {
+    // The caller's own work on the block may run on any of its streams; like the
+    // reference's synchronous gpu_mem_free, wait for the device before the block
+    // goes back to the pool, and for the release itself.
+    const int num = decode_device_id(drsc->dev_id, &kind);
+    cudaSetDevice(num);
+    cudaDeviceSynchronize();
+    cudaGetLastError();
+    const int rc = mem_free(drsc->gmem_p) == TALSH_SUCCESS ? 0 : NOT_CLEAN;
+    if (num < MAX_GPUS_PER_NODE) cudaStreamSynchronize(R.gpu[num].stream);
+    cudaGetLastError();
+    tensDevRsc_clean(drsc);
+    return rc;
+  }
   const int rc = mem_free(drsc->gmem_p) == TALSH_SUCCESS ? 0 : NOT_CLEAN;
   tensDevRsc_clean(drsc);
   return rc;
@@ -2313,6 +2335,8 @@ int talshTensorContractXL(const char *cptrn, talsh_tens_t *d, talsh_tens_t *l, t
   }
   const int es = kind_size(kind);
   if (es == 0) return TALSH_INVALID_ARGS;
+  // Copies back into these bodies may also be in flight from tasks on other GPUs.
+  for (int a = 0; a < 3; ++a) sync_pending(hp[a], shape_volume(ts[a]->shape_p) * (size_t)es);
   const int rank[3] = {op.drank, op.lrank, op.rrank};
   const int *full[3] = {d->shape_p->dims, l->shape_p->dims, r->shape_p->dims};
   // Decomposition.

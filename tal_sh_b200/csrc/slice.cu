@@ -83,20 +83,9 @@ __global__ void __launch_bounds__(kSliceThreads) slice_elems_kernel(const T *__r
   }
 }
 
-int sm_count() {
-  static int n = 0;
-  if (n == 0) {
-    int dev = 0, v = 0;
-    cudaGetDevice(&dev);
-    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0) v = 148;
-    n = v;
-  }
-  return n;
-}
-
 template <typename T, bool INSERT, bool ACC>
 int launch(const void *src, void *dst, const SliceParams &p, cudaStream_t st) {
-  const int64_t cap = (int64_t)sm_count() * 8;
+  const int64_t cap = (int64_t)current_sm_count() * 8;
   if (p.run >= 16) {
     const int64_t blocks = std::max<int64_t>(1, std::min<int64_t>((p.rows + 7) / 8, cap));
     slice_rows_kernel<T, INSERT, ACC><<<(unsigned)blocks, kSliceThreads, 0, st>>>((const T *)src, (T *)dst, p);
