@@ -381,7 +381,7 @@ def contract_summary(con):
             if isinstance(q, dict) and "tflops_fp64_equiv" in q:
                 e.update({"split_tflops": sig(q["tflops_fp64_equiv"]), "split_err": sig(q["rel_err_vs_fp64"], 2),
                           "split_x": sig(q["speedup_vs_plain"])})
-            for form in ("bf16x3", "tf32x3", "fp8"):
+            for form in ("bf16x3", "tf32x3", "fp8x3"):
                 f = con.get(name + "_" + form)
                 if isinstance(f, dict) and "tflops_fp64_equiv" in f:
                     e[form] = [sig(f["tflops_fp64_equiv"]), sig(f["rel_err_vs_fp64"], 2)]
@@ -771,11 +771,11 @@ def main():
             torch.cuda.synchronize(dev)
             link[name] = sig(2 * SLOT * (2 if name == "both" else 1) / (time.perf_counter() - t_) / 1e9)
         del dbl
-        bound = step_bytes / max(h2d / link["h2d"], d2h / link["d2h"], (h2d + d2h) / link["both"]) / 1e9
+        # seconds per step at the measured link rates (GB/s): the slower direction, or both at once
+        bound = step_bytes / max(h2d / link["h2d"], d2h / link["d2h"], (h2d + d2h) / link["both"])
         e2e = {"value": whole_job_rate(step_bytes * args.e2e_steps, world, e2e_s) / 1e9, "unit": "GB/s",
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-               "path": "talshTensorCopy (COPY_TK) + talshTensorAdd (COPY_TD), pinned Host tensors, asynchronous "
-                       "TAL-SH tasks (up to 5 in flight)",
+               "path": "talshTensorCopy COPY_TK + talshTensorAdd COPY_TD, pinned Host, async tasks",
                "link_gbs": link, "link_bound_gbs": sig(bound), "steps": args.e2e_steps}
 
     # Contractions (FP64) through talshTensorContract on GPU-resident tensors.
@@ -946,6 +946,23 @@ def bench_contractions(T, L, torch, dev):
             "rel_err_vs_fp64": errs, "int8_tops_issued": tops,
             "frac_of_int8_gemm": (tops / int8_tops) if int8_tops else None,
             "path": "talshTensorContract with talshContractSlicesSet(%d), GPU-resident" % slices}
+        # The floating-point split forms (bf16 / tf32 / e4m3 slices, fp32 sums per
+        # diagonal, FP64 recombination): rate and error of each.
+        for fname, form, fs in (("bf16x3", T.TC_SPLIT_BF16, 3), ("tf32x3", T.TC_SPLIT_TF32, 3),
+                                ("fp8x3", T.TC_SPLIT_FP8, 3)):
+            assert L.talshContractSplitFormSet(form, fs) == 0
+            try:
+                dtf = timed()
+            except AssertionError:
+                out[name + "_" + fname] = {"error": "contraction failed: %s" % L.tcLastErrorString()}
+                continue
+            finally:
+                assert L.talshContractSlicesSet(0) == 0
+            errf = float(torch.linalg.norm(got - ref) / torch.linalg.norm(ref))
+            out[name + "_" + fname] = {"tflops_fp64_equiv": flops / dtf / 1e12, "speedup_vs_plain": dt / dtf,
+                                       "ms": dtf * 1e3, "rel_err_vs_fp64": errf, "slices": fs,
+                                       "path": "talshTensorContract with talshContractSplitFormSet(%d, %d)"
+                                               % (form, fs)}
         for t in tens:
             L.talshTensorDestruct(C.byref(t))
         del views, ref, got, lv, rv

@@ -427,6 +427,14 @@ int gpu_get_device_count(int *dev_count);
  * uses the split form for R8 only.  Returns TALSH_INVALID_ARGS for other values. */
 int talshContractSlicesSet(int slices);
 int talshContractSlicesGet(void);
+/* Extension of this core (no counterpart in the reference): the split form and
+ * slice count talshTensorContract uses for R8/C8 (the forms TC_SPLIT_INT8,
+ * TC_SPLIT_BF16, TC_SPLIT_TF32, TC_SPLIT_FP8 of tcTensorContractSplitForm in
+ * talsh_b200.h; slices 0 = the form's default, else 2..7).
+ * talshContractSlicesSet(0) returns to plain FP64.  TALSH_INVALID_ARGS for
+ * other values. */
+int talshContractSplitFormSet(int form, int slices);
+int talshContractSplitFormGet(int *form, int *slices);
 #ifdef __cplusplus
 }
 #endif

@@ -102,6 +102,39 @@ int tcTensorContractSplit(int data_kind, const int *cptrn, int drank, const int 
                           int accumulative, int slices, void *scratch, size_t scratch_bytes,
                           void *stream);
 
+/* Split forms of the tensor-core contraction (tcTensorContractSplitForm). */
+#define TC_SPLIT_INT8 0 /* int8 digits, exact int32 sums (tcTensorContractSplit) */
+#define TC_SPLIT_BF16 1 /* bf16 slices, fp32 sums per diagonal (kind::f16) */
+#define TC_SPLIT_TF32 2 /* tf32 slices, fp32 sums per diagonal (kind::tf32) */
+#define TC_SPLIT_FP8 3  /* e4m3 slices with per-row power-of-two scales (kind::f8f6f4) */
+
+/* Bytes of device scratch tcTensorContractSplitForm needs (0 when the form
+ * does not apply, as for tcTensorContractSplitScratch, or for an invalid form
+ * or slice count). */
+size_t tcTensorContractSplitFormScratch(int data_kind, const int *cptrn, int drank, const int *ddims,
+                                        int lrank, const int *ldims, int rrank, const int *rdims,
+                                        int form, int slices);
+
+/* tcTensorContractSplit in a chosen form: TC_SPLIT_INT8 is that function;
+ * the floating-point forms cut each row-scaled operand into `slices` slices of
+ * bf16 (8 significant bits each), tf32 (11) or e4m3 (4), y_s = round(r_s 2^(b s)),
+ * r_{s+1} = r_s - y_s 2^(-b s) (exact in FP64), multiply the slice pairs
+ * s + t <= slices - 1 on the tensor cores with one fp32 accumulator per
+ * diagonal s + t in tensor memory (each product exact in fp32, the sums
+ * rounded to fp32) and recombine the diagonals in FP64 into D.  slices: 0 =
+ * the form's default (6 for int8, 3 otherwise), else 2..7.  The error is
+ * dominated by the fp32 sums for bf16 and tf32 (they grow with the number of
+ * tensor-core K steps: about 1e-6 relative at a contracted volume of 1024,
+ * 1e-5 to 1e-4 at 10^4 to 4x10^4) and by the dropped pairs, about
+ * 2^(-4 slices), for e4m3; callers state it per result.  The BF16x3 / TF32x3 / FP8 forms of a
+ * split-precision gpu_tensor_block_contract_dlf (reference :5847); no
+ * reference counterpart. */
+int tcTensorContractSplitForm(int data_kind, const int *cptrn, int drank, const int *ddims, int lrank,
+                              const int *ldims, int rrank, const int *rdims, void *D, const void *L,
+                              const void *R, double alpha_re, double alpha_im, int conj_bits,
+                              int accumulative, int form, int slices, void *scratch, size_t scratch_bytes,
+                              void *stream);
+
 /* Slicing: slice (+)= full[offsets : offsets + slice_dims] (0-based offsets, both
  * tensors dense column-major of the same rank and kind).  Replaces
  * gpu_tensor_block_slice (tensor_algebra_gpu_nvidia.cu:4788, a stub there) with
@@ -298,6 +331,17 @@ size_t tcContractXLLastOps(void);
  * or TALSH_INVALID_ARGS. */
 int tcContractXLPlan(int data_kind, const int *cptrn, int drank, const int *ddims, int lrank, const int *ldims,
                      int rrank, const int *rdims, size_t budget_bytes, int max_ops, int *offsets, int *extents);
+/* Number of CTAs on the current GPU that gave up one of the split-precision
+ * GEMM's bounded waits since the library was loaded, or -1 when it cannot be
+ * read (reference gpu_get_error_count, device_algebra.h:200).  A CTA that gives
+ * up waits (bounded) for its own copies in flight, frees its tensor memory and
+ * returns; the context stays usable.  talshTensorContract tasks in split
+ * precision that see the count rise finish with TALSH_TASK_ERROR. */
+int gpu_get_error_count(void);
+/* Test hook for the failure path above: while enabled, split-precision GEMM
+ * launches issue no operand copies and give up their first wait after 4096
+ * polls.  Off by default. */
+int tcTestSplitStall(int enable);
 /* Number of kernels this library launched since load (diagnostics). */
 unsigned long long tcKernelLaunchCount(void);
 /* Last CUDA error text seen by the library (diagnostics). */

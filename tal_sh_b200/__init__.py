@@ -32,6 +32,7 @@ TALSH_TASK_ERROR, TALSH_TASK_EMPTY, TALSH_TASK_SCHEDULED = 1999999, 2000000, 200
 TALSH_TASK_STARTED, TALSH_TASK_INPUT_READY = 2000002, 2000003
 TALSH_TASK_OUTPUT_READY, TALSH_TASK_COMPLETED = 2000004, 2000005
 COPY_D, COPY_M, COPY_T, COPY_K = 0, 1, 2, 3
+TC_SPLIT_INT8, TC_SPLIT_BF16, TC_SPLIT_TF32, TC_SPLIT_FP8 = 0, 1, 2, 3
 
 
 def copy_ctrl(*codes):
@@ -171,6 +172,8 @@ _PROTOS = {
     "talshTensorNorm1": (_D, [_P(Tens), _I, _I]),
     "talshContractSlicesSet": (_I, [_I]),
     "talshContractSlicesGet": (_I, []),
+    "talshContractSplitFormSet": (_I, [_I, _I]),
+    "talshContractSplitFormGet": (_I, [_P(_I), _P(_I)]),
     "talsh_get_contr_ptrn_str2dig": (_I, [_S, _P(_I), _P(_I), _P(_I), _P(_I), _P(_I)]),
     "get_contr_pattern_sym": (None, [_P(_I), _P(_I), _P(_I), _P(_I), C.c_char_p, _P(_I), _P(_I)]),
     "host_mem_register": (_I, [_V, _Z]),
@@ -257,7 +260,12 @@ _PROTOS = {
     "tcServerReplay": (_I, [_V, _I, _P(ServeTask), _P(_D), _P(C.c_uint64), _P(_D)]),
     "tcTensorContractSplit": (_I, [_I, _P(_I), _I, _P(_I), _I, _P(_I), _I, _P(_I), _V, _V, _V, _D, _D,
                                    _I, _I, _I, _V, _Z, _V]),
+    "tcTensorContractSplitForm": (_I, [_I, _P(_I), _I, _P(_I), _I, _P(_I), _I, _P(_I), _V, _V, _V, _D, _D,
+                                       _I, _I, _I, _I, _V, _Z, _V]),
+    "tcTensorContractSplitFormScratch": (_Z, [_I, _P(_I), _I, _P(_I), _I, _P(_I), _I, _P(_I), _I, _I]),
     "tcPermutePlanInfo": (_I, [_I, _I, _P(_I), _P(_I), _P(_I)]),
+    "gpu_get_error_count": (_I, []),
+    "tcTestSplitStall": (_I, [_I]),
     "tcKernelLaunchCount": (C.c_ulonglong, []),
     "tcLastErrorString": (_S, []),
 }

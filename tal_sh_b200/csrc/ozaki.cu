@@ -21,6 +21,8 @@
 // The int32 sums are exact while (S) * K * 127^2 < 2^31; longer contractions
 // are split into K chunks that accumulate into D.
 #include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_fp8.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -112,11 +114,22 @@ __device__ __forceinline__ bool mbar_try(uint64_t *bar, uint32_t parity) {
 }
 
 // Bounded wait: false (and the error flag set) when the phase never completes.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *err) {
-  for (uint32_t i = 0; i < kSpinLimit; ++i)
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *err,
+                                          uint32_t limit = kSpinLimit) {
+  for (uint32_t i = 0; i < limit; ++i)
     if (mbar_try(bar, parity)) return true;
   atomicExch(err, 1);
   return false;
+}
+
+// Count of CTAs that gave up a bounded wait, per device (as the reference's
+// gpu_error_count, tensor_algebra_gpu_nvidia.cu:189, counts kernel errors);
+// read on the host by gpu_get_error_count.
+__device__ int g_device_errors = 0;
+
+// Marks the CTA aborted; the first marker counts the CTA in g_device_errors.
+__device__ __forceinline__ void raise_abort(int *abort_flag) {
+  if (atomicExch(abort_flag, 1) == 0) atomicAdd(&g_device_errors, 1);
 }
 
 __device__ __forceinline__ void cp16(uint32_t s, const void *g) {
@@ -156,6 +169,92 @@ __global__ void __launch_bounds__(256) oz_split_rows(const double *__restrict__ 
       const double t = trunc(y);   // in [-127, 127]
       slices[s * plane + r * Kp + k] = (int8_t)(int)t;
       v = y - t;                   // exact remainder, |v| < 1
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Split forms.  The scheme above with the slices stored as int8 digits
+// (kFormInt8, exact int32 accumulation) or as floating-point slices on the
+// bf16, tf32 and e4m3 tensor-core kinds with fp32 accumulation:
+//   x 2^-e = sum_s y_s 2^(-b s) + r,   y_s = round_X(r_s 2^(b s)),
+//   r_{s+1} = r_s - y_s 2^(-b s)  (exact in FP64),
+// b = the significant bits of X (bf16 8, tf32 11, e4m3 4).  The slice pairs
+// with s + t <= S - 1 (0-based) are multiplied, each diagonal g = s + t in its
+// own fp32 accumulator (every bf16/tf32/e4m3 product is exact in fp32; the
+// accumulation rounds), and recombined in FP64 with weights 2^(-b g).  The
+// error is that of the fp32 accumulation plus the dropped pairs (about
+// 2^(-b S)), stated per result by the callers.
+// ---------------------------------------------------------------------------
+enum : int { kFormInt8 = 0, kFormBF16 = 1, kFormTF32 = 2, kFormFP8 = 3 };
+
+__host__ __device__ constexpr int form_esize(int form) { return form == kFormTF32 ? 4 : (form == kFormBF16 ? 2 : 1); }
+__host__ __device__ constexpr int form_bits(int form) {
+  return form == kFormBF16 ? 8 : (form == kFormTF32 ? 11 : (form == kFormFP8 ? 4 : 7));
+}
+
+// Rounds a double of magnitude below about 2 to the slice type; returns the
+// slice's storage bits and its exact value.
+template <int FORM>
+__device__ __forceinline__ uint32_t round_slice(double t, double &val) {
+  if constexpr (FORM == kFormBF16) {
+    const __nv_bfloat16 h = __float2bfloat16_rn((float)t);
+    val = (double)__bfloat162float(h);
+    return (uint32_t)__bfloat16_as_ushort(h);
+  } else if constexpr (FORM == kFormTF32) {
+    // round to 10 stored mantissa bits (ties away from zero); the tensor core
+    // reads only the upper 19 bits of a tf32 operand, so the lower 13 are zero
+    uint32_t u = __float_as_uint((float)t);
+    u = (u + 0x1000u) & ~0x1FFFu;
+    val = (double)__uint_as_float(u);
+    return u;
+  } else {
+    const __nv_fp8_storage_t q = __nv_cvt_float_to_fp8((float)t, __NV_SATFINITE, __NV_E4M3);
+    const __half_raw hr = __nv_cvt_fp8_to_halfraw(q, __NV_E4M3);
+    val = (double)__half2float(__half(hr));
+    return (uint32_t)q;
+  }
+}
+
+// Row split into floating-point slices: one CTA per (padded) row; 256 threads.
+// slices: [S][rows_p][Kp] elements of the form's type.
+template <int FORM>
+__global__ void __launch_bounds__(256) split_rows_float(const double *__restrict__ X, int64_t rows, int64_t K,
+                                                        int64_t rows_p, int64_t Kp, int S,
+                                                        unsigned char *__restrict__ slices, int32_t *expo) {
+  constexpr int ES = form_esize(FORM);
+  constexpr int B = form_bits(FORM);
+  const int64_t r = blockIdx.x;
+  const int tid = threadIdx.x;
+  __shared__ double red[8];
+  __shared__ int e_sh;
+  const double *x = X + r * K;
+  double mx = 0.0;
+  if (r < rows)
+    for (int64_t k = tid; k < K; k += 256) mx = fmax(mx, fabs(x[k]));
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  if ((tid & 31) == 0) red[tid >> 5] = mx;
+  __syncthreads();
+  if (tid == 0) {
+    double m = 0.0;
+    for (int w = 0; w < 8; ++w) m = fmax(m, red[w]);
+    e_sh = (m > 0.0) ? ilogb(m) + 1 : 0;
+    expo[r] = e_sh;
+  }
+  __syncthreads();
+  const int e = e_sh;
+  const int64_t plane = rows_p * Kp;
+  for (int64_t k = tid; k < Kp; k += 256) {
+    double v = (r < rows && k < K) ? scalbn(x[k], -e) : 0.0;  // |v| < 1
+    for (int s = 0; s < S; ++s) {
+      double y;
+      const uint32_t bits = round_slice<FORM>(scalbn(v, B * s), y);
+      unsigned char *dst = slices + (s * plane + r * Kp + k) * ES;
+      if constexpr (ES == 4) *reinterpret_cast<uint32_t *>(dst) = bits;
+      else if constexpr (ES == 2) *reinterpret_cast<uint16_t *>(dst) = (uint16_t)bits;
+      else *dst = (unsigned char)bits;
+      v -= scalbn(y, -B * s);  // exact: y is v 2^(B s) rounded to fewer bits
     }
   }
 }
@@ -342,6 +441,8 @@ __device__ __forceinline__ void tma_load_2d(uint32_t sdst, const CUtensorMap *ma
 }
 
 struct OzWsArgs {
+  uint32_t spin_limit;  // iterations of every bounded mbarrier wait
+  int stall_test;       // 1: the producer issues no copies, so the MMA warp's first wait runs out
   int64_t Mp, Np;
   int tiles_m, tiles_n;
   int group_m;  // m tiles per raster group
@@ -360,17 +461,47 @@ struct OzWsArgs {
 constexpr int kWsBN = 128;                    // tile columns of the pass kernel (UMMA N)
 constexpr int kWsBTile128 = kWsBN * kWsBox;   // 8 KB
 constexpr int kWsDiagPerPass = 3;             // accumulators per pass: 3 x 128 TMEM columns
-constexpr uint32_t kIdescI8N128 = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kWsBN >> 3) << 17) |
-                                  ((uint32_t)(kOzBM >> 4) << 24);
-
-__device__ __forceinline__ void mma_i8_n128(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
-                                            uint32_t accumulate) {
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
-      "l"(adesc), "l"(bdesc), "r"(kIdescI8N128), "r"(accumulate));
-}
+// Instruction descriptors, M = 128, N = 128, K-major A and B: accumulator
+// format (bits 4-5: 1 F32, 2 S32), A/B formats (bits 7-9, 10-12: signed int8
+// 1; bf16 1 and tf32 2 of kind::f16/tf32; e4m3 0 of kind::f8f6f4).
+constexpr uint32_t kIdescMN128 = ((uint32_t)(kWsBN >> 3) << 17) | ((uint32_t)(kOzBM >> 4) << 24);
+template <int FORM> struct FormMma;
+template <> struct FormMma<kFormInt8> {
+  static constexpr uint32_t idesc = (2u << 4) | (1u << 7) | (1u << 10) | kIdescMN128;
+  __device__ static void mma(uint32_t d, uint64_t a, uint64_t b, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d),
+        "l"(a), "l"(b), "r"(idesc), "r"(acc));
+  }
+};
+template <> struct FormMma<kFormBF16> {
+  static constexpr uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | kIdescMN128;
+  __device__ static void mma(uint32_t d, uint64_t a, uint64_t b, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d),
+        "l"(a), "l"(b), "r"(idesc), "r"(acc));
+  }
+};
+template <> struct FormMma<kFormTF32> {
+  static constexpr uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) | kIdescMN128;
+  __device__ static void mma(uint32_t d, uint64_t a, uint64_t b, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d),
+        "l"(a), "l"(b), "r"(idesc), "r"(acc));
+  }
+};
+template <> struct FormMma<kFormFP8> {
+  static constexpr uint32_t idesc = (1u << 4) | (0u << 7) | (0u << 10) | kIdescMN128;
+  __device__ static void mma(uint32_t d, uint64_t a, uint64_t b, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f8f6f4 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d),
+        "l"(a), "l"(b), "r"(idesc), "r"(acc));
+  }
+};
 
 __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
@@ -380,6 +511,7 @@ __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
 // passes of up to three (3 x 128 int32 TMEM columns); pass p streams K once,
 // with only the slices its diagonals use, and its epilogue adds the pass's
 // contribution into D before the next pass reuses the accumulators.
+template <int FORM>
 __global__ void __launch_bounds__(kOzWsThreads, 1)
     oz_gemm_ws_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
                       const OzWsArgs a) {
@@ -432,20 +564,24 @@ __global__ void __launch_bounds__(kOzWsThreads, 1)
   const uint32_t tmem = tmem_base_sh;
   const uint32_t sbase = (smem_u32(smem) + 1023u) & ~1023u;  // swizzled tiles need aligned bases
 
+  const uint32_t lim = a.spin_limit;
+  int64_t issued_all = 0;  // warp 0 lane 0: stage-ring iterations whose copies were issued
   if (warp == 0) {
     if (lane == 0) {
-      int64_t itg = 0;  // stage-ring iteration across passes
-      for (int p = 0; p < npass && !*(volatile int *)&abort_sh; ++p) {
+      int64_t itg = 0;     // stage-ring iteration across passes
+      int64_t issued = 0;  // iterations whose copies were issued
+      for (int p = 0; p < npass && !*(volatile int *)&abort_sh && !a.stall_test; ++p) {
         const int smax = pass_g1(p) - 1;
         const int kper = max(1, S / smax);  // boxes per slice and stage: early passes need fewer slices
         for (int64_t it = 0; it < nbox; it += kper, ++itg) {
           const int nk = (int)min((int64_t)kper, nbox - it);
           const int st = (int)(itg % nst);
-          if (itg >= nst && !mbar_wait(&empty[st], (uint32_t)(((itg / nst) - 1) & 1), a.err)) {
-            atomicExch(&abort_sh, 1);
+          if (itg >= nst && !mbar_wait(&empty[st], (uint32_t)(((itg / nst) - 1) & 1), a.err, lim)) {
+            raise_abort(&abort_sh);
             break;
           }
           if (*(volatile int *)&abort_sh) break;
+          issued = itg + 1;
           mbar_expect_tx(&full[st], (uint32_t)(nk * smax * (kWsATile + kWsBTile128)));
           const uint32_t sst = sbase + (uint32_t)(st * slot_bytes);
           for (int j = 0; j < nk; ++j) {
@@ -459,12 +595,13 @@ __global__ void __launch_bounds__(kOzWsThreads, 1)
           }
         }
       }
+      issued_all = issued;
     }
   } else if (warp == 1) {
     if (lane == 0) {
       int64_t itg = 0;
       for (int p = 0; p < npass; ++p) {
-        if (p > 0 && !mbar_wait(&drained, (uint32_t)((p - 1) & 1), a.err)) atomicExch(&abort_sh, 1);
+        if (p > 0 && !mbar_wait(&drained, (uint32_t)((p - 1) & 1), a.err, lim)) raise_abort(&abort_sh);
         if (*(volatile int *)&abort_sh) {
           mma_commit(&done);
           continue;
@@ -476,8 +613,8 @@ __global__ void __launch_bounds__(kOzWsThreads, 1)
         for (int64_t it = 0; it < nbox; it += kper, ++itg) {
           const int nk = (int)min((int64_t)kper, nbox - it);
           const int st = (int)(itg % nst);
-          if (!mbar_wait(&full[st], (uint32_t)((itg / nst) & 1), a.err)) {
-            atomicExch(&abort_sh, 1);
+          if (!mbar_wait(&full[st], (uint32_t)((itg / nst) & 1), a.err, lim)) {
+            raise_abort(&abort_sh);
             break;
           }
           asm volatile("tcgen05.fence::after_thread_sync;" ::);
@@ -493,8 +630,8 @@ __global__ void __launch_bounds__(kOzWsThreads, 1)
                   const uint32_t sa = sst + (uint32_t)((j * smax + s1 - 1) * kWsATile + kk * kWsBK);
                   const uint32_t sb =
                       sst + (uint32_t)(S * kWsATile + (j * smax + g - s1 - 1) * kWsBTile128 + kk * kWsBK);
-                  mma_i8_n128(dcol, make_desc_sw64(sa), make_desc_sw64(sb),
-                              (it > 0 || j > 0 || kk > 0 || s1 > 1) ? 1u : 0u);
+                  FormMma<FORM>::mma(dcol, make_desc_sw64(sa), make_desc_sw64(sb),
+                                     (it > 0 || j > 0 || kk > 0 || s1 > 1) ? 1u : 0u);
                 }
               }
             }
@@ -511,7 +648,8 @@ __global__ void __launch_bounds__(kOzWsThreads, 1)
     const int em = mrow ? a.ea[m] : 0;
     const int64_t dm = mrow ? a.mD[m] : 0;
     for (int p = 0; p < npass; ++p) {
-      bool ok = mbar_wait(&done, (uint32_t)(p & 1), a.err);
+      bool ok = mbar_wait(&done, (uint32_t)(p & 1), a.err, lim);
+      if (!ok) raise_abort(&abort_sh);
       ok = ok && !*(volatile int *)&abort_sh;
       ok = __all_sync(0xffffffffu, ok);
       asm volatile("tcgen05.fence::after_thread_sync;" ::);
@@ -532,9 +670,17 @@ __global__ void __launch_bounds__(kOzWsThreads, 1)
                   "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
                 : "r"(taddr));
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-            const double w = scalbn(1.0, -7 * g);
+            // diagonal weights: int8 digits 2^(-7 g) (1-based slices); float
+            // slices 2^(-b (g - 2))
+            if constexpr (FORM == kFormInt8) {
+              const double w = scalbn(1.0, -7 * g);
 #pragma unroll
-            for (int i = 0; i < 16; ++i) acc[i] += (double)(int32_t)v[i] * w;
+              for (int i = 0; i < 16; ++i) acc[i] += (double)(int32_t)v[i] * w;
+            } else {
+              const double w = scalbn(1.0, -form_bits(FORM) * (g - 2));
+#pragma unroll
+              for (int i = 0; i < 16; ++i) acc[i] += (double)__uint_as_float(v[i]) * w;
+            }
           }
           if (mrow) {
 #pragma unroll
@@ -557,6 +703,16 @@ __global__ void __launch_bounds__(kOzWsThreads, 1)
   __syncthreads();
   if (warp == 1)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(a.tmem_cols));
+  // After an abort (final once every warp has passed the barrier above), wait
+  // (bounded) until the copies of the last iteration issued into each stage
+  // have landed, so that none is in flight when the CTA exits.
+  if (warp == 0 && lane == 0 && *(volatile int *)&abort_sh) {
+    for (int st = 0; st < nst; ++st) {
+      if (issued_all <= st) continue;
+      const int64_t last = st + ((issued_all - 1 - st) / nst) * nst;
+      mbar_wait(&full[st], (uint32_t)((last / nst) & 1), a.err, lim);
+    }
+  }
 }
 
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no -lcuda).
@@ -621,17 +777,19 @@ struct OzPlan {
   size_t off_A64, off_B64, off_As, off_Bs, off_ea, off_eb, off_tab, off_err, total;
 };
 
-void oz_plan(int64_t M, int64_t N, int64_t K, int S, OzPlan &p) {
+// esize: bytes per slice element; Kp (elements) makes every slice row a whole
+// number of 64-byte blocks.
+void oz_plan(int64_t M, int64_t N, int64_t K, int S, OzPlan &p, int esize = 1) {
   p.M = M; p.N = N; p.K = K;
   p.Mp = round_up(std::max<int64_t>(M, 1), kOzBM);
   p.Np = round_up(std::max<int64_t>(N, 1), 128);  // multiple of both kernels' tile width
-  p.Kp = round_up(std::max<int64_t>(K, 1), kOzBK);
+  p.Kp = round_up(std::max<int64_t>(K, 1), kOzBK / esize);
   size_t off = 0;
   auto take = [&](size_t bytes) { const size_t o = off; off = (off + bytes + 255) & ~size_t(255); return o; };
   p.off_A64 = take((size_t)M * K * 8);
   p.off_B64 = take((size_t)N * K * 8);
-  p.off_As = take((size_t)S * p.Mp * p.Kp);
-  p.off_Bs = take((size_t)S * p.Np * p.Kp);
+  p.off_As = take((size_t)S * p.Mp * p.Kp * esize);
+  p.off_Bs = take((size_t)S * p.Np * p.Kp * esize);
   p.off_ea = take((size_t)p.Mp * 4);
   p.off_eb = take((size_t)p.Np * 4);
   p.off_tab = take(contract_tables_bytes(M, N, K));
@@ -695,6 +853,37 @@ bool has_hyper_index(const int *cptrn, int lrank, int rrank) {
 
 }  // namespace
 
+// A split-form code: the slice count in bits 0-3 (0: the form's default, 6
+// int8 digits or 3 floating-point slices), the form in bits 4-7 (kFormInt8,
+// kFormBF16, kFormTF32, kFormFP8).  A plain slice count 2..7 is the int8 form.
+struct FormCode {
+  int form = kFormInt8, S = 6;
+};
+bool decode_form(int code, FormCode &f) {
+  if (code < 0) return false;
+  f.form = (code >> 4) & 15;
+  f.S = code & 15;
+  if (f.form > kFormFP8 || (code >> 8) != 0) return false;
+  if (f.S == 0) f.S = (f.form == kFormInt8) ? 6 : 3;
+  return f.S >= 2 && f.S <= kOzMaxSlices;
+}
+
+// Failure-detection test hook (tcTestSplitStall): the next split GEMM
+// launches issue no copies and give up their first wait after 4096 polls.
+std::atomic<int> g_stall_test{0};
+
+// K elements per launch of a floating-point form (fp32 accumulation over at
+// most this many products per diagonal before the FP64 sum into D): 0 = all of
+// K; TALSH_B200_SPLIT_FP32_KCHUNK for tuning.
+int64_t fp32_kchunk() {
+  static const int64_t v = [] {
+    const char *e = std::getenv("TALSH_B200_SPLIT_FP32_KCHUNK");
+    const long long c = e ? std::atoll(e) : 0;
+    return (int64_t)(c > 0 ? c : 0);
+  }();
+  return v;
+}
+
 // 0 when the form does not apply: not R8, an operand of rank 0, an invalid
 // pattern or hyper-indices.
 size_t contract_split_scratch(int kind, const int *cptrn, int drank, const int *ddims, int lrank,
@@ -706,11 +895,38 @@ size_t contract_split_scratch(int kind, const int *cptrn, int drank, const int *
   for (int i = 0; i < lrank; ++i) (cptrn[i] > 0 ? M : K) *= ldims[i];
   for (int i = 0; i < rrank; ++i)
     if (cptrn[lrank + i] > 0) N *= rdims[i];
-  if (slices <= 0) slices = 6;
+  FormCode fc;
+  if (!decode_form(slices, fc)) return 0;
   OzPlan p;
-  oz_plan(M, N, K, slices, p);
+  oz_plan(M, N, K, fc.S, p, form_esize(fc.form));
   return p.total;
 }
+
+namespace {
+
+// The warp-specialised GEMM of one form over K-step launches [0, nkb32) in
+// chunks of kc32 steps (32 bytes each).
+template <int FORM>
+int launch_ws_form(const CUtensorMap &mapA, const CUtensorMap &mapB, OzWsArgs w, int64_t nkb32, int64_t kc32,
+                   int accumulative, int stage_bytes, cudaStream_t st) {
+  static std::atomic<uint64_t> ws_attr{0};
+  once_per_device(ws_attr, [] {
+    cudaFuncSetAttribute(oz_gemm_ws_kernel<FORM>, cudaFuncAttributeMaxDynamicSharedMemorySize, kOzWsSmem + 1024);
+  });
+  const int64_t tiles = (int64_t)w.tiles_m * w.tiles_n;
+  for (int64_t kb = 0; kb < nkb32; kb += kc32) {
+    w.kb0 = kb;
+    w.kb1 = std::min(nkb32, kb + kc32);
+    w.beta = (kb == 0) ? (accumulative ? 1 : 0) : 1;
+    oz_gemm_ws_kernel<FORM><<<(unsigned)tiles, kOzWsThreads, w.nst * stage_bytes + 1024, st>>>(mapA, mapB, w);
+    note_launch();
+    const int rc = check_launch("oz_gemm_ws_kernel");
+    if (rc != 0) return rc;
+  }
+  return TALSH_SUCCESS;
+}
+
+}  // namespace
 
 int contract_split_launch(int kind, const int *cptrn, int drank, const int *ddims, int lrank,
                           const int *ldims, int rrank, const int *rdims, void *D, const void *L,
@@ -718,12 +934,15 @@ int contract_split_launch(int kind, const int *cptrn, int drank, const int *ddim
                           size_t scratch_bytes, void *stream) {
   if (kind != R8) return TALSH_NOT_IMPLEMENTED;
   if (lrank == 0 || rrank == 0 || drank == 0) return TALSH_NOT_IMPLEMENTED;
-  if (slices <= 0) slices = 6;
-  if (slices < 2 || slices > kOzMaxSlices) return TALSH_INVALID_ARGS;
+  FormCode fc;
+  if (!decode_form(slices, fc)) return TALSH_INVALID_ARGS;
+  const int code = slices;
+  slices = fc.S;
+  const int es = form_esize(fc.form);
   if (D == nullptr || L == nullptr || R == nullptr || cptrn == nullptr) return TALSH_INVALID_ARGS;
   if (has_hyper_index(cptrn, lrank, rrank)) return TALSH_NOT_IMPLEMENTED;
   if (!elem_aligned(R8, D) || !elem_aligned(R8, L) || !elem_aligned(R8, R)) return TALSH_INVALID_ARGS;
-  const size_t need = contract_split_scratch(kind, cptrn, drank, ddims, lrank, ldims, rrank, rdims, slices);
+  const size_t need = contract_split_scratch(kind, cptrn, drank, ddims, lrank, ldims, rrank, rdims, code);
   if (need == 0 || scratch == nullptr || scratch_bytes < need) return TALSH_INVALID_ARGS;
   cudaStream_t st = (cudaStream_t)stream;
   char *base = (char *)scratch;
@@ -735,7 +954,7 @@ int contract_split_launch(int kind, const int *cptrn, int drank, const int *ddim
     for (int i = 0; i < lrank; ++i) (cptrn[i] > 0 ? M0 : K0) *= ldims[i];
     for (int i = 0; i < rrank; ++i)
       if (cptrn[lrank + i] > 0) N0 *= rdims[i];
-    oz_plan(M0, N0, K0, slices, p);
+    oz_plan(M0, N0, K0, slices, p, es);
   }
   int rc = contract_build_tables(cptrn, drank, ddims, lrank, ldims, rrank, rdims, base + p.off_tab, st, M, N,
                                  K, &mD, &nD);
@@ -753,13 +972,25 @@ int contract_split_launch(int kind, const int *cptrn, int drank, const int *ddim
   int *err = (int *)(base + p.off_err);
   cudaMemsetAsync(err, 0, sizeof(int), st);
   if (p.Mp > 0x7fffffffLL || p.Np > 0x7fffffffLL) return TALSH_LIMIT_EXCEEDED;
-  oz_split_rows<<<(unsigned)p.Mp, 256, 0, st>>>((const double *)(base + p.off_A64), M, K, p.Mp, p.Kp, slices,
-                                                As, ea);
-  note_launch();
-  oz_split_rows<<<(unsigned)p.Np, 256, 0, st>>>((const double *)(base + p.off_B64), N, K, p.Np, p.Kp, slices,
-                                                Bs, eb);
-  note_launch();
-  if ((rc = check_launch("oz_split_rows")) != 0) return rc;
+  const double *A64 = (const double *)(base + p.off_A64), *B64 = (const double *)(base + p.off_B64);
+  auto split_float = [&](auto kern) {
+    kern<<<(unsigned)p.Mp, 256, 0, st>>>(A64, M, K, p.Mp, p.Kp, slices, (unsigned char *)As, ea);
+    note_launch();
+    kern<<<(unsigned)p.Np, 256, 0, st>>>(B64, N, K, p.Np, p.Kp, slices, (unsigned char *)Bs, eb);
+    note_launch();
+  };
+  switch (fc.form) {
+    case kFormBF16: split_float(split_rows_float<kFormBF16>); break;
+    case kFormTF32: split_float(split_rows_float<kFormTF32>); break;
+    case kFormFP8: split_float(split_rows_float<kFormFP8>); break;
+    default:
+      oz_split_rows<<<(unsigned)p.Mp, 256, 0, st>>>(A64, M, K, p.Mp, p.Kp, slices, As, ea);
+      note_launch();
+      oz_split_rows<<<(unsigned)p.Np, 256, 0, st>>>(B64, N, K, p.Np, p.Kp, slices, Bs, eb);
+      note_launch();
+  }
+  if ((rc = check_launch("split rows")) != 0) return rc;
+  const int64_t Kbytes = p.Kp * es;
   // K chunks keep every int32 accumulator exact: slices * Kc * 127^2 < 2^31.
   const int64_t kc_max = ((int64_t)0x7fffffff / ((int64_t)slices * 127 * 127)) / kOzBK;
   const int64_t nkb = p.Kp / kOzBK;
@@ -780,20 +1011,26 @@ int contract_split_launch(int kind, const int *cptrn, int drank, const int *ddim
   // Warp-specialised TMA pipeline when the tensor maps can be encoded (the
   // slice matrices' row counts must fit the 32-bit TMA coordinates).
   CUtensorMap mapA, mapB;
-  const bool ws = !oz_force_simple() && (int64_t)slices * p.Mp < 0x7fffffffLL &&
-                  (int64_t)slices * p.Np < 0x7fffffffLL && make_slice_map(&mapA, As, p.Kp, slices * p.Mp, kOzBM) &&
-                  make_slice_map(&mapB, Bs, p.Kp, slices * p.Np, kWsBN);
+  const bool ws = (!oz_force_simple() || fc.form != kFormInt8) && (int64_t)slices * p.Mp < 0x7fffffffLL &&
+                  (int64_t)slices * p.Np < 0x7fffffffLL &&
+                  make_slice_map(&mapA, As, Kbytes, slices * p.Mp, kOzBM) &&
+                  make_slice_map(&mapB, Bs, Kbytes, slices * p.Np, kWsBN);
+  if (!ws && fc.form != kFormInt8) return TALSH_NOT_IMPLEMENTED;  // the float forms have no simple kernel
   if (ws) {
     const int stage_bytes = slices * (kWsATile + kWsBTile128);
     const int nst = std::max(2, std::min(8, kOzWsSmem / stage_bytes));
-    const int64_t nkb32 = p.Kp / kWsBK, kc32 = kc_max * (kOzBK / kWsBK);
+    const int64_t nkb32 = Kbytes / kWsBK;
+    int64_t kc32 = kc_max * (kOzBK / kWsBK);
+    if (fc.form != kFormInt8) {
+      const int64_t kc_el = fp32_kchunk();
+      kc32 = kc_el > 0 ? std::max<int64_t>(2, round_up(kc_el * es, kOzBK) / kWsBK) : nkb32;
+    }
     const int64_t tiles = (p.Mp / kOzBM) * (p.Np / kWsBN);
     if (tiles > 0x7fffffffLL) return TALSH_LIMIT_EXCEEDED;
-    static std::atomic<uint64_t> ws_attr{0};
-    once_per_device(ws_attr, [] {
-      cudaFuncSetAttribute(oz_gemm_ws_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kOzWsSmem + 1024);
-    });
     OzWsArgs w;
+    const bool stall = g_stall_test.load() != 0;
+    w.spin_limit = stall ? (1u << 12) : kSpinLimit;
+    w.stall_test = stall ? 1 : 0;
     w.Mp = p.Mp; w.Np = p.Np; w.S = slices; w.nst = nst;
     w.tiles_m = (int)(p.Mp / kOzBM);
     w.tiles_n = (int)(p.Np / kWsBN);
@@ -802,15 +1039,12 @@ int contract_split_launch(int kind, const int *cptrn, int drank, const int *ddim
     w.alpha = alpha_re; w.err = err;
     w.tmem_cols = 32;
     while (w.tmem_cols < (uint32_t)(std::min(slices, kWsDiagPerPass) * kWsBN)) w.tmem_cols <<= 1;
-    for (int64_t kb = 0; kb < nkb32; kb += kc32) {
-      w.kb0 = kb;
-      w.kb1 = std::min(nkb32, kb + kc32);
-      w.beta = (kb == 0) ? (accumulative ? 1 : 0) : 1;
-      oz_gemm_ws_kernel<<<(unsigned)tiles, kOzWsThreads, nst * stage_bytes + 1024, st>>>(mapA, mapB, w);
-      note_launch();
-      if ((rc = check_launch("oz_gemm_ws_kernel")) != 0) return rc;
+    switch (fc.form) {
+      case kFormBF16: return launch_ws_form<kFormBF16>(mapA, mapB, w, nkb32, kc32, accumulative, stage_bytes, st);
+      case kFormTF32: return launch_ws_form<kFormTF32>(mapA, mapB, w, nkb32, kc32, accumulative, stage_bytes, st);
+      case kFormFP8: return launch_ws_form<kFormFP8>(mapA, mapB, w, nkb32, kc32, accumulative, stage_bytes, st);
+      default: return launch_ws_form<kFormInt8>(mapA, mapB, w, nkb32, kc32, accumulative, stage_bytes, st);
     }
-    return TALSH_SUCCESS;
   }
   for (int64_t kb = 0; kb < nkb; kb += kc_max) {
     a.kb0 = kb;
@@ -857,8 +1091,8 @@ int contract_split_complex_launch(const int *cptrn, int drank, const int *ddims,
                                   double alpha_re, double alpha_im, int conj_bits, int accumulative, int slices,
                                   void *scratch, size_t scratch_bytes, void *stream) {
   if (lrank == 0 || rrank == 0 || drank == 0) return TALSH_NOT_IMPLEMENTED;
-  if (slices <= 0) slices = 6;
-  if (slices < 2 || slices > kOzMaxSlices) return TALSH_INVALID_ARGS;
+  FormCode fc;
+  if (!decode_form(slices, fc)) return TALSH_INVALID_ARGS;
   int rc = contract_validate(C8, cptrn, drank, ddims, lrank, ldims, rrank, rdims);
   if (rc) return rc;
   if (has_hyper_index(cptrn, lrank, rrank)) return TALSH_NOT_IMPLEMENTED;
@@ -892,9 +1126,20 @@ int contract_split_complex_launch(const int *cptrn, int drank, const int *ddims,
 
 }  // namespace tb
 
+namespace {
+// The int8 form's documented slice argument: 0 (6) or 2..7.
+bool plain_slices_ok(int slices) { return slices == 0 || (slices >= 2 && slices <= tb::kOzMaxSlices); }
+int form_code(int form, int slices) {
+  if (form < tb::kFormInt8 || form > tb::kFormFP8 || slices < 0 || slices > tb::kOzMaxSlices || slices == 1)
+    return -1;
+  return (form << 4) | slices;
+}
+}  // namespace
+
 extern "C" size_t tcTensorContractSplitScratch(int data_kind, const int *cptrn, int drank,
                                                const int *ddims, int lrank, const int *ldims,
                                                int rrank, const int *rdims, int slices) {
+  if (!plain_slices_ok(slices)) return 0;
   if (data_kind == C8)
     return tb::contract_split_complex_scratch(cptrn, drank, ddims, lrank, ldims, rrank, rdims, slices);
   return tb::contract_split_scratch(data_kind, cptrn, drank, ddims, lrank, ldims, rrank, rdims, slices);
@@ -905,10 +1150,53 @@ extern "C" int tcTensorContractSplit(int data_kind, const int *cptrn, int drank,
                                      const void *L, const void *R, double alpha_re, double alpha_im,
                                      int conj_bits, int accumulative, int slices, void *scratch,
                                      size_t scratch_bytes, void *stream) {
+  if (!plain_slices_ok(slices)) return TALSH_INVALID_ARGS;
   if (data_kind == C8)
     return tb::contract_split_complex_launch(cptrn, drank, ddims, lrank, ldims, rrank, rdims, D, L, R, alpha_re,
                                              alpha_im, conj_bits, accumulative, slices, scratch, scratch_bytes,
                                              stream);
   return tb::contract_split_launch(data_kind, cptrn, drank, ddims, lrank, ldims, rrank, rdims, D, L, R,
                                    alpha_re, accumulative, slices, scratch, scratch_bytes, stream);
+}
+
+extern "C" size_t tcTensorContractSplitFormScratch(int data_kind, const int *cptrn, int drank,
+                                                   const int *ddims, int lrank, const int *ldims,
+                                                   int rrank, const int *rdims, int form, int slices) {
+  const int code = form_code(form, slices);
+  if (code < 0) return 0;
+  if (data_kind == C8)
+    return tb::contract_split_complex_scratch(cptrn, drank, ddims, lrank, ldims, rrank, rdims, code);
+  return tb::contract_split_scratch(data_kind, cptrn, drank, ddims, lrank, ldims, rrank, rdims, code);
+}
+
+extern "C" int tcTensorContractSplitForm(int data_kind, const int *cptrn, int drank, const int *ddims,
+                                         int lrank, const int *ldims, int rrank, const int *rdims, void *D,
+                                         const void *L, const void *R, double alpha_re, double alpha_im,
+                                         int conj_bits, int accumulative, int form, int slices, void *scratch,
+                                         size_t scratch_bytes, void *stream) {
+  const int code = form_code(form, slices);
+  if (code < 0) return TALSH_INVALID_ARGS;
+  if (data_kind == C8)
+    return tb::contract_split_complex_launch(cptrn, drank, ddims, lrank, ldims, rrank, rdims, D, L, R, alpha_re,
+                                             alpha_im, conj_bits, accumulative, code, scratch, scratch_bytes,
+                                             stream);
+  return tb::contract_split_launch(data_kind, cptrn, drank, ddims, lrank, ldims, rrank, rdims, D, L, R,
+                                   alpha_re, accumulative, code, scratch, scratch_bytes, stream);
+}
+
+extern "C" int tcTestSplitStall(int enable) {
+  tb::g_stall_test = enable ? 1 : 0;
+  return TALSH_SUCCESS;
+}
+
+// Number of CTAs on the current device that gave up a bounded wait since the
+// library was loaded (reference gpu_get_error_count, device_algebra.h:200,
+// tensor_algebra_gpu_nvidia.cu:2315); -1 when it cannot be read.
+extern "C" int gpu_get_error_count(void) {
+  int v = 0;
+  if (cudaMemcpyFromSymbol(&v, tb::g_device_errors, sizeof(int), 0, cudaMemcpyDeviceToHost) != cudaSuccess) {
+    cudaGetLastError();
+    return -1;
+  }
+  return v;
 }

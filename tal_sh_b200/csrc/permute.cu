@@ -64,7 +64,13 @@ constexpr int kStages = 3;              // tile buffers per CTA of permute_tiled
 #define TB_STAGES_ADD8 3
 #endif
 #ifndef TB_ADD_PREFETCH
-#define TB_ADD_PREFETCH 0
+#define TB_ADD_PREFETCH 1
+#endif
+#ifndef TB_MIN_BLOCKS8
+#define TB_MIN_BLOCKS8 3  // resident CTAs per SM the K = 8 register budget is sized for
+#endif
+#ifndef TB_COPY_INPUT_MAJOR
+#define TB_COPY_INPUT_MAJOR 0  // 1: copies walk their tiles in input order, as adds do
 #endif
 constexpr bool kAddPrefetch = TB_ADD_PREFETCH != 0;
 __host__ __device__ constexpr int reg_stages(int esize, int op) {
@@ -420,7 +426,7 @@ __device__ void build_run_tables(const PermParams &P, int64_t *rIn, int32_t *rC,
 // moves each element with one asynchronous copy in and one shared load plus
 // one (vector) store out; cut-short tiles mask by class.
 template <typename T, int K, int VOUT, int OP, bool SWZ>
-__global__ void __launch_bounds__(kThreads, K <= 4 ? 4 : 3)
+__global__ void __launch_bounds__(kThreads, K <= 4 ? 4 : TB_MIN_BLOCKS8)
     permute_reg_kernel(const T *__restrict__ src, T *dst, const PermParams P) {
   constexpr int KW = K / VOUT;  // write vectors per thread
   constexpr int S = reg_stages((int)sizeof(T), OP);
@@ -843,7 +849,7 @@ int64_t balanced_grow(int64_t ext, int64_t cur) {
 // out_major: tile index order follows the output's dimensions (copies), else
 // the input's (adds, whose output sectors are read before they are written).
 int build_plan(int esize, const Fused &F, Plan &plan, int op = kOpCopy) {
-  const bool out_major = op != kOpAdd;
+  const bool out_major = op != kOpAdd && !TB_COPY_INPUT_MAJOR;
   plan.vol = F.vol;
   if (F.n <= 1) { plan.linear = true; return TALSH_SUCCESS; }
   PermParams &P = plan.P;

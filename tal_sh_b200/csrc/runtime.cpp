@@ -85,6 +85,7 @@ struct GpuCtx {
   double flops = 0.0, bytes = 0.0;
   unsigned long long tasks_ok = 0, tasks_failed = 0, try_later = 0;
   std::vector<cudaEvent_t> event_pool;
+  int device_errors = 0;  // gpu_get_error_count() as last seen
 };
 
 struct Runtime {
@@ -422,6 +423,19 @@ int task_progress(talsh_task_t *task, bool wait) {
   if (tr->finalized) return task->task_error == 0 ? TALSH_TASK_COMPLETED : TALSH_TASK_ERROR;
   cudaSetDevice(tr->gpu);
   cudaError_t e = wait ? cudaEventSynchronize(tr->ev[3]) : cudaEventQuery(tr->ev[3]);
+  if (e == cudaSuccess && tr->split_slices > 0 && !tr->finalized) {
+    // The split GEMM's bounded waits count the CTAs that gave up in a device
+    // counter: a rise since the last look fails the task.
+    const int n = gpu_get_error_count();
+    GpuCtx &G = R.gpu[tr->gpu];
+    if (n > G.device_errors) {
+      G.device_errors = n;
+      note_error_text("split-precision contraction: a bounded wait ran out on the device");
+      tr->failed = 15;
+      task_finalize(task, false);
+      return TALSH_TASK_ERROR;
+    }
+  }
   if (e == cudaSuccess) {
     task_finalize(task, true);
     return task->task_error == 0 ? TALSH_TASK_COMPLETED : TALSH_TASK_ERROR;
@@ -578,7 +592,8 @@ int schedule(OpSpec &op, int dev_id, int dev_kind, talsh_task_t *user_task) {
     const bool split_kind = (dkind == R8 && op.conj == 0) || dkind == C8;
     const size_t split =
         (sl > 0 && split_kind)
-            ? tcTensorContractSplitScratch(dkind, op.dig, op.drank, dd, op.lrank, ld, op.rrank, rd, sl)
+            ? tcTensorContractSplitFormScratch(dkind, op.dig, op.drank, dd, op.lrank, ld, op.rrank, rd, sl >> 4,
+                                               sl & 15)
             : 0;
     bool hyper = false;
     for (int i = 0; i < op.lrank && !hyper; ++i)
@@ -688,9 +703,9 @@ int schedule(OpSpec &op, int dev_id, int dev_kind, talsh_task_t *user_task) {
       case kOpContract: {
         const int *dd = op.t[0]->shape_p->dims, *ld = op.t[1]->shape_p->dims, *rd = op.t[2]->shape_p->dims;
         if (tr->split_slices > 0)
-          rc = tcTensorContractSplit(dkind, op.dig, op.drank, dd, op.lrank, ld, op.rrank, rd, tr->a[0].dptr,
-                                     tr->a[1].dptr, tr->a[2].dptr, op.sr, op.si, op.conj, op.accumulative,
-                                     tr->split_slices, tr->scratch, scratch, st);
+          rc = tcTensorContractSplitForm(dkind, op.dig, op.drank, dd, op.lrank, ld, op.rrank, rd, tr->a[0].dptr,
+                                         tr->a[1].dptr, tr->a[2].dptr, op.sr, op.si, op.conj, op.accumulative,
+                                         tr->split_slices >> 4, tr->split_slices & 15, tr->scratch, scratch, st);
         else
           rc = contract_launch(dkind, op.dig, op.drank, dd, op.lrank, ld, op.rrank, rd, tr->a[0].dptr,
                                tr->a[1].dptr, tr->a[2].dptr, op.sr, op.si, op.conj, op.accumulative,
@@ -1176,6 +1191,7 @@ int talshInit(size_t *host_buf_size, int *host_arg_max, int ngpus, int gpu_list[
     cudaMemGetInfo(&fr, &tot);
     G.budget = env ? (size_t)std::strtoull(env, nullptr, 10) : (fr / 10) * 9;
     G.used = G.peak = 0;
+    G.device_errors = std::max(0, gpu_get_error_count());
     G.in_use = true;
   }
   cudaGetLastError();
@@ -2172,62 +2188,76 @@ size_t xl_bytes(const XLBlock &b, int a, int rank, int es) {
   return v;
 }
 
-// Halves one dimension of a sub-contraction, chosen as the reference's
-// talshTensorOpDecompose2 does (talshc.cpp:3150-3294): the largest batch
-// (hyper) dimension if any, else the largest dimension of the biggest of the
-// right, left and contracted groups.  Returns false when nothing can be split.
+// One index group of a sub-contraction: its volume and its largest extent
+// (the later position on ties), as an operand position.
+struct XLGroup {
+  size_t vol = 1, top = 0;
+  int where = -1;
+  void note(size_t ext, int pos) {
+    vol *= ext;
+    if (ext >= top) { top = ext; where = pos; }
+  }
+};
+
+// Halves one dimension of a sub-contraction.  The choice follows the rule of
+// the reference's talshTensorOpDecompose2 (talshc.cpp:3150-3294), which fixes
+// the order in which partial results are summed: an index present in D, L and
+// R (a batch index) if there is one, the largest; otherwise the largest index
+// of the biggest group, comparing the indices free in R, then free in L, then
+// contracted (ties go to that order).  A batch index is halved in all three
+// blocks, a free index in D and its operand, a contracted index in L and R.
+// Returns false when nothing can be split.
 bool xl_split(const XLBlock &p, const int *dig, int drank, int lrank, int rrank, XLBlock &c1, XLBlock &c2) {
-  size_t lc = 1, ll = 1, lr = 1, lb = 1, sc = 0, sl = 0, sr = 0, sb = 0;
-  int mc = -1, ml = -1, mr = -1, mb = -1;
-  int dst[MAX_TENSOR_RANK] = {0};
+  (void)drank;
+  XLGroup con, left, right, batch;
+  int l_of_d[MAX_TENSOR_RANK] = {0};  // 1 + the L position of each D index that L carries
   for (int i = 0; i < lrank; ++i) {
-    const size_t cd = (size_t)p.dims[1][i];
+    const size_t ext = (size_t)p.dims[1][i];
     if (dig[i] < 0) {
-      lc *= cd;
-      if (cd >= sc) { sc = cd; mc = i; }
+      con.note(ext, i);
     } else if (dig[i] > 0) {
-      dst[dig[i] - 1] = i + 1;
-      ll *= cd;
-      if (cd >= sl) { sl = cd; ml = i; }
+      l_of_d[dig[i] - 1] = i + 1;
+      left.note(ext, i);
     }
   }
-  for (int i = 0; i < rrank; ++i) {
-    const size_t cd = (size_t)p.dims[2][i];
-    const int j = dig[lrank + i];
-    if (j <= 0) continue;
-    if (dst[j - 1] == 0) {
-      lr *= cd;
-      if (cd >= sr) { sr = cd; mr = lrank + i; }
-    } else {  // batch (hyper) index
-      ll /= cd;
-      lb *= cd;
-      if (cd >= sb) { sb = cd; mb = lrank + i; }
+  for (int j = 0; j < rrank; ++j) {
+    const int dpos = dig[lrank + j];
+    if (dpos <= 0) continue;
+    const size_t ext = (size_t)p.dims[2][j];
+    if (l_of_d[dpos - 1] == 0) {
+      right.note(ext, lrank + j);
+    } else {  // in L as well: a batch index, no longer counted as free in L
+      left.vol /= ext;
+      batch.note(ext, lrank + j);
     }
   }
-  if (lb <= 1 && lr <= 1 && ll <= 1 && lc <= 1) return false;
-  int d0 = -1, d1 = -1, d2 = -1;  // split positions in D, L, R (-1: not split)
-  if (lb > 1) {
-    d0 = dig[mb] - 1; d1 = dst[d0] - 1; d2 = mb - lrank;
-  } else if (lr >= ll && lr >= lc) {
-    d0 = dig[mr] - 1; d2 = mr - lrank;
-  } else if (ll >= lr && ll >= lc) {
-    d0 = dig[ml] - 1; d1 = ml;
+  if (batch.vol <= 1 && right.vol <= 1 && left.vol <= 1 && con.vol <= 1) return false;
+  int cut[3] = {-1, -1, -1};  // the halved dimension's position in D, L and R (-1: untouched)
+  if (batch.vol > 1) {
+    cut[0] = dig[batch.where] - 1;
+    cut[1] = l_of_d[cut[0]] - 1;
+    cut[2] = batch.where - lrank;
+  } else if (right.vol >= left.vol && right.vol >= con.vol) {
+    cut[0] = dig[right.where] - 1;
+    cut[2] = right.where - lrank;
+  } else if (left.vol >= right.vol && left.vol >= con.vol) {
+    cut[0] = dig[left.where] - 1;
+    cut[1] = left.where;
   } else {
-    d1 = mc; d2 = -dig[mc] - 1;
+    cut[1] = con.where;
+    cut[2] = -dig[con.where] - 1;
   }
   c1 = p;
   c2 = p;
-  const int at[3] = {d0, d1, d2};
   for (int a = 0; a < 3; ++a) {
-    const int x = at[a];
+    const int x = cut[a];
     if (x < 0) continue;
-    const int h1 = (p.dims[a][x] + 1) / 2, h2 = p.dims[a][x] - h1;
-    if (h2 <= 0) return false;
-    c1.dims[a][x] = h1;
-    c2.dims[a][x] = h2;
-    c2.off[a][x] += h1;
+    const int first = (p.dims[a][x] + 1) / 2, second = p.dims[a][x] - first;
+    if (second <= 0) return false;
+    c1.dims[a][x] = first;
+    c2.dims[a][x] = second;
+    c2.off[a][x] += first;
   }
-  (void)drank;
   return true;
 }
 
@@ -2500,8 +2530,16 @@ double talshTensorImageNorm1_cpu(const talsh_tens_t *t) {
 double talshTensorNorm1(talsh_tens_t *t, int dev_id, int dev_kind) {
   std::lock_guard<std::recursive_mutex> lk(g_mu);
   if (!R.on || t == nullptr || talshTensorIsEmpty(t) != NOPE) return -1.0;
-  double *out = nullptr;
-  if (cudaMallocHost((void **)&out, sizeof(double)) != cudaSuccess) { cudaGetLastError(); return -1.0; }
+  // One pinned result slot for the process, allocated on first use (the call
+  // is blocking and serialised by the library lock).
+  static double *out = nullptr;
+  if (out == nullptr) {
+    if (cudaMallocHost((void **)&out, sizeof(double)) != cudaSuccess) {
+      cudaGetLastError();
+      out = nullptr;
+      return -1.0;
+    }
+  }
   *out = -1.0;
   OpSpec op;
   op.kind = kOpNorm1;
@@ -2510,9 +2548,7 @@ double talshTensorNorm1(talsh_tens_t *t, int dev_id, int dev_kind) {
   op.coh_ctrl = COPY_T;  // a staged copy of a Host image is temporary
   op.norm_out = out;
   const int rc = schedule(op, dev_id, dev_kind, nullptr);
-  const double v = (rc == TALSH_SUCCESS) ? *out : -1.0;
-  cudaFreeHost(out);
-  return v;
+  return (rc == TALSH_SUCCESS) ? *out : -1.0;
 }
 double talshTensorNorm1_(talsh_tens_t *t, int dev_id, int dev_kind) { return talshTensorNorm1(t, dev_id, dev_kind); }
 
@@ -2522,7 +2558,26 @@ int talshContractSlicesSet(int slices) {
   return TALSH_SUCCESS;
 }
 
-int talshContractSlicesGet(void) { return g_r8_slices.load(); }
+int talshContractSlicesGet(void) { return g_r8_slices.load() & 15; }
+
+int talshContractSplitFormSet(int form, int slices) {
+  if (form < 0 || form > 3) return TALSH_INVALID_ARGS;
+  if (slices != 0 && (slices < 2 || slices > 7)) return TALSH_INVALID_ARGS;
+  if (form == 0 && slices == 0) {  // int8 digits at their default count
+    g_r8_slices = 6;
+    return TALSH_SUCCESS;
+  }
+  g_r8_slices = (form << 4) | slices;
+  return TALSH_SUCCESS;
+}
+
+int talshContractSplitFormGet(int *form, int *slices) {
+  if (form == nullptr || slices == nullptr) return TALSH_INVALID_ARGS;
+  const int v = g_r8_slices.load();
+  *form = (v >> 4) & 15;
+  *slices = v & 15;
+  return TALSH_SUCCESS;
+}
 
 }  // extern "C"
 

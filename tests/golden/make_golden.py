@@ -1,7 +1,8 @@
 """Generates the golden fixtures of this directory from the reference sources.
 
-Run in a container where the reference TAL-SH tree is mounted (default path
-/root/reference, override with TALSH_REFERENCE):  python tests/golden/make_golden.py
+Run where the reference TAL-SH tree sits beside the repository (../reference
+relative to the repository root; TALSH_REFERENCE overrides):
+python tests/golden/make_golden.py
 The fixtures are committed; nothing at test time reads the reference.
 
   tensor_contractions.json  the 48 benchmark patterns and shapes of the
@@ -20,8 +21,8 @@ import json
 import os
 import re
 
-REF = os.environ.get("TALSH_REFERENCE", "/root/reference")
 HERE = os.path.dirname(os.path.abspath(__file__))
+REF = os.environ.get("TALSH_REFERENCE") or os.path.normpath(os.path.join(HERE, "..", "..", "..", "reference"))
 
 
 def contractions():
