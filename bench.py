@@ -401,6 +401,9 @@ def contract_summary(con):
         bt = b.get("batched_tuned") or b.get("batched")
         out["C4"] = {"ms": sig(bt.get("ms")), "tasks_per_s": sig(bt.get("tasks_per_s")),
                      "tflops": sig(bt.get("tflops")), "x_per_task": sig(b.get("speedup_tuned", b.get("speedup")))}
+        g = b.get("graph_replay") or {}
+        if "ms" in g:
+            out["C4"]["graph_ms"] = sig(g["ms"])
     sv = con.get("C5_serve") or {}
     c5 = {}
     for k, v in sv.items():
@@ -683,22 +686,28 @@ def main():
     # used and then discarded): L crosses the link once per case.
     e2e = None
     if args.e2e_steps > 0:
-        hl = torch.empty(2 * SLOT, dtype=torch.uint8, pin_memory=True)
-        hd = torch.empty(2 * SLOT, dtype=torch.uint8, pin_memory=True)
+        # Pinned Host regions rotated between consecutive cases (as the device
+        # buffers are), so that one case's tensors do not alias the next one's.
+        HSLOT, NHSLOT = 2 * SLOT, 3
+        hl = torch.empty(NHSLOT * HSLOT, dtype=torch.uint8, pin_memory=True)
+        hd = torch.empty(NHSLOT * HSLOT, dtype=torch.uint8, pin_memory=True)
         hl.view(torch.float32).uniform_(-1.0, 1.0)
         hd.zero_()
         hb, ha = C.c_size_t(0), C.c_int(0)
         rc = L.talshInit(C.byref(hb), C.byref(ha), 1, T.ivec([dev.index or 0]), 0, None, 0, None)
         assert rc in (0, T.TALSH_ALREADY_INITIALIZED), rc
         tens = []
-        for kind, dims, o2n in cases:
+        for ci, (kind, dims, o2n) in enumerate(cases):
             lt = T.Tens(); dt_ = T.Tens()
             L.talshTensorClean(C.byref(lt)); L.talshTensorClean(C.byref(dt_))
             outd = [0] * len(dims)
             for i, p in enumerate(o2n):
                 outd[p - 1] = dims[i]
-            assert L.talshTensorConstruct(C.byref(lt), kind, len(dims), iv(dims), 0, hl.data_ptr(), -1, None, 0.0, 0.0) == 0
-            assert L.talshTensorConstruct(C.byref(dt_), kind, len(dims), iv(outd), 0, hd.data_ptr(), -1, None, 0.0, 0.0) == 0
+            off = (ci % NHSLOT) * HSLOT
+            assert L.talshTensorConstruct(C.byref(lt), kind, len(dims), iv(dims), 0, hl.data_ptr() + off, -1, None,
+                                          0.0, 0.0) == 0
+            assert L.talshTensorConstruct(C.byref(dt_), kind, len(dims), iv(outd), 0, hd.data_ptr() + off, -1, None,
+                                          0.0, 0.0) == 0
             tens.append((lt, dt_, pattern(o2n, False).encode(), pattern(o2n, True).encode()))
         h2d = d2h = 0
         for (kind, dims, o2n) in cases:
@@ -732,7 +741,7 @@ def main():
                     if rc:
                         raise RuntimeError("e2e op failed %d" % rc)
                     inflight.append(tk)
-                    if len(inflight) > 4:
+                    if len(inflight) > 5:
                         finish_oldest()
                     return
 
@@ -775,7 +784,7 @@ def main():
         bound = step_bytes / max(h2d / link["h2d"], d2h / link["d2h"], (h2d + d2h) / link["both"])
         e2e = {"value": whole_job_rate(step_bytes * args.e2e_steps, world, e2e_s) / 1e9, "unit": "GB/s",
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-               "path": "talshTensorCopy COPY_TK + talshTensorAdd COPY_TD, pinned Host, async tasks",
+               "path": "talshTensorCopy COPY_TK + talshTensorAdd COPY_TD, pinned Host (3 rotated regions), async tasks",
                "link_gbs": link, "link_bound_gbs": sig(bound), "steps": args.e2e_steps}
 
     # Contractions (FP64) through talshTensorContract on GPU-resident tensors.
@@ -1148,8 +1157,19 @@ def bench_batch(T, L, torch, dev):
             if rc:
                 raise RuntimeError("task failed %d" % rc)
 
+    # The same batch recorded once as a CUDA graph (descriptors and tables set
+    # up at creation, configurations as concurrent branches) and replayed.
+    gscr = torch.empty(need, dtype=torch.uint8, device=dev)
+    graph = C.c_void_p()
+    grc = L.tcContractBatchGraphCreate(len(tasks), arr, gscr.data_ptr(), need, s, C.byref(graph))
+
+    def replay():
+        if L.tcContractBatchGraphLaunch(graph, s):
+            raise RuntimeError("batch graph replay failed: %s" % L.tcLastErrorString())
+
     res = {}
-    for name, fn in (("batched", batched), ("per_task", per_task)):
+    legs = (("batched", batched), ("per_task", per_task)) + ((("graph_replay", replay),) if grc == 0 else ())
+    for name, fn in legs:
         fn()
         torch.cuda.synchronize(dev)
         reps = 3
@@ -1160,6 +1180,11 @@ def bench_batch(T, L, torch, dev):
         dt = (time.perf_counter() - t0) / reps
         res[name] = {"ms": dt * 1e3, "tasks_per_s": len(tasks) / dt, "tflops": flops / dt / 1e12}
     res["speedup"] = res["per_task"]["ms"] / res["batched"]["ms"]
+    if grc == 0:
+        res["graph_speedup_vs_per_task"] = res["per_task"]["ms"] / res["graph_replay"]["ms"]
+        L.tcContractBatchGraphDestroy(graph)
+    else:
+        res["graph_replay"] = {"error": "create failed %d: %s" % (grc, L.tcLastErrorString())}
     res["config"] = ("4096 tasks, operand ranks 2-6, 1-3 contracted indices, extents log-uniform [4,48], "
                      "R8/C8 alternating, operands <= 2^21 elements (seed 4096); timed host call to completion, "
                      "descriptor upload included")

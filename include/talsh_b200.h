@@ -202,6 +202,21 @@ size_t tcTensorContractBatchScratch(int ntasks, const tcContractTask *tasks);
 int tcTensorContractBatch(int ntasks, const tcContractTask *tasks, void *scratch, size_t scratch_bytes,
                           void *stream);
 
+/* A batch recorded once and replayed: tcContractBatchGraphCreate plans the
+ * tasks, uploads their descriptors into `scratch` (at least
+ * tcTensorContractBatchScratch bytes, owned by the caller and kept for the
+ * graph's life), builds their offset tables (synchronously on `stream`) and
+ * captures the GEMM work in one CUDA graph: the persistent kernels of the tile
+ * configurations (and the single-task fallbacks) run as concurrent branches.
+ * tcContractBatchGraphLaunch replays it on a stream -- the same tasks on the
+ * same operand buffers, whose contents may change between replays.  Results
+ * equal tcTensorContractBatch's bit for bit.  No reference counterpart. */
+typedef struct tcContractBatchGraph tcContractBatchGraph;
+int tcContractBatchGraphCreate(int ntasks, const tcContractTask *tasks, void *scratch, size_t scratch_bytes,
+                               void *stream, tcContractBatchGraph **graph);
+int tcContractBatchGraphLaunch(tcContractBatchGraph *graph, void *stream);
+int tcContractBatchGraphDestroy(tcContractBatchGraph *graph);
+
 /* ---------------------------------------------------------------- serving
  * A contraction server on the current GPU: tasks arrive one by one
  * (tcServerSubmit), wait for admission under a device-memory budget, and run

@@ -237,6 +237,9 @@ _PROTOS = {
     "tcTensorContractSplitScratch": (_Z, [_I, _P(_I), _I, _P(_I), _I, _P(_I), _I, _P(_I), _I]),
     "tcTensorContractBatchScratch": (_Z, [_I, _P(ContractTask)]),
     "tcTensorContractBatch": (_I, [_I, _P(ContractTask), _V, _Z, _V]),
+    "tcContractBatchGraphCreate": (_I, [_I, _P(ContractTask), _V, _Z, _V, _P(_V)]),
+    "tcContractBatchGraphLaunch": (_I, [_V, _V]),
+    "tcContractBatchGraphDestroy": (_I, [_V]),
     "tcPermuteBatchCreate": (_I, [_I, _P(PermuteTask), _I, _P(_V)]),
     "tcPermuteBatchLaunch": (_I, [_V, _V]),
     "tcPermuteBatchDestroy": (_I, [_V]),

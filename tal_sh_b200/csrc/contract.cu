@@ -1087,6 +1087,7 @@ extern "C" size_t tcTensorContractScratch(int data_kind, const int *cptrn, int d
   return tb::contract_scratch_bytes(data_kind, cptrn, drank, ddims, lrank, ldims, rrank, rdims);
 }
 
+
 extern "C" int tcTensorContract(int data_kind, const int *cptrn, int drank, const int *ddims,
                                 int lrank, const int *ldims, int rrank, const int *rdims, void *D,
                                 const void *L, const void *R, double alpha_re, double alpha_im,
@@ -1524,6 +1525,165 @@ extern "C" int tcTensorContractBatch(int ntasks, const tcContractTask *tasks, vo
   const int rc = tb::batch_plan(ntasks, tasks, bp);
   if (rc) return rc;
   return tb::batch_run(ntasks, tasks, bp, scratch, scratch_bytes, nullptr, (cudaStream_t)stream);
+}
+
+// ---------------------------------------------------------------------------
+// Graph-captured batches: the plan, the descriptor upload and the offset
+// tables are done once at creation; the GEMM work is captured in one CUDA
+// graph -- a reset of the work counters, then the persistent kernel of every
+// tile configuration (and the single-task fallbacks) as concurrent branches,
+// so one configuration's tail overlaps the others' work -- and replayed with
+// one launch.  Each tile still runs the code of the single-task kernels, so a
+// replay's results equal tcTensorContractBatch's bit for bit.
+// ---------------------------------------------------------------------------
+struct tcContractBatchGraph {
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int ntasks = 0;
+  unsigned launches = 0;
+};
+
+extern "C" int tcContractBatchGraphCreate(int ntasks, const tcContractTask *tasks, void *scratch,
+                                          size_t scratch_bytes, void *stream, tcContractBatchGraph **out) {
+  using namespace tb;
+  if (out == nullptr) return TALSH_INVALID_ARGS;
+  *out = nullptr;
+  if (ntasks < 1) return TALSH_INVALID_ARGS;
+  BatchPlan bp;
+  int rc = batch_plan(ntasks, tasks, bp);
+  if (rc) return rc;
+  if (scratch == nullptr || scratch_bytes < bp.total) return TALSH_INVALID_ARGS;
+  cudaStream_t st = (cudaStream_t)stream;
+  char *base = (char *)scratch;
+  // Descriptors, lists and prefix sums, then the offset tables, once.
+  int64_t *tabs = (int64_t *)(base + bp.off_tab);
+  int64_t max_entries = 0;
+  for (int t = 0; t < ntasks; ++t) {
+    if (bp.cfg[t] < 0) continue;
+    GemmArgs &a = bp.descs[t].a;
+    int64_t *p = tabs + bp.tab_off[t];
+    a.mL = p; a.mD = p + a.M; a.nR = a.mD + a.M; a.nD = a.nR + a.N; a.kL = a.nD + a.N; a.kR = a.kL + a.K;
+    max_entries = std::max<int64_t>(max_entries, (int64_t)a.M + a.N + a.K);
+  }
+  std::vector<char> host(bp.off_tab, 0);
+  std::memcpy(host.data() + bp.off_desc, bp.descs.data(), sizeof(BatchDesc) * ntasks);
+  for (int c = 0; c < kNumCfg; ++c) {
+    if (bp.list[c].empty()) continue;
+    std::memcpy(host.data() + bp.off_list[c], bp.list[c].data(), sizeof(int32_t) * bp.list[c].size());
+    std::memcpy(host.data() + bp.off_prefix[c], bp.prefix[c].data(), sizeof(int64_t) * bp.prefix[c].size());
+  }
+  cudaError_t e = cudaMemcpyAsync(base, host.data(), bp.off_tab, cudaMemcpyHostToDevice, st);
+  if (e != cudaSuccess) {
+    note_cuda_error("batch graph descriptor upload", (int)e);
+    return TALSH_FAILURE;
+  }
+  if (max_entries > 0) {
+    const int gx = (int)std::max<int64_t>(1, std::min<int64_t>((max_entries + 255) / 256, 64));
+    batch_tables_kernel<<<dim3(gx, ntasks), 256, 0, st>>>((const BatchDesc *)(base + bp.off_desc));
+    note_launch();
+    if ((rc = check_launch("batch_tables_kernel")) != 0) return rc;
+  }
+  if ((e = cudaStreamSynchronize(st)) != cudaSuccess) {  // the host block above goes out of scope
+    note_cuda_error("batch graph setup", (int)e);
+    return TALSH_FAILURE;
+  }
+  // Capture on a private stream: counters reset, then one branch per
+  // configuration and one for the fallbacks, joined at the end.
+  cudaStream_t cs = nullptr;
+  std::vector<cudaStream_t> br;
+  std::vector<cudaEvent_t> ev;
+  cudaGraph_t graph = nullptr;
+  unsigned launches = 0;
+  auto cleanup = [&]() {
+    for (auto x : ev) cudaEventDestroy(x);
+    for (auto x : br) cudaStreamDestroy(x);
+    if (cs) cudaStreamDestroy(cs);
+    cudaGetLastError();
+  };
+  if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess) { cleanup(); return TALSH_FAILURE; }
+  std::vector<int> used;
+  for (int c = 0; c < kNumCfg; ++c)
+    if (!bp.list[c].empty()) used.push_back(c);
+  bool fallbacks = false;
+  for (int t = 0; t < ntasks; ++t) fallbacks = fallbacks || bp.cfg[t] < 0;
+  const int nbr = (int)used.size() + (fallbacks ? 1 : 0);
+  br.assign(nbr, nullptr);
+  ev.assign(nbr + 1, nullptr);
+  for (auto &x : br)
+    if (cudaStreamCreateWithFlags(&x, cudaStreamNonBlocking) != cudaSuccess) { cleanup(); return TALSH_FAILURE; }
+  for (auto &x : ev)
+    if (cudaEventCreateWithFlags(&x, cudaEventDisableTiming) != cudaSuccess) { cleanup(); return TALSH_FAILURE; }
+  if (cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal) != cudaSuccess) { cleanup(); return TALSH_FAILURE; }
+  e = cudaMemsetAsync(base + bp.off_ctr, 0, sizeof(unsigned long long) * kNumCfg, cs);
+  cudaEventRecord(ev[nbr], cs);
+  for (int b = 0; b < nbr; ++b) cudaStreamWaitEvent(br[b], ev[nbr], 0);
+  const unsigned before = (unsigned)tcKernelLaunchCount();
+  for (size_t b = 0; b < used.size() && rc == TALSH_SUCCESS && e == cudaSuccess; ++b) {
+    const int c = used[b];
+    cudaStream_t s2 = br[b];
+    switch (c) {
+      case kCfgD64: rc = launch_dmma_batch<64, 64>(bp, c, base, s2); break;
+      case kCfgD32: rc = launch_dmma_batch<32, 32>(bp, c, base, s2); break;
+      case kCfgZ64: rc = launch_zmma_batch<64, 64>(bp, c, base, s2); break;
+      case kCfgZ32: rc = launch_zmma_batch<32, 32>(bp, c, base, s2); break;
+      case kCfgS4: rc = launch_simt_batch<float>(bp, c, base, s2); break;
+      default: rc = launch_simt_batch<float2>(bp, c, base, s2); break;
+    }
+  }
+  for (int t = 0; t < ntasks && fallbacks && rc == TALSH_SUCCESS && e == cudaSuccess; ++t) {
+    if (bp.cfg[t] >= 0) continue;
+    const tcContractTask &x = tasks[t];
+    rc = contract_launch(x.data_kind, x.cptrn, x.drank, x.ddims, x.lrank, x.ldims, x.rrank, x.rdims, x.D, x.L,
+                         x.R, x.alpha_re, x.alpha_im, x.conj_bits, x.accumulative,
+                         bp.fb_scratch[t] ? base + bp.fb_off[t] : nullptr, bp.fb_scratch[t], (void *)br[nbr - 1]);
+  }
+  launches = (unsigned)tcKernelLaunchCount() - before;
+  for (int b = 0; b < nbr; ++b) {
+    cudaEventRecord(ev[b], br[b]);
+    cudaStreamWaitEvent(cs, ev[b], 0);
+  }
+  const cudaError_t ce = cudaStreamEndCapture(cs, &graph);
+  if (rc == TALSH_SUCCESS && (e != cudaSuccess || ce != cudaSuccess)) {
+    note_cuda_error("batch graph capture", (int)(e != cudaSuccess ? e : ce));
+    rc = TALSH_FAILURE;
+  }
+  cudaGraphExec_t exec = nullptr;
+  if (rc == TALSH_SUCCESS && cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess) {
+    note_error_text("batch graph instantiation failed");
+    rc = TALSH_FAILURE;
+  }
+  cleanup();
+  if (rc != TALSH_SUCCESS) {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    return rc;
+  }
+  tcContractBatchGraph *g = new tcContractBatchGraph();
+  g->graph = graph;
+  g->exec = exec;
+  g->ntasks = ntasks;
+  g->launches = launches;
+  *out = g;
+  return TALSH_SUCCESS;
+}
+
+extern "C" int tcContractBatchGraphLaunch(tcContractBatchGraph *g, void *stream) {
+  if (g == nullptr) return TALSH_INVALID_ARGS;
+  const cudaError_t e = cudaGraphLaunch(g->exec, (cudaStream_t)stream);
+  if (e != cudaSuccess) {
+    tb::note_cuda_error("tcContractBatchGraphLaunch", (int)e);
+    return TALSH_FAILURE;
+  }
+  tb::note_launch(g->launches);
+  return TALSH_SUCCESS;
+}
+
+extern "C" int tcContractBatchGraphDestroy(tcContractBatchGraph *g) {
+  if (g == nullptr) return TALSH_INVALID_ARGS;
+  if (g->exec) cudaGraphExecDestroy(g->exec);
+  if (g->graph) cudaGraphDestroy(g->graph);
+  delete g;
+  return TALSH_SUCCESS;
 }
 
 // Autotuner: for every class present among the tasks, runs that class's tasks

@@ -1339,72 +1339,229 @@ extern "C" int tcPermutePlanInfo(int data_kind, int rank, const int *dims_in, co
 }
 
 // ---------------------------------------------------------------------------
-// Batched transposes (tcPermuteBatch*): many independent transposes and
-// transpose-adds recorded once into a CUDA graph whose branches run
-// concurrently, replayed with one launch.  Each task keeps its own tile plan
-// and kernel instantiation (the plan is chosen per permutation and extents as
-// for a single call); the graph removes the per-call host cost and lets small
-// tasks overlap on the SMs.  No reference counterpart: the reference issues one
-// gpu_tensor_block_copy / _add per call.
+// Batched transposes (tcPermuteBatch*).  Small tasks (up to kPBSmall output
+// elements) run in ONE persistent launch over device-side task descriptors:
+// every task is cut into chunks of kPBChunk output elements, the chunks of all
+// small tasks are numbered through a prefix sum (largest tasks first), and
+// each CTA takes chunk numbers from one atomic counter, finds the task by
+// binary search and writes the chunk's output elements in order (coalesced),
+// gathering each element from its input position (output coordinates by magic
+// division, the input offset as a dot product with the input strides).  The
+// arithmetic of an add is Arith<T>::axpy, as in the tiled kernels, so a
+// task's result does not depend on the path that ran it.  Larger tasks keep
+// their tiled plan (a tcTensorPermute(Add) launch).  Everything is recorded
+// once into a CUDA graph -- counter reset, the persistent launch and the
+// large tasks as concurrent branches -- and replayed with one launch.  No
+// reference counterpart: the reference issues one gpu_tensor_block_copy / _add
+// per call.
 // ---------------------------------------------------------------------------
+namespace tb {
+namespace {
+
+constexpr int64_t kPBSmall = 1 << 18;  // output elements: at most this many run in the persistent launch
+constexpr int64_t kPBChunk = 4096;     // output elements per work item
+constexpr int kPBMaxRank = TC_BATCH_MAX_RANK;
+constexpr int kPBThreads = 256;
+
+struct PBTask {
+  const void *src;
+  void *dst;
+  int64_t first_chunk;     // prefix: first work item of this task
+  int64_t vol;             // elements
+  int rank;                // output dimensions after dropping unit extents
+  int kind, add, conj;
+  double sr, si;
+  int32_t oext[kPBMaxRank];  // output extents, fastest first
+  uint32_t mg[kPBMaxRank], sh[kPBMaxRank];
+  int64_t istr[kPBMaxRank];  // input stride of each output dimension
+};
+
+template <typename T>
+__device__ __forceinline__ void pb_chunk(const PBTask &d, int64_t e0, int64_t e1) {
+  const T *src = (const T *)d.src;
+  T *dst = (T *)d.dst;
+  const bool cj = d.conj != 0;
+  for (int64_t e = e0 + threadIdx.x; e < e1; e += kPBThreads) {
+    uint32_t rem = (uint32_t)e;  // vol < 2^31 for small tasks
+    int64_t in = 0;
+#pragma unroll 1
+    for (int i = 0; i + 1 < d.rank; ++i) {
+      const uint32_t q = fast_div(rem, d.mg[i], d.sh[i]);
+      in += (int64_t)(rem - q * (uint32_t)d.oext[i]) * d.istr[i];
+      rem = q;
+    }
+    if (d.rank > 0) in += (int64_t)rem * d.istr[d.rank - 1];
+    T x = src[in];
+    if (cj) x = Arith<T>::conj(x);
+    if (d.add) dst[e] = Arith<T>::axpy(dst[e], x, d.sr, d.si);
+    else dst[e] = x;
+  }
+}
+
+__global__ void __launch_bounds__(kPBThreads) permute_batch_kernel(const PBTask *tasks, int ntasks,
+                                                                   int64_t nchunks, unsigned long long *ctr) {
+  __shared__ int64_t item_sh;
+  __shared__ int task_sh;
+  __shared__ __align__(16) PBTask d;  // the current task's descriptor
+  for (;;) {
+    if (threadIdx.x == 0) {
+      const int64_t item = (int64_t)atomicAdd(ctr, 1ull);
+      int lo = 0, hi = ntasks - 1;  // last task whose first chunk <= item
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (tasks[mid].first_chunk <= item) lo = mid; else hi = mid - 1;
+      }
+      item_sh = item;
+      task_sh = lo;
+    }
+    __syncthreads();
+    const int64_t item = item_sh;
+    if (item >= nchunks) return;
+    {
+      const uint32_t *from = reinterpret_cast<const uint32_t *>(tasks + task_sh);
+      uint32_t *to = reinterpret_cast<uint32_t *>(&d);
+      for (int w = threadIdx.x; w < (int)(sizeof(PBTask) / 4); w += kPBThreads) to[w] = from[w];
+    }
+    __syncthreads();
+    const int64_t e0 = (item - d.first_chunk) * kPBChunk;
+    const int64_t e1 = min(d.vol, e0 + kPBChunk);
+    switch (d.kind) {
+      case R4: pb_chunk<float>(d, e0, e1); break;
+      case R8: pb_chunk<double>(d, e0, e1); break;
+      case C4: pb_chunk<float2>(d, e0, e1); break;
+      default: pb_chunk<double2>(d, e0, e1); break;
+    }
+    __syncthreads();  // d and item_sh are rewritten for the next item
+  }
+}
+
+}  // namespace
+}  // namespace tb
+
 struct tcPermuteBatch {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
+  void *dev = nullptr;  // descriptors + work counter of the persistent launch
   int ntasks = 0;
+  unsigned launches = 0;
 };
 
 extern "C" int tcPermuteBatchCreate(int ntasks, const tcPermuteTask *tasks, int branches, tcPermuteBatch **out) {
+  using namespace tb;
   if (out == nullptr) return TALSH_INVALID_ARGS;
   *out = nullptr;
   if (ntasks < 1 || tasks == nullptr || branches < 1 || branches > 32) return TALSH_INVALID_ARGS;
-  branches = std::min(branches, ntasks);
-  std::vector<cudaStream_t> st(branches, nullptr);
-  std::vector<cudaEvent_t> ev(branches + 1, nullptr);
+  // Validate every task and split small (persistent launch) from large (tiled plan).
+  std::vector<PBTask> small;
+  std::vector<int> large;
+  for (int t = 0; t < ntasks; ++t) {
+    const tcPermuteTask &x = tasks[t];
+    if (x.rank < 0 || x.rank > TC_BATCH_MAX_RANK) return TALSH_INVALID_ARGS;
+    int rc = validate(x.data_kind, x.rank, x.dims, x.o2n);
+    if (rc) return rc;
+    if (x.src == nullptr || x.dst == nullptr) return TALSH_INVALID_ARGS;
+    if (!elem_aligned(x.data_kind, x.src) || !elem_aligned(x.data_kind, x.dst)) return TALSH_INVALID_ARGS;
+    int64_t vol = 1;
+    for (int i = 0; i < x.rank; ++i) vol *= x.dims[i];
+    if (vol > kPBSmall) { large.push_back(t); continue; }
+    PBTask d;
+    std::memset(&d, 0, sizeof(d));
+    d.src = x.src; d.dst = x.dst; d.vol = vol; d.kind = x.data_kind; d.add = x.add ? 1 : 0;
+    d.conj = kind_is_complex(x.data_kind) ? (x.conj ? 1 : 0) : 0;
+    d.sr = x.alpha_re; d.si = x.alpha_im;
+    if (x.add && !kind_is_complex(x.data_kind)) { d.sr = cmplx8_to_real8(x.alpha_re, x.alpha_im); d.si = 0.0; }
+    // output order (fastest first) of the non-unit input dimensions
+    int n2o[TC_BATCH_MAX_RANK];
+    for (int i = 0; i < x.rank; ++i) n2o[x.o2n[i] - 1] = i;
+    int64_t istr[TC_BATCH_MAX_RANK];
+    int64_t s_ = 1;
+    for (int i = 0; i < x.rank; ++i) { istr[i] = s_; s_ *= x.dims[i]; }
+    int r = 0;
+    for (int k = 0; k < x.rank; ++k) {
+      const int i = n2o[k];
+      if (x.dims[i] == 1) continue;
+      d.oext[r] = x.dims[i];
+      d.istr[r] = istr[i];
+      make_magic((uint32_t)x.dims[i], d.mg[r], d.sh[r]);
+      ++r;
+    }
+    d.rank = r;
+    small.push_back(d);
+  }
+  std::stable_sort(small.begin(), small.end(), [](const PBTask &a, const PBTask &b) { return a.vol > b.vol; });
+  int64_t nchunks = 0;
+  for (PBTask &d : small) { d.first_chunk = nchunks; nchunks += (d.vol + kPBChunk - 1) / kPBChunk; }
+  tcPermuteBatch *b = new tcPermuteBatch();
+  b->ntasks = ntasks;
   int rc = TALSH_SUCCESS;
-  for (int i = 0; i < branches && rc == TALSH_SUCCESS; ++i)
+  const size_t desc_bytes = (sizeof(PBTask) * small.size() + 255) & ~size_t(255);
+  if (!small.empty()) {
+    if (cudaMalloc(&b->dev, desc_bytes + 256) != cudaSuccess ||
+        cudaMemcpy(b->dev, small.data(), sizeof(PBTask) * small.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
+      note_cuda_error("tcPermuteBatchCreate descriptors", (int)cudaGetLastError());
+      rc = TALSH_FAILURE;
+    }
+  }
+  unsigned long long *ctr = b->dev ? (unsigned long long *)((char *)b->dev + desc_bytes) : nullptr;
+  // Capture: counter reset and the persistent launch on stream 0; large tasks
+  // round-robin over the other branches; all joined into stream 0.
+  const int nbr = std::max(1, std::min(branches, 1 + (int)large.size()));
+  std::vector<cudaStream_t> st(nbr, nullptr);
+  std::vector<cudaEvent_t> ev(nbr + 1, nullptr);
+  for (int i = 0; i < nbr && rc == TALSH_SUCCESS; ++i)
     if (cudaStreamCreateWithFlags(&st[i], cudaStreamNonBlocking) != cudaSuccess) rc = TALSH_FAILURE;
-  for (int i = 0; i <= branches && rc == TALSH_SUCCESS; ++i)
+  for (int i = 0; i <= nbr && rc == TALSH_SUCCESS; ++i)
     if (cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming) != cudaSuccess) rc = TALSH_FAILURE;
+  int pb_grid = 1;
+  if (rc == TALSH_SUCCESS && !small.empty()) {
+    int bps = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, permute_batch_kernel, kPBThreads, 0) != cudaSuccess ||
+        bps < 1)
+      bps = 4;
+    pb_grid = (int)std::max<int64_t>(1, std::min<int64_t>(nchunks, (int64_t)current_sm_count() * bps));
+  }
   cudaGraph_t graph = nullptr;
+  const unsigned before = (unsigned)tcKernelLaunchCount();
   if (rc == TALSH_SUCCESS) {
-    // Capture: fork every branch off stream 0, tasks round-robin over the
-    // branches, join back into stream 0.
     if (cudaStreamBeginCapture(st[0], cudaStreamCaptureModeThreadLocal) != cudaSuccess) rc = TALSH_FAILURE;
     if (rc == TALSH_SUCCESS) {
-      cudaEventRecord(ev[branches], st[0]);
-      for (int i = 1; i < branches; ++i) cudaStreamWaitEvent(st[i], ev[branches], 0);
-      for (int t = 0; t < ntasks && rc == TALSH_SUCCESS; ++t) {
-        const tcPermuteTask &x = tasks[t];
-        cudaStream_t s = st[t % branches];
-        rc = x.add ? tcTensorPermuteAdd(x.data_kind, x.rank, x.dims, x.o2n, x.src, x.dst, x.alpha_re, x.alpha_im,
-                                        x.conj, s)
-                   : tcTensorPermute(x.data_kind, x.rank, x.dims, x.o2n, x.src, x.dst, x.conj, s);
+      cudaEventRecord(ev[nbr], st[0]);
+      for (int i = 1; i < nbr; ++i) cudaStreamWaitEvent(st[i], ev[nbr], 0);
+      if (!small.empty()) {
+        cudaMemsetAsync(ctr, 0, sizeof(unsigned long long), st[0]);
+        permute_batch_kernel<<<pb_grid, kPBThreads, 0, st[0]>>>((const PBTask *)b->dev, (int)small.size(), nchunks,
+                                                                ctr);
+        note_launch();
+        rc = check_launch("permute_batch_kernel");
       }
-      for (int i = 1; i < branches; ++i) {
+      for (size_t j = 0; j < large.size() && rc == TALSH_SUCCESS; ++j) {
+        const tcPermuteTask &x = tasks[large[j]];
+        cudaStream_t s2 = st[nbr > 1 ? 1 + (int)(j % (size_t)(nbr - 1)) : 0];
+        rc = x.add ? tcTensorPermuteAdd(x.data_kind, x.rank, x.dims, x.o2n, x.src, x.dst, x.alpha_re, x.alpha_im,
+                                        x.conj, s2)
+                   : tcTensorPermute(x.data_kind, x.rank, x.dims, x.o2n, x.src, x.dst, x.conj, s2);
+      }
+      for (int i = 1; i < nbr; ++i) {
         cudaEventRecord(ev[i], st[i]);
         cudaStreamWaitEvent(st[0], ev[i], 0);
       }
       const cudaError_t e = cudaStreamEndCapture(st[0], &graph);
       if (e != cudaSuccess && rc == TALSH_SUCCESS) {
-        tb::note_cuda_error("tcPermuteBatchCreate capture", (int)e);
+        note_cuda_error("tcPermuteBatchCreate capture", (int)e);
         rc = TALSH_FAILURE;
       }
     }
   }
-  cudaGraphExec_t exec = nullptr;
-  if (rc == TALSH_SUCCESS && cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess) rc = TALSH_FAILURE;
+  b->launches = (unsigned)tcKernelLaunchCount() - before;
+  if (rc == TALSH_SUCCESS && cudaGraphInstantiate(&b->exec, graph, 0) != cudaSuccess) rc = TALSH_FAILURE;
+  b->graph = graph;
   cudaGetLastError();
   for (auto e : ev) if (e) cudaEventDestroy(e);
-  for (auto s : st) if (s) cudaStreamDestroy(s);
+  for (auto s2 : st) if (s2) cudaStreamDestroy(s2);
   if (rc != TALSH_SUCCESS) {
-    if (exec) cudaGraphExecDestroy(exec);
-    if (graph) cudaGraphDestroy(graph);
+    tcPermuteBatchDestroy(b);
     return rc;
   }
-  tcPermuteBatch *b = new tcPermuteBatch();
-  b->graph = graph;
-  b->exec = exec;
-  b->ntasks = ntasks;
   *out = b;
   return TALSH_SUCCESS;
 }
@@ -1416,7 +1573,7 @@ extern "C" int tcPermuteBatchLaunch(tcPermuteBatch *b, void *stream) {
     tb::note_cuda_error("tcPermuteBatchLaunch", (int)e);
     return TALSH_FAILURE;
   }
-  tb::note_launch((unsigned)b->ntasks);
+  tb::note_launch(b->launches);
   return TALSH_SUCCESS;
 }
 
@@ -1424,6 +1581,7 @@ extern "C" int tcPermuteBatchDestroy(tcPermuteBatch *b) {
   if (b == nullptr) return TALSH_INVALID_ARGS;
   if (b->exec) cudaGraphExecDestroy(b->exec);
   if (b->graph) cudaGraphDestroy(b->graph);
+  if (b->dev) cudaFree(b->dev);
   delete b;
   return TALSH_SUCCESS;
 }

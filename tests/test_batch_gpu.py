@@ -207,3 +207,60 @@ def test_autotune_chooses_tiles_and_keeps_results(talsh):
         lib.tcTensorContractBatchTuneReset()
     assert all(lib.tcTensorContractBatchTuned(k, mb, nb) == 0 for k in (T.R8, T.C8) for mb in range(4)
                for nb in range(4))
+
+
+def test_batch_graph_replays_equal_the_batch(talsh):
+    """tcContractBatchGraph: descriptors and tables set up once, the GEMM work
+    captured in one CUDA graph with the tile configurations as concurrent
+    branches; every replay equals tcTensorContractBatch bit for bit, also after
+    the operands' contents change between replays."""
+    torch = pytest.importorskip("torch")
+    lib = T.lib()
+    rng = np.random.default_rng(77)
+    kinds = [T.R8] * 30 + [T.C8] * 20 + [T.R4] * 6 + [T.C4] * 6
+    specs = [random_task(rng, k) for k in kinds]
+    specs.append(dict(kind=T.R8, cptrn=[2, 1], dd=[5, 6], ld=[6, 5], rd=[]))  # scalar operand: single-task path
+    dev = lambda a: torch.from_numpy(np.asarray(a).ravel(order="F").copy()).cuda()
+    s = torch.cuda.current_stream().cuda_stream
+
+    def make(out):
+        tasks = (T.ContractTask * len(specs))()
+        for t, sp, (l, r, d) in zip(tasks, specs, out):
+            t.data_kind, t.drank, t.lrank, t.rrank = sp["kind"], len(sp["dd"]), len(sp["ld"]), len(sp["rd"])
+            for i, v in enumerate(sp["cptrn"]):
+                t.cptrn[i] = v
+            for arr, name in ((sp["dd"], "ddims"), (sp["ld"], "ldims"), (sp["rd"], "rdims")):
+                for i, v in enumerate(arr):
+                    getattr(t, name)[i] = v
+            t.D, t.L, t.R = d.data_ptr(), l.data_ptr(), r.data_ptr()
+            t.alpha_re, t.alpha_im = (0.5, 0.0) if sp["kind"] in (T.R4, T.R8) else (0.5, -0.25)
+            t.conj_bits, t.accumulative = 0, 0
+        return tasks
+
+    ops = [(dev(rnd(rng, sp["ld"], sp["kind"])), dev(rnd(rng, sp["rd"], sp["kind"])),
+            dev(rnd(rng, sp["dd"] if sp["dd"] else [1], sp["kind"]))) for sp in specs]
+    ref_d = [torch.empty_like(d) for _, _, d in ops]
+    tasks_g = make(ops)
+    tasks_r = make([(l, r, d2) for (l, r, _), d2 in zip(ops, ref_d)])
+    need = lib.tcTensorContractBatchScratch(len(specs), tasks_g)
+    sc_g = torch.empty(need, dtype=torch.uint8, device="cuda")
+    sc_r = torch.empty(need, dtype=torch.uint8, device="cuda")
+    g = C.c_void_p()
+    assert lib.tcContractBatchGraphCreate(len(specs), tasks_g, sc_g.data_ptr(), need, s, C.byref(g)) == 0, \
+        lib.tcLastErrorString()
+    try:
+        for rep in range(3):
+            if rep == 2:  # new operand contents, same buffers
+                for l, r, _ in ops:
+                    l.mul_(-1.5)
+            assert lib.tcContractBatchGraphLaunch(g, s) == 0
+            assert lib.tcTensorContractBatch(len(specs), tasks_r, sc_r.data_ptr(), need, s) == 0
+            torch.cuda.synchronize()
+            for sp, (_, _, d), d2 in zip(specs, ops, ref_d):
+                assert torch.equal(d, d2), (rep, sp)
+    finally:
+        assert lib.tcContractBatchGraphDestroy(g) == 0
+    bad = C.c_void_p()
+    assert lib.tcContractBatchGraphCreate(0, tasks_g, sc_g.data_ptr(), need, s, C.byref(bad)) == T.TALSH_INVALID_ARGS
+    assert lib.tcContractBatchGraphCreate(len(specs), tasks_g, sc_g.data_ptr(), 16, s, C.byref(bad)) == \
+        T.TALSH_INVALID_ARGS

@@ -1,5 +1,7 @@
-"""Graph-captured batched transposes (tcPermuteBatch*): every task of a batch of
-uneven ranks, extents and kinds equals the oracle bit for bit after each replay."""
+"""Batched transposes (tcPermuteBatch*): small tasks in one persistent launch
+over device-side descriptors, larger ones with their tiled plan, all replayed
+from one CUDA graph; every task of a batch of uneven ranks, extents and kinds
+equals the oracle bit for bit after each replay."""
 import numpy as np
 import pytest
 
@@ -22,15 +24,22 @@ def _task(rng):
     return kind, dims, o2n, add, conj, alpha
 
 
-def test_batched_transposes_bit_exact(talsh):
+# Two tasks above the persistent launch's size limit (2^18 elements), which
+# keep their tiled plan in a branch of the same graph.
+LARGE = [(T.R8, [65, 3, 1500], [3, 1, 2], True, False, (0.5, 0.0)),
+         (T.C4, [700, 2, 300], [2, 3, 1], False, True, (1.0, 0.0))]
+
+
+@pytest.mark.parametrize("with_large", [False, True])
+def test_batched_transposes_bit_exact(talsh, with_large):
     torch = pytest.importorskip("torch")
     lib = T.lib()
     rng = np.random.default_rng(77)
-    n = 40
+    n = 40 + (len(LARGE) if with_large else 0)
     arr = (T.PermuteTask * n)()
     keep = []
     for t, x in zip(arr, range(n)):
-        kind, dims, o2n, add, conj, alpha = _task(rng)
+        kind, dims, o2n, add, conj, alpha = LARGE[x - 40] if x >= 40 else _task(rng)
         src = rand(dims, kind, rng)
         d0 = rand(O.out_dims(dims, o2n), kind, rng)
         s = torch.from_numpy(src.ravel(order="F").copy()).cuda()
