@@ -252,11 +252,10 @@ def run_cpu_baseline(cases, slices=4):
     del cs
     con = cpu_contract_rates()
     return {"value": nbytes / secs / 1e9, "unit": "GB/s", "cores": os.cpu_count() or 1, "kind": "port",
-            "sample": "%d of the %d sweep cases at full size (every %dth), each a transpose and a "
-                      "transpose-add: the oracle's cache-blocked OpenMP transpose and blocked add restating "
-                      "the reference CPU path, %.1f GB in %.2f s" % (len(idx), len(cases), slices, nbytes / 1e9, secs),
+            "sample": "%d of %d sweep cases (every %dth), full size, transpose + add, oracle blocked OpenMP "
+                      "path, %.1f GB in %.2f s" % (len(idx), len(cases), slices, nbytes / 1e9, secs),
             "contract_tflops": {k: round(v["tflops"], 4) for k, v in con.items()},
-            "contract_path": "TTGT: blocked transposes + OpenBLAS DGEMM (scipy) on all cores"}
+            "contract_path": "TTGT, blocked transposes + OpenBLAS DGEMM"}
 
 
 # ----------------------------------------------------------------- GPU side
@@ -784,7 +783,7 @@ def main():
         bound = step_bytes / max(h2d / link["h2d"], d2h / link["d2h"], (h2d + d2h) / link["both"])
         e2e = {"value": whole_job_rate(step_bytes * args.e2e_steps, world, e2e_s) / 1e9, "unit": "GB/s",
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-               "path": "talshTensorCopy COPY_TK + talshTensorAdd COPY_TD, pinned Host (3 rotated regions), async tasks",
+               "path": "talshTensorCopy COPY_TK + talshTensorAdd COPY_TD, pinned Host, async tasks",
                "link_gbs": link, "link_bound_gbs": sig(bound), "steps": args.e2e_steps}
 
     # Contractions (FP64) through talshTensorContract on GPU-resident tensors.

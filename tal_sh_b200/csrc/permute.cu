@@ -108,6 +108,9 @@ struct PermParams {
   int ta_rem, tb_rem; // extents of the last (cut-short) tile along a_last / b_last
   int pre_bA, pre_aB; // tile volume of A below b_last (b_last in A) / of B before a_last (a_last in B)
   int buf_elems;      // elements per tile buffer (whole 128-byte rows)
+  int bulk;           // 1: permute_bulk_kernel (input runs moved by bulk copies)
+  int pitch_b;        // bulk form: bytes between the rows of a tile buffer (a multiple of 16)
+  uint32_t mg_lip, sh_lip;  // magic divisor of Li_pad
   int64_t num_tiles;
   double s_re, s_im;
   const void *sdev;  // optional device scalar multiplying the scale (rank-0 operand)
@@ -603,6 +606,252 @@ __global__ void __launch_bounds__(kThreads, K <= 4 ? 4 : TB_MIN_BLOCKS8)
   }
 }
 
+// Bulk-read form of permute_reg_kernel.  Instead of one 4- or 8-byte
+// asynchronous copy per element (which makes short runs fetch well beyond
+// their bytes through the L1), every input run of a tile is moved by one bulk
+// copy (cp.async.bulk, the TMA engine) of its 16-byte-aligned cover
+// [floor16(start), ceil16(end)): the sectors read are the run's own.  Row r of
+// a stage starts at r * pitch (a multiple of 16 bytes); the run's first element
+// lands at byte (start mod 16) of its row.  That shift is the tile's
+// (src + in_base * esize) mod 16 plus the run's (rIn * esize) mod 16, so each
+// write slot keeps its row offset and the run's residue (4 bits) in registers
+// and adds the tile's residue.  A stage is complete when its mbarrier has seen
+// every thread arrive (with the byte count of the runs it copies) and every
+// byte land; each wait is bounded, counting a CTA that gives up in
+// g_permute_errors.  Writes, D prefetch and arithmetic are those of
+// permute_reg_kernel, so results are bit-identical.
+__device__ int g_permute_errors = 0;
+
+__device__ __forceinline__ void mbar_init_s(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"((uint32_t)__cvta_generic_to_shared(bar)), "r"(count));
+}
+__device__ __forceinline__ void mbar_arrive_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(
+                   (uint32_t)__cvta_generic_to_shared(bar)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_s(uint64_t *bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.b32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(ok)
+      : "r"((uint32_t)__cvta_generic_to_shared(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ void bulk_g2s(uint32_t sdst, const void *gsrc, uint32_t bytes, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(sdst),
+      "l"(gsrc), "r"(bytes), "r"((uint32_t)__cvta_generic_to_shared(bar))
+      : "memory");
+}
+
+constexpr int kBulkRunsPerThread = kMaxRuns / kThreads;  // runs a thread issues per tile (Ri <= kMaxRuns)
+constexpr uint32_t kBulkSpin = 1u << 20;                 // bounded waits (about a second at most)
+
+template <typename T, int K, int VOUT, int OP>
+__global__ void __launch_bounds__(kThreads, K <= 4 ? 4 : 3)
+    permute_bulk_kernel(const T *__restrict__ src, T *dst, const PermParams P) {
+  constexpr int KW = K / VOUT;
+  constexpr int S = reg_stages((int)sizeof(T), OP);
+  constexpr bool DPF = OP == kOpAdd && kAddPrefetch;
+  constexpr uint32_t ES = (uint32_t)sizeof(T);
+  using V = Pack<T, VOUT>;
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ TileSetup setup[kRing];
+  __shared__ DimS dimS[kMaxFR];
+  __shared__ __align__(8) uint64_t full[S];
+  const int tid = threadIdx.x;
+  const int64_t G = gridDim.x;
+
+  int32_t wg[KW];
+  uint32_t ws2[K / 2];  // row offset + element offset (bytes, 16-bit pairs)
+  uint32_t wnib = 0;    // per write element: (rIn * esize) mod 16 of its run (4 bits)
+  uint32_t wcls = 0;
+  int32_t my_rin[kBulkRunsPerThread], my_rc[kBulkRunsPerThread];
+  auto half = [](const uint32_t *a, int i) -> uint32_t { return (i & 1) ? (a[i >> 1] >> 16) : (a[i >> 1] & 0xffffu); };
+  {
+    int64_t *rIn = reinterpret_cast<int64_t *>(smem + P.off_rin);
+    int32_t *rC = reinterpret_cast<int32_t *>(smem + P.off_rc);
+    int64_t *wOut = reinterpret_cast<int64_t *>(smem + P.off_wout);
+    int32_t *wSm = reinterpret_cast<int32_t *>(smem + P.off_wsm);
+    int32_t *wC = reinterpret_cast<int32_t *>(smem + P.off_wc);
+    int32_t *ySm = reinterpret_cast<int32_t *>(smem + P.off_ysm);
+    build_run_tables<kThreads>(P, rIn, rC, wOut, wSm, wC, ySm);
+    if (tid < P.rank) {
+      DimS d;
+      d.istr = P.istr[tid];
+      d.ostr = P.ostr[tid];
+      d.ext = P.ext[tid];
+      d.tl = P.tl[tid];
+      d.nt = (int32_t)P.ntile[tid];
+      d.mg_ts = P.mg_ts[tid];
+      d.sh_ts = P.sh_ts[tid];
+      d.mg_nt = P.mg_nt[tid];
+      d.sh_nt = P.sh_nt[tid];
+      dimS[tid] = d;
+    }
+    if (tid < S) mbar_init_s(&full[tid], kThreads);
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < kBulkRunsPerThread; ++j) {
+      const int r = tid + j * kThreads;
+      my_rin[j] = r < P.Ri ? (int32_t)rIn[r] : 0;
+      my_rc[j] = r < P.Ri ? rC[r] : 0;
+    }
+    auto cls_of = [&](int ca, int cb) -> uint32_t {
+      return (ca >= P.ta_rem ? 1u : 0u) | (cb >= P.tb_rem ? 2u : 0u);
+    };
+    const int nv = P.nv, total = P.Ro * nv;
+#pragma unroll
+    for (int k = 0; k < KW; ++k) {
+      const int f = tid + k * kThreads;
+      wg[k] = 0;
+#pragma unroll
+      for (int j = 0; j < VOUT; ++j)
+        if (((k * VOUT + j) & 1) == 0) ws2[(k * VOUT + j) >> 1] = 0;
+      uint32_t c = 4u;
+      if (f < total) {
+        const int r = (int)fast_div((uint32_t)f, P.mg_nv, P.sh_nv);
+        const int y = (f - r * nv) * VOUT;
+        wg[k] = (int32_t)(wOut[r] + y);
+#pragma unroll
+        for (int j = 0; j < VOUT; ++j) {
+          const int yj = y + j;
+          const int p = wSm[r] + (P.ytab ? ySm[yj] : decompose(P.ymap, (uint32_t)yj).soff);  // r_in * Li_pad + x
+          const int rr = (int)fast_div((uint32_t)p, P.mg_lip, P.sh_lip), x = p - rr * P.Li_pad;
+          const uint32_t off = (uint32_t)rr * (uint32_t)P.pitch_b + (uint32_t)x * ES;
+          ws2[(k * VOUT + j) >> 1] |= off << (16 * ((k * VOUT + j) & 1));
+          wnib |= (uint32_t)((rIn[rr] * (int64_t)ES) & 15) << (4 * (k * VOUT + j));
+        }
+        const int cb = y / P.b_pre;
+        const int ca = P.a_in_B ? (y / P.pre_aB) % P.tl[P.a_last] : wC[r];
+        c = cls_of(ca, cb);
+      }
+      wcls |= c << (3 * k);
+    }
+    __syncthreads();  // the run tables' space becomes tile buffers
+    // The stage buffers were just written through the generic proxy; the bulk
+    // copies write them through the async proxy.
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  fill_setups(P, dimS, 0, setup);
+  fill_setups(P, dimS, 32, setup);
+  __syncthreads();
+
+  const bool cj = P.conj != 0;
+  double sr = P.s_re, si = P.s_im;
+  effective_scale<T>(P.sdev, P.sdev_kind, P.sdev_conj, sr, si);
+  const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(smem);
+  const uint32_t stage_bytes = (uint32_t)P.buf_elems * ES;
+  constexpr uint32_t kSlotStage = (uint32_t)(KW * kThreads * sizeof(V));
+  const uint32_t dbase = sbase + (uint32_t)S * stage_bytes + (uint32_t)tid * (uint32_t)sizeof(V);
+  const unsigned char *dslots = smem + (size_t)S * stage_bytes + (size_t)tid * sizeof(V);
+  const uintptr_t src_addr = reinterpret_cast<uintptr_t>(src);
+  bool failed = false;
+
+  auto issue_loads = [&](const TileSetup &St, int stage) {
+    const uintptr_t gbase = src_addr + (uintptr_t)St.in_base * ES;
+    const uint32_t sb = sbase + (uint32_t)stage * stage_bytes;
+    const uint32_t len = (uint32_t)St.li_act * ES;
+    uint32_t bytes = 0;
+#pragma unroll
+    for (int j = 0; j < kBulkRunsPerThread; ++j) {
+      const int r = tid + j * kThreads;
+      if (r < P.Ri && (P.b_in_A || my_rc[j] < St.tb_lim)) {
+        const uintptr_t a0 = gbase + (uintptr_t)(int64_t)my_rin[j] * ES;
+        bytes += (uint32_t)(((a0 + len + 15) & ~(uintptr_t)15) - (a0 & ~(uintptr_t)15));
+      }
+    }
+    mbar_arrive_tx(&full[stage], bytes);
+#pragma unroll
+    for (int j = 0; j < kBulkRunsPerThread; ++j) {
+      const int r = tid + j * kThreads;
+      if (r < P.Ri && (P.b_in_A || my_rc[j] < St.tb_lim)) {
+        const uintptr_t a0 = gbase + (uintptr_t)(int64_t)my_rin[j] * ES;
+        const uintptr_t lo = a0 & ~(uintptr_t)15;
+        const uint32_t n = (uint32_t)(((a0 + len + 15) & ~(uintptr_t)15) - lo);
+        bulk_g2s(sb + (uint32_t)r * (uint32_t)P.pitch_b, reinterpret_cast<const void *>(lo), n, &full[stage]);
+      }
+    }
+    if constexpr (DPF) {
+      const T *gd = dst + St.out_base;
+      const uint32_t db = dbase + (uint32_t)stage * kSlotStage;
+      const uint32_t m = (uint32_t)St.type | 4u;
+#pragma unroll
+      for (int k = 0; k < KW; ++k)
+        if (((wcls >> (3 * k)) & m) == 0)
+          cp_async_s<sizeof(V)>(db + (uint32_t)(k * kThreads) * (uint32_t)sizeof(V), gd + wg[k]);
+    }
+  };
+
+  int64_t t = blockIdx.x;
+#pragma unroll
+  for (int k = 0; k < S - 1; ++k) {
+    if (t + k * G < P.num_tiles) issue_loads(setup[k], k);
+    cp_async_commit();
+  }
+  for (int iter = 0; t < P.num_tiles; t += G, ++iter) {
+    const int64_t tn = t + (S - 1) * G;
+    if (tn < P.num_tiles) issue_loads(setup[(iter + S - 1) % kRing], (iter + S - 1) % S);
+    cp_async_commit();
+    if ((iter & 31) == 0 && iter > 0) fill_setups(P, dimS, iter + 32, setup);
+    cp_async_wait<S - 1>();
+    if (!failed) {  // after one wait has run out the CTA stops waiting and only finishes its loop
+      const uint32_t parity = (uint32_t)((iter / S) & 1);
+      uint32_t n = 0;
+      while (!mbar_try_s(&full[iter % S], parity))
+        if (++n == kBulkSpin) { failed = true; break; }
+    }
+    __syncthreads();
+    const TileSetup St = setup[iter % kRing];
+    const char *sbytes = reinterpret_cast<const char *>(smem) + (size_t)(iter % S) * stage_bytes;
+    const uint32_t tnib = (uint32_t)((src_addr + (uintptr_t)St.in_base * ES) & 15);
+    T *g = dst + St.out_base;
+    const uint32_t m = (uint32_t)St.type | 4u;
+    const unsigned char *ds = dslots + (size_t)(iter % S) * kSlotStage;
+    constexpr int WB = KW < 4 ? KW : 4;
+#pragma unroll
+    for (int c0 = 0; c0 < KW; c0 += WB) {
+      Pack<T, VOUT> v[WB];
+      T *gp[WB];
+      bool ok[WB];
+#pragma unroll
+      for (int u = 0; u < WB; ++u) {
+        const int k = c0 + u;
+        ok[u] = ((wcls >> (3 * k)) & m) == 0;
+        gp[u] = g + wg[k];
+        if (ok[u]) {
+#pragma unroll
+          for (int j = 0; j < VOUT; ++j) {
+            const int e = k * VOUT + j;
+            const uint32_t shift = (tnib + ((wnib >> (4 * e)) & 15u)) & 15u;
+            const T x = *reinterpret_cast<const T *>(sbytes + half(ws2, e) + shift);
+            v[u].v[j] = cj ? Arith<T>::conj(x) : x;
+          }
+        }
+      }
+      if constexpr (DPF) {
+#pragma unroll
+        for (int u = 0; u < WB; ++u) {
+          if (!ok[u]) continue;
+          V d = *reinterpret_cast<const V *>(ds + (size_t)((c0 + u) * kThreads) * sizeof(V));
+#pragma unroll
+          for (int j = 0; j < VOUT; ++j) d.v[j] = Arith<T>::axpy(d.v[j], v[u].v[j], sr, si);
+          st_pack<T, VOUT>(gp[u], d);
+        }
+      } else {
+        emit_masked<T, VOUT, OP, WB>(gp, v, ok, sr, si);
+      }
+    }
+    __syncthreads();
+  }
+  if (failed) atomicAdd(&g_permute_errors, 1);
+}
+
 // Transpose / transpose-add for plans whose tiles span more than 32-bit
 // offsets (tensors of more than 2^31 elements): positions come from the
 // shared run tables (64-bit offsets) for every element.
@@ -809,6 +1058,24 @@ int reg_k(int esize) {
   }
   if (esize >= 16) return 4;
   return forced ? forced : 8;
+}
+
+// Where the bulk-read form of the register-table kernel runs: by default for
+// elements of 8 bytes or more, copies and scalar-output adds (measured on the
+// transpose/add sweep: 4-byte elements lose to bank conflicts in the 16-byte
+// aligned rows, vector-output adds lose a little); TALSH_B200_PERMUTE_BULK=1
+// selects it for every plan it can take, 0 for none.
+int permute_bulk_mode() {
+  static const int v = [] {
+    const char *e = std::getenv("TALSH_B200_PERMUTE_BULK");
+    return e ? (std::atoi(e) != 0 ? 1 : 0) : 2;
+  }();
+  return v;
+}
+bool permute_bulk_wanted(int esize, int op, int vout) {
+  const int mode = permute_bulk_mode();
+  if (mode != 2) return mode == 1;
+  return esize >= 8 && (op != kOpAdd || vout == 1);
 }
 
 // Tile buffer budget in bytes: kTileBytes, or TALSH_B200_TILE_BYTES (4096..49152) for tuning.
@@ -1102,7 +1369,22 @@ int build_plan(int esize, const Fused &F, Plan &plan, int op = kOpCopy) {
   }();
   P.reg = (!force_generic && span_in < INT_MAX && span_out < INT_MAX && P.V <= kThreads * reg_k(esize)) ? 1 : 0;
   const int stages = P.reg ? reg_stages(esize, op) : kStages;
-  size_t bufs = (size_t)stages * buf_elems * esize;
+  // Bulk-read form: rows of pitch_b bytes (16-byte aligned, an odd number of
+  // 16-byte units), each holding a run's 16-byte-aligned cover.
+  P.bulk = 0;
+  if (P.reg && permute_bulk_wanted(esize, op, plan.vout)) {
+    int pitch = (int)(((int64_t)P.Li * esize + 15 + 15) / 16 * 16);
+    if ((pitch / 16) % 2 == 0) pitch += 16;
+    const int64_t stage_b = ((int64_t)P.Ri * pitch + 127) / 128 * 128;
+    if (stage_b + 16 < 65536) {
+      P.bulk = 1;
+      P.pitch_b = pitch;
+      P.buf_elems = (int)(stage_b / esize);
+      make_magic((uint32_t)P.Li_pad, P.mg_lip, P.sh_lip);
+    }
+  }
+  const size_t stage_elems = (size_t)P.buf_elems;
+  size_t bufs = (size_t)stages * stage_elems * esize;
   if (P.reg && op == kOpAdd && kAddPrefetch) {
     const int kreg = (P.V <= kThreads * 4) ? 4 : 8;  // the K permute_reg_kernel is launched with
     bufs += (size_t)stages * kreg * kThreads * esize;
@@ -1207,6 +1489,17 @@ int launch_typed(const Plan &plan, const void *src, void *dst, int conj, const S
     const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(P.num_tiles, (int64_t)sms * bps));
     kern<<<grid, kThreads, plan.smem, st>>>((const T *)src, (T *)dst, P);
   };
+  if (P.reg && P.bulk) {
+    auto run_b = [&](auto kc) {
+      constexpr int K = decltype(kc)::value;
+      if (vout > 1) run(permute_bulk_kernel<T, K, VEC, OP>);
+      else run(permute_bulk_kernel<T, K, 1, OP>);
+    };
+    if (P.V <= kThreads * 4) run_b(std::integral_constant<int, 4>{});
+    else run_b(std::integral_constant<int, 8>{});
+    note_launch();
+    return check_launch("permute_bulk_kernel");
+  }
   if (P.reg) {
     auto run_k = [&](auto kc) {
       constexpr int K = decltype(kc)::value;

@@ -78,7 +78,10 @@ struct PendingWrite {
 struct GpuCtx {
   bool in_use = false;
   cudaStream_t stream = nullptr;  // compute (and all work of operations without staging)
-  cudaStream_t h2d = nullptr;     // staging copies into the GPU
+  cudaStream_t h2d = nullptr;     // staging copies into the GPU (even tasks)
+  cudaStream_t h2d_b = nullptr;   // staging copies of odd tasks: one task's wait for a copy back
+                                  // does not hold up the next task's uploads
+  unsigned staged = 0;            // tasks staged so far (picks the staging stream)
   cudaStream_t d2h = nullptr;     // copies back out of the GPU
   std::vector<PendingWrite> pending;
   size_t budget = 0, used = 0, peak = 0;
@@ -222,10 +225,11 @@ void sync_pending(const void *p, size_t n) {
   }
 }
 
-// Waits for everything queued on the GPU's three streams.
+// Waits for everything queued on the GPU's streams.
 void sync_gpu_streams(int gpu) {
   GpuCtx &G = R.gpu[gpu];
   cudaStreamSynchronize(G.h2d);
+  cudaStreamSynchronize(G.h2d_b);
   cudaStreamSynchronize(G.stream);
   cudaStreamSynchronize(G.d2h);
 }
@@ -664,15 +668,20 @@ int schedule(OpSpec &op, int dev_id, int dev_kind, talsh_task_t *user_task) {
     any_out = any_out || tr->a[k].copy_back;
   }
   if (any_in) {
-    cudaStreamWaitEvent(G.h2d, tr->ev[0], 0);
+    // Consecutive tasks stage on alternating streams.  Ordering stays safe: a
+    // staging read waits for copies back into its Host range (wait_pending),
+    // and a later copy back into a range an earlier task reads follows that
+    // task's compute on the single compute stream.
+    cudaStream_t hs = (G.staged++ & 1u) ? G.h2d_b : G.h2d;
+    cudaStreamWaitEvent(hs, tr->ev[0], 0);
     // inputs first, the destination (most likely to wait for a copy back) last
     for (int k = op.nt - 1; k >= 0 && rc == TALSH_SUCCESS; --k) {
       ArgRec &a = tr->a[k];
       if (!(a.dalloc && a.need_input)) continue;
-      wait_pending(gpu, G.h2d, a.src_ptr, a.bytes);
-      rc = copy_between(a.dptr, exec_dev, a.src_ptr, a.src_dev, a.bytes, G.h2d);
+      wait_pending(gpu, hs, a.src_ptr, a.bytes);
+      rc = copy_between(a.dptr, exec_dev, a.src_ptr, a.src_dev, a.bytes, hs);
     }
-    cudaEventRecord(tr->ev[1], G.h2d);
+    cudaEventRecord(tr->ev[1], hs);
     cudaStreamWaitEvent(st, tr->ev[1], 0);
   } else {
     cudaEventRecord(tr->ev[1], st);
@@ -751,6 +760,7 @@ int schedule(OpSpec &op, int dev_id, int dev_kind, talsh_task_t *user_task) {
     // Scheduling failed after the task was recorded: the work already queued
     // must drain before its buffers can be released.
     cudaStreamSynchronize(G.h2d);
+    cudaStreamSynchronize(G.h2d_b);
     cudaStreamSynchronize(G.d2h);
     cudaStreamSynchronize(st);
     cudaGetLastError();
@@ -1180,6 +1190,7 @@ int talshInit(size_t *host_buf_size, int *host_arg_max, int ngpus, int gpu_list[
     if (cudaSetDevice(g) != cudaSuccess) { cudaGetLastError(); return TALSH_FAILURE; }
     if (cudaStreamCreateWithFlags(&G.stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithFlags(&G.h2d, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&G.h2d_b, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithFlags(&G.d2h, cudaStreamNonBlocking) != cudaSuccess)
       return TALSH_FAILURE;
     cudaMemPool_t pool;
@@ -1208,9 +1219,7 @@ int talshShutdown(void) {
     GpuCtx &G = R.gpu[g];
     if (!G.in_use) continue;
     cudaSetDevice(g);
-    cudaStreamSynchronize(G.h2d);
-    cudaStreamSynchronize(G.stream);
-    cudaStreamSynchronize(G.d2h);
+    sync_gpu_streams(g);
   }
   for (auto &kv : R.allocs) {
     if (kv.second.gpu < 0) { if (kv.second.pinned) cudaFreeHost(kv.first); else std::free(kv.first); }
@@ -1228,6 +1237,7 @@ int talshShutdown(void) {
     G.event_pool.clear();
     cudaStreamDestroy(G.stream);
     cudaStreamDestroy(G.h2d);
+    cudaStreamDestroy(G.h2d_b);
     cudaStreamDestroy(G.d2h);
     G = GpuCtx();
   }
