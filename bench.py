@@ -159,7 +159,7 @@ def measured_peak():
 
 def profile_traffic_ratio():
     """DRAM bytes / algorithmic bytes of the sweep's launches from the committed ncu summary."""
-    path = os.path.join(ROOT, "profiles", "permute_reg_kernel_c2_sweep.md")
+    path = os.path.join(ROOT, "profiles", "permute_kernels_c2_sweep.md")
     try:
         for line in open(path):
             if line.startswith("traffic_over_algorithmic:"):
