@@ -460,6 +460,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--no-contract", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-tune", action="store_true", help="skip the transpose autotuner (planner heuristics only)")
     ap.add_argument("--check-cases", type=int, default=32,
                     help="full-size sweep cases byte-compared with the oracle after the timing (0: none)")
     ap.add_argument("--detail", default=None,
@@ -580,6 +581,25 @@ def main():
         for op in ops:
             launch(op, s)
 
+    # Plan choices: the transpose autotuner times each case's candidate plans
+    # once (outside the timing) and records the fastest per class; the warm-up,
+    # the captured graph and the end-to-end calls then use the recorded table.
+    tuning = None
+    if not args.no_tune:
+        ch = C.c_int(0)
+        hist = {}
+        tt = time.perf_counter()
+        s_tune = torch.cuda.current_stream(dev).cuda_stream
+        for op in ops:
+            kind, dims, o2n, src, dst, add, _, _ = op
+            rc = L.tcTensorPermuteTune(kind, len(dims), iv(dims), iv(o2n), 1 if add else 0, src, dst, s_tune, 2,
+                                       C.byref(ch))
+            if rc != 0:
+                raise RuntimeError("tuning failed %d: %s" % (rc, L.tcLastErrorString()))
+            hist[str(ch.value)] = hist.get(str(ch.value), 0) + 1
+        torch.cuda.synchronize(dev)
+        tuning = {"ops": len(ops), "choices": dict(sorted(hist.items())), "s": sig(time.perf_counter() - tt)}
+
     # Warm-up (also fills plan/occupancy caches before graph capture).
     for _ in range(max(1, args.warmup)):
         run_sweep()
@@ -680,9 +700,10 @@ def main():
                  "gb_checked": sig(sum(5 * case_bytes(cases[i][0], cases[i][1]) for i in picked) / 1e9)}
 
     # End to end through the public API with pinned Host buffers.  Each case is a
-    # talshTensorCopy with COPY_TK (D copied back, L's device image kept) and a
-    # talshTensorAdd with COPY_TD (D staged and copied back, L's kept device image
-    # used and then discarded): L crosses the link once per case.
+    # talshTensorCopy with COPY_MK (D's result stays on the GPU, L's device image
+    # is kept), a talshTensorAdd with COPY_KD (both device images used in place,
+    # L's discarded afterwards) and an asynchronous talshTensorPlace of D back
+    # into its Host buffer (COPY_M): L crosses the link once up, D once down.
     e2e = None
     if args.e2e_steps > 0:
         # Pinned Host regions rotated between consecutive cases (as the device
@@ -707,12 +728,12 @@ def main():
                                           0.0, 0.0) == 0
             assert L.talshTensorConstruct(C.byref(dt_), kind, len(dims), iv(outd), 0, hd.data_ptr() + off, -1, None,
                                           0.0, 0.0) == 0
-            tens.append((lt, dt_, pattern(o2n, False).encode(), pattern(o2n, True).encode()))
+            tens.append((lt, dt_, pattern(o2n, False).encode(), pattern(o2n, True).encode(), hd.data_ptr() + off))
         h2d = d2h = 0
         for (kind, dims, o2n) in cases:
             b = case_bytes(kind, dims)
-            h2d += b + b  # copy: L; add: D (L's device image is kept from the copy)
-            d2h += b + b  # D after the copy and after the add
+            h2d += b  # L, uploaded by the copy and kept for the add
+            d2h += b  # D, placed back after the add
         gdev = dev.index or 0
 
         import collections
@@ -740,16 +761,18 @@ def main():
                     if rc:
                         raise RuntimeError("e2e op failed %d" % rc)
                     inflight.append(tk)
-                    if len(inflight) > 5:
+                    if len(inflight) > 8:
                         finish_oldest()
                     return
 
-            for i, (lt, dt_, pc, pa) in enumerate(tens):
+            for i, (lt, dt_, pc, pa, hptr) in enumerate(tens):
                 a = ALPHAS[i % len(ALPHAS)]
                 submit(lambda tk: L.talshTensorCopy(pc, C.byref(dt_), C.byref(lt), gdev, T.DEV_NVIDIA_GPU,
-                                                    T.COPY_TK, C.byref(tk)))
+                                                    T.COPY_MK, C.byref(tk)))
                 submit(lambda tk: L.talshTensorAdd(pa, C.byref(dt_), C.byref(lt), a[0], a[1], gdev,
-                                                   T.DEV_NVIDIA_GPU, T.COPY_TD, C.byref(tk)))
+                                                   T.DEV_NVIDIA_GPU, T.COPY_KD, C.byref(tk)))
+                submit(lambda tk: L.talshTensorPlace(C.byref(dt_), 0, T.DEV_HOST, C.c_void_p(hptr), T.COPY_M,
+                                                     C.byref(tk)))
             while inflight:
                 finish_oldest()
         e2e_step()  # warm-up
@@ -760,7 +783,7 @@ def main():
         torch.cuda.synchronize(dev)
         e2e_s = time.perf_counter() - t
         e2e_s = slowest_rank(e2e_s, world, dev)
-        for lt, dt_, _, _ in tens:
+        for lt, dt_, _, _, _ in tens:
             L.talshTensorDestruct(C.byref(lt)); L.talshTensorDestruct(C.byref(dt_))
         # the host link's own rates, for the bound: pinned 1 GiB copies each way and both at once
         link = {}
@@ -783,7 +806,8 @@ def main():
         bound = step_bytes / max(h2d / link["h2d"], d2h / link["d2h"], (h2d + d2h) / link["both"])
         e2e = {"value": whole_job_rate(step_bytes * args.e2e_steps, world, e2e_s) / 1e9, "unit": "GB/s",
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-               "path": "talshTensorCopy COPY_TK + talshTensorAdd COPY_TD, pinned Host, async tasks",
+               "path": "talshTensorCopy COPY_MK + talshTensorAdd COPY_KD + talshTensorPlace COPY_M to Host, "
+                       "pinned Host, async tasks",
                "link_gbs": link, "link_bound_gbs": sig(bound), "steps": args.e2e_steps}
 
     # Contractions (FP64) through talshTensorContract on GPU-resident tensors.
@@ -830,7 +854,7 @@ def main():
                 "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32/f64 (R4/R8)", "data": "synthetic", "config": config,
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": gpu_launches,
-                "clocks": sampler.summary(), "check_bit_exact": check, "graph": True,
+                "clocks": sampler.summary(), "check_bit_exact": check, "graph": True, "tuning": tuning,
                 "contract": contract_summary(contract)}
         print(json.dumps(line))
     if world > 1:

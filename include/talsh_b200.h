@@ -38,6 +38,36 @@ int tcTensorPermuteAdd(int data_kind, int rank, const int *dims_in, const int *o
                        const void *src, void *dst, double alpha_re, double alpha_im, int conj,
                        void *stream);
 
+/* Transpose autotuner.  Cases fall in classes by data kind, operation (copy,
+ * or add when accumulate != 0), the rank and permutation after fusing the
+ * dimensions that stay adjacent, the volume bucket (floor log2), the log2
+ * buckets of the input- and output-minor extents and whether those extents
+ * fill whole 16-byte units.  tcTensorPermuteTune runs this case with each
+ * candidate plan choice (0 the planner's heuristics, 1 bulk reads forced on, 2
+ * bulk reads off, 3 tiles of at most 4 elements per thread, 4 the other tile
+ * walk order), 1 + reps times each on `stream` (the first run is a warm-up),
+ * times them with CUDA events, and records the fastest for the class; every
+ * later tcTensorPermute / tcTensorPermuteAdd call of the class (and the tiled
+ * tasks of a permutation batch) uses it.  Results are identical under every
+ * choice; only the speed changes.  src and dst are device buffers of the case's
+ * volume; dst is overwritten (adds accumulate into it 5 x (1 + reps) times at
+ * most).  *choice receives the recorded choice (0 when the case has a single
+ * plan).  Synchronises the stream.  The reference has no autotuner: its
+ * gpu_tensor_block_copy_dlf (tensor_algebra_gpu_nvidia.cu:4806) picks a kernel
+ * by fixed rules. */
+int tcTensorPermuteTune(int data_kind, int rank, const int *dims_in, const int *o2n, int accumulate,
+                        const void *src, void *dst, void *stream, int reps, int *choice);
+/* The recorded choice of the case's class, or -1 in *choice when none. */
+int tcTensorPermuteTuned(int data_kind, int rank, const int *dims_in, const int *o2n, int accumulate,
+                         int *choice);
+/* Records `choice` (0-4) for the case's class without timing -- a saved tuning
+ * table can be restored this way -- or forgets the class's entry (choice -1).
+ * TALSH_INVALID_ARGS when the choice has no plan for this case. */
+int tcTensorPermuteTuneSet(int data_kind, int rank, const int *dims_in, const int *o2n, int accumulate,
+                           int choice);
+/* Forgets every recorded choice (the heuristics apply again). */
+void tcTensorPermuteTuneReset(void);
+
 /* dst[0..vol) = value.  Replaces gpu_tensor_block_init (:4467). */
 int tcTensorInit(int data_kind, size_t vol, void *dst, double val_re, double val_im, void *stream);
 

@@ -224,6 +224,10 @@ _PROTOS = {
     "decode_device_id": (_I, [_I, _P(_I)]),
     "tcTensorPermute": (_I, [_I, _I, _P(_I), _P(_I), _V, _V, _I, _V]),
     "tcTensorPermuteAdd": (_I, [_I, _I, _P(_I), _P(_I), _V, _V, _D, _D, _I, _V]),
+    "tcTensorPermuteTune": (_I, [_I, _I, _P(_I), _P(_I), _I, _V, _V, _V, _I, _P(_I)]),
+    "tcTensorPermuteTuned": (_I, [_I, _I, _P(_I), _P(_I), _I, _P(_I)]),
+    "tcTensorPermuteTuneSet": (_I, [_I, _I, _P(_I), _P(_I), _I, _I]),
+    "tcTensorPermuteTuneReset": (None, []),
     "tcTensorInit": (_I, [_I, _Z, _V, _D, _D, _V]),
     "tcTensorScale": (_I, [_I, _Z, _V, _D, _D, _V]),
     "tcTensorNorm1Scratch": (_Z, [_Z]),

@@ -136,10 +136,26 @@ __device__ __forceinline__ void cp16(uint32_t s, const void *g) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(g));
 }
 
+// Tiled slice layout (the one the warp-specialised GEMM reads): 128-row x
+// 64-byte tiles, the S slices of one (row tile, K box) adjacent, and every
+// tile stored as the shared-memory image of a 64-byte-swizzled load -- the
+// 16-byte chunk c of tile row i sits at chunk c ^ ((i >> 1) & 3), the layout
+// make_desc_sw64 describes.  One contiguous bulk copy then moves the slices of
+// a box into a stage.  kb: byte offset in the row; nbox: 64-byte boxes per row.
+#ifndef TB_SPLIT_TILED
+#define TB_SPLIT_TILED 1
+#endif
+__device__ __forceinline__ int64_t tiled_off(int64_t r, int64_t kb, int s, int S, int64_t nbox) {
+  const int64_t tile = ((r >> 7) * nbox + (kb >> 6)) * S + s;
+  const int i = (int)(r & 127);
+  const int c = (int)((kb >> 4) & 3) ^ ((i >> 1) & 3);
+  return tile * 8192 + i * 64 + c * 16 + (kb & 15);
+}
+
 // Row split: one CTA per (padded) row; 256 threads.
 __global__ void __launch_bounds__(256) oz_split_rows(const double *__restrict__ X, int64_t rows,
                                                      int64_t K, int64_t rows_p, int64_t Kp, int S,
-                                                     int8_t *__restrict__ slices, int32_t *expo) {
+                                                     int8_t *__restrict__ slices, int32_t *expo, int tiled) {
   const int64_t r = blockIdx.x;
   const int tid = threadIdx.x;
   __shared__ double red[8];
@@ -167,7 +183,7 @@ __global__ void __launch_bounds__(256) oz_split_rows(const double *__restrict__ 
     for (int s = 0; s < S; ++s) {
       const double y = v * 128.0;  // |y| < 128
       const double t = trunc(y);   // in [-127, 127]
-      slices[s * plane + r * Kp + k] = (int8_t)(int)t;
+      slices[tiled ? tiled_off(r, k, s, S, Kp >> 6) : s * plane + r * Kp + k] = (int8_t)(int)t;
       v = y - t;                   // exact remainder, |v| < 1
     }
   }
@@ -217,11 +233,13 @@ __device__ __forceinline__ uint32_t round_slice(double t, double &val) {
 }
 
 // Row split into floating-point slices: one CTA per (padded) row; 256 threads.
-// slices: [S][rows_p][Kp] elements of the form's type.
+// slices: [S][rows_p][Kp] elements of the form's type, or the tiled layout
+// (tiled_off) when tiled != 0.
 template <int FORM>
 __global__ void __launch_bounds__(256) split_rows_float(const double *__restrict__ X, int64_t rows, int64_t K,
                                                         int64_t rows_p, int64_t Kp, int S,
-                                                        unsigned char *__restrict__ slices, int32_t *expo) {
+                                                        unsigned char *__restrict__ slices, int32_t *expo,
+                                                        int tiled) {
   constexpr int ES = form_esize(FORM);
   constexpr int B = form_bits(FORM);
   const int64_t r = blockIdx.x;
@@ -250,7 +268,8 @@ __global__ void __launch_bounds__(256) split_rows_float(const double *__restrict
     for (int s = 0; s < S; ++s) {
       double y;
       const uint32_t bits = round_slice<FORM>(scalbn(v, B * s), y);
-      unsigned char *dst = slices + (s * plane + r * Kp + k) * ES;
+      unsigned char *dst = slices + (tiled ? tiled_off(r, k * ES, s, S, (Kp * ES) >> 6)
+                                           : (s * plane + r * Kp + k) * ES);
       if constexpr (ES == 4) *reinterpret_cast<uint32_t *>(dst) = bits;
       else if constexpr (ES == 2) *reinterpret_cast<uint16_t *>(dst) = (uint16_t)bits;
       else *dst = (unsigned char)bits;
@@ -440,7 +459,18 @@ __device__ __forceinline__ void tma_load_2d(uint32_t sdst, const CUtensorMap *ma
       : "memory");
 }
 
+// Contiguous global -> shared bulk copy completing on an mbarrier (16-byte
+// aligned addresses, size a multiple of 16).
+__device__ __forceinline__ void bulk_load(uint32_t sdst, const void *gsrc, uint32_t bytes, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(sdst),
+      "l"(gsrc), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+
 struct OzWsArgs {
+  const unsigned char *At, *Bt;  // tiled slices (tiled_off), or null: copies through the tensor maps
+  int64_t nbox;                  // 64-byte K boxes per slice row
   uint32_t spin_limit;  // iterations of every bounded mbarrier wait
   int stall_test;       // 1: the producer issues no copies, so the MMA warp's first wait runs out
   int64_t Mp, Np;
@@ -465,6 +495,8 @@ constexpr int kWsDiagPerPass = 3;             // accumulators per pass: 3 x 128 
 // format (bits 4-5: 1 F32, 2 S32), A/B formats (bits 7-9, 10-12: signed int8
 // 1; bf16 1 and tf32 2 of kind::f16/tf32; e4m3 0 of kind::f8f6f4).
 constexpr uint32_t kIdescMN128 = ((uint32_t)(kWsBN >> 3) << 17) | ((uint32_t)(kOzBM >> 4) << 24);
+// M = 256 (a CTA pair, cta_group::2), N = 128.
+constexpr uint32_t kIdescPair = ((uint32_t)(kWsBN >> 3) << 17) | ((uint32_t)(256 >> 4) << 24);
 template <int FORM> struct FormMma;
 template <> struct FormMma<kFormInt8> {
   static constexpr uint32_t idesc = (2u << 4) | (1u << 7) | (1u << 10) | kIdescMN128;
@@ -473,6 +505,13 @@ template <> struct FormMma<kFormInt8> {
         "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d),
         "l"(a), "l"(b), "r"(idesc), "r"(acc));
+  }
+  static constexpr uint32_t idesc_pair = (2u << 4) | (1u << 7) | (1u << 10) | kIdescPair;
+  __device__ static void mma_pair(uint32_t d, uint64_t a, uint64_t b, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::2.kind::i8 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d),
+        "l"(a), "l"(b), "r"(idesc_pair), "r"(acc));
   }
 };
 template <> struct FormMma<kFormBF16> {
@@ -483,6 +522,13 @@ template <> struct FormMma<kFormBF16> {
         "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d),
         "l"(a), "l"(b), "r"(idesc), "r"(acc));
   }
+  static constexpr uint32_t idesc_pair = (1u << 4) | (1u << 7) | (1u << 10) | kIdescPair;
+  __device__ static void mma_pair(uint32_t d, uint64_t a, uint64_t b, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d),
+        "l"(a), "l"(b), "r"(idesc_pair), "r"(acc));
+  }
 };
 template <> struct FormMma<kFormTF32> {
   static constexpr uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) | kIdescMN128;
@@ -492,6 +538,13 @@ template <> struct FormMma<kFormTF32> {
         "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d),
         "l"(a), "l"(b), "r"(idesc), "r"(acc));
   }
+  static constexpr uint32_t idesc_pair = (1u << 4) | (2u << 7) | (2u << 10) | kIdescPair;
+  __device__ static void mma_pair(uint32_t d, uint64_t a, uint64_t b, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::2.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d),
+        "l"(a), "l"(b), "r"(idesc_pair), "r"(acc));
+  }
 };
 template <> struct FormMma<kFormFP8> {
   static constexpr uint32_t idesc = (1u << 4) | (0u << 7) | (0u << 10) | kIdescMN128;
@@ -500,6 +553,13 @@ template <> struct FormMma<kFormFP8> {
         "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::1.kind::f8f6f4 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d),
         "l"(a), "l"(b), "r"(idesc), "r"(acc));
+  }
+  static constexpr uint32_t idesc_pair = (1u << 4) | (0u << 7) | (0u << 10) | kIdescPair;
+  __device__ static void mma_pair(uint32_t d, uint64_t a, uint64_t b, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::2.kind::f8f6f4 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d),
+        "l"(a), "l"(b), "r"(idesc_pair), "r"(acc));
   }
 };
 
@@ -555,8 +615,10 @@ __global__ void __launch_bounds__(kOzWsThreads, 1)
     mbar_init(&drained, 128);
     abort_sh = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::);
-    asm volatile("prefetch.tensormap [%0];" ::"l"((uint64_t)&mapA) : "memory");
-    asm volatile("prefetch.tensormap [%0];" ::"l"((uint64_t)&mapB) : "memory");
+    if (a.At == nullptr) {
+      asm volatile("prefetch.tensormap [%0];" ::"l"((uint64_t)&mapA) : "memory");
+      asm volatile("prefetch.tensormap [%0];" ::"l"((uint64_t)&mapB) : "memory");
+    }
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::);
   __syncthreads();
@@ -585,6 +647,16 @@ __global__ void __launch_bounds__(kOzWsThreads, 1)
           mbar_expect_tx(&full[st], (uint32_t)(nk * smax * (kWsATile + kWsBTile128)));
           const uint32_t sst = sbase + (uint32_t)(st * slot_bytes);
           for (int j = 0; j < nk; ++j) {
+            if (a.At != nullptr) {
+              // slices 0 .. smax-1 of box (tm or tn, kb0/2 + it + j) are adjacent
+              const int64_t box = a.kb0 / 2 + it + j;
+              const uint32_t bytes = (uint32_t)(smax * kWsATile);
+              bulk_load(sst + (uint32_t)(j * smax * kWsATile),
+                        a.At + ((int64_t)tm * a.nbox + box) * S * kWsATile, bytes, &full[st]);
+              bulk_load(sst + (uint32_t)(S * kWsATile + j * smax * kWsBTile128),
+                        a.Bt + ((int64_t)tn * a.nbox + box) * S * kWsBTile128, bytes, &full[st]);
+              continue;
+            }
             const int kx = (int)((a.kb0 + 2 * (it + j)) * kWsBK);
             for (int s = 0; s < smax; ++s) {
               const uint32_t sa = sst + (uint32_t)((j * smax + s) * kWsATile);
@@ -656,7 +728,22 @@ __global__ void __launch_bounds__(kOzWsThreads, 1)
       const int g0 = pass_g0(p), g1 = pass_g1(p);
       const bool first = (p == 0);
       if (ok) {
+        const bool rd = !(first && !a.beta);  // D is read (accumulated into) in this pass
         for (int c = 0; c < kWsBN / 16; ++c) {
+          // The chunk's D addresses and old values first: the 16 loads are in
+          // flight together while the accumulators are read from tensor memory.
+          double *ptr[16];
+          double old[16];
+          int esc[16];
+#pragma unroll
+          for (int i = 0; i < 16; ++i) {
+            const int64_t n = (int64_t)tn * kWsBN + c * 16 + i;
+            const bool ok = mrow && n < a.N;
+            ptr[i] = ok ? a.D + dm + a.nD[n] : nullptr;
+            esc[i] = ok ? em + a.eb[n] : 0;
+          }
+#pragma unroll
+          for (int i = 0; i < 16; ++i) old[i] = (rd && ptr[i] != nullptr) ? *ptr[i] : 0.0;
           double acc[16];
 #pragma unroll
           for (int i = 0; i < 16; ++i) acc[i] = 0.0;
@@ -682,16 +769,11 @@ __global__ void __launch_bounds__(kOzWsThreads, 1)
               for (int i = 0; i < 16; ++i) acc[i] += (double)__uint_as_float(v[i]) * w;
             }
           }
-          if (mrow) {
 #pragma unroll
-            for (int i = 0; i < 16; ++i) {
-              const int64_t n = (int64_t)tn * kWsBN + c * 16 + i;
-              if (n < a.N) {
-                double *ptr = a.D + dm + a.nD[n];
-                const double val = a.alpha * scalbn(acc[i], em + a.eb[n]);
-                *ptr = (first && !a.beta) ? val : (*ptr + val);
-              }
-            }
+          for (int i = 0; i < 16; ++i) {
+            if (ptr[i] == nullptr) continue;
+            const double val = a.alpha * scalbn(acc[i], esc[i]);
+            *ptr[i] = rd ? old[i] + val : val;
           }
         }
       }
@@ -713,6 +795,307 @@ __global__ void __launch_bounds__(kOzWsThreads, 1)
       mbar_wait(&full[st], (uint32_t)((last / nst) & 1), a.err, lim);
     }
   }
+}
+
+// ---------------------------------------------------------------------------
+// Pair (cta_group::2) form of the warp-specialised GEMM.  Two CTAs of a
+// cluster compute one 256 x 128 tile: each holds 128 rows of A and 64 rows of
+// B per slice in its shared memory, and the even CTA issues MMAs of M = 256
+// that read both CTAs' operands (each SM multiplies its own A rows by all of
+// B; the B halves are exchanged between the pair), so every SM streams 25 %
+// fewer operand bytes and its tensor core reads half the B bytes from shared
+// memory per MMA.  Every SM keeps its own rows' accumulators in its tensor
+// memory (3 diagonals x 128 columns per pass, as in the single-CTA form).
+// Synchronisation: both CTAs' copies complete on the even CTA's "full"
+// barriers (the copies carry .cta_group::2); the even CTA's commits arrive on
+// "empty" and "done" in both CTAs (.multicast::cluster on tcgen05.commit);
+// both CTAs' epilogue threads arrive on the even CTA's "drained" barrier.
+// Every wait on an mbarrier is bounded; the two cluster barriers (after the
+// barrier set-up and before the tensor memory is freed) are reached by every
+// thread on every path.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t cluster_ctarank() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+__device__ __forceinline__ void cluster_sync_all() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+// Shared::cluster address of the same shared variable in CTA `rank` of the cluster.
+__device__ __forceinline__ uint32_t mapa_rank(uint32_t saddr, uint32_t rank) {
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(saddr), "r"(rank));
+  return r;
+}
+// 2-D tensor copy whose completion is counted on the even CTA's barrier
+// (`bar_cluster`, a shared::cluster address); no multicast.
+__device__ __forceinline__ void tma_load_2d_pair(uint32_t sdst, const CUtensorMap *map, int x, int y,
+                                                 uint32_t bar_cluster) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, "
+      "%3}], [%4];" ::"r"(sdst),
+      "l"((uint64_t)map), "r"(x), "r"(y), "r"(bar_cluster)
+      : "memory");
+}
+// Arrival on `bar` (same shared offset) in both CTAs of the pair once every
+// previously issued MMA of this thread has completed.
+__device__ __forceinline__ void mma_commit_pair(uint64_t *bar) {
+  asm volatile(
+      "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;" ::"r"(
+          smem_u32(bar)),
+      "h"((uint16_t)3)
+      : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_cluster(uint32_t bar_cluster) {
+  asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(bar_cluster) : "memory");
+}
+// Waits with cluster-scope acquire (the phase may be completed by the peer CTA).
+__device__ __forceinline__ bool mbar_try_cluster(uint64_t *bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.b32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ bool mbar_wait_cluster(uint64_t *bar, uint32_t parity, int *err, uint32_t limit) {
+  for (uint32_t i = 0; i < limit; ++i)
+    if (mbar_try_cluster(bar, parity)) return true;
+  atomicExch(err, 1);
+  return false;
+}
+
+constexpr int kPairBTile = 64 * kWsBox;  // 4 KB: this CTA's 64 rows of a B slice box
+
+struct OzPairArgs {
+  uint32_t spin_limit;
+  int64_t Mp, Np;
+  int tiles_m2, tiles_n;  // 256-row and 128-column tiles
+  int group_m;            // pair tiles along m per raster group
+  int64_t kb0, kb1;
+  int S, nst;
+  const int32_t *ea, *eb;
+  double *D;
+  const int64_t *mD, *nD;
+  int64_t M, N;
+  double alpha;
+  int beta;
+  int *err;
+  uint32_t tmem_cols;
+};
+
+template <int FORM>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kOzWsThreads, 1)
+    oz_gemm_pair_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
+                        const OzPairArgs a) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  constexpr int kMaxStages = 8;
+  __shared__ __align__(8) uint64_t full[kMaxStages], empty[kMaxStages], done, drained;
+  __shared__ uint32_t tmem_base_sh;
+  __shared__ int abort_sh;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const uint32_t rank = cluster_ctarank();
+  const int S = a.S, nst = a.nst;
+  const int slot_bytes = S * (kWsATile + kPairBTile);
+  const int npass = (S + kWsDiagPerPass - 1) / kWsDiagPerPass;
+  int tm, tn;  // 256-row tile of the pair, 128-column tile
+  {
+    const int id = blockIdx.x >> 1;
+    const int per_group = a.group_m * a.tiles_n;
+    const int grp = id / per_group;
+    const int first_m = grp * a.group_m;
+    const int gm = min(a.group_m, a.tiles_m2 - first_m);
+    const int r = id - grp * per_group;
+    tm = first_m + r % gm;
+    tn = r / gm;
+  }
+  const int64_t nkb = a.kb1 - a.kb0;
+  const int64_t nbox = (nkb + 1) / 2;
+  auto pass_g0 = [&](int p) { return 2 + p * kWsDiagPerPass; };
+  auto pass_g1 = [&](int p) { return min(S + 1, pass_g0(p) + kWsDiagPerPass - 1); };
+
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base_sh)),
+                 "r"(a.tmem_cols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::);
+  }
+  if (tid == 0) {
+    for (int i = 0; i < nst; ++i) {
+      mbar_init(&full[i], 1);
+      mbar_init(&empty[i], 1);
+    }
+    mbar_init(&done, 1);
+    mbar_init(&drained, 256);  // both CTAs' epilogue threads
+    abort_sh = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::);
+    asm volatile("prefetch.tensormap [%0];" ::"l"((uint64_t)&mapA) : "memory");
+    asm volatile("prefetch.tensormap [%0];" ::"l"((uint64_t)&mapB) : "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::);
+  __syncthreads();
+  cluster_sync_all();  // the even CTA's barriers exist before the odd CTA signals them
+  asm volatile("tcgen05.fence::after_thread_sync;" ::);
+  const uint32_t tmem = tmem_base_sh;
+  const uint32_t sbase = (smem_u32(smem) + 1023u) & ~1023u;
+  const uint32_t lim = a.spin_limit;
+
+  int64_t issued_all = 0;  // warp 0 lane 0: stage-ring iterations whose copies were issued
+  if (warp == 0) {
+    if (lane == 0) {
+      int64_t itg = 0;
+      for (int p = 0; p < npass && !*(volatile int *)&abort_sh; ++p) {
+        const int smax = pass_g1(p) - 1;
+        const int kper = max(1, S / smax);
+        for (int64_t it = 0; it < nbox; it += kper, ++itg) {
+          const int nk = (int)min((int64_t)kper, nbox - it);
+          const int st = (int)(itg % nst);
+          if (itg >= nst && !mbar_wait_cluster(&empty[st], (uint32_t)(((itg / nst) - 1) & 1), a.err, lim)) {
+            raise_abort(&abort_sh);
+            break;
+          }
+          issued_all = itg + 1;
+          // the even CTA expects the bytes of both CTAs' copies of this stage
+          if (rank == 0) mbar_expect_tx(&full[st], (uint32_t)(2 * nk * smax * (kWsATile + kPairBTile)));
+          const uint32_t fbar = mapa_rank(smem_u32(&full[st]), 0);
+          const uint32_t sst = sbase + (uint32_t)(st * slot_bytes);
+          for (int j = 0; j < nk; ++j) {
+            const int kx = (int)((a.kb0 + 2 * (it + j)) * kWsBK);
+            for (int s = 0; s < smax; ++s) {
+              const uint32_t sa = sst + (uint32_t)((j * smax + s) * kWsATile);
+              const uint32_t sb = sst + (uint32_t)(S * kWsATile + (j * smax + s) * kPairBTile);
+              tma_load_2d_pair(sa, &mapA, kx, (int)(s * a.Mp + tm * 256 + rank * 128), fbar);
+              tma_load_2d_pair(sb, &mapB, kx, (int)(s * a.Np + tn * kWsBN + rank * 64), fbar);
+            }
+          }
+        }
+      }
+    }
+  } else if (warp == 1) {
+    if (rank == 0 && lane == 0) {
+      int64_t itg = 0;
+      for (int p = 0; p < npass; ++p) {
+        if (p > 0 && !mbar_wait_cluster(&drained, (uint32_t)((p - 1) & 1), a.err, lim)) raise_abort(&abort_sh);
+        if (*(volatile int *)&abort_sh) {
+          mma_commit_pair(&done);
+          continue;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::);
+        const int g0 = pass_g0(p), g1 = pass_g1(p);
+        const int smax = g1 - 1;
+        const int kper = max(1, S / smax);
+        for (int64_t it = 0; it < nbox; it += kper, ++itg) {
+          const int nk = (int)min((int64_t)kper, nbox - it);
+          const int st = (int)(itg % nst);
+          if (!mbar_wait_cluster(&full[st], (uint32_t)((itg / nst) & 1), a.err, lim)) {
+            raise_abort(&abort_sh);
+            break;
+          }
+          asm volatile("tcgen05.fence::after_thread_sync;" ::);
+          const uint32_t sst = sbase + (uint32_t)(st * slot_bytes);
+          for (int j = 0; j < nk; ++j) {
+            const int nsteps = (2 * (it + j) + 1 < nkb) ? 2 : 1;
+            for (int kk = 0; kk < nsteps; ++kk) {
+              for (int g = g0; g <= g1; ++g) {
+                const uint32_t dcol = tmem + (uint32_t)((g - g0) * kWsBN);
+                for (int s1 = 1; s1 < g; ++s1) {
+                  const uint32_t sa = sst + (uint32_t)((j * smax + s1 - 1) * kWsATile + kk * kWsBK);
+                  const uint32_t sb =
+                      sst + (uint32_t)(S * kWsATile + (j * smax + g - s1 - 1) * kPairBTile + kk * kWsBK);
+                  FormMma<FORM>::mma_pair(dcol, make_desc_sw64(sa), make_desc_sw64(sb),
+                                          (it > 0 || j > 0 || kk > 0 || s1 > 1) ? 1u : 0u);
+                }
+              }
+            }
+          }
+          mma_commit_pair(&empty[st]);
+        }
+        mma_commit_pair(&done);
+      }
+    }
+  } else {
+    const int q = warp & 3;
+    const int64_t m = (int64_t)tm * 256 + rank * 128 + q * 32 + lane;
+    const bool mrow = m < a.M;
+    const int em = mrow ? a.ea[m] : 0;
+    const int64_t dm = mrow ? a.mD[m] : 0;
+    const uint32_t drained0 = mapa_rank(smem_u32(&drained), 0);
+    for (int p = 0; p < npass; ++p) {
+      bool ok = mbar_wait_cluster(&done, (uint32_t)(p & 1), a.err, lim);
+      if (!ok) raise_abort(&abort_sh);
+      ok = ok && !*(volatile int *)&abort_sh;
+      ok = __all_sync(0xffffffffu, ok);
+      asm volatile("tcgen05.fence::after_thread_sync;" ::);
+      const int g0 = pass_g0(p), g1 = pass_g1(p);
+      const bool first = (p == 0);
+      if (ok) {
+        const bool rd = !(first && !a.beta);
+        for (int c = 0; c < kWsBN / 16; ++c) {
+          double *ptr[16];
+          double old[16];
+          int esc[16];
+#pragma unroll
+          for (int i = 0; i < 16; ++i) {
+            const int64_t n = (int64_t)tn * kWsBN + c * 16 + i;
+            const bool okn = mrow && n < a.N;
+            ptr[i] = okn ? a.D + dm + a.nD[n] : nullptr;
+            esc[i] = okn ? em + a.eb[n] : 0;
+          }
+#pragma unroll
+          for (int i = 0; i < 16; ++i) old[i] = (rd && ptr[i] != nullptr) ? *ptr[i] : 0.0;
+          double acc[16];
+#pragma unroll
+          for (int i = 0; i < 16; ++i) acc[i] = 0.0;
+          for (int g = g0; g <= g1; ++g) {
+            uint32_t v[16];
+            const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)((g - g0) * kWsBN + c * 16);
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+                  "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]),
+                  "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+                : "r"(taddr));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if constexpr (FORM == kFormInt8) {
+              const double w = scalbn(1.0, -7 * g);
+#pragma unroll
+              for (int i = 0; i < 16; ++i) acc[i] += (double)(int32_t)v[i] * w;
+            } else {
+              const double w = scalbn(1.0, -form_bits(FORM) * (g - 2));
+#pragma unroll
+              for (int i = 0; i < 16; ++i) acc[i] += (double)__uint_as_float(v[i]) * w;
+            }
+          }
+#pragma unroll
+          for (int i = 0; i < 16; ++i) {
+            if (ptr[i] == nullptr) continue;
+            const double val = a.alpha * scalbn(acc[i], esc[i]);
+            *ptr[i] = rd ? old[i] + val : val;
+          }
+        }
+      }
+      asm volatile("tcgen05.fence::before_thread_sync;" ::);
+      mbar_arrive_cluster(drained0);  // the pass's accumulators of this CTA have been read
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::);
+  __syncthreads();
+  // After an abort, the even CTA waits (bounded) for the last phase of every
+  // stage it expected, so that no copy of the pair is in flight at exit.
+  if (rank == 0 && warp == 0 && lane == 0 && *(volatile int *)&abort_sh) {
+    for (int st = 0; st < nst; ++st) {
+      if (issued_all <= st) continue;
+      const int64_t last = st + ((issued_all - 1 - st) / nst) * nst;
+      mbar_wait_cluster(&full[st], (uint32_t)((last / nst) & 1), a.err, lim);
+    }
+  }
+  cluster_sync_all();  // no MMA, copy or arrival of the pair is outstanding
+  asm volatile("tcgen05.fence::after_thread_sync;" ::);
+  if (warp == 1)
+    asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(a.tmem_cols));
 }
 
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no -lcuda).
@@ -781,7 +1164,7 @@ struct OzPlan {
 // number of 64-byte blocks.
 void oz_plan(int64_t M, int64_t N, int64_t K, int S, OzPlan &p, int esize = 1) {
   p.M = M; p.N = N; p.K = K;
-  p.Mp = round_up(std::max<int64_t>(M, 1), kOzBM);
+  p.Mp = round_up(std::max<int64_t>(M, 1), 2 * kOzBM);  // whole 256-row tiles of the CTA-pair kernel
   p.Np = round_up(std::max<int64_t>(N, 1), 128);  // multiple of both kernels' tile width
   p.Kp = round_up(std::max<int64_t>(K, 1), kOzBK / esize);
   size_t off = 0;
@@ -904,6 +1287,48 @@ size_t contract_split_scratch(int kind, const int *cptrn, int drank, const int *
 
 namespace {
 
+// The CTA-pair kernel or the single-CTA kernel (TALSH_B200_SPLIT_PAIR=1 / 0;
+// the default is kSplitPairDefault).
+constexpr bool kSplitPairDefault = false;
+bool split_pair_enabled() {
+  static const bool v = [] {
+    const char *e = std::getenv("TALSH_B200_SPLIT_PAIR");
+    return e ? std::atoi(e) != 0 : kSplitPairDefault;
+  }();
+  return v;
+}
+
+// Stage ring of the pair kernel, plus 1 KB of alignment slack and 8 KB of
+// guard after the ring (an MMA's B operand never reaches past its tile; the
+// guard keeps every descriptor-addressed read inside the allocation).
+constexpr int kOzPairSmem = 216 * 1024;
+constexpr int kOzPairExtra = 1024 + 8192;
+
+// The CTA-pair GEMM of one form over K-step launches [0, nkb32) in chunks of
+// kc32 steps.
+template <int FORM>
+int launch_pair_form(const CUtensorMap &mapA, const CUtensorMap &mapB, OzPairArgs w, int64_t nkb32, int64_t kc32,
+                     int accumulative, int stage_bytes, cudaStream_t st) {
+  static std::atomic<uint64_t> pair_attr{0};
+  once_per_device(pair_attr, [] {
+    cudaFuncSetAttribute(oz_gemm_pair_kernel<FORM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         kOzPairSmem + kOzPairExtra);
+  });
+  const int64_t ctas = 2 * (int64_t)w.tiles_m2 * w.tiles_n;
+  if (ctas > 0x7fffffffLL) return TALSH_LIMIT_EXCEEDED;
+  for (int64_t kb = 0; kb < nkb32; kb += kc32) {
+    w.kb0 = kb;
+    w.kb1 = std::min(nkb32, kb + kc32);
+    w.beta = (kb == 0) ? (accumulative ? 1 : 0) : 1;
+    oz_gemm_pair_kernel<FORM><<<(unsigned)ctas, kOzWsThreads, w.nst * stage_bytes + kOzPairExtra, st>>>(mapA, mapB,
+                                                                                                      w);
+    note_launch();
+    const int rc = check_launch("oz_gemm_pair_kernel");
+    if (rc != 0) return rc;
+  }
+  return TALSH_SUCCESS;
+}
+
 // The warp-specialised GEMM of one form over K-step launches [0, nkb32) in
 // chunks of kc32 steps (32 bytes each).
 template <int FORM>
@@ -973,10 +1398,18 @@ int contract_split_launch(int kind, const int *cptrn, int drank, const int *ddim
   cudaMemsetAsync(err, 0, sizeof(int), st);
   if (p.Mp > 0x7fffffffLL || p.Np > 0x7fffffffLL) return TALSH_LIMIT_EXCEEDED;
   const double *A64 = (const double *)(base + p.off_A64), *B64 = (const double *)(base + p.off_B64);
+  // The warp-specialised GEMM reads the tiled layout with bulk copies; the
+  // single-loop int8 kernel (TALSH_B200_SPLIT_SIMPLE=1) reads [S][rows][Kp].
+  const bool simple = oz_force_simple() && fc.form == kFormInt8;
+  // The pair kernel reads [S][rows][Kp] through tensor maps (its copies
+  // complete on the even CTA's barriers); the stall test runs the single-CTA one.
+  const bool pair = !simple && g_stall_test.load() == 0 && split_pair_enabled() &&
+                    (int64_t)slices * p.Mp < 0x7fffffffLL && (int64_t)slices * p.Np < 0x7fffffffLL;
+  const int tiled = (TB_SPLIT_TILED && !simple && !pair) ? 1 : 0;
   auto split_float = [&](auto kern) {
-    kern<<<(unsigned)p.Mp, 256, 0, st>>>(A64, M, K, p.Mp, p.Kp, slices, (unsigned char *)As, ea);
+    kern<<<(unsigned)p.Mp, 256, 0, st>>>(A64, M, K, p.Mp, p.Kp, slices, (unsigned char *)As, ea, tiled);
     note_launch();
-    kern<<<(unsigned)p.Np, 256, 0, st>>>(B64, N, K, p.Np, p.Kp, slices, (unsigned char *)Bs, eb);
+    kern<<<(unsigned)p.Np, 256, 0, st>>>(B64, N, K, p.Np, p.Kp, slices, (unsigned char *)Bs, eb, tiled);
     note_launch();
   };
   switch (fc.form) {
@@ -984,9 +1417,9 @@ int contract_split_launch(int kind, const int *cptrn, int drank, const int *ddim
     case kFormTF32: split_float(split_rows_float<kFormTF32>); break;
     case kFormFP8: split_float(split_rows_float<kFormFP8>); break;
     default:
-      oz_split_rows<<<(unsigned)p.Mp, 256, 0, st>>>(A64, M, K, p.Mp, p.Kp, slices, As, ea);
+      oz_split_rows<<<(unsigned)p.Mp, 256, 0, st>>>(A64, M, K, p.Mp, p.Kp, slices, As, ea, tiled);
       note_launch();
-      oz_split_rows<<<(unsigned)p.Np, 256, 0, st>>>(B64, N, K, p.Np, p.Kp, slices, Bs, eb);
+      oz_split_rows<<<(unsigned)p.Np, 256, 0, st>>>(B64, N, K, p.Np, p.Kp, slices, Bs, eb, tiled);
       note_launch();
   }
   if ((rc = check_launch("split rows")) != 0) return rc;
@@ -1011,23 +1444,49 @@ int contract_split_launch(int kind, const int *cptrn, int drank, const int *ddim
   // Warp-specialised TMA pipeline when the tensor maps can be encoded (the
   // slice matrices' row counts must fit the 32-bit TMA coordinates).
   CUtensorMap mapA, mapB;
-  const bool ws = (!oz_force_simple() || fc.form != kFormInt8) && (int64_t)slices * p.Mp < 0x7fffffffLL &&
-                  (int64_t)slices * p.Np < 0x7fffffffLL &&
-                  make_slice_map(&mapA, As, Kbytes, slices * p.Mp, kOzBM) &&
-                  make_slice_map(&mapB, Bs, Kbytes, slices * p.Np, kWsBN);
+  std::memset(&mapA, 0, sizeof(mapA));
+  std::memset(&mapB, 0, sizeof(mapB));
+  const int64_t nkb32 = Kbytes / kWsBK;
+  int64_t kc32 = kc_max * (kOzBK / kWsBK);  // K steps per launch
+  if (fc.form != kFormInt8) {
+    const int64_t kc_el = fp32_kchunk();
+    kc32 = kc_el > 0 ? std::max<int64_t>(2, round_up(kc_el * es, kOzBK) / kWsBK) : nkb32;
+  }
+  if (pair && make_slice_map(&mapA, As, Kbytes, slices * p.Mp, kOzBM) &&
+      make_slice_map(&mapB, Bs, Kbytes, slices * p.Np, 64)) {
+    const int stage_bytes = slices * (kWsATile + kPairBTile);
+    OzPairArgs w;
+    w.spin_limit = kSpinLimit;
+    w.Mp = p.Mp; w.Np = p.Np; w.S = slices;
+    w.nst = std::max(2, std::min(8, kOzPairSmem / stage_bytes));
+    w.tiles_m2 = (int)(p.Mp / (2 * kOzBM));
+    w.tiles_n = (int)(p.Np / kWsBN);
+    w.group_m = std::max(1, ws_group_m() / 2);
+    w.ea = ea; w.eb = eb; w.D = (double *)D; w.mD = mD; w.nD = nD; w.M = M; w.N = N;
+    w.alpha = alpha_re; w.err = err;
+    w.tmem_cols = 32;
+    while (w.tmem_cols < (uint32_t)(std::min(slices, kWsDiagPerPass) * kWsBN)) w.tmem_cols <<= 1;
+    switch (fc.form) {
+      case kFormBF16: return launch_pair_form<kFormBF16>(mapA, mapB, w, nkb32, kc32, accumulative, stage_bytes, st);
+      case kFormTF32: return launch_pair_form<kFormTF32>(mapA, mapB, w, nkb32, kc32, accumulative, stage_bytes, st);
+      case kFormFP8: return launch_pair_form<kFormFP8>(mapA, mapB, w, nkb32, kc32, accumulative, stage_bytes, st);
+      default: return launch_pair_form<kFormInt8>(mapA, mapB, w, nkb32, kc32, accumulative, stage_bytes, st);
+    }
+  }
+  const bool ws = !simple && (tiled || ((int64_t)slices * p.Mp < 0x7fffffffLL &&
+                                        (int64_t)slices * p.Np < 0x7fffffffLL &&
+                                        make_slice_map(&mapA, As, Kbytes, slices * p.Mp, kOzBM) &&
+                                        make_slice_map(&mapB, Bs, Kbytes, slices * p.Np, kWsBN)));
   if (!ws && fc.form != kFormInt8) return TALSH_NOT_IMPLEMENTED;  // the float forms have no simple kernel
   if (ws) {
     const int stage_bytes = slices * (kWsATile + kWsBTile128);
     const int nst = std::max(2, std::min(8, kOzWsSmem / stage_bytes));
-    const int64_t nkb32 = Kbytes / kWsBK;
-    int64_t kc32 = kc_max * (kOzBK / kWsBK);
-    if (fc.form != kFormInt8) {
-      const int64_t kc_el = fp32_kchunk();
-      kc32 = kc_el > 0 ? std::max<int64_t>(2, round_up(kc_el * es, kOzBK) / kWsBK) : nkb32;
-    }
     const int64_t tiles = (p.Mp / kOzBM) * (p.Np / kWsBN);
     if (tiles > 0x7fffffffLL) return TALSH_LIMIT_EXCEEDED;
     OzWsArgs w;
+    w.At = tiled ? (const unsigned char *)As : nullptr;
+    w.Bt = tiled ? (const unsigned char *)Bs : nullptr;
+    w.nbox = Kbytes / kWsBox;
     const bool stall = g_stall_test.load() != 0;
     w.spin_limit = stall ? (1u << 12) : kSpinLimit;
     w.stall_test = stall ? 1 : 0;

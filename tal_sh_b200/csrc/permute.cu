@@ -24,6 +24,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <climits>
 #include <cstdlib>
 #include <cstring>
@@ -1113,10 +1114,18 @@ int64_t balanced_grow(int64_t ext, int64_t cur) {
   return ext;
 }
 
+// Plan choices the transpose autotuner (tcTensorPermuteTune) can override;
+// the defaults are the heuristics of build_plan.
+struct PlanCfg {
+  int bulk = -1;   // -1: permute_bulk_wanted decides; 0: never; 1: wherever the plan allows it
+  int small = 0;   // 1: tiles of at most 4 elements per thread (more resident CTAs per SM)
+  int flip = 0;    // 1: walk the tiles in the other tensor's dimension order
+};
+
 // out_major: tile index order follows the output's dimensions (copies), else
 // the input's (adds, whose output sectors are read before they are written).
-int build_plan(int esize, const Fused &F, Plan &plan, int op = kOpCopy) {
-  const bool out_major = op != kOpAdd && !TB_COPY_INPUT_MAJOR;
+int build_plan(int esize, const Fused &F, Plan &plan, int op = kOpCopy, const PlanCfg &cfg = PlanCfg()) {
+  const bool out_major = (op != kOpAdd && !TB_COPY_INPUT_MAJOR) != (cfg.flip != 0);
   plan.vol = F.vol;
   if (F.n <= 1) { plan.linear = true; return TALSH_SUCCESS; }
   PermParams &P = plan.P;
@@ -1132,7 +1141,7 @@ int build_plan(int esize, const Fused &F, Plan &plan, int op = kOpCopy) {
 
   // Tile budget: at most reg_k(esize) elements per thread of the register-table
   // kernel.  Small tensors get smaller tiles so that every SM still holds a few.
-  int elems_max = std::min(tile_bytes() / esize, kThreads * reg_k(esize));
+  int elems_max = std::min(tile_bytes() / esize, kThreads * (cfg.small ? 4 : reg_k(esize)));
   {
     const int64_t slots = 148LL * kMinBlocks * 2;
     while (elems_max / 2 >= 1024 && F.vol / elems_max < slots) elems_max /= 2;  // floor 1024: every plan fits
@@ -1372,7 +1381,7 @@ int build_plan(int esize, const Fused &F, Plan &plan, int op = kOpCopy) {
   // Bulk-read form: rows of pitch_b bytes (16-byte aligned, an odd number of
   // 16-byte units), each holding a run's 16-byte-aligned cover.
   P.bulk = 0;
-  if (P.reg && permute_bulk_wanted(esize, op, plan.vout)) {
+  if (P.reg && (cfg.bulk < 0 ? permute_bulk_wanted(esize, op, plan.vout) : cfg.bulk == 1)) {
     int pitch = (int)(((int64_t)P.Li * esize + 15 + 15) / 16 * 16);
     if ((pitch / 16) % 2 == 0) pitch += 16;
     const int64_t stage_b = ((int64_t)P.Ri * pitch + 127) / 128 * 128;
@@ -1540,6 +1549,67 @@ int validate(int kind, int rank, const int *dims, const int *o2n) {
   return TALSH_SUCCESS;
 }
 
+// ---------------------------------------------------------------------------
+// Transpose autotuner.  Cases fall in classes by element kind, operation, the
+// fused rank and permutation, the volume bucket (floor log2), the buckets of
+// the input- and output-minor extents and whether those extents fill whole
+// 16-byte units; tcTensorPermuteTune times the candidate plan choices of one
+// case (CUDA events) and records the fastest for its class, which every later
+// call of that class then uses.  Candidates: the heuristics, bulk reads
+// forced on, bulk reads off, small tiles (4 elements per thread), and the
+// other tile walk order.  Results do not depend on the choice (the same
+// element arithmetic runs in every kernel), only the speed does.
+// ---------------------------------------------------------------------------
+constexpr int kTuneConfigs = 5;
+PlanCfg tune_cfg(int code) {
+  PlanCfg c;
+  switch (code) {
+    case 1: c.bulk = 1; break;
+    case 2: c.bulk = 0; break;
+    case 3: c.small = 1; break;
+    case 4: c.flip = 1; break;
+    default: break;
+  }
+  return c;
+}
+
+int ilog2_64(int64_t x) {
+  int b = 0;
+  while (x > 1) { x >>= 1; ++b; }
+  return b;
+}
+
+// Class key of a fused case (0: not tunable -- straight copies and fused ranks
+// above 6).
+uint64_t tune_key(int kind, int op, const Fused &F) {
+  if (F.n < 2 || F.n > 6) return 0;
+  const int esize = kind_size(kind);
+  int q0 = 0;
+  for (int i = 0; i < F.n; ++i)
+    if (F.perm[i] == 0) q0 = i;
+  uint64_t k = (uint64_t)(kind & 3);
+  k = (k << 1) | (uint64_t)(op == kOpAdd);
+  k = (k << 3) | (uint64_t)F.n;
+  for (int i = 0; i < F.n; ++i) k = (k << 3) | (uint64_t)F.perm[i];
+  k = (k << 6) | (uint64_t)std::min(63, ilog2_64(F.vol));
+  k = (k << 5) | (uint64_t)std::min(31, ilog2_64(F.ext[0]));
+  k = (k << 5) | (uint64_t)std::min(31, ilog2_64(F.ext[q0]));
+  k = (k << 1) | (uint64_t)((F.ext[0] * esize) % 16 == 0);
+  k = (k << 1) | (uint64_t)((F.ext[q0] * esize) % 16 == 0);
+  return k | (uint64_t(1) << 63);
+}
+
+std::mutex g_tune_mu;
+std::unordered_map<uint64_t, int> g_tune_table;
+std::atomic<int> g_tune_entries{0};
+
+int tuned_choice(uint64_t key) {
+  if (key == 0 || g_tune_entries.load(std::memory_order_relaxed) == 0) return -1;
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  auto it = g_tune_table.find(key);
+  return it == g_tune_table.end() ? -1 : it->second;
+}
+
 template <int OP>
 int permute_entry(int kind, int rank, const int *dims, const int *o2n, const void *src, void *dst,
                   int conj, const ScaleArgs &sc, void *stream) {
@@ -1551,8 +1621,9 @@ int permute_entry(int kind, int rank, const int *dims, const int *o2n, const voi
   Fused F;
   if (rank == 0) { F.n = 0; F.vol = 1; }
   else if ((rc = fuse_dims(rank, dims, o2n, F)) != 0) return rc;
+  const int choice = tuned_choice(tune_key(kind, OP, F));
   Plan plan;
-  if ((rc = build_plan(kind_size(kind), F, plan, OP)) != 0) return rc;
+  if ((rc = build_plan(kind_size(kind), F, plan, OP, tune_cfg(choice))) != 0) return rc;
   cudaStream_t st = (cudaStream_t)stream;
   switch (kind) {
     case R4: return launch_typed<float, OP>(plan, src, dst, conj, sc, st);
@@ -1580,6 +1651,132 @@ extern "C" int tcTensorPermuteAdd(int data_kind, int rank, const int *dims_in, c
   sc.si = alpha_im;
   if (!tb::kind_is_complex(data_kind)) { sc.sr = tb::cmplx8_to_real8(alpha_re, alpha_im); sc.si = 0.0; }
   return tb::permute_entry<tb::kOpAdd>(data_kind, rank, dims_in, o2n, src, dst, conj, sc, stream);
+}
+
+namespace tb {
+namespace {
+template <int OP>
+int launch_kind(int kind, const Plan &plan, const void *src, void *dst, const ScaleArgs &sc, cudaStream_t st) {
+  switch (kind) {
+    case R4: return launch_typed<float, OP>(plan, src, dst, 0, sc, st);
+    case R8: return launch_typed<double, OP>(plan, src, dst, 0, sc, st);
+    case C4: return launch_typed<float2, OP>(plan, src, dst, 0, sc, st);
+    case C8: return launch_typed<double2, OP>(plan, src, dst, 0, sc, st);
+  }
+  return TALSH_INVALID_ARGS;
+}
+}  // namespace
+}  // namespace tb
+
+extern "C" int tcTensorPermuteTune(int data_kind, int rank, const int *dims_in, const int *o2n, int accumulate,
+                                   const void *src, void *dst, void *stream, int reps, int *choice) {
+  using namespace tb;
+  int rc = validate(data_kind, rank, dims_in, o2n);
+  if (rc) return rc;
+  if (src == nullptr || dst == nullptr || reps < 1 || choice == nullptr) return TALSH_INVALID_ARGS;
+  if (!elem_aligned(data_kind, src) || !elem_aligned(data_kind, dst)) return TALSH_INVALID_ARGS;
+  *choice = 0;
+  Fused F;
+  if (rank == 0) return TALSH_SUCCESS;
+  if ((rc = fuse_dims(rank, dims_in, o2n, F)) != 0) return rc;
+  const int op = accumulate ? kOpAdd : kOpCopy;
+  const uint64_t key = tune_key(data_kind, op, F);
+  if (key == 0) return TALSH_SUCCESS;  // one plan only
+  const int esize = kind_size(data_kind);
+  Plan plans[kTuneConfigs];
+  bool live[kTuneConfigs] = {false};
+  for (int c = 0; c < kTuneConfigs; ++c) {
+    if (build_plan(esize, F, plans[c], op, tune_cfg(c)) != 0) continue;
+    live[c] = true;
+    for (int d = 0; d < c && live[c]; ++d)  // a choice that changes nothing is not timed twice
+      if (live[d] && plans[d].linear == plans[c].linear && plans[d].smem == plans[c].smem &&
+          std::memcmp(&plans[d].P, &plans[c].P, sizeof(PermParams)) == 0)
+        live[c] = false;
+  }
+  if (!live[0]) return TALSH_FAILURE;
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+    cudaGetLastError();
+    if (e0) cudaEventDestroy(e0);
+    return TALSH_FAILURE;
+  }
+  ScaleArgs sc;
+  sc.sr = 1.0;
+  int best = 0;
+  float best_ms = 0.0f;
+  for (int c = 0; c < kTuneConfigs && rc == TALSH_SUCCESS; ++c) {
+    if (!live[c]) continue;
+    float ms = 0.0f;
+    for (int r = 0; r <= reps && rc == TALSH_SUCCESS; ++r) {  // the first run warms up
+      cudaEventRecord(e0, st);
+      rc = (op == kOpAdd) ? launch_kind<kOpAdd>(data_kind, plans[c], src, dst, sc, st)
+                          : launch_kind<kOpCopy>(data_kind, plans[c], src, dst, sc, st);
+      cudaEventRecord(e1, st);
+      if (rc == TALSH_SUCCESS && cudaEventSynchronize(e1) != cudaSuccess) rc = TALSH_FAILURE;
+      float dt = 0.0f;
+      if (rc == TALSH_SUCCESS && r > 0 && cudaEventElapsedTime(&dt, e0, e1) == cudaSuccess) ms += dt;
+    }
+    if (rc == TALSH_SUCCESS && (c == 0 || ms < best_ms)) {
+      best_ms = ms;
+      best = c;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaGetLastError();
+  if (rc != TALSH_SUCCESS) return rc;
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune_table[key] = best;
+    g_tune_entries.store((int)g_tune_table.size());
+  }
+  *choice = best;
+  return TALSH_SUCCESS;
+}
+
+extern "C" int tcTensorPermuteTuned(int data_kind, int rank, const int *dims_in, const int *o2n, int accumulate,
+                                    int *choice) {
+  using namespace tb;
+  int rc = validate(data_kind, rank, dims_in, o2n);
+  if (rc) return rc;
+  if (choice == nullptr) return TALSH_INVALID_ARGS;
+  *choice = -1;
+  if (rank == 0) return TALSH_SUCCESS;
+  Fused F;
+  if ((rc = fuse_dims(rank, dims_in, o2n, F)) != 0) return rc;
+  *choice = tuned_choice(tune_key(data_kind, accumulate ? kOpAdd : kOpCopy, F));
+  return TALSH_SUCCESS;
+}
+
+extern "C" int tcTensorPermuteTuneSet(int data_kind, int rank, const int *dims_in, const int *o2n, int accumulate,
+                                      int choice) {
+  using namespace tb;
+  int rc = validate(data_kind, rank, dims_in, o2n);
+  if (rc) return rc;
+  if (choice < -1 || choice >= kTuneConfigs) return TALSH_INVALID_ARGS;
+  if (rank == 0) return TALSH_SUCCESS;
+  Fused F;
+  if ((rc = fuse_dims(rank, dims_in, o2n, F)) != 0) return rc;
+  const uint64_t key = tune_key(data_kind, accumulate ? kOpAdd : kOpCopy, F);
+  if (key == 0) return TALSH_SUCCESS;
+  if (choice >= 0) {  // the plan of the choice must exist for this case
+    Plan plan;
+    if (build_plan(kind_size(data_kind), F, plan, accumulate ? kOpAdd : kOpCopy, tune_cfg(choice)) != 0)
+      return TALSH_INVALID_ARGS;
+  }
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  if (choice < 0) g_tune_table.erase(key);
+  else g_tune_table[key] = choice;
+  g_tune_entries.store((int)g_tune_table.size());
+  return TALSH_SUCCESS;
+}
+
+extern "C" void tcTensorPermuteTuneReset(void) {
+  using namespace tb;
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune_table.clear();
+  g_tune_entries.store(0);
 }
 
 namespace tb {

@@ -1955,14 +1955,25 @@ int talshTensorPlace(talsh_tens_t *t, int dev_id, int dev_kind, void *dev_mem, i
   TaskRec *tr = new TaskRec();
   tr->gpu = gpu;
   tr->st = G.stream;
-  tr->nargs = 0;  // placement has its own bookkeeping below
+  tr->nargs = 0;  // set below for a move: the source is discarded when the task completes
+  // A copy of a GPU image to the Host runs on the copy-back stream after the
+  // work queued on the compute stream (which may still be producing the
+  // image), so it overlaps later tasks' compute and staging; other
+  // placements run on the compute stream.
+  const bool to_host = (dvk == DEV_HOST);
+  cudaStream_t cs = to_host ? G.d2h : G.stream;
   for (auto &e : tr->ev) e = event_get(gpu);
   cudaEventRecord(tr->ev[0], G.stream);
-  cudaEventRecord(tr->ev[1], G.stream);
-  wait_pending(gpu, G.stream, t->dev_rsc[src].gmem_p, bytes);
-  int rc = copy_between(dst, flat, t->dev_rsc[src].gmem_p, t->dev_rsc[src].dev_id, bytes, G.stream);
-  cudaEventRecord(tr->ev[2], G.stream);
-  cudaEventRecord(tr->ev[3], G.stream);
+  if (to_host) cudaStreamWaitEvent(cs, tr->ev[0], 0);
+  cudaEventRecord(tr->ev[1], cs);
+  wait_pending(gpu, cs, t->dev_rsc[src].gmem_p, bytes);
+  int rc = copy_between(dst, flat, t->dev_rsc[src].gmem_p, t->dev_rsc[src].dev_id, bytes, cs);
+  if (to_host && rc == TALSH_SUCCESS) note_pending(gpu, dst, bytes, cs);
+  cudaEventRecord(tr->ev[2], cs);
+  cudaEventRecord(tr->ev[3], cs);
+  // A kept source may be written by later work on the compute stream: that
+  // work waits for the copy.
+  if (to_host && copy_ctrl == COPY_K) cudaStreamWaitEvent(G.stream, tr->ev[3], 0);
   tk->task_p = tr;
   tk->task_error = -1;
   tk->dev_kind = DEV_NVIDIA_GPU;
@@ -1980,9 +1991,11 @@ int talshTensorPlace(talsh_tens_t *t, int dev_id, int dev_kind, void *dev_mem, i
     if (task == nullptr) talshTaskDestroy(tk);
     return TALSH_FAILURE;
   }
-  // The new image becomes visible right away (reads of it are ordered on the
-  // same stream); the moved source is discarded once the copy finished.
-  if (t->ndev >= t->dev_rsc_len) { cudaStreamSynchronize(G.stream); if (owned) mem_free(dst); return TALSH_LIMIT_EXCEEDED; }
+  // The new image becomes visible right away (reads of a GPU image are ordered
+  // on the compute stream; staging reads of a Host image wait for the copy,
+  // which is recorded as pending); a moved source becomes unavailable now and
+  // is discarded when the task completes (task_finalize applies COPY_M).
+  if (t->ndev >= t->dev_rsc_len) { sync_gpu_streams(gpu); if (owned) mem_free(dst); return TALSH_LIMIT_EXCEEDED; }
   const int k = t->ndev++;
   t->dev_rsc[k].dev_id = flat;
   t->dev_rsc[k].gmem_p = dst;
@@ -1991,8 +2004,14 @@ int talshTensorPlace(talsh_tens_t *t, int dev_id, int dev_kind, void *dev_mem, i
   t->data_kind[k] = t->data_kind[src];
   t->avail[k] = YEP;
   if (copy_ctrl == COPY_M) {
-    sync_gpu_streams(gpu);
-    image_discard(t, src);
+    ArgRec &a = tr->a[0];
+    a.t = t;
+    a.src_dev = t->dev_rsc[src].dev_id;
+    a.src_ptr = t->dev_rsc[src].gmem_p;
+    a.coh = COPY_M;
+    a.bytes = bytes;
+    tr->nargs = 1;
+    t->avail[src] = NOPE;
   }
   if (task == nullptr) {
     int stats = 0;

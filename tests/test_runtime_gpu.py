@@ -71,6 +71,40 @@ def test_coherence_move_and_place(talsh):
         assert t.destruct() == 0
 
 
+def test_chain_with_asynchronous_place(talsh):
+    """A transpose and a transpose-add that keep D on the GPU between them
+    (COPY_MK, then COPY_KD), then an asynchronous talshTensorPlace(COPY_M) of D
+    into its Host buffer: one upload of L, one copy back of D, bit-exact with
+    the oracle; the moved GPU image is discarded when the place task completes,
+    L's kept image by the add."""
+    L = talsh
+    rng = np.random.default_rng(5)
+    for kind in (T.R4, T.R8, T.C8):
+        A = rand((17, 31, 6), kind, rng)
+        D = fort(np.zeros((6, 17, 31), dtype=A.dtype))
+        d, a = host_tensor(D), host_tensor(A)
+        tasks = [T.Task() for _ in range(3)]
+        for tk in tasks:
+            L.talshTaskClean(C.byref(tk))
+        assert L.talshTensorCopy(b"D(c,a,b)=L(a,b,c)", d.ref, a.ref, 0, T.DEV_NVIDIA_GPU, T.COPY_MK,
+                                 C.byref(tasks[0])) == 0
+        assert L.talshTensorAdd(b"D(c,a,b)+=L(a,b,c)", d.ref, a.ref, 0.5, 0.0, 0, T.DEV_NVIDIA_GPU, T.COPY_KD,
+                                C.byref(tasks[1])) == 0
+        assert L.talshTensorPlace(d.ref, 0, T.DEV_HOST, C.c_void_p(D.ctypes.data), T.COPY_M,
+                                  C.byref(tasks[2])) == 0
+        st = C.c_int()
+        for tk in tasks:
+            assert L.talshTaskWait(C.byref(tk), C.byref(st)) == 0 and st.value == T.TALSH_TASK_COMPLETED
+            assert L.talshTaskDestruct(C.byref(tk)) == 0
+        ref = O.permute(A, [2, 3, 1])
+        O.tensor_add(ref, A, [2, 3, 1], 0.5)
+        assert same_bits(D, ref), kind
+        assert [img[0] for img in d.images()] == [0]
+        assert [img[0] for img in a.images()] == [0]
+        for t in (d, a):
+            assert t.destruct() == 0
+
+
 def test_gpu_resident_tensors(talsh):
     """Tensors constructed on the GPU stay there; chains of operations run without transfers."""
     L = talsh
