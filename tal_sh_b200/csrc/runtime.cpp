@@ -1925,7 +1925,13 @@ int talshTensorPlace(talsh_tens_t *t, int dev_id, int dev_kind, void *dev_mem, i
     decode_device_id(t->dev_rsc[i].dev_id, &dk);
     if (src < 0 || dk == DEV_HOST) src = i;
   }
-  if (src < 0) return TALSH_NOT_FOUND;
+  if (src < 0) {
+    // Every image held by a task still in flight: the placement can run once
+    // that task has completed (as for the operations).
+    bool held = false;
+    for (int i = 0; i < t->ndev; ++i) held = held || t->avail[i] != YEP;
+    return held ? TRY_LATER : TALSH_NOT_FOUND;
+  }
   int es = 0;
   tens_valid_data_kind(t->data_kind[src], &es);
   const size_t bytes = shape_volume(t->shape_p) * (size_t)es;

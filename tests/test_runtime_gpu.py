@@ -86,16 +86,25 @@ def test_chain_with_asynchronous_place(talsh):
         tasks = [T.Task() for _ in range(3)]
         for tk in tasks:
             L.talshTaskClean(C.byref(tk))
-        assert L.talshTensorCopy(b"D(c,a,b)=L(a,b,c)", d.ref, a.ref, 0, T.DEV_NVIDIA_GPU, T.COPY_MK,
-                                 C.byref(tasks[0])) == 0
-        assert L.talshTensorAdd(b"D(c,a,b)+=L(a,b,c)", d.ref, a.ref, 0.5, 0.0, 0, T.DEV_NVIDIA_GPU, T.COPY_KD,
-                                C.byref(tasks[1])) == 0
-        assert L.talshTensorPlace(d.ref, 0, T.DEV_HOST, C.c_void_p(D.ctypes.data), T.COPY_M,
-                                  C.byref(tasks[2])) == 0
         st = C.c_int()
-        for tk in tasks:
+
+        def wait(tk):
             assert L.talshTaskWait(C.byref(tk), C.byref(st)) == 0 and st.value == T.TALSH_TASK_COMPLETED
             assert L.talshTaskDestruct(C.byref(tk)) == 0
+
+        assert L.talshTensorCopy(b"D(c,a,b)=L(a,b,c)", d.ref, a.ref, 0, T.DEV_NVIDIA_GPU, T.COPY_MK,
+                                 C.byref(tasks[0])) == 0
+        # D is held by the copy until it completes: a later operation on it is refused for now
+        assert L.talshTensorPlace(d.ref, 0, T.DEV_HOST, C.c_void_p(D.ctypes.data), T.COPY_M,
+                                  C.byref(tasks[2])) == T.TRY_LATER
+        wait(tasks[0])
+        assert L.talshTensorAdd(b"D(c,a,b)+=L(a,b,c)", d.ref, a.ref, 0.5, 0.0, 0, T.DEV_NVIDIA_GPU, T.COPY_KD,
+                                C.byref(tasks[1])) == 0
+        wait(tasks[1])
+        assert [img[0] for img in d.images()] == [GPU0]  # moved to the GPU by the copy, kept by the add
+        assert L.talshTensorPlace(d.ref, 0, T.DEV_HOST, C.c_void_p(D.ctypes.data), T.COPY_M,
+                                  C.byref(tasks[2])) == 0
+        wait(tasks[2])
         ref = O.permute(A, [2, 3, 1])
         O.tensor_add(ref, A, [2, 3, 1], 0.5)
         assert same_bits(D, ref), kind

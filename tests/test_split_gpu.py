@@ -114,8 +114,6 @@ def _run_complex(torch, pattern, ext, slices, alpha, conj, acc=True, seed=0):
     assert rc == 0, (rc, L.tcLastErrorString())
     torch.cuda.synchronize()
     got = d.cpu().numpy().reshape(dd, order="F")
-    if raw:
-        return got.tobytes(order="F")
     ref = D0.copy(order="F")
     assert O.tensor_contract(ref, Lh, Rh, dig, alpha[0], alpha[1], conj, acc) == 0
     term = ref - (D0 if acc else 0)
