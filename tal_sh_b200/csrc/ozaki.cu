@@ -495,8 +495,8 @@ constexpr int kWsDiagPerPass = 3;             // accumulators per pass: 3 x 128 
 // format (bits 4-5: 1 F32, 2 S32), A/B formats (bits 7-9, 10-12: signed int8
 // 1; bf16 1 and tf32 2 of kind::f16/tf32; e4m3 0 of kind::f8f6f4).
 constexpr uint32_t kIdescMN128 = ((uint32_t)(kWsBN >> 3) << 17) | ((uint32_t)(kOzBM >> 4) << 24);
-// M = 256 (a CTA pair, cta_group::2), N = 128.
-constexpr uint32_t kIdescPair = ((uint32_t)(kWsBN >> 3) << 17) | ((uint32_t)(256 >> 4) << 24);
+// M = 256 (a CTA pair, cta_group::2), N = 256.
+constexpr uint32_t kIdescPair = ((uint32_t)(256 >> 3) << 17) | ((uint32_t)(256 >> 4) << 24);
 template <int FORM> struct FormMma;
 template <> struct FormMma<kFormInt8> {
   static constexpr uint32_t idesc = (2u << 4) | (1u << 7) | (1u << 10) | kIdescMN128;
@@ -799,13 +799,13 @@ __global__ void __launch_bounds__(kOzWsThreads, 1)
 
 // ---------------------------------------------------------------------------
 // Pair (cta_group::2) form of the warp-specialised GEMM.  Two CTAs of a
-// cluster compute one 256 x 128 tile: each holds 128 rows of A and 64 rows of
-// B per slice in its shared memory, and the even CTA issues MMAs of M = 256
-// that read both CTAs' operands (each SM multiplies its own A rows by all of
-// B; the B halves are exchanged between the pair), so every SM streams 25 %
-// fewer operand bytes and its tensor core reads half the B bytes from shared
-// memory per MMA.  Every SM keeps its own rows' accumulators in its tensor
-// memory (3 diagonals x 128 columns per pass, as in the single-CTA form).
+// cluster compute one 256 x 256 tile: each holds 128 rows of A and 128 rows
+// of B per slice in its shared memory, and the even CTA issues MMAs of
+// M = 256, N = 256 that read both CTAs' operands (each SM multiplies its own
+// A rows by all of B; the B halves are exchanged between the pair), so one
+// instruction does four times the work of the single-CTA form's 128 x 128.
+// Every SM keeps its own rows' accumulators in its tensor memory: 2
+// diagonals x 256 columns per pass, three passes for six slices.
 // Synchronisation: both CTAs' copies complete on the even CTA's "full"
 // barriers (the copies carry .cta_group::2); the even CTA's commits arrive on
 // "empty" and "done" in both CTAs (.multicast::cluster on tcgen05.commit);
@@ -869,7 +869,9 @@ __device__ __forceinline__ bool mbar_wait_cluster(uint64_t *bar, uint32_t parity
   return false;
 }
 
-constexpr int kPairBTile = 64 * kWsBox;  // 4 KB: this CTA's 64 rows of a B slice box
+constexpr int kPairBN = 256;                 // tile columns of the pair (UMMA N)
+constexpr int kPairDiag = 2;                 // accumulators per pass: 2 x 256 TMEM columns
+constexpr int kPairBTile = 128 * kWsBox;     // 8 KB: this CTA's 128 rows of a B slice box
 
 struct OzPairArgs {
   uint32_t spin_limit;
@@ -901,7 +903,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kOzWsThreads, 1)
   const uint32_t rank = cluster_ctarank();
   const int S = a.S, nst = a.nst;
   const int slot_bytes = S * (kWsATile + kPairBTile);
-  const int npass = (S + kWsDiagPerPass - 1) / kWsDiagPerPass;
+  const int npass = (S + kPairDiag - 1) / kPairDiag;
   int tm, tn;  // 256-row tile of the pair, 128-column tile
   {
     const int id = blockIdx.x >> 1;
@@ -915,8 +917,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kOzWsThreads, 1)
   }
   const int64_t nkb = a.kb1 - a.kb0;
   const int64_t nbox = (nkb + 1) / 2;
-  auto pass_g0 = [&](int p) { return 2 + p * kWsDiagPerPass; };
-  auto pass_g1 = [&](int p) { return min(S + 1, pass_g0(p) + kWsDiagPerPass - 1); };
+  auto pass_g0 = [&](int p) { return 2 + p * kPairDiag; };
+  auto pass_g1 = [&](int p) { return min(S + 1, pass_g0(p) + kPairDiag - 1); };
 
   if (warp == 1) {
     asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base_sh)),
@@ -968,7 +970,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kOzWsThreads, 1)
               const uint32_t sa = sst + (uint32_t)((j * smax + s) * kWsATile);
               const uint32_t sb = sst + (uint32_t)(S * kWsATile + (j * smax + s) * kPairBTile);
               tma_load_2d_pair(sa, &mapA, kx, (int)(s * a.Mp + tm * 256 + rank * 128), fbar);
-              tma_load_2d_pair(sb, &mapB, kx, (int)(s * a.Np + tn * kWsBN + rank * 64), fbar);
+              tma_load_2d_pair(sb, &mapB, kx, (int)(s * a.Np + tn * kPairBN + rank * 128), fbar);
             }
           }
         }
@@ -1000,7 +1002,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kOzWsThreads, 1)
             const int nsteps = (2 * (it + j) + 1 < nkb) ? 2 : 1;
             for (int kk = 0; kk < nsteps; ++kk) {
               for (int g = g0; g <= g1; ++g) {
-                const uint32_t dcol = tmem + (uint32_t)((g - g0) * kWsBN);
+                const uint32_t dcol = tmem + (uint32_t)((g - g0) * kPairBN);
                 for (int s1 = 1; s1 < g; ++s1) {
                   const uint32_t sa = sst + (uint32_t)((j * smax + s1 - 1) * kWsATile + kk * kWsBK);
                   const uint32_t sb =
@@ -1033,13 +1035,13 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kOzWsThreads, 1)
       const bool first = (p == 0);
       if (ok) {
         const bool rd = !(first && !a.beta);
-        for (int c = 0; c < kWsBN / 16; ++c) {
+        for (int c = 0; c < kPairBN / 16; ++c) {
           double *ptr[16];
           double old[16];
           int esc[16];
 #pragma unroll
           for (int i = 0; i < 16; ++i) {
-            const int64_t n = (int64_t)tn * kWsBN + c * 16 + i;
+            const int64_t n = (int64_t)tn * kPairBN + c * 16 + i;
             const bool okn = mrow && n < a.N;
             ptr[i] = okn ? a.D + dm + a.nD[n] : nullptr;
             esc[i] = okn ? em + a.eb[n] : 0;
@@ -1051,7 +1053,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kOzWsThreads, 1)
           for (int i = 0; i < 16; ++i) acc[i] = 0.0;
           for (int g = g0; g <= g1; ++g) {
             uint32_t v[16];
-            const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)((g - g0) * kWsBN + c * 16);
+            const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)((g - g0) * kPairBN + c * 16);
             asm volatile(
                 "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
                 : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
@@ -1165,7 +1167,7 @@ struct OzPlan {
 void oz_plan(int64_t M, int64_t N, int64_t K, int S, OzPlan &p, int esize = 1) {
   p.M = M; p.N = N; p.K = K;
   p.Mp = round_up(std::max<int64_t>(M, 1), 2 * kOzBM);  // whole 256-row tiles of the CTA-pair kernel
-  p.Np = round_up(std::max<int64_t>(N, 1), 128);  // multiple of both kernels' tile width
+  p.Np = round_up(std::max<int64_t>(N, 1), 256);  // whole tiles of every kernel (the pair's are 256 wide)
   p.Kp = round_up(std::max<int64_t>(K, 1), kOzBK / esize);
   size_t off = 0;
   auto take = [&](size_t bytes) { const size_t o = off; off = (off + bytes + 255) & ~size_t(255); return o; };
@@ -1287,15 +1289,20 @@ size_t contract_split_scratch(int kind, const int *cptrn, int drank, const int *
 
 namespace {
 
-// The CTA-pair kernel or the single-CTA kernel (TALSH_B200_SPLIT_PAIR=1 / 0;
-// the default is kSplitPairDefault).
-constexpr bool kSplitPairDefault = false;
-bool split_pair_enabled() {
-  static const bool v = [] {
+// Which GEMM runs: the CTA-pair kernel (256 x 256 tiles) when its tiles give
+// every SM work (two CTAs per tile), else the single-CTA kernel (128 x 128
+// tiles, four times as many); TALSH_B200_SPLIT_PAIR=1 / 0 forces one.
+int split_pair_mode() {
+  static const int v = [] {
     const char *e = std::getenv("TALSH_B200_SPLIT_PAIR");
-    return e ? std::atoi(e) != 0 : kSplitPairDefault;
+    return e ? (std::atoi(e) != 0 ? 1 : 0) : -1;
   }();
   return v;
+}
+bool split_pair_wanted(int64_t Mp, int64_t Np) {
+  const int mode = split_pair_mode();
+  if (mode >= 0) return mode == 1;
+  return 2 * (Mp / 256) * (Np / 256) >= current_sm_count();
 }
 
 // Stage ring of the pair kernel, plus 1 KB of alignment slack and 8 KB of
@@ -1403,7 +1410,7 @@ int contract_split_launch(int kind, const int *cptrn, int drank, const int *ddim
   const bool simple = oz_force_simple() && fc.form == kFormInt8;
   // The pair kernel reads [S][rows][Kp] through tensor maps (its copies
   // complete on the even CTA's barriers); the stall test runs the single-CTA one.
-  const bool pair = !simple && g_stall_test.load() == 0 && split_pair_enabled() &&
+  const bool pair = !simple && g_stall_test.load() == 0 && split_pair_wanted(p.Mp, p.Np) &&
                     (int64_t)slices * p.Mp < 0x7fffffffLL && (int64_t)slices * p.Np < 0x7fffffffLL;
   const int tiled = (TB_SPLIT_TILED && !simple && !pair) ? 1 : 0;
   auto split_float = [&](auto kern) {
@@ -1453,19 +1460,19 @@ int contract_split_launch(int kind, const int *cptrn, int drank, const int *ddim
     kc32 = kc_el > 0 ? std::max<int64_t>(2, round_up(kc_el * es, kOzBK) / kWsBK) : nkb32;
   }
   if (pair && make_slice_map(&mapA, As, Kbytes, slices * p.Mp, kOzBM) &&
-      make_slice_map(&mapB, Bs, Kbytes, slices * p.Np, 64)) {
+      make_slice_map(&mapB, Bs, Kbytes, slices * p.Np, 128)) {
     const int stage_bytes = slices * (kWsATile + kPairBTile);
     OzPairArgs w;
     w.spin_limit = kSpinLimit;
     w.Mp = p.Mp; w.Np = p.Np; w.S = slices;
     w.nst = std::max(2, std::min(8, kOzPairSmem / stage_bytes));
     w.tiles_m2 = (int)(p.Mp / (2 * kOzBM));
-    w.tiles_n = (int)(p.Np / kWsBN);
+    w.tiles_n = (int)(p.Np / kPairBN);
     w.group_m = std::max(1, ws_group_m() / 2);
     w.ea = ea; w.eb = eb; w.D = (double *)D; w.mD = mD; w.nD = nD; w.M = M; w.N = N;
     w.alpha = alpha_re; w.err = err;
     w.tmem_cols = 32;
-    while (w.tmem_cols < (uint32_t)(std::min(slices, kWsDiagPerPass) * kWsBN)) w.tmem_cols <<= 1;
+    while (w.tmem_cols < (uint32_t)(std::min(slices, kPairDiag) * kPairBN)) w.tmem_cols <<= 1;
     switch (fc.form) {
       case kFormBF16: return launch_pair_form<kFormBF16>(mapA, mapB, w, nkb32, kc32, accumulative, stage_bytes, st);
       case kFormTF32: return launch_pair_form<kFormTF32>(mapA, mapB, w, nkb32, kc32, accumulative, stage_bytes, st);
