@@ -1342,20 +1342,21 @@ int build_plan(int esize, const Fused &F, Plan &plan, int op = kOpCopy, const Pl
   fill_map(P.wmap, P.wb_dims, P.nwb, true, P.a_in_B ? -1 : P.a_last);
   fill_map(P.ymap, P.b_dims, P.nb, false, -1);
   // Output vector width: every output run start, run length and partial run
-  // length must be a multiple of 16 bytes.  Reads are element-granular
+  // length must be a multiple of the vector (16 bytes, or 8 bytes for 4-byte
+  // elements when 16 do not divide them).  Reads are element-granular
   // asynchronous copies and need no alignment beyond the element.
   const int vec = 16 / esize;
   plan.vin = 1;
   plan.vout = 1;
-  if (vec > 1) {
-    bool ok = (P.Lo % vec) == 0;
+  for (int v = vec; v > 1 && plan.vout == 1 && (v == vec || esize == 4); v /= 2) {
+    bool ok = (P.Lo % v) == 0;
     const int64_t partial = P.ext[P.b_last] % P.tl[P.b_last];
-    if (partial && ((int64_t)P.b_pre * partial) % vec) ok = false;
+    if (partial && ((int64_t)P.b_pre * partial) % v) ok = false;
     for (int i = 0; i < n && ok; ++i) {
-      if (!inB[i] && P.tl[i] > 1 && P.ostr[i] % vec) ok = false;       // run offsets
-      if (P.ntile[i] > 1 && (P.tl[i] * P.ostr[i]) % vec) ok = false;   // tile bases
+      if (!inB[i] && P.tl[i] > 1 && P.ostr[i] % v) ok = false;       // run offsets
+      if (P.ntile[i] > 1 && (P.tl[i] * P.ostr[i]) % v) ok = false;   // tile bases
     }
-    if (ok) plan.vout = vec;
+    if (ok) plan.vout = v;
   }
   // Shared memory: the stage buffers and the run tables.  Each buffer is
   // rounded up to whole 128-byte rows: the swizzle permutes within rows.  The
@@ -1487,8 +1488,11 @@ int launch_typed(const Plan &plan, const void *src, void *dst, int conj, const S
   P.sdev_kind = sc.sdev_kind;
   P.sdev_conj = sc.sdev_conj;
   constexpr int VEC = 16 / sizeof(T);
-  const bool dst_al = ((uintptr_t)dst % 16) == 0;
-  const int vout = (plan.vout > 1 && dst_al) ? VEC : 1;
+  // 4-byte elements may also run with 8-byte vectors (VOUT 2), on the
+  // register-table and bulk kernels
+  int vout = plan.vout;
+  if (vout != VEC && (VEC != 4 || !P.reg)) vout = 1;
+  if (vout > 1 && ((uintptr_t)dst % ((uintptr_t)vout * sizeof(T))) != 0) vout = 1;
   P.y_step = (P.ymap.n >= 1 && P.ymap.ext[0] % vout == 0) ? 1 : 0;
   P.nv = P.Lo / vout;
   make_magic((uint32_t)P.nv, P.mg_nv, P.sh_nv);
@@ -1501,8 +1505,11 @@ int launch_typed(const Plan &plan, const void *src, void *dst, int conj, const S
   if (P.reg && P.bulk) {
     auto run_b = [&](auto kc) {
       constexpr int K = decltype(kc)::value;
-      if (vout > 1) run(permute_bulk_kernel<T, K, VEC, OP>);
-      else run(permute_bulk_kernel<T, K, 1, OP>);
+      if (vout == VEC) run(permute_bulk_kernel<T, K, VEC, OP>);
+      else if constexpr (VEC == 4) {
+        if (vout == 2) run(permute_bulk_kernel<T, K, 2, OP>);
+        else run(permute_bulk_kernel<T, K, 1, OP>);
+      } else run(permute_bulk_kernel<T, K, 1, OP>);
     };
     if (P.V <= kThreads * 4) run_b(std::integral_constant<int, 4>{});
     else run_b(std::integral_constant<int, 8>{});
@@ -1512,13 +1519,16 @@ int launch_typed(const Plan &plan, const void *src, void *dst, int conj, const S
   if (P.reg) {
     auto run_k = [&](auto kc) {
       constexpr int K = decltype(kc)::value;
-      if (P.swz) {
-        if (vout > 1) run(permute_reg_kernel<T, K, VEC, OP, true>);
-        else run(permute_reg_kernel<T, K, 1, OP, true>);
-      } else {
-        if (vout > 1) run(permute_reg_kernel<T, K, VEC, OP, false>);
-        else run(permute_reg_kernel<T, K, 1, OP, false>);
-      }
+      auto pick = [&](auto swz) {
+        constexpr bool SW = decltype(swz)::value;
+        if (vout == VEC) run(permute_reg_kernel<T, K, VEC, OP, SW>);
+        else if constexpr (VEC == 4) {
+          if (vout == 2) run(permute_reg_kernel<T, K, 2, OP, SW>);
+          else run(permute_reg_kernel<T, K, 1, OP, SW>);
+        } else run(permute_reg_kernel<T, K, 1, OP, SW>);
+      };
+      if (P.swz) pick(std::true_type{});
+      else pick(std::false_type{});
     };
     if (P.V <= kThreads * 4) run_k(std::integral_constant<int, 4>{});
     else run_k(std::integral_constant<int, 8>{});
