@@ -142,9 +142,6 @@ __device__ __forceinline__ void cp16(uint32_t s, const void *g) {
 // 16-byte chunk c of tile row i sits at chunk c ^ ((i >> 1) & 3), the layout
 // make_desc_sw64 describes.  One contiguous bulk copy then moves the slices of
 // a box into a stage.  kb: byte offset in the row; nbox: 64-byte boxes per row.
-#ifndef TB_SPLIT_TILED
-#define TB_SPLIT_TILED 1
-#endif
 __device__ __forceinline__ int64_t tiled_off(int64_t r, int64_t kb, int s, int S, int64_t nbox) {
   const int64_t tile = ((r >> 7) * nbox + (kb >> 6)) * S + s;
   const int i = (int)(r & 127);
@@ -429,13 +426,14 @@ __global__ void __launch_bounds__(kOzThreads, 1) oz_gemm_kernel(const OzArgs a) 
 }
 
 // ---------------------------------------------------------------------------
-// Warp-specialised mainloop.  Warp 0: one thread issues the TMA tile copies of
-// each stage (2-D tensor maps over the slice matrices, 64-byte x rows boxes
-// with the 64-byte swizzle: two UMMA K steps per box, half the TMA requests of
-// 32-byte boxes).  Warp 1: one
-// thread issues the MMAs of a stage once its copies have landed and commits
-// them to the stage's "empty" barrier; warp 1 also owns the tensor memory.
-// Warps 2-5: epilogue, TMEM lane quadrant (warp % 4).
+// Warp-specialised mainloop (single CTA per 128 x 128 tile).  Warp 0: one
+// thread fills each stage with bulk copies of the tiled slice layout (64-byte
+// x 128-row swizzled tiles: two UMMA K steps per box, the slices of a box
+// adjacent, one copy per operand and box).  Warp 1: one thread issues the MMAs
+// of a stage once its copies have landed and commits them to the stage's
+// "empty" barrier; warp 1 also owns the tensor memory.  Warps 2-5: epilogue,
+// TMEM lane quadrant (warp % 4).  The pair kernel further down reads the same
+// boxes through 2-D tensor maps over the plain slice layout.
 // ---------------------------------------------------------------------------
 constexpr int kOzWsThreads = 192;
 constexpr int kWsBK = 32;                    // K bytes of one UMMA K step
@@ -469,7 +467,7 @@ __device__ __forceinline__ void bulk_load(uint32_t sdst, const void *gsrc, uint3
 }
 
 struct OzWsArgs {
-  const unsigned char *At, *Bt;  // tiled slices (tiled_off), or null: copies through the tensor maps
+  const unsigned char *At, *Bt;  // tiled slices (tiled_off)
   int64_t nbox;                  // 64-byte K boxes per slice row
   uint32_t spin_limit;  // iterations of every bounded mbarrier wait
   int stall_test;       // 1: the producer issues no copies, so the MMA warp's first wait runs out
@@ -573,8 +571,7 @@ __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
 // contribution into D before the next pass reuses the accumulators.
 template <int FORM>
 __global__ void __launch_bounds__(kOzWsThreads, 1)
-    oz_gemm_ws_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
-                      const OzWsArgs a) {
+    oz_gemm_ws_kernel(const OzWsArgs a) {
   extern __shared__ __align__(128) unsigned char smem[];
   constexpr int kMaxStages = 8;
   __shared__ __align__(8) uint64_t full[kMaxStages], empty[kMaxStages], done, drained;
@@ -615,10 +612,6 @@ __global__ void __launch_bounds__(kOzWsThreads, 1)
     mbar_init(&drained, 128);
     abort_sh = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::);
-    if (a.At == nullptr) {
-      asm volatile("prefetch.tensormap [%0];" ::"l"((uint64_t)&mapA) : "memory");
-      asm volatile("prefetch.tensormap [%0];" ::"l"((uint64_t)&mapB) : "memory");
-    }
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::);
   __syncthreads();
@@ -647,23 +640,13 @@ __global__ void __launch_bounds__(kOzWsThreads, 1)
           mbar_expect_tx(&full[st], (uint32_t)(nk * smax * (kWsATile + kWsBTile128)));
           const uint32_t sst = sbase + (uint32_t)(st * slot_bytes);
           for (int j = 0; j < nk; ++j) {
-            if (a.At != nullptr) {
-              // slices 0 .. smax-1 of box (tm or tn, kb0/2 + it + j) are adjacent
-              const int64_t box = a.kb0 / 2 + it + j;
-              const uint32_t bytes = (uint32_t)(smax * kWsATile);
-              bulk_load(sst + (uint32_t)(j * smax * kWsATile),
-                        a.At + ((int64_t)tm * a.nbox + box) * S * kWsATile, bytes, &full[st]);
-              bulk_load(sst + (uint32_t)(S * kWsATile + j * smax * kWsBTile128),
-                        a.Bt + ((int64_t)tn * a.nbox + box) * S * kWsBTile128, bytes, &full[st]);
-              continue;
-            }
-            const int kx = (int)((a.kb0 + 2 * (it + j)) * kWsBK);
-            for (int s = 0; s < smax; ++s) {
-              const uint32_t sa = sst + (uint32_t)((j * smax + s) * kWsATile);
-              const uint32_t sb = sst + (uint32_t)(S * kWsATile + (j * smax + s) * kWsBTile128);
-              tma_load_2d(sa, &mapA, kx, (int)(s * a.Mp + tm * kOzBM), &full[st]);
-              tma_load_2d(sb, &mapB, kx, (int)(s * a.Np + tn * kWsBN), &full[st]);
-            }
+            // slices 0 .. smax-1 of box (tm or tn, kb0/2 + it + j) are adjacent
+            const int64_t box = a.kb0 / 2 + it + j;
+            const uint32_t bytes = (uint32_t)(smax * kWsATile);
+            bulk_load(sst + (uint32_t)(j * smax * kWsATile),
+                      a.At + ((int64_t)tm * a.nbox + box) * S * kWsATile, bytes, &full[st]);
+            bulk_load(sst + (uint32_t)(S * kWsATile + j * smax * kWsBTile128),
+                      a.Bt + ((int64_t)tn * a.nbox + box) * S * kWsBTile128, bytes, &full[st]);
           }
         }
       }
@@ -1339,7 +1322,7 @@ int launch_pair_form(const CUtensorMap &mapA, const CUtensorMap &mapB, OzPairArg
 // The warp-specialised GEMM of one form over K-step launches [0, nkb32) in
 // chunks of kc32 steps (32 bytes each).
 template <int FORM>
-int launch_ws_form(const CUtensorMap &mapA, const CUtensorMap &mapB, OzWsArgs w, int64_t nkb32, int64_t kc32,
+int launch_ws_form(OzWsArgs w, int64_t nkb32, int64_t kc32,
                    int accumulative, int stage_bytes, cudaStream_t st) {
   static std::atomic<uint64_t> ws_attr{0};
   once_per_device(ws_attr, [] {
@@ -1350,7 +1333,7 @@ int launch_ws_form(const CUtensorMap &mapA, const CUtensorMap &mapB, OzWsArgs w,
     w.kb0 = kb;
     w.kb1 = std::min(nkb32, kb + kc32);
     w.beta = (kb == 0) ? (accumulative ? 1 : 0) : 1;
-    oz_gemm_ws_kernel<FORM><<<(unsigned)tiles, kOzWsThreads, w.nst * stage_bytes + 1024, st>>>(mapA, mapB, w);
+    oz_gemm_ws_kernel<FORM><<<(unsigned)tiles, kOzWsThreads, w.nst * stage_bytes + 1024, st>>>(w);
     note_launch();
     const int rc = check_launch("oz_gemm_ws_kernel");
     if (rc != 0) return rc;
@@ -1408,11 +1391,19 @@ int contract_split_launch(int kind, const int *cptrn, int drank, const int *ddim
   // The warp-specialised GEMM reads the tiled layout with bulk copies; the
   // single-loop int8 kernel (TALSH_B200_SPLIT_SIMPLE=1) reads [S][rows][Kp].
   const bool simple = oz_force_simple() && fc.form == kFormInt8;
-  // The pair kernel reads [S][rows][Kp] through tensor maps (its copies
-  // complete on the even CTA's barriers); the stall test runs the single-CTA one.
+  const int64_t Kbytes = p.Kp * es;
+  // The pair kernel reads [S][rows][Kp] through 2-D tensor maps (its copies
+  // complete on the even CTA's barriers; the maps need 32-bit row
+  // coordinates); the single-CTA kernel reads the tiled layout by bulk copies;
+  // the stall test runs the single-CTA kernel.
+  CUtensorMap mapA, mapB;
+  std::memset(&mapA, 0, sizeof(mapA));
+  std::memset(&mapB, 0, sizeof(mapB));
   const bool pair = !simple && g_stall_test.load() == 0 && split_pair_wanted(p.Mp, p.Np) &&
-                    (int64_t)slices * p.Mp < 0x7fffffffLL && (int64_t)slices * p.Np < 0x7fffffffLL;
-  const int tiled = (TB_SPLIT_TILED && !simple && !pair) ? 1 : 0;
+                    (int64_t)slices * p.Mp < 0x7fffffffLL && (int64_t)slices * p.Np < 0x7fffffffLL &&
+                    make_slice_map(&mapA, As, Kbytes, slices * p.Mp, kOzBM) &&
+                    make_slice_map(&mapB, Bs, Kbytes, slices * p.Np, 128);
+  const int tiled = (!simple && !pair) ? 1 : 0;
   auto split_float = [&](auto kern) {
     kern<<<(unsigned)p.Mp, 256, 0, st>>>(A64, M, K, p.Mp, p.Kp, slices, (unsigned char *)As, ea, tiled);
     note_launch();
@@ -1430,7 +1421,6 @@ int contract_split_launch(int kind, const int *cptrn, int drank, const int *ddim
       note_launch();
   }
   if ((rc = check_launch("split rows")) != 0) return rc;
-  const int64_t Kbytes = p.Kp * es;
   // K chunks keep every int32 accumulator exact: slices * Kc * 127^2 < 2^31.
   const int64_t kc_max = ((int64_t)0x7fffffff / ((int64_t)slices * 127 * 127)) / kOzBK;
   const int64_t nkb = p.Kp / kOzBK;
@@ -1450,17 +1440,13 @@ int contract_split_launch(int kind, const int *cptrn, int drank, const int *ddim
   if (grid.y > 65535) return TALSH_LIMIT_EXCEEDED;
   // Warp-specialised TMA pipeline when the tensor maps can be encoded (the
   // slice matrices' row counts must fit the 32-bit TMA coordinates).
-  CUtensorMap mapA, mapB;
-  std::memset(&mapA, 0, sizeof(mapA));
-  std::memset(&mapB, 0, sizeof(mapB));
   const int64_t nkb32 = Kbytes / kWsBK;
   int64_t kc32 = kc_max * (kOzBK / kWsBK);  // K steps per launch
   if (fc.form != kFormInt8) {
     const int64_t kc_el = fp32_kchunk();
     kc32 = kc_el > 0 ? std::max<int64_t>(2, round_up(kc_el * es, kOzBK) / kWsBK) : nkb32;
   }
-  if (pair && make_slice_map(&mapA, As, Kbytes, slices * p.Mp, kOzBM) &&
-      make_slice_map(&mapB, Bs, Kbytes, slices * p.Np, 128)) {
+  if (pair) {
     const int stage_bytes = slices * (kWsATile + kPairBTile);
     OzPairArgs w;
     w.spin_limit = kSpinLimit;
@@ -1480,19 +1466,15 @@ int contract_split_launch(int kind, const int *cptrn, int drank, const int *ddim
       default: return launch_pair_form<kFormInt8>(mapA, mapB, w, nkb32, kc32, accumulative, stage_bytes, st);
     }
   }
-  const bool ws = !simple && (tiled || ((int64_t)slices * p.Mp < 0x7fffffffLL &&
-                                        (int64_t)slices * p.Np < 0x7fffffffLL &&
-                                        make_slice_map(&mapA, As, Kbytes, slices * p.Mp, kOzBM) &&
-                                        make_slice_map(&mapB, Bs, Kbytes, slices * p.Np, kWsBN)));
-  if (!ws && fc.form != kFormInt8) return TALSH_NOT_IMPLEMENTED;  // the float forms have no simple kernel
-  if (ws) {
+  if (!tiled && fc.form != kFormInt8) return TALSH_NOT_IMPLEMENTED;  // the float forms have no simple kernel
+  if (tiled) {
     const int stage_bytes = slices * (kWsATile + kWsBTile128);
     const int nst = std::max(2, std::min(8, kOzWsSmem / stage_bytes));
     const int64_t tiles = (p.Mp / kOzBM) * (p.Np / kWsBN);
     if (tiles > 0x7fffffffLL) return TALSH_LIMIT_EXCEEDED;
     OzWsArgs w;
-    w.At = tiled ? (const unsigned char *)As : nullptr;
-    w.Bt = tiled ? (const unsigned char *)Bs : nullptr;
+    w.At = (const unsigned char *)As;
+    w.Bt = (const unsigned char *)Bs;
     w.nbox = Kbytes / kWsBox;
     const bool stall = g_stall_test.load() != 0;
     w.spin_limit = stall ? (1u << 12) : kSpinLimit;
@@ -1506,10 +1488,10 @@ int contract_split_launch(int kind, const int *cptrn, int drank, const int *ddim
     w.tmem_cols = 32;
     while (w.tmem_cols < (uint32_t)(std::min(slices, kWsDiagPerPass) * kWsBN)) w.tmem_cols <<= 1;
     switch (fc.form) {
-      case kFormBF16: return launch_ws_form<kFormBF16>(mapA, mapB, w, nkb32, kc32, accumulative, stage_bytes, st);
-      case kFormTF32: return launch_ws_form<kFormTF32>(mapA, mapB, w, nkb32, kc32, accumulative, stage_bytes, st);
-      case kFormFP8: return launch_ws_form<kFormFP8>(mapA, mapB, w, nkb32, kc32, accumulative, stage_bytes, st);
-      default: return launch_ws_form<kFormInt8>(mapA, mapB, w, nkb32, kc32, accumulative, stage_bytes, st);
+      case kFormBF16: return launch_ws_form<kFormBF16>(w, nkb32, kc32, accumulative, stage_bytes, st);
+      case kFormTF32: return launch_ws_form<kFormTF32>(w, nkb32, kc32, accumulative, stage_bytes, st);
+      case kFormFP8: return launch_ws_form<kFormFP8>(w, nkb32, kc32, accumulative, stage_bytes, st);
+      default: return launch_ws_form<kFormInt8>(w, nkb32, kc32, accumulative, stage_bytes, st);
     }
   }
   for (int64_t kb = 0; kb < nkb; kb += kc_max) {
