@@ -310,7 +310,27 @@ int find_image(const talsh_tens_t *t, int dev_id, const void *p) {
   return -1;
 }
 
+// The image a task made unavailable, or -1 when a later task has dropped it
+// already (an output's other images are discarded when the next operation on
+// it is scheduled); the same body may meanwhile be a second, available image
+// (a placement back into the same Host buffer), which is not this task's.
+int find_held_image(const talsh_tens_t *t, int dev_id, const void *p) {
+  for (int i = 0; i < t->ndev; ++i)
+    if (t->dev_rsc[i].dev_id == dev_id && t->dev_rsc[i].gmem_p == p && t->avail[i] != YEP) return i;
+  return -1;
+}
+
 // Preferred image for execution on [dvk, dvn]: that device, then that kind, then Host.
+// GPU bodies that became images of their tensors when the task writing them
+// was scheduled (a moved output, a kept or moved staged input, an output kept
+// in place), mapped to their GPU until that task completes.  Work on the same
+// GPU's compute stream is ordered after the writer and may use them at once;
+// work that would read them from anywhere else waits for the task.
+struct TaskRec;
+std::unordered_map<const void *, const TaskRec *> g_early;  // body -> the task writing it
+
+bool early_image(const talsh_tens_t *t, int i) { return g_early.count(t->dev_rsc[i].gmem_p) != 0; }
+
 int choose_image(const talsh_tens_t *t, int dvk, int dvn) {
   int same_kind = -1, host = -1;
   for (int i = 0; i < t->ndev; ++i) {
@@ -318,6 +338,7 @@ int choose_image(const talsh_tens_t *t, int dvk, int dvn) {
     int dk = DEV_NULL;
     const int dn = decode_device_id(t->dev_rsc[i].dev_id, &dk);
     if (dn < 0) continue;
+    if (dk == DEV_NVIDIA_GPU && early_image(t, i) && !(dvk == DEV_NVIDIA_GPU && dn == dvn)) continue;
     if (dk == dvk) {
       if (dn == dvn) return i;
       if (same_kind < 0) same_kind = i;
@@ -338,6 +359,8 @@ struct ArgRec {
   bool output = false;
   bool need_input = true;
   bool copy_back = false;  // output copied back into the source image
+  bool early = false;      // the GPU body became an image of the tensor at submission
+  bool held = false;       // the source image was made unavailable at submission
   size_t bytes = 0;
 };
 
@@ -378,8 +401,15 @@ int task_finalize(talsh_task_t *task, bool success) {
     ArgRec &a = tr->a[i];
     talsh_tens_t *t = a.t;
     if (t == nullptr || !healthy(t)) { rc = TALSH_FAILURE; continue; }
-    int img = find_image(t, a.src_dev, a.src_ptr);
-    if (a.dalloc) {
+    int img = a.held ? find_held_image(t, a.src_dev, a.src_ptr) : find_image(t, a.src_dev, a.src_ptr);
+    void *early_body = a.early ? (a.dalloc ? a.dptr : a.src_ptr) : nullptr;
+    if (early_body) {
+      const auto it = g_early.find(early_body);
+      if (it != g_early.end() && it->second == tr) g_early.erase(it);
+    }
+    if (a.dalloc && a.early) {
+      a.dptr = nullptr;  // an image of the tensor since the task was scheduled
+    } else if (a.dalloc) {
       if (success && (a.coh == COPY_M || a.coh == COPY_K) && t->ndev < t->dev_rsc_len) {
         const int k = t->ndev++;
         t->dev_rsc[k].dev_id = encode_device_id(DEV_NVIDIA_GPU, tr->gpu);
@@ -393,17 +423,22 @@ int task_finalize(talsh_task_t *task, bool success) {
       }
       a.dptr = nullptr;
     }
-    if (img < 0) continue;
-    if (success && (a.coh == COPY_D || a.coh == COPY_M)) {
-      if (t->avail[img] == NOPE) {
-        if (t->ndev > 1) {
-          if (image_discard(t, img) != TALSH_SUCCESS) rc = NOT_CLEAN;
-        } else {
-          t->avail[img] = YEP;
-        }
+    // Only a source image this task made unavailable is released or dropped
+    // here: later tasks may already have taken over the others.
+    if (img >= 0 && a.held) {
+      if (success && (a.coh == COPY_D || a.coh == COPY_M) && t->ndev > 1) {
+        if (image_discard(t, img) != TALSH_SUCCESS) rc = NOT_CLEAN;
+      } else {
+        t->avail[img] = YEP;
       }
-    } else {
-      t->avail[img] = YEP;
+    }
+    // A failed task's staged body holds no result: it stops being an image.
+    if (!success && a.dalloc && early_body) {
+      for (int j = 0; j < t->ndev; ++j)
+        if (t->dev_rsc[j].gmem_p == early_body) {
+          if (image_discard(t, j) != TALSH_SUCCESS) rc = NOT_CLEAN;
+          break;
+        }
     }
   }
   if (tr->scratch) { mem_free(tr->scratch); tr->scratch = nullptr; }
@@ -546,7 +581,7 @@ int schedule(OpSpec &op, int dev_id, int dev_kind, talsh_task_t *user_task) {
       // Every image held by a task still in flight (its output, or a moved
       // input): the operation can run once that task has completed.
       bool held = false;
-      for (int i = 0; i < op.t[k]->ndev; ++i) held = held || op.t[k]->avail[i] != YEP;
+      for (int i = 0; i < op.t[k]->ndev; ++i) held = held || op.t[k]->avail[i] != YEP || early_image(op.t[k], i);
       return held ? TRY_LATER : TALSH_FAILURE;
     }
   }
@@ -621,17 +656,45 @@ int schedule(OpSpec &op, int dev_id, int dev_kind, talsh_task_t *user_task) {
     }
   }
   // Resources acquired: commit image bookkeeping (reference: discard other
-  // output images, mark moved/discarded sources unavailable).
+  // output images, mark moved/discarded sources unavailable).  GPU bodies that
+  // outlive the task (a moved output, an output kept in place, a kept or
+  // moved staged input) become images right away, usable by later work on
+  // this GPU's compute stream (g_early); the rest wait for the task.
+  auto register_early = [&](talsh_tens_t *t, ArgRec &a) {
+    if (t->ndev >= t->dev_rsc_len) return;
+    const int k = t->ndev++;
+    t->dev_rsc[k].dev_id = exec_dev;
+    t->dev_rsc[k].gmem_p = a.dptr;
+    t->dev_rsc[k].buf_entry = -1;
+    t->dev_rsc[k].mem_attached = 0;
+    t->data_kind[k] = dkind;
+    t->avail[k] = YEP;
+    g_early[a.dptr] = tr;
+    a.early = true;
+  };
   if (op.kind != kOpNorm1 && op.kind != kOpPlace) {
     talsh_tens_t *D = op.t[0];
-    const int di = find_image(D, tr->a[0].src_dev, tr->a[0].src_ptr);
+    ArgRec &a0 = tr->a[0];
+    const int di = find_image(D, a0.src_dev, a0.src_ptr);
     image_discard_other(D, di);
-    D->avail[0] = NOPE;
+    if (!a0.dalloc && (a0.coh == COPY_K || a0.coh == COPY_M)) {
+      g_early[a0.src_ptr] = tr;  // written in place on this GPU and kept
+      a0.early = true;
+    } else {
+      D->avail[0] = NOPE;
+      a0.held = true;
+      if (a0.dalloc && a0.coh == COPY_M) register_early(D, a0);
+    }
   }
   for (int k = (op.kind == kOpNorm1 || op.kind == kOpPlace) ? 0 : 1; k < op.nt; ++k) {
     ArgRec &a = tr->a[k];
     const int i = find_image(a.t, a.src_dev, a.src_ptr);
-    if (a.coh == COPY_D || (a.coh == COPY_M && a.src_dev != exec_dev)) a.t->avail[i] = NOPE;
+    if (a.coh == COPY_D || (a.coh == COPY_M && a.src_dev != exec_dev)) {
+      a.t->avail[i] = NOPE;
+      a.held = true;
+    }
+    if (op.kind != kOpNorm1 && op.kind != kOpPlace && a.dalloc && (a.coh == COPY_K || a.coh == COPY_M))
+      register_early(a.t, a);
   }
 
   talsh_task_t *task = user_task;
@@ -1915,21 +1978,23 @@ int talshTensorPlace(talsh_tens_t *t, int dev_id, int dev_kind, void *dev_mem, i
   if (dvk == DEV_NVIDIA_GPU && (dvn >= MAX_GPUS_PER_NODE || !R.gpu[dvn].in_use)) return TALSH_INVALID_ARGS;
   // Source image: one on the destination device means nothing to do.
   int src = -1;
+  bool held = false;
   for (int i = 0; i < t->ndev; ++i) {
-    if (t->avail[i] != YEP) continue;
+    if (t->avail[i] != YEP) { held = true; continue; }
     if (t->dev_rsc[i].dev_id == flat) {
       if (task) { talshTaskClean(task); task->task_error = 0; }
       return TALSH_SUCCESS;
     }
     int dk = DEV_NULL;
     decode_device_id(t->dev_rsc[i].dev_id, &dk);
+    // a GPU image still being written is copied to the Host on its own GPU's
+    // streams (ordered after the writer), but not to another GPU
+    if (dk == DEV_NVIDIA_GPU && dvk == DEV_NVIDIA_GPU && early_image(t, i)) { held = true; continue; }
     if (src < 0 || dk == DEV_HOST) src = i;
   }
   if (src < 0) {
     // Every image held by a task still in flight: the placement can run once
     // that task has completed (as for the operations).
-    bool held = false;
-    for (int i = 0; i < t->ndev; ++i) held = held || t->avail[i] != YEP;
     return held ? TRY_LATER : TALSH_NOT_FOUND;
   }
   int es = 0;
@@ -2016,6 +2081,7 @@ int talshTensorPlace(talsh_tens_t *t, int dev_id, int dev_kind, void *dev_mem, i
     a.src_ptr = t->dev_rsc[src].gmem_p;
     a.coh = COPY_M;
     a.bytes = bytes;
+    a.held = true;
     tr->nargs = 1;
     t->avail[src] = NOPE;
   }

@@ -92,19 +92,17 @@ def test_chain_with_asynchronous_place(talsh):
             assert L.talshTaskWait(C.byref(tk), C.byref(st)) == 0 and st.value == T.TALSH_TASK_COMPLETED
             assert L.talshTaskDestruct(C.byref(tk)) == 0
 
+        # The copy's result (moved to the GPU) and L's kept GPU copy are images
+        # as soon as the copy is scheduled, so the add and the placement are
+        # accepted at once and run after it in stream order.
         assert L.talshTensorCopy(b"D(c,a,b)=L(a,b,c)", d.ref, a.ref, 0, T.DEV_NVIDIA_GPU, T.COPY_MK,
                                  C.byref(tasks[0])) == 0
-        # D is held by the copy until it completes: a later operation on it is refused for now
-        assert L.talshTensorPlace(d.ref, 0, T.DEV_HOST, C.c_void_p(D.ctypes.data), T.COPY_M,
-                                  C.byref(tasks[2])) == T.TRY_LATER
-        wait(tasks[0])
         assert L.talshTensorAdd(b"D(c,a,b)+=L(a,b,c)", d.ref, a.ref, 0.5, 0.0, 0, T.DEV_NVIDIA_GPU, T.COPY_KD,
                                 C.byref(tasks[1])) == 0
-        wait(tasks[1])
-        assert [img[0] for img in d.images()] == [GPU0]  # moved to the GPU by the copy, kept by the add
         assert L.talshTensorPlace(d.ref, 0, T.DEV_HOST, C.c_void_p(D.ctypes.data), T.COPY_M,
                                   C.byref(tasks[2])) == 0
-        wait(tasks[2])
+        for tk in tasks:
+            wait(tk)
         ref = O.permute(A, [2, 3, 1])
         O.tensor_add(ref, A, [2, 3, 1], 0.5)
         assert same_bits(D, ref), kind
@@ -112,6 +110,23 @@ def test_chain_with_asynchronous_place(talsh):
         assert [img[0] for img in a.images()] == [0]
         for t in (d, a):
             assert t.destruct() == 0
+    # An output staged as a temporary (COPY_T) is held until its task completes.
+    A = rand((17, 31, 6), T.R8, rng)
+    D = fort(np.zeros((6, 17, 31)))
+    d, a = host_tensor(D), host_tensor(A)
+    tk, tk2 = T.Task(), T.Task()
+    L.talshTaskClean(C.byref(tk)); L.talshTaskClean(C.byref(tk2))
+    assert L.talshTensorCopy(b"D(c,a,b)=L(a,b,c)", d.ref, a.ref, 0, T.DEV_NVIDIA_GPU, T.COPY_TT, C.byref(tk)) == 0
+    rc = L.talshTensorPlace(d.ref, 0, T.DEV_NVIDIA_GPU, None, T.COPY_K, C.byref(tk2))
+    assert rc in (0, T.TRY_LATER)  # TRY_LATER unless the copy already completed
+    st = C.c_int()
+    assert L.talshTaskWait(C.byref(tk), C.byref(st)) == 0 and st.value == T.TALSH_TASK_COMPLETED
+    if rc == 0:
+        assert L.talshTaskWait(C.byref(tk2), C.byref(st)) == 0
+    L.talshTaskDestruct(C.byref(tk)); L.talshTaskDestruct(C.byref(tk2))
+    assert same_bits(D, O.permute(A, [2, 3, 1]))
+    for t in (d, a):
+        assert t.destruct() == 0
 
 
 def test_gpu_resident_tensors(talsh):
