@@ -385,6 +385,9 @@ def contract_summary(con):
                 if isinstance(f, dict) and "tflops_fp64_equiv" in f:
                     e[form] = [sig(f["tflops_fp64_equiv"]), sig(f["rel_err_vs_fp64"], 2)]
             out[name] = e
+    ct = con.get("C1_transpose")
+    if isinstance(ct, dict) and "gbs" in ct:
+        out["C1_transpose"] = {"us": sig(ct["us"]), "gbs": sig(ct["gbs"]), "bit_exact": ct["bit_exact"]}
     cx = con.get("complex") or {}
     if isinstance(cx.get("C3b_c8"), dict) and "tflops" in cx["C3b_c8"]:
         e = {"plain_tflops": sig(cx["C3b_c8"]["tflops"]), "plain_err": sig(cx["C3b_c8"]["rel_err_vs_fp64"], 2)}
@@ -1014,6 +1017,25 @@ def bench_contractions(T, L, torch, dev):
         for t in tens:
             L.talshTensorDestruct(C.byref(t))
         del views, ref, got, lv, rv
+    # The C1 transpose D(i,c,a,b)=L(a,b,c,i) on the 32^4 R8 tensor (8 MiB each way,
+    # L2-resident across repetitions), through the device ABI, byte-checked.
+    lt = torch.randn(32 ** 4, dtype=torch.float64, device=dev)
+    dt_ = torch.empty_like(lt)
+    s = torch.cuda.current_stream(dev).cuda_stream
+    dims, o2n = T.ivec([32] * 4), T.ivec([3, 4, 2, 1])
+    for _ in range(3):
+        assert L.tcTensorPermute(T.R8, 4, dims, o2n, lt.data_ptr(), dt_.data_ptr(), 0, s) == 0
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 200
+    e0.record()
+    for _ in range(reps):
+        L.tcTensorPermute(T.R8, 4, dims, o2n, lt.data_ptr(), dt_.data_ptr(), 0, s)
+    e1.record()
+    torch.cuda.synchronize(dev)
+    us = e0.elapsed_time(e1) * 1e3 / reps
+    ref = lt.view(32, 32, 32, 32).permute(2, 3, 1, 0).contiguous().view(-1)  # [i][c][b][a] -> [b][a][c][i]
+    out["C1_transpose"] = {"us": us, "gbs": 2 * 8 * 32 ** 4 / (us * 1e-6) / 1e9,
+                           "bit_exact": bool(torch.equal(dt_, ref)), "note": "8 MiB each way, L2-resident"}
     return out
 
 
