@@ -1565,21 +1565,21 @@ int validate(int kind, int rank, const int *dims, const int *o2n) {
 // the input- and output-minor extents and whether those extents fill whole
 // 16-byte units; tcTensorPermuteTune times the candidate plan choices of one
 // case (CUDA events) and records the fastest for its class, which every later
-// call of that class then uses.  Candidates: the heuristics, bulk reads
-// forced on, bulk reads off, small tiles (4 elements per thread), and the
-// other tile walk order.  Results do not depend on the choice (the same
+// call of that class then uses.  Candidates: every combination of the read
+// path (heuristics, bulk reads on, off), the tile size (heuristics, at most 4
+// elements per thread) and the tile walk order.  Results do not depend on the choice (the same
 // element arithmetic runs in every kernel), only the speed does.
 // ---------------------------------------------------------------------------
-constexpr int kTuneConfigs = 5;
+// choice = bulk + 3 small + 6 flip: bulk 0 the heuristics, 1 bulk reads on, 2 off;
+// small 1: tiles of at most 4 elements per thread; flip 1: the other tile order.
+constexpr int kTuneConfigs = 12;
 PlanCfg tune_cfg(int code) {
   PlanCfg c;
-  switch (code) {
-    case 1: c.bulk = 1; break;
-    case 2: c.bulk = 0; break;
-    case 3: c.small = 1; break;
-    case 4: c.flip = 1; break;
-    default: break;
-  }
+  if (code <= 0 || code >= kTuneConfigs) return c;
+  const int b = code % 3;
+  c.bulk = b == 0 ? -1 : (b == 1 ? 1 : 0);
+  c.small = (code / 3) % 2;
+  c.flip = code / 6;
   return c;
 }
 
