@@ -595,7 +595,7 @@ def main():
         s_tune = torch.cuda.current_stream(dev).cuda_stream
         for op in ops:
             kind, dims, o2n, src, dst, add, _, _ = op
-            rc = L.tcTensorPermuteTune(kind, len(dims), iv(dims), iv(o2n), 1 if add else 0, src, dst, s_tune, 2,
+            rc = L.tcTensorPermuteTune(kind, len(dims), iv(dims), iv(o2n), 1 if add else 0, src, dst, s_tune, 1,
                                        C.byref(ch))
             if rc != 0:
                 raise RuntimeError("tuning failed %d: %s" % (rc, L.tcLastErrorString()))

@@ -1120,6 +1120,7 @@ struct PlanCfg {
   int bulk = -1;   // -1: permute_bulk_wanted decides; 0: never; 1: wherever the plan allows it
   int small = 0;   // 1: tiles of at most 4 elements per thread (more resident CTAs per SM)
   int flip = 0;    // 1: walk the tiles in the other tensor's dimension order
+  int grow = -1;   // tile growth: -1 the shorter run first, 0 input runs first, 1 output runs first
 };
 
 // out_major: tile index order follows the output's dimensions (copies), else
@@ -1226,7 +1227,8 @@ int build_plan(int esize, const Fused &F, Plan &plan, int op = kOpCopy, const Pl
     if (G.V * 2 > elems_max) break;
     bool done = false;
     for (int pass = 0; pass < 2 && !done; ++pass) {
-      const bool growA = (pass == 0) ? (G.Li <= G.Lo) : !(G.Li <= G.Lo);
+      const bool firstA = cfg.grow < 0 ? (G.Li <= G.Lo) : (cfg.grow == 0);
+      const bool growA = (pass == 0) ? firstA : !firstA;
       int na2 = na, nb2 = nb;
       int64_t tA2 = tA, tB2 = tB;
       if (growA) {
@@ -1567,19 +1569,23 @@ int validate(int kind, int rank, const int *dims, const int *o2n) {
 // case (CUDA events) and records the fastest for its class, which every later
 // call of that class then uses.  Candidates: every combination of the read
 // path (heuristics, bulk reads on, off), the tile size (heuristics, at most 4
-// elements per thread) and the tile walk order.  Results do not depend on the choice (the same
+// elements per thread), the tile walk order and the tile's growth order
+// (heuristics, input runs first, output runs first).  Results do not depend on the choice (the same
 // element arithmetic runs in every kernel), only the speed does.
 // ---------------------------------------------------------------------------
-// choice = bulk + 3 small + 6 flip: bulk 0 the heuristics, 1 bulk reads on, 2 off;
-// small 1: tiles of at most 4 elements per thread; flip 1: the other tile order.
-constexpr int kTuneConfigs = 12;
+// choice = bulk + 3 small + 6 flip + 12 grow: bulk 0 the heuristics, 1 bulk
+// reads on, 2 off; small 1: tiles of at most 4 elements per thread; flip 1: the
+// other tile order; grow 0 the heuristics (the shorter run grows first), 1
+// input runs first, 2 output runs first.
+constexpr int kTuneConfigs = 36;
 PlanCfg tune_cfg(int code) {
   PlanCfg c;
   if (code <= 0 || code >= kTuneConfigs) return c;
   const int b = code % 3;
   c.bulk = b == 0 ? -1 : (b == 1 ? 1 : 0);
   c.small = (code / 3) % 2;
-  c.flip = code / 6;
+  c.flip = (code / 6) % 2;
+  c.grow = code / 12 - 1;
   return c;
 }
 
