@@ -1121,6 +1121,7 @@ struct PlanCfg {
   int small = 0;   // 1: tiles of at most 4 elements per thread (more resident CTAs per SM)
   int flip = 0;    // 1: walk the tiles in the other tensor's dimension order
   int grow = -1;   // tile growth: -1 the shorter run first, 0 input runs first, 1 output runs first
+  int longrun = 0; // 1: the initial runs span at least twice the usual elements
 };
 
 // out_major: tile index order follows the output's dimensions (copies), else
@@ -1147,7 +1148,7 @@ int build_plan(int esize, const Fused &F, Plan &plan, int op = kOpCopy, const Pl
     const int64_t slots = 148LL * kMinBlocks * 2;
     while (elems_max / 2 >= 1024 && F.vol / elems_max < slots) elems_max /= 2;  // floor 1024: every plan fits
   }
-  const int run_min = esize >= 16 ? 16 : 32;
+  const int run_min = (esize >= 16 ? 16 : 32) * (cfg.longrun ? 2 : 1);
   // Initial groups: shortest prefixes reaching run_min elements.
   int na = 0, nb = 0;
   int64_t tA = 1, tB = 1;
@@ -1569,15 +1570,17 @@ int validate(int kind, int rank, const int *dims, const int *o2n) {
 // case (CUDA events) and records the fastest for its class, which every later
 // call of that class then uses.  Candidates: every combination of the read
 // path (heuristics, bulk reads on, off), the tile size (heuristics, at most 4
-// elements per thread), the tile walk order and the tile's growth order
-// (heuristics, input runs first, output runs first).  Results do not depend on the choice (the same
+// elements per thread), the tile walk order, the tile's growth order
+// (heuristics, input runs first, output runs first) and the initial run
+// length (the planner's minimum, twice that).  Results do not depend on the choice (the same
 // element arithmetic runs in every kernel), only the speed does.
 // ---------------------------------------------------------------------------
-// choice = bulk + 3 small + 6 flip + 12 grow: bulk 0 the heuristics, 1 bulk
-// reads on, 2 off; small 1: tiles of at most 4 elements per thread; flip 1: the
-// other tile order; grow 0 the heuristics (the shorter run grows first), 1
-// input runs first, 2 output runs first.
-constexpr int kTuneConfigs = 36;
+// choice = bulk + 3 small + 6 flip + 12 grow + 36 longrun: bulk 0 the
+// heuristics, 1 bulk reads on, 2 off; small 1: tiles of at most 4 elements per
+// thread; flip 1: the other tile order; grow 0 the heuristics (the shorter run
+// grows first), 1 input runs first, 2 output runs first; longrun 1: initial
+// runs of at least 64 elements (32 for 16-byte elements) instead of 32 (16).
+constexpr int kTuneConfigs = 72;
 PlanCfg tune_cfg(int code) {
   PlanCfg c;
   if (code <= 0 || code >= kTuneConfigs) return c;
@@ -1585,7 +1588,8 @@ PlanCfg tune_cfg(int code) {
   c.bulk = b == 0 ? -1 : (b == 1 ? 1 : 0);
   c.small = (code / 3) % 2;
   c.flip = (code / 6) % 2;
-  c.grow = code / 12 - 1;
+  c.grow = (code / 12) % 3 - 1;
+  c.longrun = code / 36;
   return c;
 }
 
