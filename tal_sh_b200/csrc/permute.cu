@@ -1121,7 +1121,7 @@ struct PlanCfg {
   int small = 0;   // 1: tiles of at most 4 elements per thread (more resident CTAs per SM)
   int flip = 0;    // 1: walk the tiles in the other tensor's dimension order
   int grow = -1;   // tile growth: -1 the shorter run first, 0 input runs first, 1 output runs first
-  int longrun = 0; // 1: the initial runs span at least twice the usual elements
+  int longrun = 0; // initial runs of at least 2^longrun times the usual elements
 };
 
 // out_major: tile index order follows the output's dimensions (copies), else
@@ -1148,7 +1148,7 @@ int build_plan(int esize, const Fused &F, Plan &plan, int op = kOpCopy, const Pl
     const int64_t slots = 148LL * kMinBlocks * 2;
     while (elems_max / 2 >= 1024 && F.vol / elems_max < slots) elems_max /= 2;  // floor 1024: every plan fits
   }
-  const int run_min = (esize >= 16 ? 16 : 32) * (cfg.longrun ? 2 : 1);
+  const int run_min = (esize >= 16 ? 16 : 32) << cfg.longrun;
   // Initial groups: shortest prefixes reaching run_min elements.
   int na = 0, nb = 0;
   int64_t tA = 1, tB = 1;
@@ -1572,15 +1572,16 @@ int validate(int kind, int rank, const int *dims, const int *o2n) {
 // path (heuristics, bulk reads on, off), the tile size (heuristics, at most 4
 // elements per thread), the tile walk order, the tile's growth order
 // (heuristics, input runs first, output runs first) and the initial run
-// length (the planner's minimum, twice that).  Results do not depend on the choice (the same
+// length (the planner's minimum, twice or four times that).  Results do not depend on the choice (the same
 // element arithmetic runs in every kernel), only the speed does.
 // ---------------------------------------------------------------------------
 // choice = bulk + 3 small + 6 flip + 12 grow + 36 longrun: bulk 0 the
 // heuristics, 1 bulk reads on, 2 off; small 1: tiles of at most 4 elements per
 // thread; flip 1: the other tile order; grow 0 the heuristics (the shorter run
-// grows first), 1 input runs first, 2 output runs first; longrun 1: initial
-// runs of at least 64 elements (32 for 16-byte elements) instead of 32 (16).
-constexpr int kTuneConfigs = 72;
+// grows first), 1 input runs first, 2 output runs first; longrun 1 / 2:
+// initial runs of at least 2 / 4 times the usual 32 elements (16 for 16-byte
+// elements).
+constexpr int kTuneConfigs = 108;
 PlanCfg tune_cfg(int code) {
   PlanCfg c;
   if (code <= 0 || code >= kTuneConfigs) return c;
