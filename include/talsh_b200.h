@@ -48,12 +48,14 @@ int tcTensorPermuteAdd(int data_kind, int rank, const int *dims_in, const int *o
  * elements per thread; f = 1: the other tile walk order; g: 0 the planner's
  * tile growth (the shorter run first), 1 input runs first, 2 output runs
  * first; r = 1 / 2: initial runs of 2 / 4 times the planner's minimum length;
- * 0 is the planner's heuristics throughout), 1 + reps times each on `stream` (the first run is a warm-up),
+ * add 108 to keep the full tile budget for small tensors, which the planner
+ * otherwise shrinks so that every SM gets tiles; 0 is the planner's
+ * heuristics throughout), 1 + reps times each on `stream` (the first run is a warm-up),
  * times them with CUDA events, and records the fastest for the class; every
  * later tcTensorPermute / tcTensorPermuteAdd call of the class (and the tiled
  * tasks of a permutation batch) uses it.  Results are identical under every
  * choice; only the speed changes.  src and dst are device buffers of the case's
- * volume; dst is overwritten (adds accumulate into it 108 x (1 + reps) times
+ * volume; dst is overwritten (adds accumulate into it 216 x (1 + reps) times
  * at most).  *choice receives the recorded choice (0 when the case has a single
  * plan).  Synchronises the stream.  The reference has no autotuner: its
  * gpu_tensor_block_copy_dlf (tensor_algebra_gpu_nvidia.cu:4806) picks a kernel
@@ -63,7 +65,7 @@ int tcTensorPermuteTune(int data_kind, int rank, const int *dims_in, const int *
 /* The recorded choice of the case's class, or -1 in *choice when none. */
 int tcTensorPermuteTuned(int data_kind, int rank, const int *dims_in, const int *o2n, int accumulate,
                          int *choice);
-/* Records `choice` (0-107) for the case's class without timing -- a saved tuning
+/* Records `choice` (0-215) for the case's class without timing -- a saved tuning
  * table can be restored this way -- or forgets the class's entry (choice -1).
  * TALSH_INVALID_ARGS when the choice has no plan for this case. */
 int tcTensorPermuteTuneSet(int data_kind, int rank, const int *dims_in, const int *o2n, int accumulate,

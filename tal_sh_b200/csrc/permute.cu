@@ -1122,6 +1122,7 @@ struct PlanCfg {
   int flip = 0;    // 1: walk the tiles in the other tensor's dimension order
   int grow = -1;   // tile growth: -1 the shorter run first, 0 input runs first, 1 output runs first
   int longrun = 0; // initial runs of at least 2^longrun times the usual elements
+  int keep = 0;    // 1: small tensors keep the full tile budget
 };
 
 // out_major: tile index order follows the output's dimensions (copies), else
@@ -1146,7 +1147,7 @@ int build_plan(int esize, const Fused &F, Plan &plan, int op = kOpCopy, const Pl
   int elems_max = std::min(tile_bytes() / esize, kThreads * (cfg.small ? 4 : reg_k(esize)));
   {
     const int64_t slots = 148LL * kMinBlocks * 2;
-    while (elems_max / 2 >= 1024 && F.vol / elems_max < slots) elems_max /= 2;  // floor 1024: every plan fits
+    while (!cfg.keep && elems_max / 2 >= 1024 && F.vol / elems_max < slots) elems_max /= 2;  // floor 1024: every plan fits
   }
   const int run_min = (esize >= 16 ? 16 : 32) << cfg.longrun;
   // Initial groups: shortest prefixes reaching run_min elements.
@@ -1571,8 +1572,9 @@ int validate(int kind, int rank, const int *dims, const int *o2n) {
 // call of that class then uses.  Candidates: every combination of the read
 // path (heuristics, bulk reads on, off), the tile size (heuristics, at most 4
 // elements per thread), the tile walk order, the tile's growth order
-// (heuristics, input runs first, output runs first) and the initial run
-// length (the planner's minimum, twice or four times that).  Results do not depend on the choice (the same
+// (heuristics, input runs first, output runs first), the initial run length
+// (the planner's minimum, twice or four times that) and, for small tensors,
+// the tile budget (shrunk so that every SM gets tiles, or kept).  Results do not depend on the choice (the same
 // element arithmetic runs in every kernel), only the speed does.
 // ---------------------------------------------------------------------------
 // choice = bulk + 3 small + 6 flip + 12 grow + 36 longrun: bulk 0 the
@@ -1580,8 +1582,8 @@ int validate(int kind, int rank, const int *dims, const int *o2n) {
 // thread; flip 1: the other tile order; grow 0 the heuristics (the shorter run
 // grows first), 1 input runs first, 2 output runs first; longrun 1 / 2:
 // initial runs of at least 2 / 4 times the usual 32 elements (16 for 16-byte
-// elements).
-constexpr int kTuneConfigs = 108;
+// elements); keep 1 (code + 108): small tensors keep the full tile budget.
+constexpr int kTuneConfigs = 216;
 PlanCfg tune_cfg(int code) {
   PlanCfg c;
   if (code <= 0 || code >= kTuneConfigs) return c;
@@ -1590,7 +1592,8 @@ PlanCfg tune_cfg(int code) {
   c.small = (code / 3) % 2;
   c.flip = (code / 6) % 2;
   c.grow = (code / 12) % 3 - 1;
-  c.longrun = code / 36;
+  c.longrun = (code / 36) % 3;
+  c.keep = code / 108;
   return c;
 }
 

@@ -42,7 +42,7 @@ def test_tune_table_without_gpu(built):
     kind, dims, o2n = CASES[0]
     args = (kind, len(dims), T.ivec(dims), T.ivec(o2n))
     assert L.tcTensorPermuteTuned(*args, 0, C.byref(ch)) == 0 and ch.value == -1
-    for choice in range(108):
+    for choice in range(216):
         rc = L.tcTensorPermuteTuneSet(*args, 1, choice)
         assert rc in (0, T.TALSH_INVALID_ARGS)
         if rc == 0:
@@ -58,7 +58,7 @@ def test_tune_table_without_gpu(built):
     assert L.tcTensorPermuteTuneSet(*args, 0, -1) == 0
     assert L.tcTensorPermuteTuned(*args, 0, C.byref(ch)) == 0 and ch.value == -1
     # invalid arguments
-    assert L.tcTensorPermuteTuneSet(*args, 0, 108) == T.TALSH_INVALID_ARGS
+    assert L.tcTensorPermuteTuneSet(*args, 0, 216) == T.TALSH_INVALID_ARGS
     assert L.tcTensorPermuteTuneSet(*args, 0, -2) == T.TALSH_INVALID_ARGS
     assert L.tcTensorPermuteTuned(kind, len(dims), T.ivec(dims), T.ivec([1, 1, 2, 3, 4, 5]), 0,
                                   C.byref(ch)) == T.TALSH_INVALID_ARGS
@@ -110,7 +110,7 @@ def test_every_choice_bit_exact(talsh):
             ref_copy = O.permute(Lh, o2n).tobytes(order="F")
             ref = D0.copy(order="F")
             O.tensor_add(ref, Lh, o2n, 0.5)
-            for choice in range(108):
+            for choice in range(216):
                 for acc in (0, 1):
                     rc = L.tcTensorPermuteTuneSet(kind, len(dims), T.ivec(dims), T.ivec(o2n), acc, choice)
                     assert rc in (0, T.TALSH_INVALID_ARGS)
@@ -120,7 +120,7 @@ def test_every_choice_bit_exact(talsh):
                 tried += 1
     finally:
         L.tcTensorPermuteTuneReset()
-    assert tried == 108 * len(CASES)
+    assert tried == 216 * len(CASES)
 
 
 @pytest.mark.gpu
@@ -140,7 +140,7 @@ def test_tune_records_a_choice(talsh):
             for acc in (0, 1):
                 rc = L.tcTensorPermuteTune(*args, acc, lt.data_ptr(), dt.data_ptr(), s, 2, C.byref(ch))
                 assert rc == 0, L.tcLastErrorString()
-                assert 0 <= ch.value <= 107
+                assert 0 <= ch.value <= 215
                 assert L.tcTensorPermuteTuned(*args, acc, C.byref(ch2)) == 0
                 straight = len(o2n) > 1 and list(o2n) == sorted(o2n)
                 assert ch2.value == (-1 if straight else ch.value)
