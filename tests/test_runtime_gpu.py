@@ -237,3 +237,52 @@ def test_host_mem_register_pins_caller_memory(talsh):
     finally:
         assert L.host_mem_unregister(p) == 0
     assert L.host_mem_unregister(p) == 1
+
+
+class _DeviceBlock:
+    """A device pointer seen by torch through the CUDA array interface (no copy)."""
+
+    def __init__(self, ptr, n):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": "<f8", "data": (ptr, False), "strides": None,
+                                          "version": 2}
+
+
+def test_device_resource_memory_from_caller_streams(talsh):
+    """tensDevRsc_allocate_mem on GPU 0 (flat device 1) returns a block that is ready
+    when the call returns, as the reference's synchronous gpu_mem_alloc
+    (mem_manager.cpp:779) is: a caller fills it at once from a stream of its own and
+    reads it back, the library permutes into it, and tensDevRsc_free_mem takes it back
+    only after the device has finished with it, over several allocate / free cycles."""
+    import torch
+    L = talsh
+    pp = C.POINTER(T.DevRsc)()
+    assert L.tensDevRsc_create(C.byref(pp)) == 0
+    d = pp
+    n = 1 << 20
+    rng = np.random.default_rng(17)
+    A = rand((128, 64, 128), T.R8, rng)
+    src = torch.from_numpy(A.ravel(order="F").copy()).cuda()
+    ref = O.permute(A, [3, 1, 2])
+    side = torch.cuda.Stream()
+    try:
+        for it in range(4):
+            assert L.tensDevRsc_allocate_mem(d, 1, n * 8, T.NOPE) == 0
+            assert L.tensDevRsc_device_id(d) == 1
+            g = C.c_void_p()
+            assert L.tensDevRsc_get_gmem_ptr(d, C.byref(g)) == 0 and g.value
+            blk = torch.as_tensor(_DeviceBlock(g.value, n), device="cuda")
+            with torch.cuda.stream(side):
+                blk.fill_(it + 0.5)
+                assert bool((blk == it + 0.5).all().item())
+            side.synchronize()
+            s = torch.cuda.current_stream().cuda_stream
+            assert L.tcTensorPermute(T.R8, 3, T.ivec([128, 64, 128]), T.ivec([3, 1, 2]), src.data_ptr(), g.value,
+                                     0, s) == 0
+            torch.cuda.synchronize()
+            got = blk.cpu().numpy().reshape((64, 128, 128), order="F")
+            assert same_bits(got, ref), it
+            del blk
+            assert L.tensDevRsc_free_mem(d) == 0 and L.tensDevRsc_is_empty(d) == T.YEP
+    finally:
+        L.tensDevRsc_release_all(d)
+        assert L.tensDevRsc_destroy(d) == 0
